@@ -1,0 +1,141 @@
+/*
+ * scg.h -- C ABI of the B200 search library (libscgpu.so).
+ *
+ * The drop-in boundary for the search path of marker68/second-candidate:
+ * plain pointers and sizes, int status returns, no C++ or CUDA types.  The
+ * reference's own C++ classes (PQQuery, MultiQuery, SCQuery, Encoder,
+ * SCEncoder) are header-only and non-virtual; the drop-in headers under
+ * second-candidate_b200/cpp/ keep their names and signatures and forward to
+ * these entry points.  Each declaration names the reference interface it
+ * replaces (file:line in the reference tree).
+ *
+ * Status codes: SCG_OK (0) or a negative SCG_ERR_*; scg_last_error() returns
+ * the message of the last failure on the calling thread.  Device-side caps
+ * (cell budgets, iteration limits) end a query with a status, never a trap.
+ */
+#ifndef SCG_H_
+#define SCG_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SCG_OK 0
+#define SCG_ERR_ARG (-1)    /* invalid argument or shape                        */
+#define SCG_ERR_OOM (-2)    /* device or host allocation failed                 */
+#define SCG_ERR_IO (-3)     /* file missing, short or malformed                 */
+#define SCG_ERR_CUDA (-4)   /* CUDA runtime error                               */
+#define SCG_ERR_CAP (-5)    /* a per-query device budget was exceeded           */
+#define SCG_ERR_STATE (-6)  /* call order (e.g. search before codebooks/index)  */
+
+/* Search modes: the three reference entry points. */
+#define SCG_IVFADC 0  /* PQQuery::search_ivfadc      query.h:202-325        */
+#define SCG_IMI 1     /* MultiQuery::search_multi2   multi_query.h:62-273   */
+#define SCG_SC2 2     /* SCQuery::search_mr_ivf      sc_query.h:60-256      */
+
+/* Arithmetic of the per-query tables and of the ADC sum. */
+#define SCG_FP32_EXACT 0 /* the reference's float operations in its order     */
+#define SCG_FAST 1       /* tensor-core tables, fused per-vector term         */
+
+typedef struct scg_index scg_index;
+
+typedef struct {
+    int mode;       /* SCG_IVFADC / SCG_IMI / SCG_SC2                              */
+    int R;          /* results per query (1..1024)                                 */
+    int w;          /* cell cap: popped cells (IVFADC, IMI) or non-empty cells (SC) */
+    int T;          /* candidate target: stop after the cell that reaches T         */
+    int precision;  /* SCG_FP32_EXACT or SCG_FAST                                   */
+    int rerank;     /* 0: ADC distances; -1: exact distance for every candidate
+                       (the reference's real_dist branch); L>0: ADC shortlist of L
+                       re-ranked by exact distance                                  */
+} scg_search_params;
+
+/* Message of the last failing call on this thread (always NUL-terminated). */
+int scg_last_error(char *buf, int len);
+
+/* Creates an empty index on CUDA device `device`.  Replaces the PQQuery /
+ * MultiQuery / SCQuery constructors (query.cpp:19-32, multi_query.cpp:15-17,
+ * sc_query.cpp:17-25). */
+int scg_index_create(scg_index **out, int device);
+
+/* Frees all device memory of the index.  Replaces ~PQQuery (query.cpp:37-61). */
+int scg_index_destroy(scg_index *h);
+
+/* Codebooks from memory: cq is [mc][kc][dim/mc], pq is [mp][kp][dim/mp]
+ * (the arrays load_codebook fills, sc_utilities.h:897-980). */
+int scg_load_codebooks(scg_index *h, const float *cq, int kc, int mc,
+                       const float *pq, int kp, int mp, int dim);
+
+/* Codebooks from two .ctr_ files.  Replaces PQQuery::load_codebooks
+ * (query.cpp:66-75). */
+int scg_load_codebooks_file(scg_index *h, const char *cq_path, const char *pq_path);
+
+/* The CSR index: L[ncells] inclusive prefix counts, pid[N], codes[N][mp] in
+ * cell order (the arrays PQQuery::load_encoded_data builds, query.cpp:82-165).
+ * ncells must be kc^mc (IVFADC/IMI) or kc^2 (SC, mc = 1). */
+int scg_load_csr(scg_index *h, const int *L, const int *pid, const uint8_t *codes,
+                 int64_t N, int64_t ncells);
+
+/* Reads an .edat_ file with kc^nc cells (nc = mc for IVFADC/IMI indexes, 2 for
+ * second-candidate indexes).  Replaces PQQuery::load_encoded_data
+ * (query.cpp:82-165) and SCQuery::load_encoded_data (sc_query.cpp:36-123). */
+int scg_load_encoded_file(scg_index *h, const char *path, int nc);
+
+/* Raw vectors [N][dim] (float), for the exact-distance branch and re-rank.
+ * Replaces PQQuery::load_data (query.h:82-86). */
+int scg_load_raw(scg_index *h, const float *X, int64_t N);
+
+/* Query-independent tables: ||c||^2, ||r||^2, 2<c,r> and the per-vector ADC
+ * term of the fast form.  Replaces PQQuery::pre_compute1 (query.h:91-149). */
+int scg_precompute(scg_index *h);
+
+/* Batched search with HOST buffers: Q[nq][dim] in, ids[nq][R], dists[nq][R],
+ * sums[nq] out (sums may be NULL).  Each query returns its top min(R, sum)
+ * candidates in ascending distance (equal distances by id); unused slots hold
+ * id -1 and distance +inf.  `sum` is the candidate count the reference
+ * returns by reference.  Replaces one call per query of search_ivfadc
+ * (query.h:202), search_multi2 (multi_query.h:62) or search_mr_ivf
+ * (sc_query.h:60); per-query tables (pre_compute2, query.h:154-184) are built
+ * inside. */
+int scg_search(scg_index *h, const scg_search_params *p, const float *Q, int nq,
+               int *ids, float *dists, int *sums);
+
+/* The same with DEVICE buffers, enqueued on `stream` (a cudaStream_t, or NULL
+ * for the index's own stream); returns once the work is enqueued and
+ * synchronises only to read the status word. */
+int scg_search_device(scg_index *h, const scg_search_params *p, const float *dQ, int nq,
+                      int *d_ids, float *d_dists, int *d_sums, void *stream);
+
+/* Per-query candidate targets (device pointer to nq ints) for the next
+ * scg_search_device call; NULL restores the single T of the parameters. */
+int scg_set_query_targets(scg_index *h, const int *d_T);
+
+/* Budgets of the traversal: the most cells one query may enumerate
+ * (default 131072).  Larger budgets cost device memory per resident CTA. */
+int scg_set_cell_budget(scg_index *h, int max_cells);
+
+/* Encoder: X[n][dim] float rows -> cid[n][mc] (uint16) and codes[n][mp]
+ * (uint8), first-minimum argmin with double accumulation exactly as
+ * Encoder::encode<T> (encoder.h:69-192).  Host buffers. */
+int scg_encode(scg_index *h, const float *X, int64_t n, uint16_t *cid, uint8_t *codes);
+
+/* Second-candidate encoder (mc = 1): cid[n][nc] nearest coarse centroids in
+ * ascending distance, codes of the residual to the nearest, as
+ * SCEncoder::encode<T> (sc_encoder.h:205-332).  Host buffers. */
+int scg_sc_encode(scg_index *h, const float *X, int64_t n, int nc, uint16_t *cid,
+                  uint8_t *codes);
+
+/* Device-buffer form of the two encoders (X, cid, codes on the device). */
+int scg_encode_device(scg_index *h, const float *dX, int64_t n, int nc, uint16_t *d_cid,
+                      uint8_t *d_codes, void *stream);
+
+/* Index facts: dim, mc, kc, mp, kp, N (any pointer may be NULL). */
+int scg_index_info(scg_index *h, int *dim, int *mc, int *kc, int *mp, int *kp, int64_t *N);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,514 @@
+// C ABI of libscgpu.so (include/scg.h): the index handle, loaders, and the
+// host orchestration of the batched search and the encoders.
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "scg_internal.cuh"
+
+namespace scg {
+
+static thread_local std::string g_err;
+
+void set_error(const std::string &msg) { g_err = msg; }
+int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+int cuda_fail(cudaError_t e, const char *what) {
+    g_err = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? SCG_ERR_OOM : SCG_ERR_CUDA;
+}
+
+// Grow-only device buffer.
+struct DevBuf {
+    void *p = nullptr;
+    size_t n = 0;
+    int ensure(size_t bytes) {
+        if (bytes <= n) return SCG_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+        n = bytes;
+        return SCG_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    template <class T>
+    T *as() const {
+        return (T *)p;
+    }
+};
+
+}  // namespace scg
+
+using namespace scg;
+
+struct scg_index {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    int dim = 0, mc = 0, kc = 0, mp = 0, kp = 0;
+    int64_t N = 0;
+    int64_t ncells = 0;
+    bool have_codebooks = false, have_csr = false, precomputed = false;
+    int cap_rec = 131072;
+    const int *d_Tq = nullptr;
+    DevBuf cq, pq, norm_c, norm_r, dot_cr, off, pid, codes, raw;
+    // batch workspace
+    DevBuf q, dqc, dqr, qn, qsum, ids, dists, sums, nvis, empty, status, counter;
+    DevBuf rec_key, rec_rank, rec_cnt, vis_cell, vis_pre;
+    int *h_status = nullptr;  // pinned
+    std::mutex mu;
+};
+
+namespace {
+
+int set_device(scg_index *h) {
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    return SCG_OK;
+}
+
+bool read_file(const char *path, std::vector<unsigned char> &buf) {
+    std::ifstream f(path, std::ios::binary | std::ios::ate);
+    if (!f) return false;
+    std::streamsize n = f.tellg();
+    if (n < 0) return false;
+    f.seekg(0);
+    buf.resize((size_t)n);
+    return n == 0 || (bool)f.read((char *)buf.data(), n);
+}
+
+// Reads a .ctr_ file: float {k, m, dim} then k*dim floats
+// (load_codebook, sc_utilities.h:897-980).
+int read_ctr(const char *path, std::vector<float> &c, int &k, int &m, int &dim) {
+    std::vector<unsigned char> b;
+    if (!path || !read_file(path, b)) return fail(SCG_ERR_IO, std::string("cannot read codebook ") + (path ? path : "(null)"));
+    if (b.size() < 12) return fail(SCG_ERR_IO, std::string("codebook too short: ") + path);
+    float hdr[3];
+    memcpy(hdr, b.data(), 12);
+    k = (int)hdr[0];
+    m = (int)hdr[1];
+    dim = (int)hdr[2];
+    if (k <= 0 || m <= 0 || dim <= 0 || dim % m != 0)
+        return fail(SCG_ERR_IO, std::string("bad codebook header in ") + path);
+    size_t need = (size_t)k * dim;
+    if (b.size() < 12 + need * 4) return fail(SCG_ERR_IO, std::string("codebook truncated: ") + path);
+    c.resize(need);
+    memcpy(c.data(), b.data() + 12, need * 4);
+    return SCG_OK;
+}
+
+int64_t ipow(int64_t b, int e) {
+    int64_t r = 1;
+    for (int i = 0; i < e; i++) r *= b;
+    return r;
+}
+
+int check_ready(scg_index *h) {
+    if (!h) return fail(SCG_ERR_ARG, "null index");
+    if (!h->have_codebooks) return fail(SCG_ERR_STATE, "codebooks not loaded");
+    if (!h->have_csr) return fail(SCG_ERR_STATE, "encoded data not loaded");
+    if (!h->precomputed) return fail(SCG_ERR_STATE, "scg_precompute not called");
+    return SCG_OK;
+}
+
+int check_params(scg_index *h, const scg_search_params *p, int nq) {
+    if (!p) return fail(SCG_ERR_ARG, "null params");
+    if (nq < 0) return fail(SCG_ERR_ARG, "nq < 0");
+    if (p->R < 1 || p->R > 1024) return fail(SCG_ERR_ARG, "R must be in [1, 1024]");
+    if (p->precision != SCG_FP32_EXACT) return fail(SCG_ERR_ARG, "precision not supported by this build");
+    if (p->rerank != 0) return fail(SCG_ERR_ARG, "rerank not supported by this build");
+    switch (p->mode) {
+        case SCG_IVFADC:
+            if (h->mc != 1 || h->ncells != h->kc) return fail(SCG_ERR_ARG, "This search method is for IVFADC only");
+            break;
+        case SCG_IMI:
+            if (h->mc != 2 || h->ncells != (int64_t)h->kc * h->kc)
+                return fail(SCG_ERR_ARG, "This search method is for Multi-D-ADC-2 only");
+            break;
+        case SCG_SC2:
+            if (h->mc != 1 || h->ncells != (int64_t)h->kc * h->kc)
+                return fail(SCG_ERR_ARG, "This search method is for MultiRank IVFADC only");
+            break;
+        default:
+            return fail(SCG_ERR_ARG, "unknown search mode");
+    }
+    if (h->kc > 65535) return fail(SCG_ERR_ARG, "kc must be < 65536");
+    return SCG_OK;
+}
+
+int run_search(scg_index *h, const scg_search_params *p, const float *dQ, int nq, int *d_ids, float *d_d,
+               int *d_sums, cudaStream_t s) {
+    int rc;
+    const int R = p->R;
+    if ((rc = h->dqc.ensure(sizeof(float) * (size_t)nq * h->mc * h->kc))) return rc;
+    if ((rc = h->dqr.ensure(sizeof(float) * (size_t)nq * h->mp * h->kp))) return rc;
+    if ((rc = h->qn.ensure(sizeof(float) * (size_t)nq * 2))) return rc;
+    if ((rc = h->qsum.ensure(sizeof(float) * (size_t)nq))) return rc;
+    if ((rc = h->nvis.ensure(sizeof(int) * (size_t)nq))) return rc;
+    if ((rc = h->empty.ensure(sizeof(int) * (size_t)nq))) return rc;
+    if ((rc = h->status.ensure(sizeof(int) * 4))) return rc;
+    if ((rc = h->counter.ensure(sizeof(int) * 4))) return rc;
+    int per_sm = search_max_blocks_per_sm(p->mode, h->kc, h->mp, h->kp);
+    if (per_sm < 1) return fail(SCG_ERR_ARG, "search kernel does not fit on an SM for this shape");
+    int grid = h->num_sms * per_sm;
+    if (grid > nq) grid = nq;
+    if (grid < 1) grid = 1;
+    size_t slot = (size_t)h->cap_rec;
+    if ((rc = h->rec_key.ensure(4 * slot * grid))) return rc;
+    if ((rc = h->rec_rank.ensure(4 * slot * grid))) return rc;
+    if ((rc = h->rec_cnt.ensure(4 * slot * grid))) return rc;
+    if ((rc = h->vis_cell.ensure(4 * (slot + 1) * grid))) return rc;
+    if ((rc = h->vis_pre.ensure(4 * (slot + 1) * grid))) return rc;
+
+    TablesArgs ta;
+    ta.dim = h->dim; ta.mc = h->mc; ta.kc = h->kc; ta.mp = h->mp; ta.kp = h->kp; ta.nq = nq;
+    ta.Q = dQ;
+    ta.cq = h->cq.as<float>(); ta.pq = h->pq.as<float>();
+    ta.norm_c = h->norm_c.as<float>(); ta.norm_r = h->norm_r.as<float>();
+    ta.dqc = h->dqc.as<float>(); ta.dqr = h->dqr.as<float>();
+    ta.qn = h->qn.as<float>(); ta.qsum = h->qsum.as<float>();
+    launch_tables_exact(ta, s);
+
+    SCG_CUDA(cudaMemsetAsync(h->status.p, 0, sizeof(int) * 4, s));
+    SCG_CUDA(cudaMemsetAsync(h->counter.p, 0, sizeof(int) * 4, s));
+    SearchArgs sa;
+    memset(&sa, 0, sizeof(sa));
+    sa.mode = p->mode; sa.dim = h->dim; sa.mc = h->mc; sa.kc = h->kc; sa.mp = h->mp; sa.kp = h->kp;
+    sa.nq = nq; sa.R = R; sa.w = p->w; sa.T = p->T; sa.precision = p->precision;
+    sa.Tq = h->d_Tq;
+    sa.dqc = ta.dqc; sa.dqr = ta.dqr; sa.qn = ta.qn; sa.qsum = ta.qsum;
+    sa.off = h->off.as<uint32_t>(); sa.pid = h->pid.as<int>(); sa.codes = h->codes.as<uint8_t>();
+    sa.dot_cr = h->dot_cr.as<float>();
+    sa.vterm = nullptr;
+    sa.ncells = (uint64_t)h->ncells;
+    sa.N = h->N;
+    sa.rec_key = h->rec_key.as<uint32_t>(); sa.rec_rank = h->rec_rank.as<uint32_t>();
+    sa.rec_cnt = h->rec_cnt.as<uint32_t>();
+    sa.vis_cell = h->vis_cell.as<uint32_t>(); sa.vis_pre = h->vis_pre.as<uint32_t>();
+    sa.cap_rec = h->cap_rec;
+    sa.qcounter = h->counter.as<int>();
+    sa.out_ids = d_ids; sa.out_d = d_d; sa.out_sum = d_sums;
+    sa.out_nvis = h->nvis.as<int>(); sa.out_empty = h->empty.as<int>();
+    sa.status = h->status.as<int>();
+    if (nq > 0 && (rc = search_launch(sa, grid, s))) return rc;
+    SCG_CUDA(cudaMemcpyAsync(h->h_status, h->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SCG_CUDA(cudaStreamSynchronize(s));
+    int st = *h->h_status;
+    if (st & ST_CELL_BUDGET)
+        return fail(SCG_ERR_CAP, "a query enumerated more cells than the cell budget; raise it with scg_set_cell_budget");
+    if (st & ST_TIE_OVERFLOW) return fail(SCG_ERR_CAP, "too many cells tie exactly at the cut key");
+    if (st & ST_ITER_CAP) return fail(SCG_ERR_CAP, "cell selection did not converge within its round cap");
+    if (st) return fail(SCG_ERR_CUDA, "search kernel reported status " + std::to_string(st));
+    return SCG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int scg_last_error(char *buf, int len) {
+    if (!buf || len <= 0) return SCG_ERR_ARG;
+    snprintf(buf, (size_t)len, "%s", g_err.c_str());
+    return SCG_OK;
+}
+
+int scg_index_create(scg_index **out, int device) {
+    if (!out) return fail(SCG_ERR_ARG, "null output pointer");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceCount");
+    if (device < 0 || device >= n) return fail(SCG_ERR_ARG, "no such CUDA device");
+    scg_index *h = new scg_index();
+    h->device = device;
+    e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_status, sizeof(int) * 4);
+    if (e != cudaSuccess) {
+        delete h;
+        return cuda_fail(e, "scg_index_create");
+    }
+    *out = h;
+    return SCG_OK;
+}
+
+int scg_index_destroy(scg_index *h) {
+    if (!h) return SCG_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    DevBuf *all[] = {&h->cq, &h->pq, &h->norm_c, &h->norm_r, &h->dot_cr, &h->off, &h->pid, &h->codes,
+                     &h->raw, &h->q, &h->dqc, &h->dqr, &h->qn, &h->qsum, &h->ids, &h->dists, &h->sums,
+                     &h->nvis, &h->empty, &h->status, &h->counter, &h->rec_key, &h->rec_rank,
+                     &h->rec_cnt, &h->vis_cell, &h->vis_pre};
+    for (DevBuf *b : all) b->release();
+    if (h->h_status) cudaFreeHost(h->h_status);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return SCG_OK;
+}
+
+int scg_load_codebooks(scg_index *h, const float *cq, int kc, int mc, const float *pq, int kp, int mp, int dim) {
+    if (!h || !cq || !pq) return fail(SCG_ERR_ARG, "null argument");
+    if (kc <= 0 || mc <= 0 || kp <= 0 || mp <= 0 || dim <= 0) return fail(SCG_ERR_ARG, "non-positive shape");
+    if (dim % mc || dim % mp || mp % mc) return fail(SCG_ERR_ARG, "dim must divide by mc and mp, mp by mc");
+    if (mc > 2) return fail(SCG_ERR_ARG, "mc must be 1 or 2");
+    if (kp > 256) return fail(SCG_ERR_ARG, "kp must be <= 256 (uint8 codes)");
+    std::lock_guard<std::mutex> g(h->mu);
+    int rc;
+    if ((rc = set_device(h))) return rc;
+    if ((rc = h->cq.ensure(sizeof(float) * (size_t)kc * dim))) return rc;
+    if ((rc = h->pq.ensure(sizeof(float) * (size_t)kp * dim))) return rc;
+    SCG_CUDA(cudaMemcpy(h->cq.p, cq, sizeof(float) * (size_t)kc * dim, cudaMemcpyHostToDevice));
+    SCG_CUDA(cudaMemcpy(h->pq.p, pq, sizeof(float) * (size_t)kp * dim, cudaMemcpyHostToDevice));
+    h->dim = dim; h->mc = mc; h->kc = kc; h->mp = mp; h->kp = kp;
+    h->have_codebooks = true;
+    h->precomputed = false;
+    return SCG_OK;
+}
+
+int scg_load_codebooks_file(scg_index *h, const char *cq_path, const char *pq_path) {
+    std::vector<float> c, p;
+    int kc, mc, dc, kp, mp, dp, rc;
+    if ((rc = read_ctr(cq_path, c, kc, mc, dc))) return rc;
+    if ((rc = read_ctr(pq_path, p, kp, mp, dp))) return rc;
+    if (dc != dp) return fail(SCG_ERR_IO, "codebook dimensions differ");
+    return scg_load_codebooks(h, c.data(), kc, mc, p.data(), kp, mp, dc);
+}
+
+int scg_load_csr(scg_index *h, const int *L, const int *pid, const uint8_t *codes, int64_t N, int64_t ncells) {
+    if (!h || !L || (N > 0 && (!pid || !codes))) return fail(SCG_ERR_ARG, "null argument");
+    if (!h->have_codebooks) return fail(SCG_ERR_STATE, "load codebooks before encoded data");
+    if (N < 0 || N > 0xfffffffeLL) return fail(SCG_ERR_ARG, "N out of range");
+    int64_t imi_cells = ipow(h->kc, h->mc), sc_cells = (int64_t)h->kc * h->kc;
+    if (ncells != imi_cells && !(h->mc == 1 && ncells == sc_cells))
+        return fail(SCG_ERR_ARG, "ncells must be kc^mc or kc^2 (second-candidate)");
+    std::vector<uint32_t> off((size_t)ncells + 1);
+    off[0] = 0;
+    int prev = 0;
+    for (int64_t c = 0; c < ncells; c++) {
+        if (L[c] < prev) return fail(SCG_ERR_ARG, "L must be a non-decreasing inclusive prefix");
+        prev = L[c];
+        off[(size_t)c + 1] = (uint32_t)L[c];
+    }
+    if ((int64_t)prev != N) return fail(SCG_ERR_ARG, "L[ncells-1] must equal N");
+    for (int64_t i = 0; i < N * h->mp; i++)
+        if (codes[i] >= h->kp) return fail(SCG_ERR_ARG, "a code is not below kp");
+    for (int64_t i = 0; i < N; i++)
+        if (pid[i] < 0) return fail(SCG_ERR_ARG, "negative pid");
+    std::lock_guard<std::mutex> g(h->mu);
+    int rc;
+    if ((rc = set_device(h))) return rc;
+    if ((rc = h->off.ensure(sizeof(uint32_t) * off.size()))) return rc;
+    if ((rc = h->pid.ensure(sizeof(int) * (size_t)(N ? N : 1)))) return rc;
+    if ((rc = h->codes.ensure((size_t)(N ? N : 1) * h->mp))) return rc;
+    SCG_CUDA(cudaMemcpy(h->off.p, off.data(), sizeof(uint32_t) * off.size(), cudaMemcpyHostToDevice));
+    if (N) {
+        SCG_CUDA(cudaMemcpy(h->pid.p, pid, sizeof(int) * (size_t)N, cudaMemcpyHostToDevice));
+        SCG_CUDA(cudaMemcpy(h->codes.p, codes, (size_t)N * h->mp, cudaMemcpyHostToDevice));
+    }
+    h->N = N;
+    h->ncells = ncells;
+    h->have_csr = true;
+    return SCG_OK;
+}
+
+int scg_load_encoded_file(scg_index *h, const char *path, int nc) {
+    if (!h || !path) return fail(SCG_ERR_ARG, "null argument");
+    if (!h->have_codebooks) return fail(SCG_ERR_STATE, "load codebooks before encoded data");
+    int64_t ncells = ipow(h->kc, nc);
+    std::vector<unsigned char> b;
+    if (!read_file(path, b)) return fail(SCG_ERR_IO, std::string("cannot read ") + path);
+    if (b.size() < 8) return fail(SCG_ERR_IO, "encoded file too short");
+    int hdr[2];
+    memcpy(hdr, b.data(), 8);
+    int64_t N = hdr[1];
+    if (N < 0) return fail(SCG_ERR_IO, "negative N in encoded file");
+    std::vector<int> L((size_t)ncells), pid((size_t)(N ? N : 1));
+    std::vector<uint8_t> codes((size_t)(N ? N : 1) * h->mp);
+    size_t pos = 8;
+    int64_t base = 0, acc = 0;
+    for (int64_t c = 0; c < ncells; c++) {
+        if (pos + 4 > b.size()) return fail(SCG_ERR_IO, "encoded file truncated (cell lengths)");
+        int l;
+        memcpy(&l, b.data() + pos, 4);
+        pos += 4;
+        if (l < 0 || base + l > N) return fail(SCG_ERR_IO, "encoded file: bad cell length");
+        if (l > 0) {
+            size_t need = (size_t)l * 4 + (size_t)l * h->mp;
+            if (pos + need > b.size()) return fail(SCG_ERR_IO, "encoded file truncated (cell data)");
+            memcpy(pid.data() + base, b.data() + pos, (size_t)l * 4);
+            pos += (size_t)l * 4;
+            memcpy(codes.data() + base * h->mp, b.data() + pos, (size_t)l * h->mp);
+            pos += (size_t)l * h->mp;
+            base += l;
+        }
+        acc += l;
+        L[(size_t)c] = (int)acc;
+    }
+    if (base != N) return fail(SCG_ERR_IO, "encoded file: cell lengths do not sum to N");
+    return scg_load_csr(h, L.data(), pid.data(), codes.data(), N, ncells);
+}
+
+int scg_load_raw(scg_index *h, const float *X, int64_t N) {
+    if (!h || !X) return fail(SCG_ERR_ARG, "null argument");
+    if (!h->have_codebooks) return fail(SCG_ERR_STATE, "load codebooks first");
+    std::lock_guard<std::mutex> g(h->mu);
+    int rc;
+    if ((rc = set_device(h))) return rc;
+    if ((rc = h->raw.ensure(sizeof(float) * (size_t)N * h->dim))) return rc;
+    SCG_CUDA(cudaMemcpy(h->raw.p, X, sizeof(float) * (size_t)N * h->dim, cudaMemcpyHostToDevice));
+    return SCG_OK;
+}
+
+int scg_precompute(scg_index *h) {
+    if (!h) return fail(SCG_ERR_ARG, "null index");
+    if (!h->have_codebooks) return fail(SCG_ERR_STATE, "codebooks not loaded");
+    std::lock_guard<std::mutex> g(h->mu);
+    int rc;
+    if ((rc = set_device(h))) return rc;
+    if ((rc = h->norm_c.ensure(sizeof(float) * (size_t)h->mc * h->kc))) return rc;
+    if ((rc = h->norm_r.ensure(sizeof(float) * (size_t)h->mp * h->kp))) return rc;
+    if ((rc = h->dot_cr.ensure(sizeof(float) * (size_t)h->kc * h->kp * h->mp))) return rc;
+    launch_precompute1(h->dim, h->mc, h->kc, h->mp, h->kp, h->cq.as<float>(), h->pq.as<float>(),
+                       h->norm_c.as<float>(), h->norm_r.as<float>(), h->dot_cr.as<float>(), h->stream);
+    SCG_CUDA(cudaGetLastError());
+    SCG_CUDA(cudaStreamSynchronize(h->stream));
+    h->precomputed = true;
+    return SCG_OK;
+}
+
+int scg_search_device(scg_index *h, const scg_search_params *p, const float *dQ, int nq, int *d_ids, float *d_dists,
+                      int *d_sums, void *stream) {
+    int rc;
+    if ((rc = check_ready(h))) return rc;
+    if ((rc = check_params(h, p, nq))) return rc;
+    if (nq > 0 && (!dQ || !d_ids || !d_dists || !d_sums)) return fail(SCG_ERR_ARG, "null buffer");
+    std::lock_guard<std::mutex> g(h->mu);
+    if ((rc = set_device(h))) return rc;
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+    return run_search(h, p, dQ, nq, d_ids, d_dists, d_sums, s);
+}
+
+int scg_search(scg_index *h, const scg_search_params *p, const float *Q, int nq, int *ids, float *dists, int *sums) {
+    int rc;
+    if ((rc = check_ready(h))) return rc;
+    if ((rc = check_params(h, p, nq))) return rc;
+    if (nq > 0 && (!Q || !ids || !dists)) return fail(SCG_ERR_ARG, "null buffer");
+    std::lock_guard<std::mutex> g(h->mu);
+    if ((rc = set_device(h))) return rc;
+    if (nq == 0) return SCG_OK;
+    cudaStream_t s = h->stream;
+    const int R = p->R;
+    if ((rc = h->q.ensure(sizeof(float) * (size_t)nq * h->dim))) return rc;
+    if ((rc = h->ids.ensure(sizeof(int) * (size_t)nq * R))) return rc;
+    if ((rc = h->dists.ensure(sizeof(float) * (size_t)nq * R))) return rc;
+    if ((rc = h->sums.ensure(sizeof(int) * (size_t)nq))) return rc;
+    SCG_CUDA(cudaMemcpyAsync(h->q.p, Q, sizeof(float) * (size_t)nq * h->dim, cudaMemcpyHostToDevice, s));
+    const int *saved = h->d_Tq;
+    h->d_Tq = nullptr;
+    rc = run_search(h, p, h->q.as<float>(), nq, h->ids.as<int>(), h->dists.as<float>(), h->sums.as<int>(), s);
+    h->d_Tq = saved;
+    if (rc) return rc;
+    SCG_CUDA(cudaMemcpyAsync(ids, h->ids.p, sizeof(int) * (size_t)nq * R, cudaMemcpyDeviceToHost, s));
+    SCG_CUDA(cudaMemcpyAsync(dists, h->dists.p, sizeof(float) * (size_t)nq * R, cudaMemcpyDeviceToHost, s));
+    if (sums) SCG_CUDA(cudaMemcpyAsync(sums, h->sums.p, sizeof(int) * (size_t)nq, cudaMemcpyDeviceToHost, s));
+    SCG_CUDA(cudaStreamSynchronize(s));
+    return SCG_OK;
+}
+
+int scg_set_query_targets(scg_index *h, const int *d_T) {
+    if (!h) return fail(SCG_ERR_ARG, "null index");
+    h->d_Tq = d_T;
+    return SCG_OK;
+}
+
+int scg_set_cell_budget(scg_index *h, int max_cells) {
+    if (!h) return fail(SCG_ERR_ARG, "null index");
+    if (max_cells < 64) return fail(SCG_ERR_ARG, "cell budget must be >= 64");
+    h->cap_rec = max_cells;
+    return SCG_OK;
+}
+
+int scg_encode_device(scg_index *h, const float *dX, int64_t n, int nc, uint16_t *d_cid, uint8_t *d_codes,
+                      void *stream) {
+    if (!h) return fail(SCG_ERR_ARG, "null index");
+    if (!h->have_codebooks) return fail(SCG_ERR_STATE, "codebooks not loaded");
+    if (n < 0) return fail(SCG_ERR_ARG, "n < 0");
+    if (n > 0 && (!dX || !d_cid || !d_codes)) return fail(SCG_ERR_ARG, "null buffer");
+    if (nc != 0 && nc != 2 && nc != 3) return fail(SCG_ERR_ARG, "nc must be 0 (IVF/IMI), 2 or 3");
+    if (nc && h->mc != 1) return fail(SCG_ERR_ARG, "the second-candidate encoder needs mc = 1");
+    if (nc > h->kc) return fail(SCG_ERR_ARG, "nc > kc");
+    int mcp = nc ? 1 : h->mc;
+    size_t smem = sizeof(float) * (8192 + (size_t)(h->dim / mcp) * 64 + (size_t)h->dim * 64);
+    if (smem > 227 * 1024) return fail(SCG_ERR_ARG, "dimension too large for the encoder's shared-memory tile");
+    std::lock_guard<std::mutex> g(h->mu);
+    int rc;
+    if ((rc = set_device(h))) return rc;
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+    EncodeArgs a;
+    a.dim = h->dim; a.mc = h->mc; a.kc = h->kc; a.mp = h->mp; a.kp = h->kp; a.nc = nc; a.n = n;
+    a.X = dX; a.cq = h->cq.as<float>(); a.pq = h->pq.as<float>(); a.cid = d_cid; a.codes = d_codes;
+    launch_encode(a, s);
+    SCG_CUDA(cudaGetLastError());
+    SCG_CUDA(cudaStreamSynchronize(s));
+    return SCG_OK;
+}
+
+static int encode_host(scg_index *h, const float *X, int64_t n, int nc, uint16_t *cid, uint8_t *codes) {
+    if (!h) return fail(SCG_ERR_ARG, "null index");
+    if (!h->have_codebooks) return fail(SCG_ERR_STATE, "codebooks not loaded");
+    if (n <= 0) return n == 0 ? SCG_OK : fail(SCG_ERR_ARG, "n < 0");
+    if (!X || !cid || !codes) return fail(SCG_ERR_ARG, "null buffer");
+    int rc;
+    if ((rc = set_device(h))) return rc;
+    int ncid = nc ? nc : h->mc;
+    DevBuf x, c, k;
+    if ((rc = x.ensure(sizeof(float) * (size_t)n * h->dim))) return rc;
+    if ((rc = c.ensure(sizeof(uint16_t) * (size_t)n * ncid))) { x.release(); return rc; }
+    if ((rc = k.ensure((size_t)n * h->mp))) { x.release(); c.release(); return rc; }
+    cudaError_t e = cudaMemcpy(x.p, X, sizeof(float) * (size_t)n * h->dim, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        rc = scg_encode_device(h, x.as<float>(), n, nc, c.as<uint16_t>(), k.as<uint8_t>(), nullptr);
+        if (rc == SCG_OK) {
+            e = cudaMemcpy(cid, c.p, sizeof(uint16_t) * (size_t)n * ncid, cudaMemcpyDeviceToHost);
+            if (e == cudaSuccess) e = cudaMemcpy(codes, k.p, (size_t)n * h->mp, cudaMemcpyDeviceToHost);
+        }
+    }
+    x.release(); c.release(); k.release();
+    if (e != cudaSuccess) return cuda_fail(e, "encode copies");
+    return rc;
+}
+
+int scg_encode(scg_index *h, const float *X, int64_t n, uint16_t *cid, uint8_t *codes) {
+    return encode_host(h, X, n, 0, cid, codes);
+}
+
+int scg_sc_encode(scg_index *h, const float *X, int64_t n, int nc, uint16_t *cid, uint8_t *codes) {
+    if (nc < 2) return fail(SCG_ERR_ARG, "nc must be >= 2");
+    return encode_host(h, X, n, nc, cid, codes);
+}
+
+int scg_index_info(scg_index *h, int *dim, int *mc, int *kc, int *mp, int *kp, int64_t *N) {
+    if (!h) return fail(SCG_ERR_ARG, "null index");
+    if (dim) *dim = h->dim;
+    if (mc) *mc = h->mc;
+    if (kc) *kc = h->kc;
+    if (mp) *mp = h->mp;
+    if (kp) *kp = h->kp;
+    if (N) *N = h->N;
+    return SCG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,104 @@
+// Internal declarations shared by the CUDA translation units of libscgpu.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "scg.h"
+
+namespace scg {
+
+// ---------------------------------------------------------------------------
+// Host-side error plumbing
+
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+
+#define SCG_CUDA(call)                                         \
+    do {                                                       \
+        cudaError_t _e = (call);                               \
+        if (_e != cudaSuccess) return ::scg::cuda_fail(_e, #call); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Device helpers
+
+// Order-preserving map of a float onto uint32 (negative zero maps as zero).
+__device__ __forceinline__ uint32_t f2o(float f) {
+    uint32_t u = __float_as_uint(f);
+    if (u == 0x80000000u) u = 0u;
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float o2f(uint32_t o) {
+    uint32_t u = (o & 0x80000000u) ? (o & 0x7fffffffu) : ~o;
+    return __uint_as_float(u);
+}
+
+// Status word bits written by kernels (never a trap).
+enum : int {
+    ST_OK = 0,
+    ST_CELL_BUDGET = 1,   // a query enumerated more cells than the budget
+    ST_TIE_OVERFLOW = 2,  // more exact key ties at the cut than the tie buffer
+    ST_ITER_CAP = 4,      // an iteration cap was reached
+    ST_BAD_ARG = 8,
+};
+
+// ---------------------------------------------------------------------------
+// Kernel launch wrappers (defined in the .cu files)
+
+struct TablesArgs {
+    int dim, mc, kc, mp, kp, nq;
+    const float *Q;        // [nq][dim]
+    const float *cq, *pq;  // codebooks
+    const float *norm_c, *norm_r;
+    float *dqc;            // [nq][mc*kc]
+    float *dqr;            // [nq][mp*kp]
+    float *qn;             // [nq][2] half norms (IMI) or [nq][2] = {q_sum, 0}
+    float *qsum;           // [nq]
+};
+
+void launch_precompute1(int dim, int mc, int kc, int mp, int kp, const float *cq, const float *pq,
+                        float *norm_c, float *norm_r, float *dot_cr, cudaStream_t s);
+void launch_tables_exact(const TablesArgs &a, cudaStream_t s);
+
+struct SearchArgs {
+    int mode, dim, mc, kc, mp, kp, nq, R, w, T;
+    int precision;
+    const int *Tq;          // optional per-query T
+    const float *dqc, *dqr, *qn, *qsum;
+    const uint32_t *off;    // [ncells+1] exclusive offsets
+    const int *pid;
+    const uint8_t *codes;
+    const float *dot_cr;
+    const float *vterm;     // per-vector term of the fast form (may be null)
+    uint64_t ncells;
+    int64_t N;
+    // per-CTA scratch slots
+    uint32_t *rec_key, *rec_rank, *rec_cnt;  // [slots][cap_rec]
+    uint32_t *vis_cell, *vis_pre;            // [slots][cap_rec + 1]
+    int cap_rec;
+    int *qcounter;                           // dynamic query counter
+    // outputs
+    int *out_ids;
+    float *out_d;
+    int *out_sum, *out_nvis, *out_empty;
+    int *status;
+};
+
+size_t search_smem_bytes(int mode, int kc, int mp, int kp);
+int search_launch(const SearchArgs &a, int grid, cudaStream_t s);
+int search_max_blocks_per_sm(int mode, int kc, int mp, int kp);
+
+struct EncodeArgs {
+    int dim, mc, kc, mp, kp, nc;  // nc = 0: IVF/IMI encoder; nc >= 2: SC encoder
+    int64_t n;
+    const float *X, *cq, *pq;
+    uint16_t *cid;
+    uint8_t *codes;
+};
+void launch_encode(const EncodeArgs &a, cudaStream_t s);
+
+}  // namespace scg

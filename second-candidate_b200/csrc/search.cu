@@ -1,0 +1,802 @@
+// Fused batched search: per query, coarse ranking -> multi-sequence cell
+// selection -> ADC scan with a fused top-R.  One CTA works on one query at a
+// time and takes the next query from a global counter, so queries with
+// uneven posting-list totals balance across the persistent grid.
+//
+// Cell selection.  The reference walks the grid of rank pairs (h1, h2) of two
+// sorted coarse lists with a binary heap (multi_query.h:133-205,
+// sc_query.h:112-186) and stops after the first cell at which the candidate
+// total reaches T (or the cell cap w).  The visited set is therefore a
+// prefix of the cells sorted by key(h1,h2) = A[h1] + B[h2].  Here the prefix
+// is found without a serial heap:
+//   1. rounds of "all cells with key <= tau": tau is bisected so that the
+//      staircase {key <= tau} holds about a target number of cells (one
+//      binary search per row, all rows in parallel); the new cells of the
+//      round are enumerated, their lengths read from the CSR offsets and
+//      kept as records (key, rank pair, length) in a per-CTA scratch slot;
+//   2. once the totals reach T (or w), the exact cut key is found by a radix
+//      select over the last round's records, weighted by length (or by
+//      cell count for the w rule);
+//   3. cells tied at the cut key are taken in (rank1, rank2) order until the
+//      rule fires -- the order an exact priority queue yields.
+// The ADC scan then walks the visited cells' candidates with one candidate
+// per thread, adds the table entries in the reference's order, and keeps
+// the R smallest (distance, id) pairs: a threshold filter feeds a shared
+// buffer that is merged by a bitonic sort when full.
+#include "scg_internal.cuh"
+
+namespace scg {
+
+namespace {
+
+constexpr int NT = 512;
+constexpr int NWARP = NT / 32;
+constexpr int HBITS = 11;
+constexpr int HBINS = 1 << HBITS;
+constexpr int TIECAP = 64;
+constexpr int MERGE_N = 4096;
+constexpr int MAX_ROUNDS = 64;
+
+struct CellWin {
+    uint32_t pre;    // candidates before this cell (flat index)
+    uint32_t start;  // CSR start
+    float d0;        // per-cell constant of the ADC sum
+    uint32_t h34;    // h3 | h4 << 16
+};
+
+__host__ __device__ __forceinline__ int next_pow2(int x) {
+    int p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+__host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+struct Smem {
+    uint64_t *LA, *LB;
+    uint16_t *rowc, *rowp;
+    uint32_t *rowpre;
+    float *lut;
+    unsigned char *uni;
+};
+
+__host__ __device__ inline size_t carve(int mode, int kc, int mp, int kp, Smem *s, unsigned char *base) {
+    int kcP = next_pow2(kc);
+    size_t off = 0;
+    size_t la = (size_t)kcP * 8;
+    size_t lb = (mode == SCG_IMI) ? (size_t)kcP * 8 : 0;
+    if (s) s->LA = (uint64_t *)(base + off);
+    off += la;
+    if (s) s->LB = (mode == SCG_IMI) ? (uint64_t *)(base + off) : s->LA;
+    off += lb;
+    if (s) s->rowc = (uint16_t *)(base + off);
+    off += align16((size_t)kc * 2);
+    if (s) s->rowp = (uint16_t *)(base + off);
+    off += align16((size_t)kc * 2);
+    if (s) s->rowpre = (uint32_t *)(base + off);
+    off += align16((size_t)(kc + 1) * 4);
+    if (s) s->lut = (float *)(base + off);
+    off += align16((size_t)mp * kp * 4);
+    if (s) s->uni = base + off;
+    size_t trav = (size_t)HBINS * 4 + (size_t)TIECAP * 8;
+    size_t scan = (size_t)MERGE_N * 8 + (size_t)NT * sizeof(CellWin);
+    off += (trav > scan ? trav : scan);
+    return off;
+}
+
+// ---------------------------------------------------------------------------
+// Block-wide helpers (NT threads, all threads must call)
+
+__device__ __forceinline__ uint64_t warp_sum64(uint64_t v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sums three values over the block.
+__device__ void block_sum3(uint64_t &a, uint64_t &b, uint64_t &c, uint64_t *red) {
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    a = warp_sum64(a);
+    b = warp_sum64(b);
+    c = warp_sum64(c);
+    __syncthreads();
+    if (lane == 0) {
+        red[wid] = a;
+        red[NWARP + wid] = b;
+        red[2 * NWARP + wid] = c;
+    }
+    __syncthreads();
+    uint64_t x = 0, y = 0, z = 0;
+    for (int i = 0; i < NWARP; i++) {
+        x += red[i];
+        y += red[NWARP + i];
+        z += red[2 * NWARP + i];
+    }
+    a = x;
+    b = y;
+    c = z;
+    __syncthreads();
+}
+
+__device__ uint64_t block_sum(uint64_t v, uint64_t *red) {
+    uint64_t b = 0, c = 0;
+    block_sum3(v, b, c, red);
+    return v;
+}
+
+// Exclusive scan of one u64 per thread; returns the exclusive prefix and the
+// block total.
+__device__ uint64_t block_exscan(uint64_t v, uint64_t *red, uint64_t &total) {
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint64_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    __syncthreads();
+    if (lane == 31) red[wid] = x;
+    __syncthreads();
+    uint64_t wpre = 0, tot = 0;
+    for (int i = 0; i < NWARP; i++) {
+        uint64_t r = red[i];
+        if (i < wid) wpre += r;
+        tot += r;
+    }
+    total = tot;
+    __syncthreads();
+    return wpre + x - v;
+}
+
+__device__ void bitonic_sort64(uint64_t *key, int n) {
+    for (int k = 2; k <= n; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < n; i += NT) {
+                int ixj = i ^ j;
+                if (ixj > i) {
+                    uint64_t x = key[i], y = key[ixj];
+                    bool up = (i & k) == 0;
+                    if ((x > y) == up) {
+                        key[i] = y;
+                        key[ixj] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+
+struct Lists {
+    const uint64_t *LA, *LB;
+    int kc, kB;
+    bool ivf;
+    __device__ __forceinline__ float a(int h) const { return o2f((uint32_t)(LA[h] >> 32)); }
+    __device__ __forceinline__ float b(int h) const { return ivf ? 0.0f : o2f((uint32_t)(LB[h] >> 32)); }
+    __device__ __forceinline__ uint32_t ta(int h) const { return (uint32_t)LA[h]; }
+    __device__ __forceinline__ uint32_t tb(int h) const { return (uint32_t)LB[h]; }
+    // number of h2 in [0, kB) with f2o(a + B[h2]) <= tau
+    __device__ __forceinline__ int row_count(float av, uint32_t tau) const {
+        if (f2o(__fadd_rn(av, b(0))) > tau) return 0;
+        int lo = 1, hi = kB;  // answer in [1, kB]
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (f2o(__fadd_rn(av, b(mid - 1))) <= tau) lo = mid;
+            else hi = mid - 1;
+        }
+        return lo;
+    }
+};
+
+__device__ uint64_t staircase_count(const Lists &L, uint32_t tau, uint64_t *red) {
+    uint64_t c = 0;
+    for (int h = threadIdx.x; h < L.kc; h += NT) c += (uint64_t)L.row_count(L.a(h), tau);
+    return block_sum(c, red);
+}
+
+// Radix select over the last round's records [r0, r1): the smallest key x
+// with base + sum_{key <= x} weight >= need.  weight: 0 = length, 1 = one per
+// cell, 2 = one per non-empty cell.  Returns x and sets *below to
+// base + sum_{key < x} weight.
+__device__ uint32_t radix_cut(const uint32_t *rk, const uint32_t *rc, int r0, int r1, uint32_t lo,
+                              uint32_t hi, uint64_t base, uint64_t need, int weight, uint32_t *hist,
+                              uint64_t *red, uint64_t *below, uint32_t *s_bin, uint64_t *s_acc) {
+    uint32_t range = hi - lo;
+    int nbits = range ? 32 - __clz(range) : 0;
+    uint32_t prefix = 0;
+    uint64_t acc = base;
+    int shift = nbits;
+    while (shift > 0) {
+        int db = shift < HBITS ? shift : HBITS;
+        shift -= db;
+        int nb = 1 << db;
+        for (int i = threadIdx.x; i < nb; i += NT) hist[i] = 0;
+        __syncthreads();
+        int hs = shift + db;
+        for (int r = r0 + threadIdx.x; r < r1; r += NT) {
+            uint32_t rel = rk[r] - lo;
+            if (hs < 32 && (rel >> hs) != (prefix >> hs)) continue;
+            uint32_t dg = (rel >> shift) & (nb - 1);
+            uint32_t c = rc[r];
+            uint32_t wt = weight == 0 ? c : (weight == 1 ? 1u : (c > 0 ? 1u : 0u));
+            if (wt) atomicAdd(&hist[dg], wt);
+        }
+        __syncthreads();
+        // first bin at which acc + inclusive prefix >= need
+        int per = (nb + NT - 1) / NT;
+        int b0 = threadIdx.x * per;
+        uint64_t mine = 0;
+        for (int i = 0; i < per; i++)
+            if (b0 + i < nb) mine += hist[b0 + i];
+        uint64_t tot;
+        uint64_t ex = block_exscan(mine, red, tot);
+        uint64_t run = acc + ex;
+        for (int i = 0; i < per; i++) {
+            int bb = b0 + i;
+            if (bb >= nb) break;
+            uint64_t nxt = run + hist[bb];
+            if (run < need && nxt >= need) {
+                *s_bin = (uint32_t)bb;
+                *s_acc = run;
+            }
+            run = nxt;
+        }
+        __syncthreads();
+        prefix |= (*s_bin) << shift;
+        acc = *s_acc;
+        __syncthreads();
+    }
+    if (nbits == 0) {
+        // all keys equal lo: everything below is the base
+        acc = base;
+    }
+    *below = acc;
+    return lo + prefix;
+}
+
+__device__ __forceinline__ uint32_t cell_of(const Lists &L, bool ivf, uint32_t rank) {
+    int h1 = rank >> 16, h2 = rank & 0xffff;
+    return ivf ? L.ta(h1) : L.ta(h1) * (uint32_t)L.kc + L.tb(h2);
+}
+
+struct QState {
+    int err;
+    uint32_t tau;
+    uint32_t s_bin;
+    uint64_t s_acc;
+    uint32_t kappa;
+    uint32_t rank_cut;
+    int take_all;
+    int nties;
+    uint64_t sumv, nv, nev;
+    int nvis;
+    // scan
+    int ncur, npend;
+    uint64_t thr;
+    int clo, cn;
+    uint32_t wend;
+};
+
+__global__ void __launch_bounds__(NT) k_search(SearchArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint64_t red[3 * NWARP];
+    __shared__ QState st;
+    __shared__ int s_q;
+    Smem S;
+    carve(a.mode, a.kc, a.mp, a.kp, &S, smem);
+    const int tid = threadIdx.x;
+    const int kc = a.kc, mp = a.mp, kp = a.kp;
+    const int kcP = next_pow2(kc);
+    const bool imi = a.mode == SCG_IMI, sc = a.mode == SCG_SC2, ivf = a.mode == SCG_IVFADC;
+    const int kB = ivf ? 1 : kc;
+    const int cap = a.cap_rec;
+    uint32_t *rec_key = a.rec_key + (size_t)blockIdx.x * cap;
+    uint32_t *rec_rank = a.rec_rank + (size_t)blockIdx.x * cap;
+    uint32_t *rec_cnt = a.rec_cnt + (size_t)blockIdx.x * cap;
+    uint32_t *vis_cell = a.vis_cell + (size_t)blockIdx.x * (cap + 1);
+    uint32_t *vis_pre = a.vis_pre + (size_t)blockIdx.x * (cap + 1);
+    uint32_t *hist = (uint32_t *)S.uni;
+    uint64_t *ties = (uint64_t *)(S.uni + (size_t)HBINS * 4);
+    uint64_t *topk = (uint64_t *)S.uni;
+    CellWin *win = (CellWin *)(S.uni + (size_t)MERGE_N * 8);
+    const int bsI = kp * mp / a.mc;  // dot_cr block of one coarse centroid
+    const uint64_t total_cells = (uint64_t)kc * kB - (sc ? 1 : 0);
+    const double avg_density = (double)a.N / (double)(a.ncells ? a.ncells : 1);
+
+    for (;;) {
+        if (tid == 0) s_q = atomicAdd(a.qcounter, 1);
+        __syncthreads();
+        const int q = s_q;
+        if (q >= a.nq) break;
+        const int T = a.Tq ? a.Tq[q] : a.T;
+        const int w = a.w;
+        const int R = a.R;
+        const float *dqc = a.dqc + (size_t)q * a.mc * kc;
+        const float qn0 = a.qn[2 * q], qn1 = a.qn[2 * q + 1], qs = a.qsum[q];
+
+        // (1) sorted coarse lists (sort_id/nth_element_id with M = kc;
+        //     multi_query.h:114-128, sc_query.h:98-106, query.h:230-234):
+        //     key | centroid id, equal keys by id.
+        for (int h = tid; h < kcP; h += NT) {
+            if (h < kc) {
+                float ka = __fadd_rn(imi ? qn0 : qs, dqc[h]);
+                S.LA[h] = ((uint64_t)f2o(ka) << 32) | (uint32_t)h;
+                if (imi) {
+                    float kb = __fadd_rn(qn1, dqc[kc + h]);
+                    S.LB[h] = ((uint64_t)f2o(kb) << 32) | (uint32_t)h;
+                }
+            } else {
+                S.LA[h] = ~0ull;
+                if (imi) S.LB[h] = ~0ull;
+            }
+        }
+        for (int i = tid; i < mp * kp; i += NT) S.lut[i] = a.dqr[(size_t)q * mp * kp + i];
+        if (tid == 0) st.err = 0;
+        __syncthreads();
+        bitonic_sort64(S.LA, kcP);
+        if (imi) bitonic_sort64(S.LB, kcP);
+        Lists L{S.LA, S.LB, kc, kB, ivf};
+
+        // IMI and SC test the rules before each pop (multi_query.h:151,
+        // sc_query.h:130); IVFADC pops first and tests after
+        // (query.h:249-259), so T <= 0 still visits one cell there.
+        const bool nothing = (w <= 0) || (!ivf && T <= 0);
+        uint64_t needT = (uint64_t)(T > 0 ? T : 0);
+        uint64_t needW = (uint64_t)(w > 0 ? w : 0);
+        if (ivf && T <= 0) {
+            needT = ~0ull;
+            needW = 1;
+        }
+
+        // (2) rounds of staircase enumeration
+        for (int h = tid; h < kc; h += NT) S.rowp[h] = (sc && h == 0) ? 1 : 0;
+        uint64_t Ssum = 0, Ncell = 0, NEc = 0;  // totals over enumerated cells
+        uint64_t S0 = 0, N0 = 0, NE0 = 0;
+        int nrec = 0, r0 = 0;
+        bool trig = false;
+        uint32_t tau_prev = 0;
+        const uint32_t lo_key = f2o(__fadd_rn(L.a(0), L.b(0)));
+        const uint32_t hi_key = f2o(__fadd_rn(L.a(kc - 1), L.b(kB - 1)));
+        uint64_t target = 0;
+        {
+            double t0 = (T > 0 ? (double)T : 1.0) / (avg_density > 1e-9 ? avg_density : 1e-9);
+            target = (uint64_t)(t0 * 0.75) + 64;
+            if (sc) target += 1;
+        }
+        __syncthreads();
+        int round = 0;
+        if (!nothing) {
+            for (; round < MAX_ROUNDS; round++) {
+                uint64_t grid_cells = (uint64_t)kc * kB;
+                if (target > grid_cells) target = grid_cells;
+                if (!sc && needW < target) {
+                    // the w rule caps popped cells: never enumerate past w
+                    uint64_t tw = needW;
+                    if (tw < Ncell + 1) tw = Ncell + 1;
+                    if (tw < target) target = tw;
+                }
+                // bisection for tau: smallest key with staircase count >= target
+                uint32_t lo = round == 0 ? lo_key : tau_prev + 1, hi = hi_key;
+                uint64_t thi = target + target / 4 + 32;
+                if (lo > hi) lo = hi;
+                int it = 0;
+                while (lo < hi && it < 40) {
+                    uint32_t mid = lo + ((hi - lo) >> 1);
+                    uint64_t c = staircase_count(L, mid, red);
+                    if (c >= target) {
+                        hi = mid;
+                        if (c <= thi) break;
+                    } else {
+                        lo = mid + 1;
+                    }
+                    it++;
+                }
+                const uint32_t tau = hi;
+                tau_prev = tau;
+                // row counts at tau and the new cells per row
+                uint32_t mycnt = 0;
+                const int per = (kc + NT - 1) / NT;
+                const int hb = tid * per;
+                for (int i = 0; i < per; i++) {
+                    int h = hb + i;
+                    if (h >= kc) break;
+                    int c = L.row_count(L.a(h), tau);
+                    int p0 = S.rowp[h];
+                    if (c < p0) c = p0;
+                    S.rowc[h] = (uint16_t)(c > 65535 ? 65535 : c);
+                    mycnt += (uint32_t)(c - p0);
+                }
+                uint64_t tot_new;
+                uint64_t ex = block_exscan(mycnt, red, tot_new);
+                {
+                    uint32_t run = (uint32_t)ex;
+                    for (int i = 0; i < per; i++) {
+                        int h = hb + i;
+                        if (h >= kc) break;
+                        S.rowpre[h] = run;
+                        run += (uint32_t)(S.rowc[h] - S.rowp[h]);
+                    }
+                    if (tid == 0) S.rowpre[kc] = (uint32_t)tot_new;
+                }
+                if ((uint64_t)nrec + tot_new > (uint64_t)cap) {
+                    if (tid == 0) {
+                        st.err = 1;
+                        atomicOr(a.status, ST_CELL_BUDGET);
+                    }
+                    __syncthreads();
+                    break;
+                }
+                __syncthreads();
+                const int nnew = (int)tot_new;
+                uint64_t ls = 0, lne = 0, dummy = 0;
+                for (int idx = tid; idx < nnew; idx += NT) {
+                    // row of idx: last h with rowpre[h] <= idx
+                    int lo2 = 0, hi2 = kc - 1;
+                    while (lo2 < hi2) {
+                        int mid = (lo2 + hi2 + 1) >> 1;
+                        if (S.rowpre[mid] <= (uint32_t)idx) lo2 = mid;
+                        else hi2 = mid - 1;
+                    }
+                    int h1 = lo2;
+                    int h2 = S.rowp[h1] + (idx - (int)S.rowpre[h1]);
+                    float key = __fadd_rn(L.a(h1), L.b(h2));
+                    uint32_t rank = ((uint32_t)h1 << 16) | (uint32_t)h2;
+                    uint32_t cell = cell_of(L, ivf, rank);
+                    uint32_t c = a.off[cell + 1] - a.off[cell];
+                    if (sc && cell == 0) c = 0;  // sc_query.h:138-140
+                    rec_key[nrec + idx] = f2o(key);
+                    rec_rank[nrec + idx] = rank;
+                    rec_cnt[nrec + idx] = c;
+                    ls += c;
+                    lne += (c > 0);
+                }
+                block_sum3(ls, lne, dummy, red);
+                S0 = Ssum;
+                N0 = Ncell;
+                NE0 = NEc;
+                r0 = nrec;
+                nrec += nnew;
+                Ssum += ls;
+                Ncell += (uint64_t)nnew;
+                NEc += lne;
+                for (int h = tid; h < kc; h += NT) S.rowp[h] = S.rowc[h];
+                __syncthreads();
+                uint64_t wcnt = sc ? NEc : Ncell;
+                trig = (Ssum >= needT) || (wcnt >= needW);
+                if (trig || Ncell >= total_cells || tau >= hi_key) break;
+                // next target from the density seen so far
+                double dens = Ncell ? (double)Ssum / (double)Ncell : avg_density;
+                if (dens < 1e-6) dens = avg_density > 1e-6 ? avg_density : 1e-6;
+                double need_cells = (double)(needT - Ssum) / dens;
+                uint64_t grow = (uint64_t)(need_cells * 1.25) + 64;
+                uint64_t minimum = Ncell / 4 + 64;
+                target = Ncell + (sc ? 1 : 0) + (grow > minimum ? grow : minimum);
+            }
+            if (round >= MAX_ROUNDS && tid == 0) {
+                st.err = 1;
+                atomicOr(a.status, ST_ITER_CAP);
+            }
+        }
+        __syncthreads();
+        const bool qerr = st.err != 0;
+
+        // (3) the cut within the last round
+        if (!nothing && !qerr && trig) {
+            uint32_t lo = 0xffffffffu, hi = 0;
+            for (int r = r0 + tid; r < nrec; r += NT) {
+                uint32_t k = rec_key[r];
+                lo = min(lo, k);
+                hi = max(hi, k);
+            }
+            // block min / max through the reduction buffer
+            uint64_t mn = lo, mx = hi;
+            {
+                int lane = tid & 31, wid = tid >> 5;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    mn = min(mn, (uint64_t)__shfl_xor_sync(0xffffffffu, mn, o));
+                    mx = max(mx, (uint64_t)__shfl_xor_sync(0xffffffffu, mx, o));
+                }
+                __syncthreads();
+                if (lane == 0) {
+                    red[wid] = mn;
+                    red[NWARP + wid] = mx;
+                }
+                __syncthreads();
+                mn = 0xffffffffu;
+                mx = 0;
+                for (int i = 0; i < NWARP; i++) {
+                    mn = min(mn, red[i]);
+                    mx = max(mx, red[NWARP + i]);
+                }
+                __syncthreads();
+            }
+            uint32_t klo = (uint32_t)mn, khi = (uint32_t)mx;
+            uint32_t kap = 0xffffffffu;
+            uint64_t below;
+            if (Ssum >= needT)
+                kap = radix_cut(rec_key, rec_cnt, r0, nrec, klo, khi, S0, needT, 0, hist, red, &below,
+                                &st.s_bin, &st.s_acc);
+            uint64_t wcnt = sc ? NEc : Ncell;
+            if (wcnt >= needW) {
+                uint32_t kw = radix_cut(rec_key, rec_cnt, r0, nrec, klo, khi, sc ? NE0 : N0, needW,
+                                        sc ? 2 : 1, hist, red, &below, &st.s_bin, &st.s_acc);
+                if (kw < kap) kap = kw;
+            }
+            // totals strictly below kappa, and the ties at kappa
+            uint64_t ls = 0, ln = 0, lne = 0;
+            if (tid == 0) st.nties = 0;
+            __syncthreads();
+            for (int r = r0 + tid; r < nrec; r += NT) {
+                uint32_t k = rec_key[r];
+                if (k < kap) {
+                    uint32_t c = rec_cnt[r];
+                    ls += c;
+                    ln += 1;
+                    lne += (c > 0);
+                } else if (k == kap) {
+                    int slot = atomicAdd(&st.nties, 1);
+                    if (slot < TIECAP) ties[slot] = ((uint64_t)rec_rank[r] << 32) | rec_cnt[r];
+                }
+            }
+            block_sum3(ls, ln, lne, red);
+            if (tid == 0) {
+                uint64_t s = S0 + ls, n = N0 + ln, ne = NE0 + lne;
+                int nt = st.nties;
+                if (nt > TIECAP) {
+                    st.err = 1;
+                    atomicOr(a.status, ST_TIE_OVERFLOW);
+                    nt = TIECAP;
+                }
+                // ties in rank order (an exact priority queue's order)
+                for (int i = 1; i < nt; i++) {
+                    uint64_t v = ties[i];
+                    int j = i - 1;
+                    while (j >= 0 && ties[j] > v) {
+                        ties[j + 1] = ties[j];
+                        j--;
+                    }
+                    ties[j + 1] = v;
+                }
+                uint32_t rc_ = 0;
+                for (int i = 0; i < nt; i++) {
+                    uint32_t c = (uint32_t)ties[i];
+                    s += c;
+                    n += 1;
+                    ne += (c > 0);
+                    rc_ = (uint32_t)(ties[i] >> 32);
+                    if (s >= needT || (sc ? ne : n) >= needW) break;
+                }
+                st.kappa = kap;
+                st.rank_cut = rc_;
+                st.take_all = 0;
+                st.sumv = s;
+                st.nv = n;
+                st.nev = ne;
+            }
+            __syncthreads();
+        } else if (tid == 0) {
+            st.kappa = 0xffffffffu;
+            st.rank_cut = 0xffffffffu;
+            st.take_all = 1;
+            st.sumv = nothing ? 0 : Ssum;
+            st.nv = nothing ? 0 : Ncell;
+            st.nev = nothing ? 0 : NEc;
+        }
+        __syncthreads();
+
+        // (4) visited non-empty cells -> (cell, prefix) list
+        int nvis = 0;
+        if (!nothing && !st.err) {
+            const uint32_t kap = st.kappa, rcut = st.rank_cut;
+            const bool all = st.take_all != 0;
+            uint64_t pos = 0, runc = 0;
+            for (int base = 0; base < nrec; base += NT) {
+                int r = base + tid;
+                bool f = false;
+                uint32_t c = 0, rank = 0;
+                if (r < nrec) {
+                    c = rec_cnt[r];
+                    rank = rec_rank[r];
+                    uint32_t k = rec_key[r];
+                    bool inc = all || r < r0 || k < kap || (k == kap && rank <= rcut);
+                    f = inc && c > 0;
+                }
+                uint64_t v = f ? ((1ull << 40) | c) : 0ull;
+                uint64_t tot;
+                uint64_t ex = block_exscan(v, red, tot);
+                if (f) {
+                    uint64_t p = pos + (ex >> 40);
+                    vis_cell[p] = cell_of(L, ivf, rank);
+                    vis_pre[p] = (uint32_t)(runc + (ex & 0xffffffffffull));
+                }
+                pos += tot >> 40;
+                runc += tot & 0xffffffffffull;
+            }
+            nvis = (int)pos;
+            if (tid == 0) {
+                vis_pre[nvis] = (uint32_t)runc;
+                st.sumv = runc;  // the candidates of the visited cells
+            }
+        }
+        if (tid == 0) st.nvis = nvis;
+        __syncthreads();
+        nvis = st.nvis;
+        const bool qerr2 = st.err != 0;
+        const uint32_t Svis = (nvis > 0) ? (uint32_t)st.sumv : 0u;
+
+        // (5) ADC scan with the fused top-R
+        if (tid == 0) {
+            st.ncur = 0;
+            st.npend = 0;
+            st.thr = ~0ull;
+            st.clo = 0;
+            st.cn = 0;
+            st.wend = 0;
+        }
+        __syncthreads();
+        if (!qerr2 && nvis > 0) {
+            uint32_t flat0 = 0;
+            while (flat0 < Svis) {
+                // restage the cell window when the current one is consumed
+                if (flat0 >= st.wend) {
+                    int clo = st.clo + st.cn;
+                    __syncthreads();
+                    int c = clo + tid;
+                    if (c < nvis) {
+                        uint32_t cell = vis_cell[c];
+                        CellWin cw;
+                        cw.pre = vis_pre[c];
+                        cw.start = a.off[cell];
+                        uint32_t h3, h4;
+                        if (imi) {
+                            h3 = cell / (uint32_t)kc;
+                            h4 = cell - h3 * (uint32_t)kc;
+                            cw.d0 = __fadd_rn(__fadd_rn(qs, dqc[h3]), dqc[kc + h4]);
+                        } else if (sc) {
+                            h3 = cell / (uint32_t)kc;
+                            h4 = 0;
+                            cw.d0 = __fadd_rn(qs, dqc[h3]);
+                        } else {
+                            h3 = cell;
+                            h4 = 0;
+                            cw.d0 = __fadd_rn(qs, dqc[h3]);
+                        }
+                        cw.h34 = h3 | (h4 << 16);
+                        win[tid] = cw;
+                    }
+                    __syncthreads();
+                    if (tid == 0) {
+                        int cn = min(NT, nvis - clo);
+                        st.clo = clo;
+                        st.cn = cn;
+                        st.wend = (clo + cn < nvis) ? vis_pre[clo + cn] : Svis;
+                    }
+                    __syncthreads();
+                }
+                // make room for this round's candidates
+                if (st.ncur + st.npend + NT > MERGE_N) {
+                    int n = st.ncur + st.npend;
+                    int np2 = next_pow2(n);
+                    for (int i = n + tid; i < np2; i += NT) topk[i] = ~0ull;
+                    __syncthreads();
+                    bitonic_sort64(topk, np2);
+                    if (tid == 0) {
+                        int keep = n < R ? n : R;
+                        st.ncur = keep;
+                        st.npend = 0;
+                        st.thr = keep == R ? topk[R - 1] : ~0ull;
+                    }
+                    __syncthreads();
+                }
+                const uint32_t wend = st.wend;
+                const uint32_t flat = flat0 + tid;
+                const uint64_t thr = st.thr;
+                const int cn = st.cn;
+                if (flat < wend) {
+                    // window cell containing flat
+                    int lo2 = 0, hi2 = cn - 1;
+                    while (lo2 < hi2) {
+                        int mid = (lo2 + hi2 + 1) >> 1;
+                        if (win[mid].pre <= flat) lo2 = mid;
+                        else hi2 = mid - 1;
+                    }
+                    const CellWin cw = win[lo2];
+                    const uint32_t pos = cw.start + (flat - cw.pre);
+                    const uint8_t *cp = a.codes + (size_t)pos * mp;
+                    float d = cw.d0;
+                    const uint32_t h3 = cw.h34 & 0xffffu, h4 = cw.h34 >> 16;
+                    if (imi) {
+                        // multi_query.h:237-254: two adds per subspace
+                        const int half = mp >> 1;
+                        const float *r1 = a.dot_cr + (size_t)h3 * bsI;
+                        const float *r2 = a.dot_cr + (size_t)(h4 + kc - 1) * bsI;
+                        for (int k = 0; k < mp; k++) {
+                            int bc = k * kp + cp[k];
+                            d = __fadd_rn(d, S.lut[bc]);
+                            d = __fadd_rn(d, __ldg((k < half ? r1 : r2) + bc));
+                        }
+                    } else {
+                        // query.h:295-306, sc_query.h:222-229: pair sum per subspace
+                        const float *r1 = a.dot_cr + (size_t)h3 * bsI;
+                        for (int k = 0; k < mp; k++) {
+                            int bc = k * kp + cp[k];
+                            d = __fadd_rn(d, __fadd_rn(S.lut[bc], __ldg(r1 + bc)));
+                        }
+                    }
+                    uint32_t du = f2o(d);
+                    if (du <= (uint32_t)(thr >> 32)) {
+                        uint64_t e = ((uint64_t)du << 32) | (uint32_t)a.pid[pos];
+                        if (e < thr) {
+                            int slot = atomicAdd(&st.npend, 1);
+                            topk[st.ncur + slot] = e;
+                        }
+                    }
+                }
+                uint32_t step = wend > flat0 ? wend - flat0 : 0u;
+                if (step > (uint32_t)NT) step = NT;
+                __syncthreads();
+                if (step == 0) {
+                    // cannot happen with consistent prefixes; stop instead of spinning
+                    if (tid == 0) atomicOr(a.status, ST_ITER_CAP);
+                    break;
+                }
+                flat0 += step;
+            }
+            // final merge
+            int n = st.ncur + st.npend;
+            int np2 = next_pow2(n > 1 ? n : 2);
+            for (int i = n + tid; i < np2; i += NT) topk[i] = ~0ull;
+            __syncthreads();
+            bitonic_sort64(topk, np2);
+        }
+        __syncthreads();
+        // (6) outputs
+        {
+            int n = (qerr2 || nvis == 0) ? 0 : st.ncur + st.npend;
+            int keep = n < R ? n : R;
+            for (int j = tid; j < R; j += NT) {
+                size_t o = (size_t)q * R + j;
+                if (j < keep) {
+                    uint64_t e = topk[j];
+                    a.out_ids[o] = (int)(uint32_t)e;
+                    a.out_d[o] = o2f((uint32_t)(e >> 32));
+                } else {
+                    a.out_ids[o] = -1;
+                    a.out_d[o] = __int_as_float(0x7f800000);
+                }
+            }
+            if (tid == 0) {
+                a.out_sum[q] = qerr2 ? -1 : (int)(nothing ? 0 : st.sumv);
+                if (a.out_nvis) a.out_nvis[q] = nvis;
+                if (a.out_empty) a.out_empty[q] = qerr2 ? 0 : (int)(st.nv - st.nev);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+}  // namespace
+
+size_t search_smem_bytes(int mode, int kc, int mp, int kp) { return carve(mode, kc, mp, kp, nullptr, nullptr); }
+
+int search_max_blocks_per_sm(int mode, int kc, int mp, int kp) {
+    size_t smem = search_smem_bytes(mode, kc, mp, kp);
+    cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search, NT, smem);
+    return nb;
+}
+
+int search_launch(const SearchArgs &a, int grid, cudaStream_t s) {
+    size_t smem = search_smem_bytes(a.mode, a.kc, a.mp, a.kp);
+    cudaError_t e = cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_search)");
+    k_search<<<grid, NT, smem, s>>>(a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "k_search launch");
+    return SCG_OK;
+}
+
+}  // namespace scg

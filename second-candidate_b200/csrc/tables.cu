@@ -1,0 +1,174 @@
+// ADC tables: query-independent (pre_compute1) and per-query (pre_compute2).
+//
+// The exact form reproduces the reference's float arithmetic: every dot
+// product is a sequential loop in which each multiply and each add rounds on
+// its own (__fmul_rn / __fadd_rn, so nothing is contracted into an FMA), in
+// the reference's order.  Entries are therefore bit-identical to
+// PQQuery::pre_compute1 / pre_compute2 (query.h:91-184) with BLAS sdot taken
+// as the sequential loop.
+#include "scg_internal.cuh"
+
+namespace scg {
+
+namespace {
+
+__device__ __forceinline__ float seq_dot(const float *x, const float *y, int n) {
+    float d = 0.0f;
+    for (int k = 0; k < n; k++) d = __fadd_rn(d, __fmul_rn(x[k], y[k]));
+    return d;
+}
+
+// norm_c (query.h:105-114) and norm_r (query.h:116-125): one thread per centroid.
+__global__ void k_norms(const float *__restrict__ C, int rows, int len, float *__restrict__ out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= rows) return;
+    const float *c = C + (size_t)i * len;
+    float d = 0.0f;
+    for (int k = 0; k < len; k++) {
+        float t = c[k];
+        d = __fadd_rn(d, __fmul_rn(t, t));
+    }
+    out[i] = d;
+}
+
+// dot_cr[((i*kc + j)*(mp/mc) + i1)*kp + j1] = 2 * <cq[i][j] chunk i1, pq[i*(mp/mc)+i1][j1]>
+// (query.h:127-147): one thread per entry.
+__global__ void k_dot_cr(const float *__restrict__ cq, const float *__restrict__ pq, int mc, int kc,
+                         int mp, int kp, int bsc, int bsp, float *__restrict__ dot_cr) {
+    size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    size_t total = (size_t)kc * kp * mp;
+    if (e >= total) return;
+    int per = mp / mc;
+    int j1 = (int)(e % kp);
+    size_t t = e / kp;
+    int i1 = (int)(t % per);
+    t /= per;
+    int j = (int)(t % kc);
+    int i = (int)(t / kc);
+    const float *c = cq + ((size_t)i * kc + j) * bsc + (size_t)i1 * bsp;
+    const float *r = pq + (((size_t)i * per + i1) * kp + j1) * bsp;
+    dot_cr[e] = __fmul_rn(2.0f, seq_dot(c, r, bsp));
+}
+
+constexpr int QT = 16;    // queries per block
+constexpr int ET = 128;   // table entries per block (one per thread)
+constexpr int KCH = 32;   // dimensions staged per step
+
+// Per-query tables (query.h:154-184, intended sequencing):
+//   dqc[q][i*kc + j] = (norm_c[i*kc+j] - d) - d,  d = sum_t q[i*bsc+t] * cq[i][j][t]
+//   dqr[q][k*kp + j] = (norm_r[k*kp+j] - d) - d,  d = sum_t q[k*bsp+t] * pq[k][j][t]
+// Blocks cover (segment tile, query tile); a segment is one coarse part or one
+// PQ subspace.  Each thread owns one table entry and keeps QT sequential
+// accumulators; dimensions are staged through shared memory in chunks.
+__global__ void __launch_bounds__(ET) k_tables_exact(TablesArgs a, int ctiles, int ptiles) {
+    __shared__ float qs[QT][KCH];
+    __shared__ float cs[KCH][ET + 1];
+    int tile = blockIdx.x;
+    int seg, e0, seglen, len, qoff;
+    const float *cent;
+    const float *norm;
+    float *out;
+    int outstride, outoff;
+    if (tile < a.mc * ctiles) {
+        seg = tile / ctiles;
+        e0 = (tile % ctiles) * ET;
+        seglen = a.kc;
+        len = a.dim / a.mc;
+        qoff = seg * len;
+        cent = a.cq + (size_t)seg * a.kc * len;
+        norm = a.norm_c + (size_t)seg * a.kc;
+        out = a.dqc;
+        outstride = a.mc * a.kc;
+        outoff = seg * a.kc;
+    } else {
+        tile -= a.mc * ctiles;
+        seg = tile / ptiles;
+        e0 = (tile % ptiles) * ET;
+        seglen = a.kp;
+        len = a.dim / a.mp;
+        qoff = seg * len;
+        cent = a.pq + (size_t)seg * a.kp * len;
+        norm = a.norm_r + (size_t)seg * a.kp;
+        out = a.dqr;
+        outstride = a.mp * a.kp;
+        outoff = seg * a.kp;
+    }
+    int q0 = blockIdx.y * QT;
+    int t = threadIdx.x;
+    int e = e0 + t;
+    float acc[QT];
+#pragma unroll
+    for (int i = 0; i < QT; i++) acc[i] = 0.0f;
+    for (int k0 = 0; k0 < len; k0 += KCH) {
+        int kn = min(KCH, len - k0);
+        for (int i = t; i < QT * KCH; i += ET) {
+            int qq = i / KCH, kk = i % KCH;
+            int q = q0 + qq;
+            qs[qq][kk] = (q < a.nq && kk < kn) ? a.Q[(size_t)q * a.dim + qoff + k0 + kk] : 0.0f;
+        }
+        for (int i = t; i < ET * KCH; i += ET) {
+            int ee = i / KCH, kk = i % KCH;
+            int eg = e0 + ee;
+            cs[kk][ee] = (eg < seglen && kk < kn) ? cent[(size_t)eg * len + k0 + kk] : 0.0f;
+        }
+        __syncthreads();
+        for (int kk = 0; kk < kn; kk++) {
+            float c = cs[kk][t];
+#pragma unroll
+            for (int i = 0; i < QT; i++) acc[i] = __fadd_rn(acc[i], __fmul_rn(qs[i][kk], c));
+        }
+        __syncthreads();
+    }
+    if (e < seglen) {
+        float nv = norm[e];
+#pragma unroll
+        for (int i = 0; i < QT; i++) {
+            int q = q0 + i;
+            if (q < a.nq) out[(size_t)q * outstride + outoff + e] = __fsub_rn(__fsub_rn(nv, acc[i]), acc[i]);
+        }
+    }
+}
+
+// Query norms: per coarse part (multi_query.h:102-112) and the total the
+// ADC uses (q_sum: the sum of the part norms for IMI, the sequential sum over
+// all dimensions for IVFADC / SC, query.h:223-228, sc_query.h:91-96).
+__global__ void k_query_norms(const float *__restrict__ Q, int nq, int dim, int mc,
+                              float *__restrict__ qn, float *__restrict__ qsum) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    const float *x = Q + (size_t)q * dim;
+    int bsc = dim / mc;
+    float n[2] = {0.0f, 0.0f};
+    for (int i = 0; i < mc && i < 2; i++) {
+        float d = 0.0f;
+        for (int j = 0; j < bsc; j++) {
+            float t = x[i * bsc + j];
+            d = __fadd_rn(d, __fmul_rn(t, t));
+        }
+        n[i] = d;
+    }
+    qn[2 * q] = n[0];
+    qn[2 * q + 1] = n[1];
+    qsum[q] = (mc == 2) ? __fadd_rn(__fadd_rn(0.0f, n[0]), n[1]) : n[0];
+}
+
+}  // namespace
+
+void launch_precompute1(int dim, int mc, int kc, int mp, int kp, const float *cq, const float *pq,
+                        float *norm_c, float *norm_r, float *dot_cr, cudaStream_t s) {
+    int bsc = dim / mc, bsp = dim / mp;
+    k_norms<<<(mc * kc + 255) / 256, 256, 0, s>>>(cq, mc * kc, bsc, norm_c);
+    k_norms<<<(mp * kp + 255) / 256, 256, 0, s>>>(pq, mp * kp, bsp, norm_r);
+    size_t total = (size_t)kc * kp * mp;
+    k_dot_cr<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(cq, pq, mc, kc, mp, kp, bsc, bsp, dot_cr);
+}
+
+void launch_tables_exact(const TablesArgs &a, cudaStream_t s) {
+    if (a.nq <= 0) return;
+    int ctiles = (a.kc + ET - 1) / ET, ptiles = (a.kp + ET - 1) / ET;
+    dim3 grid(a.mc * ctiles + a.mp * ptiles, (a.nq + QT - 1) / QT);
+    k_tables_exact<<<grid, ET, 0, s>>>(a, ctiles, ptiles);
+    k_query_norms<<<(a.nq + 127) / 128, 128, 0, s>>>(a.Q, a.nq, a.dim, a.mc, a.qn, a.qsum);
+}
+
+}  // namespace scg

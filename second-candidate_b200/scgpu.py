@@ -1,0 +1,174 @@
+"""Python binding of libscgpu.so (the C ABI in include/scg.h) via ctypes.
+
+Used by the tests and by bench.py.  The library is built in-tree by
+build.py; loading fails loudly when it cannot be built or loaded -- there is
+no CPU fallback.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libscgpu.so")
+
+IVFADC, IMI, SC2 = 0, 1, 2
+FP32_EXACT, FAST = 0, 1
+
+ERRORS = {-1: "SCG_ERR_ARG", -2: "SCG_ERR_OOM", -3: "SCG_ERR_IO", -4: "SCG_ERR_CUDA",
+          -5: "SCG_ERR_CAP", -6: "SCG_ERR_STATE"}
+
+EXPORTS = ["scg_last_error", "scg_index_create", "scg_index_destroy", "scg_load_codebooks",
+           "scg_load_codebooks_file", "scg_load_csr", "scg_load_encoded_file", "scg_load_raw",
+           "scg_precompute", "scg_search", "scg_search_device", "scg_set_query_targets",
+           "scg_set_cell_budget", "scg_encode", "scg_sc_encode", "scg_encode_device",
+           "scg_index_info"]
+
+
+class ScgError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s: %s" % (ERRORS.get(code, code), msg))
+        self.code = code
+
+
+class SearchParams(ctypes.Structure):
+    _fields_ = [("mode", ctypes.c_int), ("R", ctypes.c_int), ("w", ctypes.c_int),
+                ("T", ctypes.c_int), ("precision", ctypes.c_int), ("rerank", ctypes.c_int)]
+
+
+_lib = None
+
+
+def load(build_if_missing=True):
+    """Loads libscgpu.so, building it first when it is missing or stale."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if build_if_missing:
+        import importlib.util
+        spec = importlib.util.spec_from_file_location("scg_build", os.path.join(HERE, "build.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        mod.build()
+    _lib = ctypes.CDLL(LIB_PATH)
+    for name in EXPORTS:
+        getattr(_lib, name).restype = ctypes.c_int
+    return _lib
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def _check(rc):
+    if rc != 0:
+        buf = ctypes.create_string_buffer(1024)
+        _lib.scg_last_error(buf, 1024)
+        raise ScgError(rc, buf.value.decode(errors="replace"))
+
+
+class Index:
+    """One device-resident index (codebooks, CSR codes, tables)."""
+
+    def __init__(self, device=0):
+        lib = load()
+        self._h = ctypes.c_void_p()
+        _check(lib.scg_index_create(ctypes.byref(self._h), device))
+
+    def close(self):
+        if self._h:
+            _lib.scg_index_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def load_codebooks(self, cq, kc, mc, pq, kp, mp, dim):
+        cq = np.ascontiguousarray(cq, np.float32)
+        pq = np.ascontiguousarray(pq, np.float32)
+        _check(_lib.scg_load_codebooks(self._h, _ptr(cq), kc, mc, _ptr(pq), kp, mp, dim))
+        self.dim, self.mc, self.kc, self.mp, self.kp = dim, mc, kc, mp, kp
+
+    def load_codebooks_file(self, cq_path, pq_path):
+        _check(_lib.scg_load_codebooks_file(self._h, cq_path.encode(), pq_path.encode()))
+        self._refresh_info()
+
+    def _refresh_info(self):
+        v = [ctypes.c_int() for _ in range(5)]
+        n = ctypes.c_int64()
+        _check(_lib.scg_index_info(self._h, *[ctypes.byref(x) for x in v], ctypes.byref(n)))
+        self.dim, self.mc, self.kc, self.mp, self.kp = (x.value for x in v)
+        self.N = n.value
+
+    def load_csr(self, L, pid, codes):
+        L = np.ascontiguousarray(L, np.int32)
+        pid = np.ascontiguousarray(pid, np.int32)
+        codes = np.ascontiguousarray(codes, np.uint8)
+        _check(_lib.scg_load_csr(self._h, _ptr(L), _ptr(pid), _ptr(codes),
+                                 ctypes.c_int64(pid.shape[0]), ctypes.c_int64(L.shape[0])))
+        self.N = pid.shape[0]
+
+    def load_encoded_file(self, path, nc):
+        _check(_lib.scg_load_encoded_file(self._h, path.encode(), nc))
+        self._refresh_info()
+
+    def load_raw(self, X):
+        X = np.ascontiguousarray(X, np.float32)
+        _check(_lib.scg_load_raw(self._h, _ptr(X), ctypes.c_int64(X.shape[0])))
+
+    def precompute(self):
+        _check(_lib.scg_precompute(self._h))
+
+    def set_cell_budget(self, n):
+        _check(_lib.scg_set_cell_budget(self._h, n))
+
+    def search(self, mode, Q, R, w, T, precision=FP32_EXACT, rerank=0):
+        """Host-buffer search: returns (ids[nq,R], dists[nq,R], sums[nq])."""
+        Q = np.ascontiguousarray(Q, np.float32).reshape(-1, self.dim)
+        nq = Q.shape[0]
+        ids = np.empty((nq, R), np.int32)
+        d = np.empty((nq, R), np.float32)
+        sums = np.empty(nq, np.int32)
+        p = SearchParams(mode, R, w, T, precision, rerank)
+        _check(_lib.scg_search(self._h, ctypes.byref(p), _ptr(Q), nq, _ptr(ids), _ptr(d), _ptr(sums)))
+        return ids, d, sums
+
+    def search_device(self, mode, dQ_ptr, nq, R, w, T, d_ids, d_d, d_sums, stream=None,
+                      precision=FP32_EXACT, rerank=0):
+        """Device-buffer search; arguments are raw device addresses (ints)."""
+        p = SearchParams(mode, R, w, T, precision, rerank)
+        _check(_lib.scg_search_device(self._h, ctypes.byref(p), ctypes.c_void_p(dQ_ptr), nq,
+                                      ctypes.c_void_p(d_ids), ctypes.c_void_p(d_d),
+                                      ctypes.c_void_p(d_sums),
+                                      ctypes.c_void_p(stream) if stream else None))
+
+    def set_query_targets(self, d_T_ptr):
+        _check(_lib.scg_set_query_targets(self._h, ctypes.c_void_p(d_T_ptr) if d_T_ptr else None))
+
+    def encode(self, X):
+        X = np.ascontiguousarray(X, np.float32)
+        n = X.shape[0]
+        cid = np.empty((n, self.mc), np.uint16)
+        codes = np.empty((n, self.mp), np.uint8)
+        _check(_lib.scg_encode(self._h, _ptr(X), ctypes.c_int64(n), _ptr(cid), _ptr(codes)))
+        return cid, codes
+
+    def sc_encode(self, X, nc=2):
+        X = np.ascontiguousarray(X, np.float32)
+        n = X.shape[0]
+        cid = np.empty((n, nc), np.uint16)
+        codes = np.empty((n, self.mp), np.uint8)
+        _check(_lib.scg_sc_encode(self._h, _ptr(X), ctypes.c_int64(n), nc, _ptr(cid), _ptr(codes)))
+        return cid, codes
+
+    def encode_device(self, dX_ptr, n, nc, d_cid, d_codes, stream=None):
+        _check(_lib.scg_encode_device(self._h, ctypes.c_void_p(dX_ptr), ctypes.c_int64(n), nc,
+                                      ctypes.c_void_p(d_cid), ctypes.c_void_p(d_codes),
+                                      ctypes.c_void_p(stream) if stream else None))

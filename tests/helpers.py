@@ -1,0 +1,42 @@
+"""Shared helpers of the test suite (fixtures on disk, comparisons)."""
+import glob
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def golden_cases():
+    return sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def load_case(path):
+    z = np.load(path)
+    return {k: z[k] for k in z.files}
+
+
+def oracle_index(O, g):
+    D, mc, kc, mp, kp = (int(g[k]) for k in ("D", "mc", "kc", "mp", "kp"))
+    return O.Index(D, mc, kc, mp, kp, g["cq"], g["pq"], g["L"], g["pid"], g["icodes"],
+                   raw=g["X"].astype(np.float32))
+
+
+def same_topk(ids_a, d_a, ids_b, d_b, n):
+    """True when two top-n lists agree: identical distances position by
+    position, and identical ids except inside runs of equal distance (where
+    the ids must agree as sets, and a run cut by the n-th position may differ)."""
+    ids_a, ids_b = np.asarray(ids_a)[:n], np.asarray(ids_b)[:n]
+    d_a, d_b = np.asarray(d_a)[:n], np.asarray(d_b)[:n]
+    if not np.array_equal(d_a, d_b):
+        return False
+    if n == 0:
+        return True
+    last = d_a[n - 1]
+    for v in np.unique(d_a):
+        m = d_a == v
+        if v == last:
+            continue
+        if set(ids_a[m].tolist()) != set(ids_b[m].tolist()):
+            return False
+    return True

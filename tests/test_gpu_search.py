@@ -1,0 +1,142 @@
+"""Parity of the CUDA search (through the C ABI) with the oracle and with the
+reference's golden vectors."""
+import os
+
+import numpy as np
+import pytest
+
+import helpers
+import oracle as O
+import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+MODES = {O.IVFADC: 0, O.IMI: 1, O.SC: 2}
+
+
+@pytest.fixture(scope="module")
+def scg():
+    import scgpu
+    scgpu.load()
+    return scgpu
+
+
+def gpu_index(scgpu, D, mc, kc, mp, kp, cq, pq, L, pid, codes):
+    g = scgpu.Index(0)
+    g.load_codebooks(cq, kc, mc, pq, kp, mp, D)
+    g.load_csr(L, pid, codes)
+    g.precompute()
+    return g
+
+
+def check_against_oracle(ix, g, mode, Q, R, w, T):
+    ids, d, sums = g.search(MODES[mode], Q, R, w, T)
+    oi, od, osum = ix.search(mode, Q, R, w, T, order=O.ORDER_EXACT)
+    assert np.array_equal(sums, osum), (sums, osum)
+    assert np.array_equal(d, od)
+    assert np.array_equal(ids, oi)
+    return ids, d, sums
+
+
+@pytest.mark.parametrize("path", helpers.golden_cases(), ids=lambda p: os.path.basename(p)[:-4])
+def test_golden_cases(scg, oracle_mod, path):
+    c = helpers.load_case(path)
+    ix = helpers.oracle_index(O, c)
+    D, mc, kc, mp, kp = (int(c[k]) for k in ("D", "mc", "kc", "mp", "kp"))
+    g = gpu_index(scg, D, mc, kc, mp, kp, c["cq"], c["pq"], c["L"], c["pid"], c["icodes"])
+    mode, R = int(c["mode"]), int(c["R"])
+    same_as_ref = 0
+    total = 0
+    for ri, (T, w) in enumerate(c["rules"]):
+        ids, d, sums = check_against_oracle(ix, g, mode, c["Q"], R, int(w), int(T))
+        # against the reference itself: identical wherever its heap visited
+        # the same cells as the exact order
+        for i in range(c["Q"].shape[0]):
+            total += 1
+            if sums[i] == c["r%d_sum" % ri][i]:
+                m = min(R, int(sums[i]))
+                rid, rd = c["r%d_top_ids" % ri][i][:m], c["r%d_top_d" % ri][i][:m]
+                o = np.lexsort((rid, rd))
+                if helpers.same_topk(ids[i], d[i], rid[o], rd[o], m):
+                    same_as_ref += 1
+    g.close()
+    assert same_as_ref >= 0.6 * total
+
+
+@pytest.mark.parametrize("mode,mc,kc", [(O.IVFADC, 1, 64), (O.IMI, 2, 48), (O.SC, 1, 48)])
+def test_random_index_parity(scg, oracle_mod, mode, mc, kc):
+    D, mp, kp = 64, 8, 256
+    mix = W.Mixture(D, 16, 20.0, "u8", seed=21 + mode)
+    X = mix.sample(40000, seed=22)
+    Q = mix.sample(60, seed=23)
+    cq, pq = W.train_codebooks(X[:5000], mc, kc, mp, kp, 4, seed=24)
+    if mode == O.SC:
+        cid, codes = O.sc_encode(D, kc, mp, kp, 2, cq, pq, X)
+        L, pid, co, _ = O.distribution(O.SC, kc, 1, 2, cid, codes)
+    else:
+        cid, codes = O.encode((D, mc, kc, mp, kp), cq, pq, X)
+        L, pid, co, _ = O.distribution(mode, kc, mc, 0, cid, codes)
+    ix = O.Index(D, mc, kc, mp, kp, cq, pq, L, pid, co)
+    g = gpu_index(scg, D, mc, kc, mp, kp, cq, pq, L, pid, co)
+    w = kc if mode == O.IVFADC else 1 << 20
+    for T in (1, 700, 5000):
+        for R in (1, 100):
+            check_against_oracle(ix, g, mode, Q, R, w, T)
+    # w caps: popped cells (IVFADC, IMI) or non-empty cells (SC)
+    check_against_oracle(ix, g, mode, Q, 50, 5, 5000)
+    # T beyond N: every cell is visited
+    check_against_oracle(ix, g, mode, Q[:5], 1024, w, 10 ** 8)
+    g.close()
+
+
+def test_edge_cases(scg, oracle_mod):
+    c = helpers.load_case(os.path.join(helpers.GOLDEN, "imi_d32.npz"))
+    ix = helpers.oracle_index(O, c)
+    D, mc, kc, mp, kp = (int(c[k]) for k in ("D", "mc", "kc", "mp", "kp"))
+    g = gpu_index(scg, D, mc, kc, mp, kp, c["cq"], c["pq"], c["L"], c["pid"], c["icodes"])
+    Q = c["Q"]
+    # nothing to visit: T <= 0 or w <= 0
+    ids, d, sums = g.search(1, Q, 10, 1 << 20, 0)
+    assert (sums == 0).all() and (ids == -1).all() and np.isinf(d).all()
+    ids, d, sums = g.search(1, Q, 10, 0, 100)
+    assert (sums == 0).all()
+    # one query, empty batch, R larger than the candidates
+    check_against_oracle(ix, g, O.IMI, Q[:1], 1024, 1 << 20, 30)
+    ids, d, sums = g.search(1, Q[:0], 10, 1 << 20, 30)
+    assert ids.shape == (0, 10)
+    # a budget too small is an error, never a silent truncation
+    import scgpu
+    g.set_cell_budget(64)
+    with pytest.raises(scgpu.ScgError) as e:
+        g.search(1, Q, 10, 1 << 20, 2900)
+    assert e.value.code == -5
+    g.set_cell_budget(131072)
+    check_against_oracle(ix, g, O.IMI, Q, 10, 1 << 20, 2900)
+    # wrong mode for the index is refused like the reference's cerr/return
+    with pytest.raises(scgpu.ScgError):
+        g.search(2, Q, 10, 1 << 20, 30)
+    with pytest.raises(scgpu.ScgError):
+        g.search(1, Q, 0, 1 << 20, 30)
+    g.close()
+
+
+def test_file_loaders(scg, oracle_mod, tmp_path):
+    import formats
+    c = helpers.load_case(os.path.join(helpers.GOLDEN, "sc_d32.npz"))
+    D, mc, kc, mp, kp = (int(c[k]) for k in ("D", "mc", "kc", "mp", "kp"))
+    formats.write_ctr(tmp_path / "cq.ctr_", c["cq"], kc, mc, D)
+    formats.write_ctr(tmp_path / "pq.ctr_", c["pq"], kp, mp, D)
+    formats.write_edat(tmp_path / "x_mr2_ivf.edat_", c["L"], c["pid"], c["icodes"])
+    g = scg.Index(0)
+    g.load_codebooks_file(str(tmp_path / "cq.ctr_"), str(tmp_path / "pq.ctr_"))
+    g.load_encoded_file(str(tmp_path / "x_mr2_ivf.edat_"), 2)
+    g.precompute()
+    ix = helpers.oracle_index(O, c)
+    check_against_oracle(ix, g, O.SC, c["Q"], 20, 1 << 20, 300)
+    # truncated files are I/O errors
+    raw = open(tmp_path / "x_mr2_ivf.edat_", "rb").read()
+    open(tmp_path / "bad.edat_", "wb").write(raw[: len(raw) // 2])
+    with pytest.raises(scg.ScgError) as e:
+        g.load_encoded_file(str(tmp_path / "bad.edat_"), 2)
+    assert e.value.code == -3
+    g.close()

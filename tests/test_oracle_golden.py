@@ -1,0 +1,81 @@
+"""The C restatement (oracle/) against golden vectors produced by the
+reference itself (tests/golden/make_golden.py)."""
+import numpy as np
+import pytest
+
+import helpers
+import oracle as O
+
+CASES = helpers.golden_cases()
+
+
+@pytest.fixture(scope="module", params=CASES, ids=lambda p: p.split("/")[-1][:-4])
+def case(request, oracle_mod):
+    return helpers.load_case(request.param)
+
+
+def test_tables(case):
+    ix = helpers.oracle_index(O, case)
+    assert np.array_equal(ix.norm_c, case["norm_c"])
+    assert np.array_equal(ix.norm_r, case["norm_r"])
+    assert np.array_equal(ix.dot_cr, case["dot_cr"])
+    dqc, dqr = O.pre_compute2(ix.cfg, ix.cq, ix.pq, ix.norm_c, ix.norm_r, case["Q"][0])
+    assert np.array_equal(dqc, case["dqc0"])
+    assert np.array_equal(dqr, case["dqr0"])
+
+
+def test_encoder_and_distribution(case):
+    D, mc, kc, mp, kp = (int(case[k]) for k in ("D", "mc", "kc", "mp", "kp"))
+    X = case["X"].astype(np.float32)
+    if int(case["mode"]) == O.SC:
+        cid, codes = O.sc_encode(D, kc, mp, kp, 2, case["cq"], case["pq"], X)
+        L, pid, co, _ = O.distribution(O.SC, kc, 1, 2, cid, codes)
+    else:
+        cid, codes = O.encode((D, mc, kc, mp, kp), case["cq"], case["pq"], X)
+        L, pid, co, _ = O.distribution(int(case["mode"]), kc, mc, 0, cid, codes)
+    assert np.array_equal(cid, case["cid"])
+    assert np.array_equal(codes, case["codes"])
+    assert np.array_equal(L, case["L"])
+    assert np.array_equal(pid, case["pid"])
+    assert np.array_equal(co, case["icodes"])
+
+
+def test_search_heap_order_matches_reference(case):
+    ix = helpers.oracle_index(O, case)
+    mode = int(case["mode"])
+    Q = case["Q"]
+    R = int(case["R"])
+    for ri, (T, w) in enumerate(case["rules"]):
+        off = case["r%d_cand_off" % ri]
+        for i in range(Q.shape[0]):
+            r = ix.search_one(mode, Q[i], int(w), int(T), order=O.ORDER_HEAP)
+            assert r["sum"] == case["r%d_sum" % ri][i]
+            if mode == O.IMI:
+                assert r["empty"] == case["r%d_empty" % ri][i]
+            o = np.lexsort((r["dist"], r["ids"]))
+            assert np.array_equal(r["ids"][o], case["r%d_cand_ids" % ri][off[i]:off[i + 1]])
+            assert np.array_equal(r["dist"][o], case["r%d_cand_d" % ri][off[i]:off[i + 1]])
+        # top-R: the reference sorts when sum >= R (IVFADC, IMI) and leaves
+        # the R selected unsorted for SC (sc_query.h:250-252)
+        ids, d, sums = ix.search(mode, Q, R, int(w), int(T), order=O.ORDER_HEAP)
+        for i in range(Q.shape[0]):
+            m = min(R, int(sums[i]))
+            ri_ids, ri_d = case["r%d_top_ids" % ri][i][:m], case["r%d_top_d" % ri][i][:m]
+            if sums[i] < R or mode == O.SC:
+                o = np.lexsort((ri_ids, ri_d))
+                ri_ids, ri_d = ri_ids[o], ri_d[o]
+            assert helpers.same_topk(ids[i], d[i], ri_ids, ri_d, m)
+
+
+def test_exact_order_differs_only_at_the_boundary(case):
+    """The exact priority order visits a prefix of the same key order; where
+    it differs from the reference heap the candidate counts differ by whole
+    boundary cells and the candidate sets overlap in all cells but those."""
+    ix = helpers.oracle_index(O, case)
+    mode = int(case["mode"])
+    for ri, (T, w) in enumerate(case["rules"]):
+        for i in range(case["Q"].shape[0]):
+            a = ix.search_one(mode, case["Q"][i], int(w), int(T), order=O.ORDER_HEAP)
+            b = ix.search_one(mode, case["Q"][i], int(w), int(T), order=O.ORDER_EXACT)
+            ca, cb = set(a["cells"].tolist()), set(b["cells"].tolist())
+            assert len(ca ^ cb) <= 4
