@@ -1,0 +1,333 @@
+"""Benchmark of the batched search on one B200 (or N replicas).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload C2] [--cache DIR]
+
+A step is one batched search of the workload's whole query set, inputs
+already resident on the device.  Default workload: the 10,000,000 x 128
+inverted multi-index (2 x 1024 coarse centroids per half, residual PQ 8 x
+256), 10,000 queries, T = 30,000 candidates, top-100 -- the configuration the
+headline metric is quoted on.  Data is synthetic and seeded (see
+second-candidate_b200/workloads.py).
+
+Prints one JSON line (rank 0).  `value` is the whole-job QPS (all replicas);
+`e2e` is the same metric through the public host-buffer entry point with the
+host<->device copies inside the timed region; `cpu_baseline` is the
+reference's own search (compiled from its sources, oracle/_ref) on the host
+cores with all threads on a bounded query sample; `roofline` is for the
+fused selection + scan kernel.
+
+`--impl reference` times only the reference's CPU search (rank 0; other
+ranks exit at once) on the same workload and prints the same line with
+"impl": "reference".
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "second-candidate_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+METRIC = "QPS at recall@100 (BF16 batched vs FP32 plain vs CPU); p50/p99 latency"
+MODE_IDS = {"ivfadc": 0, "imi": 1, "sc": 2}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p["hbm_gbs"], p["bf16_tflops"], "measured"
+    except Exception:
+        return 6650.0, 1590.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the
+    timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if not self.p:
+            return None
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except Exception:
+            self.p.kill()
+            out, _ = self.p.communicate()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def cpu_reference(w, seconds_target=12.0, threads=None, mode=None):
+    """Times the reference's own search (oracle/_ref/libscref.so, all host
+    threads) on a bounded sample of the workload's queries.  Falls back to
+    the C restatement when the reference build is not present."""
+    import oracle as O
+    cfg = w["cfg"]
+    threads = threads or os.cpu_count()
+    mode = MODE_IDS[cfg["mode"]] if mode is None else mode
+    mcp = 1 if cfg["mode"] == "sc" else cfg["mc"]
+    ix = O.Index(cfg["D"], mcp, cfg["kc"], cfg["mp"], cfg["kp"], w["cq"], w["pq"], w["L"], w["pid"],
+                 w["codes"])
+    Q = w["Q"]
+    T = cfg["T"] if isinstance(cfg["T"], int) else cfg["T"][0]
+    R, wcap = cfg["R"], cfg["w"]
+    if O.ref_available():
+        kind = "reference"
+
+        def run(qs):
+            ids, d, sums, sec = O.ref_search_batch(ix, mode, qs, R, wcap, T, nthreads=threads)
+            return ids, sec
+    else:
+        kind = "port"
+        threads = 1
+
+        def run(qs):
+            t0 = time.perf_counter()
+            ids, d, sums = ix.search(mode, qs, R, wcap, T, order=O.ORDER_HEAP)
+            return ids, time.perf_counter() - t0
+    probe = min(Q.shape[0], max(4 * threads, 32))
+    _, sec = run(Q[:probe])
+    per_q = sec / probe
+    n = int(min(Q.shape[0], max(probe, seconds_target / max(per_q, 1e-9))))
+    ids, sec = run(Q[:n])
+    from workloads import recall_at
+    return {"value": n / sec, "unit": "queries/s", "cores": threads, "kind": kind,
+            "sample": "first %d of %d queries, one batch, %s" % (n, Q.shape[0], "OpenMP over queries"),
+            "seconds": sec, "recall@100": recall_at(ids, w["gt"][:n], min(100, R))}
+
+
+def workload_desc(cfg):
+    if cfg["mode"] == "imi":
+        idx = "IMI 2x%d, residual PQ %dx%d" % (cfg["kc"], cfg["mp"], cfg["kp"])
+    elif cfg["mode"] == "sc":
+        idx = "second-candidate kc=%d, residual PQ %dx%d" % (cfg["kc"], cfg["mp"], cfg["kp"])
+    else:
+        idx = "IVFADC kc=%d, PQ %dx%d" % (cfg["kc"], cfg["mp"], cfg["kp"])
+    return "%s: N=%d D=%d %s, Q=%d, T=%s, R=%d" % (cfg["name"], cfg["N"], cfg["D"], idx, cfg["nq"],
+                                                    cfg["T"], cfg["R"])
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="C2")
+    ap.add_argument("--cache", default="/tmp/scg_bench_cache")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    import torch
+    import workloads as W
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        hbm, _, _ = peaks()
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        w = W.build_gpu_workload(args.workload, cache_dir=args.cache, log=log)
+        cfg = w["cfg"]
+        vals = []
+        for i in range(args.warmup + args.steps):
+            r = cpu_reference(w, seconds_target=2.0)
+            if i >= args.warmup:
+                vals.append(r)
+        qps = sum(v["value"] for v in vals) / len(vals)
+        line = {"impl": "reference", "metric": METRIC, "value": qps, "unit": "queries/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1000.0 * statistics.mean(v["seconds"] for v in vals),
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic", "recall@100": vals[-1]["recall@100"],
+                "config": {"workload": workload_desc(cfg), "parallelism": "host threads"},
+                "cpu_baseline": {"value": qps, "unit": "queries/s", "cores": vals[-1]["cores"],
+                                 "kind": vals[-1]["kind"], "sample": vals[-1]["sample"]},
+                "e2e": {"value": qps, "unit": "queries/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import scgpu
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    w = W.build_gpu_workload(args.workload, cache_dir=args.cache, log=log)
+    cfg = w["cfg"]
+    mode = MODE_IDS[cfg["mode"]]
+    mcp = 1 if cfg["mode"] == "sc" else cfg["mc"]
+    R, wcap = cfg["R"], cfg["w"]
+    T = cfg["T"] if isinstance(cfg["T"], int) else cfg["T"][0]
+    nq = w["Q"].shape[0]
+
+    ix = scgpu.Index(local)
+    ix.load_codebooks(w["cq"], cfg["kc"], mcp, w["pq"], cfg["kp"], cfg["mp"], cfg["D"])
+    ix.load_csr(w["L"], w["pid"], w["codes"])
+    ix.precompute()
+
+    dQ = torch.from_numpy(w["Q"]).to(dev)
+    d_ids = torch.empty(nq * R, dtype=torch.int32, device=dev)
+    d_d = torch.empty(nq * R, dtype=torch.float32, device=dev)
+    d_s = torch.empty(nq, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    def step():
+        ix.search_device(mode, dQ.data_ptr(), nq, R, wcap, T, d_ids.data_ptr(), d_d.data_ptr(),
+                         d_s.data_ptr(), stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    clocks = Clocks(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    times, kern = [], []
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    for _ in range(args.steps):
+        flush.zero_()
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        kern.append(ix.last_timings())
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    total_ms = sum(times)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ck = clocks.stop()
+
+    ids = d_ids.view(nq, R).cpu().numpy()
+    sums = d_s.cpu().numpy()
+    nvis, empty = ix.last_query_stats(nq)
+    recall = W.recall_at(ids, w["gt"], min(100, R))
+
+    # roofline of the fused selection + scan kernel: algorithmic bytes = the
+    # codes of every scanned candidate + 8 bytes of CSR offsets per visited
+    # cell + 4 bytes per returned id
+    search_ms = statistics.mean(k[1] for k in kern)
+    tables_ms = statistics.mean(k[0] for k in kern)
+    alg_bytes = float(sums.astype(np.int64).sum() * cfg["mp"] + 8 * nvis.astype(np.int64).sum() + 4 * nq * R)
+    hbm, _, peak_kind = peaks()
+    achieved = alg_bytes / (search_ms / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get("k_search:" + args.workload)
+        except Exception:
+            traffic = None
+
+    # end to end through the public host-buffer entry point
+    Qh = torch.from_numpy(w["Q"]).pin_memory().numpy()
+    e2e_times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        hid, hd, hs = ix.search(mode, Qh, R, wcap, T)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            e2e_times.append(dt)
+    e2e_qps = nq * len(e2e_times) / sum(e2e_times) * world
+    same = bool(np.array_equal(hid, ids))
+
+    line = {
+        "metric": METRIC, "value": nq * args.steps * world / (total_ms / 1e3), "unit": "queries/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": workload_desc(cfg), "precision": "fp32-exact (the reference's float order)",
+                   "l2": "flushed between steps (256 MB write)", "parallelism": "replicas" if world > 1 else "1 GPU",
+                   "timing": "CUDA events per step on the launching stream"},
+        "recall@100": recall,
+        "latency_ms": {"p50": float(np.percentile(times, 50)), "p99": float(np.percentile(times, 99)),
+                       "what": "whole batch of %d queries" % nq},
+        "kernels_ms": {"tables": tables_ms, "select_scan": search_ms},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
+                     "kernel": "k_search (selection + ADC scan + top-R)",
+                     "alg_bytes_per_launch": alg_bytes},
+        "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": int(nq * cfg["D"] * 4),
+                "d2h_bytes_per_step": int(nq * R * 8 + nq * 4), "same_ids_as_device_path": same},
+        "gpu_launches": 3 * args.steps,
+        "clocks": ck,
+        "candidates_per_query": float(sums.mean()), "cells_per_query": float(nvis.mean() + empty.mean()),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_reference(w)
+        except Exception as ex:  # reported, never silently dropped
+            line["cpu_baseline"] = {"unavailable": repr(ex)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ix.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

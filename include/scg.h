@@ -132,6 +132,16 @@ int scg_sc_encode(scg_index *h, const float *X, int64_t n, int nc, uint16_t *cid
 int scg_encode_device(scg_index *h, const float *dX, int64_t n, int nc, uint16_t *d_cid,
                       uint8_t *d_codes, void *stream);
 
+/* Per-query facts of the last search call on this index: visited non-empty
+ * cells and visited empty cells (the `e` output of search_multi2,
+ * multi_query.h:170), host buffers of nq ints (either may be NULL). */
+int scg_last_query_stats(scg_index *h, int *nvis, int *empty, int nq);
+
+/* Device time in milliseconds of the kernels of the last search call,
+ * measured with CUDA events on its stream: ms[0] the per-query tables,
+ * ms[1] the fused selection + scan.  n is the capacity of ms. */
+int scg_last_timings(scg_index *h, float *ms, int n);
+
 /* Index facts: dim, mc, kc, mp, kp, N (any pointer may be NULL). */
 int scg_index_info(scg_index *h, int *dim, int *mc, int *kc, int *mp, int *kp, int64_t *N);
 

@@ -67,6 +67,8 @@ struct scg_index {
     DevBuf q, dqc, dqr, qn, qsum, ids, dists, sums, nvis, empty, status, counter;
     DevBuf rec_key, rec_rank, rec_cnt, vis_cell, vis_pre;
     int *h_status = nullptr;  // pinned
+    int last_nq = 0;
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     std::mutex mu;
 };
 
@@ -178,7 +180,9 @@ int run_search(scg_index *h, const scg_search_params *p, const float *dQ, int nq
     ta.norm_c = h->norm_c.as<float>(); ta.norm_r = h->norm_r.as<float>();
     ta.dqc = h->dqc.as<float>(); ta.dqr = h->dqr.as<float>();
     ta.qn = h->qn.as<float>(); ta.qsum = h->qsum.as<float>();
+    SCG_CUDA(cudaEventRecord(h->ev[0], s));
     launch_tables_exact(ta, s);
+    SCG_CUDA(cudaEventRecord(h->ev[1], s));
 
     SCG_CUDA(cudaMemsetAsync(h->status.p, 0, sizeof(int) * 4, s));
     SCG_CUDA(cudaMemsetAsync(h->counter.p, 0, sizeof(int) * 4, s));
@@ -202,6 +206,8 @@ int run_search(scg_index *h, const scg_search_params *p, const float *dQ, int nq
     sa.out_nvis = h->nvis.as<int>(); sa.out_empty = h->empty.as<int>();
     sa.status = h->status.as<int>();
     if (nq > 0 && (rc = search_launch(sa, grid, s))) return rc;
+    SCG_CUDA(cudaEventRecord(h->ev[2], s));
+    h->last_nq = nq;
     SCG_CUDA(cudaMemcpyAsync(h->h_status, h->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     SCG_CUDA(cudaStreamSynchronize(s));
     int st = *h->h_status;
@@ -236,6 +242,7 @@ int scg_index_create(scg_index **out, int device) {
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_status, sizeof(int) * 4);
+    for (int i = 0; i < 3 && e == cudaSuccess; i++) e = cudaEventCreate(&h->ev[i]);
     if (e != cudaSuccess) {
         delete h;
         return cuda_fail(e, "scg_index_create");
@@ -254,6 +261,8 @@ int scg_index_destroy(scg_index *h) {
                      &h->rec_cnt, &h->vis_cell, &h->vis_pre};
     for (DevBuf *b : all) b->release();
     if (h->h_status) cudaFreeHost(h->h_status);
+    for (int i = 0; i < 3; i++)
+        if (h->ev[i]) cudaEventDestroy(h->ev[i]);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return SCG_OK;
@@ -498,6 +507,30 @@ int scg_encode(scg_index *h, const float *X, int64_t n, uint16_t *cid, uint8_t *
 int scg_sc_encode(scg_index *h, const float *X, int64_t n, int nc, uint16_t *cid, uint8_t *codes) {
     if (nc < 2) return fail(SCG_ERR_ARG, "nc must be >= 2");
     return encode_host(h, X, n, nc, cid, codes);
+}
+
+int scg_last_query_stats(scg_index *h, int *nvis, int *empty, int nq) {
+    if (!h) return fail(SCG_ERR_ARG, "null index");
+    if (nq < 0 || nq > h->last_nq) return fail(SCG_ERR_ARG, "nq exceeds the last search's batch");
+    std::lock_guard<std::mutex> g(h->mu);
+    int rc;
+    if ((rc = set_device(h))) return rc;
+    if (nvis && nq) SCG_CUDA(cudaMemcpy(nvis, h->nvis.p, sizeof(int) * (size_t)nq, cudaMemcpyDeviceToHost));
+    if (empty && nq) SCG_CUDA(cudaMemcpy(empty, h->empty.p, sizeof(int) * (size_t)nq, cudaMemcpyDeviceToHost));
+    return SCG_OK;
+}
+
+int scg_last_timings(scg_index *h, float *ms, int n) {
+    if (!h || !ms) return fail(SCG_ERR_ARG, "null argument");
+    if (h->last_nq <= 0) return fail(SCG_ERR_STATE, "no search has run");
+    std::lock_guard<std::mutex> g(h->mu);
+    int rc;
+    if ((rc = set_device(h))) return rc;
+    float t[2];
+    SCG_CUDA(cudaEventElapsedTime(&t[0], h->ev[0], h->ev[1]));
+    SCG_CUDA(cudaEventElapsedTime(&t[1], h->ev[1], h->ev[2]));
+    for (int i = 0; i < n && i < 2; i++) ms[i] = t[i];
+    return SCG_OK;
 }
 
 int scg_index_info(scg_index *h, int *dim, int *mc, int *kc, int *mp, int *kp, int64_t *N) {

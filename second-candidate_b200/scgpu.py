@@ -22,7 +22,7 @@ EXPORTS = ["scg_last_error", "scg_index_create", "scg_index_destroy", "scg_load_
            "scg_load_codebooks_file", "scg_load_csr", "scg_load_encoded_file", "scg_load_raw",
            "scg_precompute", "scg_search", "scg_search_device", "scg_set_query_targets",
            "scg_set_cell_budget", "scg_encode", "scg_sc_encode", "scg_encode_device",
-           "scg_index_info"]
+           "scg_index_info", "scg_last_query_stats", "scg_last_timings"]
 
 
 class ScgError(RuntimeError):
@@ -151,6 +151,17 @@ class Index:
 
     def set_query_targets(self, d_T_ptr):
         _check(_lib.scg_set_query_targets(self._h, ctypes.c_void_p(d_T_ptr) if d_T_ptr else None))
+
+    def last_query_stats(self, nq):
+        nvis = np.empty(nq, np.int32)
+        empty = np.empty(nq, np.int32)
+        _check(_lib.scg_last_query_stats(self._h, _ptr(nvis), _ptr(empty), nq))
+        return nvis, empty
+
+    def last_timings(self):
+        ms = np.zeros(2, np.float32)
+        _check(_lib.scg_last_timings(self._h, _ptr(ms), 2))
+        return float(ms[0]), float(ms[1])
 
     def encode(self, X):
         X = np.ascontiguousarray(X, np.float32)

@@ -151,3 +151,190 @@ def recall_at(ids, gt, R):
     whose true nearest neighbour is among the first R returned ids."""
     ids = np.asarray(ids)[:, :R]
     return float((ids == np.asarray(gt)[:, None]).any(axis=1).mean())
+
+
+# ---------------------------------------------------------------------------
+# Full-size workloads, built on the GPU (data preparation for bench.py; the
+# timed search never runs through this code).
+
+def _torch_kmeans(X, k, iters, seed):
+    """k-means++ seeding, then Lloyd steps (float32 distances, float64 means)
+    on a CUDA tensor X [n, d]."""
+    import torch
+    g = torch.Generator(device=X.device).manual_seed(seed)
+    n, d = X.shape
+    C = torch.empty(k, d, device=X.device, dtype=torch.float32)
+    C[0] = X[torch.randint(0, n, (1,), generator=g, device=X.device)]
+    closest = ((X - C[0]) ** 2).sum(1)
+    for i in range(1, k):
+        p = closest.clamp_min(0)
+        s = p.sum()
+        if float(s) <= 0:
+            j = torch.randint(0, n, (1,), generator=g, device=X.device)
+        else:
+            j = torch.multinomial(p / s, 1, generator=g)
+        C[i] = X[j]
+        closest = torch.minimum(closest, ((X - C[i]) ** 2).sum(1))
+    Xn = (X * X).sum(1, keepdim=True)
+    Xd = X.double()
+    for _ in range(iters):
+        dist = Xn + (C * C).sum(1)[None, :] - 2.0 * (X @ C.T)
+        lab = dist.argmin(1)
+        sums = torch.zeros(k, d, dtype=torch.float64, device=X.device).index_add_(0, lab, Xd)
+        cnt = torch.bincount(lab, minlength=k)
+        nz = cnt > 0
+        C[nz] = (sums[nz] / cnt[nz, None].double()).float()
+    return C
+
+
+def _torch_nearest(X, C):
+    import torch
+    Xn = (X * X).sum(1, keepdim=True)
+    out = torch.empty(X.shape[0], dtype=torch.long, device=X.device)
+    for s in range(0, X.shape[0], 1 << 18):
+        x = X[s:s + (1 << 18)]
+        out[s:s + x.shape[0]] = (Xn[s:s + x.shape[0]] + (C * C).sum(1)[None] - 2.0 * x @ C.T).argmin(1)
+    return out
+
+
+def build_gpu_workload(name, seed=1234, cache_dir=None, log=print):
+    """Generates config `name` on cuda:0 and returns a dict of host arrays:
+    cq, pq (codebooks), L, pid, codes (CSR index in cell order), Q (queries),
+    gt (exact nearest neighbour of each query) and the shape facts.  The
+    index is encoded by the library's exact encoder (bit-identical to the
+    reference's Encoder/SCEncoder) and bucketed by cell id in row order (as
+    Encoder::distribution does).  With cache_dir the result is kept as .npz
+    and reused."""
+    import hashlib
+    import os
+    import time
+
+    import torch
+
+    cfg = dict(CONFIGS[name])
+    key = hashlib.sha1(repr((name, seed, sorted(cfg.items()), 3)).encode()).hexdigest()[:16]
+    path = os.path.join(cache_dir, "%s_%s.npz" % (cfg["name"], key)) if cache_dir else None
+    if path and os.path.exists(path):
+        z = np.load(path)
+        out = {k: z[k] for k in z.files}
+        out.update(cfg=cfg)
+        log("workload %s loaded from cache" % cfg["name"])
+        return out
+
+    import scgpu
+    t0 = time.time()
+    dev = torch.device("cuda:0")
+    torch.backends.cuda.matmul.allow_tf32 = False
+    N, D, mc, kc, mp, kp = cfg["N"], cfg["D"], cfg["mc"], cfg["kc"], cfg["mp"], cfg["kp"]
+    sc = cfg["mode"] == "sc"
+    g = torch.Generator(device=dev).manual_seed(seed)
+    kind = "u8" if cfg["sigma"] >= 1 else ("unit01" if name == "C4" else "sphere")
+    if kind == "u8":
+        means = torch.rand(cfg["comps"], D, generator=g, device=dev) * 128.0
+    elif kind == "unit01":
+        means = 0.2 + 0.6 * torch.rand(cfg["comps"], D, generator=g, device=dev)
+    else:
+        means = torch.randn(cfg["comps"], D, generator=g, device=dev)
+        means /= means.norm(dim=1, keepdim=True)
+
+    def sample(n):
+        comp = torch.randint(0, cfg["comps"], (n,), generator=g, device=dev)
+        x = means[comp] + cfg["sigma"] * torch.randn(n, D, generator=g, device=dev)
+        if kind == "u8":
+            x = x.round_().clamp_(0, 255)
+        elif kind == "unit01":
+            x = x.clamp_(0.0, 1.0)
+        else:
+            x /= x.norm(dim=1, keepdim=True).clamp_min(1e-12)
+        return x.contiguous()
+
+    X = sample(N)
+    Q = sample(cfg["nq"])
+    log("generated %d x %d in %.1fs" % (N, D, time.time() - t0))
+    # codebooks: coarse (k-means per part, or one zero centroid), residual PQ
+    tr = X[: cfg["train"]]
+    mcp = 1 if sc else mc
+    bsc, bsp = D // mcp, D // mp
+    if kc == 1:
+        cq = torch.zeros(mcp, 1, bsc, device=dev)
+    else:
+        cq = torch.stack([_torch_kmeans(tr[:, i * bsc:(i + 1) * bsc].contiguous(), kc, cfg["iters"], seed + 11 * i)
+                          for i in range(mcp)])
+    resid = tr.clone()
+    for i in range(mcp):
+        part = tr[:, i * bsc:(i + 1) * bsc].contiguous()
+        resid[:, i * bsc:(i + 1) * bsc] -= cq[i][_torch_nearest(part, cq[i])]
+    pq = torch.stack([_torch_kmeans(resid[:, j * bsp:(j + 1) * bsp].contiguous(), kp, cfg["iters"], seed + 101 + 7 * j)
+                      for j in range(mp)])
+    cq_h = cq.cpu().numpy().astype(np.float32).ravel()
+    pq_h = pq.cpu().numpy().astype(np.float32).ravel()
+    log("trained codebooks in %.1fs" % (time.time() - t0))
+    # exact encoding with the library's encoder
+    ix = scgpu.Index(0)
+    ix.load_codebooks(cq_h, kc, mcp, pq_h, kp, mp, D)
+    nc = 2 if sc else 0
+    ncid = 2 if sc else mcp
+    cid = torch.empty(N, ncid, dtype=torch.int16, device=dev)
+    codes = torch.empty(N, mp, dtype=torch.uint8, device=dev)
+    step = 1 << 22
+    for s in range(0, N, step):
+        n = min(step, N - s)
+        ix.encode_device(X[s:s + n].data_ptr(), n, nc, cid[s:s + n].data_ptr(), codes[s:s + n].data_ptr())
+    torch.cuda.synchronize()
+    ix.close()
+    log("encoded in %.1fs" % (time.time() - t0))
+    c = cid.to(torch.int64) & 0xFFFF
+    cell = c[:, 0] * kc + c[:, 1] if ncid == 2 else c[:, 0]
+    ncells = kc * kc if (sc or mc == 2) else kc
+    cell_sorted, perm = torch.sort(cell, stable=True)
+    counts = torch.bincount(cell, minlength=ncells)
+    L = counts.cumsum(0).to(torch.int32)
+    codes_sorted = codes[perm]
+    # exact nearest neighbour of each query (float32 distances are exact for
+    # integer data; ties resolve to the lowest id)
+    gt = exact_nn_torch(X, Q)
+    log("index + ground truth in %.1fs" % (time.time() - t0))
+    out = dict(cq=cq_h, pq=pq_h, L=L.cpu().numpy(), pid=perm.to(torch.int32).cpu().numpy(),
+               codes=codes_sorted.cpu().numpy(), Q=Q.cpu().numpy(), gt=gt.cpu().numpy())
+    del X, codes, cid, cell, perm, codes_sorted
+    torch.cuda.empty_cache()
+    if path:
+        os.makedirs(cache_dir, exist_ok=True)
+        tmp = path + ".%d.tmp.npz" % os.getpid()
+        np.savez(tmp, **out)
+        os.replace(tmp, path)
+    out.update(cfg=cfg)
+    return out
+
+
+def exact_nn_torch(X, Q, qchunk=1024, bchunk=1 << 20):
+    """Exact 1-NN of each row of Q among the rows of X (CUDA tensors)."""
+    import torch
+    best = torch.full((Q.shape[0],), float("inf"), device=Q.device, dtype=torch.float64)
+    arg = torch.zeros(Q.shape[0], dtype=torch.long, device=Q.device)
+    for qs in range(0, Q.shape[0], qchunk):
+        q = Q[qs:qs + qchunk]
+        qn = (q.double() ** 2).sum(1)
+        bb = torch.full((q.shape[0],), float("inf"), device=Q.device, dtype=torch.float64)
+        ba = torch.zeros(q.shape[0], dtype=torch.long, device=Q.device)
+        for bs in range(0, X.shape[0], bchunk):
+            x = X[bs:bs + bchunk]
+            d = (x * x).sum(1)[None, :] - 2.0 * (q @ x.T)
+            # keep 4 candidates per chunk, decide among them in float64
+            v, j = torch.topk(d, 4, dim=1, largest=False)
+            cand = x[j]  # [q, 4, D]
+            dd = ((cand.double() - q.double()[:, None, :]) ** 2).sum(2)
+            jj = j + bs
+            # lowest id among equal float64 distances
+            order = torch.argsort(jj, dim=1)
+            dd = torch.gather(dd, 1, order)
+            jj = torch.gather(jj, 1, order)
+            m, mi = dd.min(1)
+            pick = torch.gather(jj, 1, mi[:, None])[:, 0]
+            better = (m < bb) | ((m == bb) & (pick < ba))
+            bb = torch.where(better, m, bb)
+            ba = torch.where(better, pick, ba)
+        best[qs:qs + q.shape[0]] = bb
+        arg[qs:qs + q.shape[0]] = ba
+        del qn
+    return arg
