@@ -160,6 +160,7 @@ def main():
     ap.add_argument("--workload", default="C2")
     ap.add_argument("--cache", default="/tmp/scg_bench_cache")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="fast", choices=["fast", "fp32"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -228,9 +229,32 @@ def main():
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
-    def step():
+    prec = scgpu.FAST if args.precision == "fast" else scgpu.FP32_EXACT
+
+    def step(p=None):
         ix.search_device(mode, dQ.data_ptr(), nq, R, wcap, T, d_ids.data_ptr(), d_d.data_ptr(),
-                         d_s.data_ptr(), stream=stream.cuda_stream)
+                         d_s.data_ptr(), stream=stream.cuda_stream, precision=prec if p is None else p)
+
+    # the plain FP32 form (the reference's float order), for comparison
+    plain = None
+    if args.precision == "fast":
+        for _ in range(2):
+            step(scgpu.FP32_EXACT)
+        torch.cuda.synchronize()
+        pt = []
+        for _ in range(3):
+            flush.zero_()
+            e0p = torch.cuda.Event(enable_timing=True)
+            e1p = torch.cuda.Event(enable_timing=True)
+            e0p.record(stream)
+            step(scgpu.FP32_EXACT)
+            e1p.record(stream)
+            e1p.synchronize()
+            pt.append(e0p.elapsed_time(e1p))
+        pids = d_ids.view(nq, R).cpu().numpy()
+        plain = {"value": nq / (statistics.mean(pt) / 1e3), "unit": "queries/s",
+                 "recall@100": W.recall_at(pids, w["gt"], min(100, R)), "ms_per_step": statistics.mean(pt),
+                 "kernels_ms": dict(zip(("tables", "select_scan"), ix.last_timings()))}
 
     for _ in range(args.warmup):
         step()
@@ -288,7 +312,7 @@ def main():
     e2e_times = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        hid, hd, hs = ix.search(mode, Qh, R, wcap, T)
+        hid, hd, hs = ix.search(mode, Qh, R, wcap, T, precision=prec)
         dt = time.perf_counter() - t0
         if i >= args.warmup:
             e2e_times.append(dt)
@@ -300,10 +324,13 @@ def main():
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": workload_desc(cfg), "precision": "fp32-exact (the reference's float order)",
+        "config": {"workload": workload_desc(cfg),
+                   "precision": ("fast: FP32 tables + fused per-vector term" if args.precision == "fast"
+                                 else "fp32-exact (the reference's float order)"),
                    "l2": "flushed between steps (256 MB write)", "parallelism": "replicas" if world > 1 else "1 GPU",
                    "timing": "CUDA events per step on the launching stream"},
         "recall@100": recall,
+        "fp32_plain": plain,
         "latency_ms": {"p50": float(np.percentile(times, 50)), "p99": float(np.percentile(times, 99)),
                        "what": "whole batch of %d queries" % nq},
         "kernels_ms": {"tables": tables_ms, "select_scan": search_ms},

@@ -142,6 +142,10 @@ int scg_last_query_stats(scg_index *h, int *nvis, int *empty, int nq);
  * ms[1] the fused selection + scan.  n is the capacity of ms. */
 int scg_last_timings(scg_index *h, float *ms, int n);
 
+/* Copies the cell lengths back as the reference's inclusive prefix L[ncells]
+ * (the array PQQuery::entropy reads, query.cpp:168-182). */
+int scg_cell_counts(scg_index *h, int *L, int64_t ncells);
+
 /* Index facts: dim, mc, kc, mp, kp, N (any pointer may be NULL). */
 int scg_index_info(scg_index *h, int *dim, int *mc, int *kc, int *mp, int *kp, int64_t *N);
 

@@ -62,7 +62,8 @@ struct scg_index {
     bool have_codebooks = false, have_csr = false, precomputed = false;
     int cap_rec = 131072;
     const int *d_Tq = nullptr;
-    DevBuf cq, pq, norm_c, norm_r, dot_cr, off, pid, codes, raw;
+    DevBuf cq, pq, norm_c, norm_r, dot_cr, off, pid, codes, raw, vterm;
+    bool have_vterm = false;
     // batch workspace
     DevBuf q, dqc, dqr, qn, qsum, ids, dists, sums, nvis, empty, status, counter;
     DevBuf rec_key, rec_rank, rec_cnt, vis_cell, vis_pre;
@@ -128,7 +129,7 @@ int check_params(scg_index *h, const scg_search_params *p, int nq) {
     if (!p) return fail(SCG_ERR_ARG, "null params");
     if (nq < 0) return fail(SCG_ERR_ARG, "nq < 0");
     if (p->R < 1 || p->R > 1024) return fail(SCG_ERR_ARG, "R must be in [1, 1024]");
-    if (p->precision != SCG_FP32_EXACT) return fail(SCG_ERR_ARG, "precision not supported by this build");
+    if (p->precision != SCG_FP32_EXACT && p->precision != SCG_FAST) return fail(SCG_ERR_ARG, "unknown precision");
     if (p->rerank != 0) return fail(SCG_ERR_ARG, "rerank not supported by this build");
     switch (p->mode) {
         case SCG_IVFADC:
@@ -173,6 +174,14 @@ int run_search(scg_index *h, const scg_search_params *p, const float *dQ, int nq
     if ((rc = h->vis_cell.ensure(4 * (slot + 1) * grid))) return rc;
     if ((rc = h->vis_pre.ensure(4 * (slot + 1) * grid))) return rc;
 
+    if (p->precision == SCG_FAST && !h->have_vterm) {
+        // the fast form's per-vector term (one float per database vector)
+        if ((rc = h->vterm.ensure(sizeof(float) * (size_t)(h->N ? h->N : 1)))) return rc;
+        launch_vterm(p->mode, h->kc, h->mp, h->kp, h->mc, (uint64_t)h->ncells, h->N, h->off.as<uint32_t>(),
+                     h->codes.as<uint8_t>(), h->norm_r.as<float>(), h->dot_cr.as<float>(), h->vterm.as<float>(), s);
+        SCG_CUDA(cudaGetLastError());
+        h->have_vterm = true;
+    }
     TablesArgs ta;
     ta.dim = h->dim; ta.mc = h->mc; ta.kc = h->kc; ta.mp = h->mp; ta.kp = h->kp; ta.nq = nq;
     ta.Q = dQ;
@@ -180,6 +189,7 @@ int run_search(scg_index *h, const scg_search_params *p, const float *dQ, int nq
     ta.norm_c = h->norm_c.as<float>(); ta.norm_r = h->norm_r.as<float>();
     ta.dqc = h->dqc.as<float>(); ta.dqr = h->dqr.as<float>();
     ta.qn = h->qn.as<float>(); ta.qsum = h->qsum.as<float>();
+    ta.fast = p->precision == SCG_FAST;
     SCG_CUDA(cudaEventRecord(h->ev[0], s));
     launch_tables_exact(ta, s);
     SCG_CUDA(cudaEventRecord(h->ev[1], s));
@@ -194,7 +204,7 @@ int run_search(scg_index *h, const scg_search_params *p, const float *dQ, int nq
     sa.dqc = ta.dqc; sa.dqr = ta.dqr; sa.qn = ta.qn; sa.qsum = ta.qsum;
     sa.off = h->off.as<uint32_t>(); sa.pid = h->pid.as<int>(); sa.codes = h->codes.as<uint8_t>();
     sa.dot_cr = h->dot_cr.as<float>();
-    sa.vterm = nullptr;
+    sa.vterm = h->vterm.as<float>();
     sa.ncells = (uint64_t)h->ncells;
     sa.N = h->N;
     sa.rec_key = h->rec_key.as<uint32_t>(); sa.rec_rank = h->rec_rank.as<uint32_t>();
@@ -256,7 +266,7 @@ int scg_index_destroy(scg_index *h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     DevBuf *all[] = {&h->cq, &h->pq, &h->norm_c, &h->norm_r, &h->dot_cr, &h->off, &h->pid, &h->codes,
-                     &h->raw, &h->q, &h->dqc, &h->dqr, &h->qn, &h->qsum, &h->ids, &h->dists, &h->sums,
+                     &h->raw, &h->vterm, &h->q, &h->dqc, &h->dqr, &h->qn, &h->qsum, &h->ids, &h->dists, &h->sums,
                      &h->nvis, &h->empty, &h->status, &h->counter, &h->rec_key, &h->rec_rank,
                      &h->rec_cnt, &h->vis_cell, &h->vis_pre};
     for (DevBuf *b : all) b->release();
@@ -284,6 +294,7 @@ int scg_load_codebooks(scg_index *h, const float *cq, int kc, int mc, const floa
     h->dim = dim; h->mc = mc; h->kc = kc; h->mp = mp; h->kp = kp;
     h->have_codebooks = true;
     h->precomputed = false;
+    h->have_vterm = false;
     return SCG_OK;
 }
 
@@ -330,6 +341,7 @@ int scg_load_csr(scg_index *h, const int *L, const int *pid, const uint8_t *code
     h->N = N;
     h->ncells = ncells;
     h->have_csr = true;
+    h->have_vterm = false;
     return SCG_OK;
 }
 
@@ -395,6 +407,7 @@ int scg_precompute(scg_index *h) {
     SCG_CUDA(cudaGetLastError());
     SCG_CUDA(cudaStreamSynchronize(h->stream));
     h->precomputed = true;
+    h->have_vterm = false;
     return SCG_OK;
 }
 
@@ -530,6 +543,17 @@ int scg_last_timings(scg_index *h, float *ms, int n) {
     SCG_CUDA(cudaEventElapsedTime(&t[0], h->ev[0], h->ev[1]));
     SCG_CUDA(cudaEventElapsedTime(&t[1], h->ev[1], h->ev[2]));
     for (int i = 0; i < n && i < 2; i++) ms[i] = t[i];
+    return SCG_OK;
+}
+
+int scg_cell_counts(scg_index *h, int *L, int64_t ncells) {
+    if (!h || !L) return fail(SCG_ERR_ARG, "null argument");
+    if (!h->have_csr) return fail(SCG_ERR_STATE, "encoded data not loaded");
+    if (ncells != h->ncells) return fail(SCG_ERR_ARG, "ncells differs from the loaded index");
+    std::lock_guard<std::mutex> g(h->mu);
+    int rc;
+    if ((rc = set_device(h))) return rc;
+    SCG_CUDA(cudaMemcpy(L, h->off.as<uint32_t>() + 1, sizeof(int) * (size_t)ncells, cudaMemcpyDeviceToHost));
     return SCG_OK;
 }
 

@@ -58,11 +58,14 @@ struct TablesArgs {
     float *dqr;            // [nq][mp*kp]
     float *qn;             // [nq][2] half norms (IMI) or [nq][2] = {q_sum, 0}
     float *qsum;           // [nq]
+    int fast;              // 0: the reference's float order; 1: FMA dots, LUT = -2<q,r>
 };
 
 void launch_precompute1(int dim, int mc, int kc, int mp, int kp, const float *cq, const float *pq,
                         float *norm_c, float *norm_r, float *dot_cr, cudaStream_t s);
 void launch_tables_exact(const TablesArgs &a, cudaStream_t s);
+void launch_vterm(int mode, int kc, int mp, int kp, int mc, uint64_t ncells, int64_t N, const uint32_t *off,
+                  const uint8_t *codes, const float *norm_r, const float *dot_cr, float *vterm, cudaStream_t s);
 
 struct SearchArgs {
     int mode, dim, mc, kc, mp, kp, nq, R, w, T;

@@ -29,7 +29,8 @@ namespace scg {
 
 namespace {
 
-constexpr int NT = 512;
+constexpr int NT = 256;
+constexpr int CPT = 4;  // candidates per thread per scan round
 constexpr int NWARP = NT / 32;
 constexpr int HBITS = 11;
 constexpr int HBINS = 1 << HBITS;
@@ -260,6 +261,47 @@ __device__ __forceinline__ uint32_t cell_of(const Lists &L, bool ivf, uint32_t r
     return ivf ? L.ta(h1) : L.ta(h1) * (uint32_t)L.kc + L.tb(h2);
 }
 
+// The mp code bytes of one candidate.  MPC > 0: mp == MPC, loaded with
+// 16/8/4-byte vector loads (rows are MPC-byte aligned); MPC == 0: any mp,
+// byte loads on demand.
+template <int MPC>
+struct CodeWords {
+    uint32_t w[(MPC + 3) / 4];
+    __device__ __forceinline__ void load(const uint8_t *codes, uint32_t pos, int) {
+        const uint8_t *p = codes + (size_t)pos * MPC;
+        if constexpr (MPC % 16 == 0) {
+#pragma unroll
+            for (int i = 0; i < MPC / 16; i++) {
+                uint4 v = __ldg((const uint4 *)p + i);
+                w[4 * i] = v.x; w[4 * i + 1] = v.y; w[4 * i + 2] = v.z; w[4 * i + 3] = v.w;
+            }
+        } else if constexpr (MPC % 8 == 0) {
+#pragma unroll
+            for (int i = 0; i < MPC / 8; i++) {
+                uint2 v = __ldg((const uint2 *)p + i);
+                w[2 * i] = v.x; w[2 * i + 1] = v.y;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < MPC / 4; i++) w[i] = __ldg((const uint32_t *)p + i);
+        }
+    }
+    __device__ __forceinline__ int n(int) const { return MPC; }
+    __device__ __forceinline__ uint32_t code(int k) const { return (w[k >> 2] >> ((k & 3) * 8)) & 0xffu; }
+};
+
+template <>
+struct CodeWords<0> {
+    const uint8_t *p;
+    int m;
+    __device__ __forceinline__ void load(const uint8_t *codes, uint32_t pos, int mp) {
+        p = codes + (size_t)pos * mp;
+        m = mp;
+    }
+    __device__ __forceinline__ int n(int mp) const { return mp; }
+    __device__ __forceinline__ uint32_t code(int k) const { return __ldg(p + k); }
+};
+
 struct QState {
     int err;
     uint32_t tau;
@@ -278,7 +320,8 @@ struct QState {
     uint32_t wend;
 };
 
-__global__ void __launch_bounds__(NT) k_search(SearchArgs a) {
+template <int MPC>
+__global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint64_t red[3 * NWARP];
     __shared__ QState st;
@@ -289,6 +332,7 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a) {
     const int kc = a.kc, mp = a.mp, kp = a.kp;
     const int kcP = next_pow2(kc);
     const bool imi = a.mode == SCG_IMI, sc = a.mode == SCG_SC2, ivf = a.mode == SCG_IVFADC;
+    const bool fast = a.precision == SCG_FAST;
     const int kB = ivf ? 1 : kc;
     const int cap = a.cap_rec;
     uint32_t *rec_key = a.rec_key + (size_t)blockIdx.x * cap;
@@ -676,7 +720,7 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a) {
                     __syncthreads();
                 }
                 // make room for this round's candidates
-                if (st.ncur + st.npend + NT > MERGE_N) {
+                if (st.ncur + st.npend + NT * CPT > MERGE_N) {
                     int n = st.ncur + st.npend;
                     int np2 = next_pow2(n);
                     for (int i = n + tid; i < np2; i += NT) topk[i] = ~0ull;
@@ -691,43 +735,65 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a) {
                     __syncthreads();
                 }
                 const uint32_t wend = st.wend;
-                const uint32_t flat = flat0 + tid;
                 const uint64_t thr = st.thr;
                 const int cn = st.cn;
-                if (flat < wend) {
-                    // window cell containing flat
-                    int lo2 = 0, hi2 = cn - 1;
-                    while (lo2 < hi2) {
-                        int mid = (lo2 + hi2 + 1) >> 1;
-                        if (win[mid].pre <= flat) lo2 = mid;
-                        else hi2 = mid - 1;
+                // CPT candidates per thread, all loads issued before the sums
+                uint32_t pos[CPT];
+                float dd[CPT];
+                uint32_t h34[CPT];
+                CodeWords<MPC> cw_[CPT];
+#pragma unroll
+                for (int j = 0; j < CPT; j++) {
+                    const uint32_t flat = flat0 + tid + j * NT;
+                    pos[j] = 0xffffffffu;
+                    if (flat < wend) {
+                        int lo2 = 0, hi2 = cn - 1;
+                        while (lo2 < hi2) {
+                            int mid = (lo2 + hi2 + 1) >> 1;
+                            if (win[mid].pre <= flat) lo2 = mid;
+                            else hi2 = mid - 1;
+                        }
+                        const CellWin cw = win[lo2];
+                        pos[j] = cw.start + (flat - cw.pre);
+                        dd[j] = cw.d0;
+                        h34[j] = cw.h34;
+                        cw_[j].load(a.codes, pos[j], mp);
                     }
-                    const CellWin cw = win[lo2];
-                    const uint32_t pos = cw.start + (flat - cw.pre);
-                    const uint8_t *cp = a.codes + (size_t)pos * mp;
-                    float d = cw.d0;
-                    const uint32_t h3 = cw.h34 & 0xffffu, h4 = cw.h34 >> 16;
-                    if (imi) {
+                }
+                if (fast) {
+#pragma unroll
+                    for (int j = 0; j < CPT; j++)
+                        if (pos[j] != 0xffffffffu) dd[j] = __fadd_rn(dd[j], __ldg(a.vterm + pos[j]));
+                }
+#pragma unroll
+                for (int j = 0; j < CPT; j++) {
+                    if (pos[j] == 0xffffffffu) continue;
+                    float d = dd[j];
+                    const uint32_t h3 = h34[j] & 0xffffu, h4 = h34[j] >> 16;
+                    if (fast) {
+                        // d0 + per-vector term + sum_k LUT[k][c_k]
+                        for (int k = 0; k < cw_[j].n(mp); k++) d = __fadd_rn(d, S.lut[k * kp + cw_[j].code(k)]);
+                    } else if (imi) {
                         // multi_query.h:237-254: two adds per subspace
                         const int half = mp >> 1;
                         const float *r1 = a.dot_cr + (size_t)h3 * bsI;
                         const float *r2 = a.dot_cr + (size_t)(h4 + kc - 1) * bsI;
-                        for (int k = 0; k < mp; k++) {
-                            int bc = k * kp + cp[k];
+                        for (int k = 0; k < cw_[j].n(mp); k++) {
+                            int bc = k * kp + cw_[j].code(k);
                             d = __fadd_rn(d, S.lut[bc]);
                             d = __fadd_rn(d, __ldg((k < half ? r1 : r2) + bc));
                         }
                     } else {
                         // query.h:295-306, sc_query.h:222-229: pair sum per subspace
                         const float *r1 = a.dot_cr + (size_t)h3 * bsI;
-                        for (int k = 0; k < mp; k++) {
-                            int bc = k * kp + cp[k];
+                        for (int k = 0; k < cw_[j].n(mp); k++) {
+                            int bc = k * kp + cw_[j].code(k);
                             d = __fadd_rn(d, __fadd_rn(S.lut[bc], __ldg(r1 + bc)));
                         }
                     }
                     uint32_t du = f2o(d);
                     if (du <= (uint32_t)(thr >> 32)) {
-                        uint64_t e = ((uint64_t)du << 32) | (uint32_t)a.pid[pos];
+                        uint64_t e = ((uint64_t)du << 32) | (uint32_t)a.pid[pos[j]];
                         if (e < thr) {
                             int slot = atomicAdd(&st.npend, 1);
                             topk[st.ncur + slot] = e;
@@ -735,7 +801,7 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a) {
                     }
                 }
                 uint32_t step = wend > flat0 ? wend - flat0 : 0u;
-                if (step > (uint32_t)NT) step = NT;
+                if (step > (uint32_t)(NT * CPT)) step = NT * CPT;
                 __syncthreads();
                 if (step == 0) {
                     // cannot happen with consistent prefixes; stop instead of spinning
@@ -781,22 +847,44 @@ __global__ void __launch_bounds__(NT) k_search(SearchArgs a) {
 
 size_t search_smem_bytes(int mode, int kc, int mp, int kp) { return carve(mode, kc, mp, kp, nullptr, nullptr); }
 
+template <int MPC>
+static int occupancy(size_t smem) {
+    cudaFuncSetAttribute(k_search<MPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<MPC>, NT, smem);
+    return nb;
+}
+
 int search_max_blocks_per_sm(int mode, int kc, int mp, int kp) {
     size_t smem = search_smem_bytes(mode, kc, mp, kp);
-    cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search, NT, smem);
-    return nb;
+    switch (mp) {
+        case 4: return occupancy<4>(smem);
+        case 8: return occupancy<8>(smem);
+        case 16: return occupancy<16>(smem);
+        case 32: return occupancy<32>(smem);
+        default: return occupancy<0>(smem);
+    }
+}
+
+template <int MPC>
+static int launch(const SearchArgs &a, int grid, size_t smem, cudaStream_t s) {
+    cudaError_t e = cudaFuncSetAttribute(k_search<MPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_search)");
+    k_search<MPC><<<grid, NT, smem, s>>>(a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "k_search launch");
+    return SCG_OK;
 }
 
 int search_launch(const SearchArgs &a, int grid, cudaStream_t s) {
     size_t smem = search_smem_bytes(a.mode, a.kc, a.mp, a.kp);
-    cudaError_t e = cudaFuncSetAttribute(k_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_search)");
-    k_search<<<grid, NT, smem, s>>>(a);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(e, "k_search launch");
-    return SCG_OK;
+    switch (a.mp) {
+        case 4: return launch<4>(a, grid, smem, s);
+        case 8: return launch<8>(a, grid, smem, s);
+        case 16: return launch<16>(a, grid, smem, s);
+        case 32: return launch<32>(a, grid, smem, s);
+        default: return launch<0>(a, grid, smem, s);
+    }
 }
 
 }  // namespace scg

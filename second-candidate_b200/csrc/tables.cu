@@ -112,15 +112,25 @@ __global__ void __launch_bounds__(ET) k_tables_exact(TablesArgs a, int ctiles, i
             cs[kk][ee] = (eg < seglen && kk < kn) ? cent[(size_t)eg * len + k0 + kk] : 0.0f;
         }
         __syncthreads();
-        for (int kk = 0; kk < kn; kk++) {
-            float c = cs[kk][t];
+        if (a.fast) {
+            for (int kk = 0; kk < kn; kk++) {
+                float c = cs[kk][t];
 #pragma unroll
-            for (int i = 0; i < QT; i++) acc[i] = __fadd_rn(acc[i], __fmul_rn(qs[i][kk], c));
+                for (int i = 0; i < QT; i++) acc[i] = fmaf(qs[i][kk], c, acc[i]);
+            }
+        } else {
+            for (int kk = 0; kk < kn; kk++) {
+                float c = cs[kk][t];
+#pragma unroll
+                for (int i = 0; i < QT; i++) acc[i] = __fadd_rn(acc[i], __fmul_rn(qs[i][kk], c));
+            }
         }
         __syncthreads();
     }
     if (e < seglen) {
-        float nv = norm[e];
+        // the fast form keeps ||r||^2 in the per-vector term: its LUT is -2<q,r>
+        const bool lut_only = a.fast && out == a.dqr;
+        float nv = lut_only ? 0.0f : norm[e];
 #pragma unroll
         for (int i = 0; i < QT; i++) {
             int q = q0 + i;
@@ -152,7 +162,52 @@ __global__ void k_query_norms(const float *__restrict__ Q, int nq, int dim, int 
     qsum[q] = (mc == 2) ? __fadd_rn(__fadd_rn(0.0f, n[0]), n[1]) : n[0];
 }
 
+// Per-vector term of the fast ADC form, in CSR order:
+//   vterm[p] = sum_k ( ||r_k(c_k)||^2 + 2<c_part(k), r_k(c_k)> )
+// so that ||q - c - r||^2 = q_sum + dqc(cell) + vterm + sum_k (-2<q_k, r_k>).
+__global__ void k_vterm(int mode, int kc, int mp, int kp, int mc, uint64_t ncells, int64_t N,
+                        const uint32_t *__restrict__ off, const uint8_t *__restrict__ codes,
+                        const float *__restrict__ norm_r, const float *__restrict__ dot_cr,
+                        float *__restrict__ vterm) {
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    // cell of CSR position p: last c with off[c] <= p
+    uint64_t lo = 0, hi = ncells - 1;
+    while (lo < hi) {
+        uint64_t mid = (lo + hi + 1) >> 1;
+        if ((int64_t)off[mid] <= p) lo = mid;
+        else hi = mid - 1;
+    }
+    uint32_t cell = (uint32_t)lo;
+    int bs = kp * mp / mc;
+    const float *r1, *r2;
+    if (mode == SCG_IMI) {
+        uint32_t h3 = cell / (uint32_t)kc, h4 = cell - h3 * (uint32_t)kc;
+        r1 = dot_cr + (size_t)h3 * bs;
+        r2 = dot_cr + (size_t)(h4 + kc - 1) * bs;
+    } else {
+        uint32_t h3 = (mode == SCG_SC2) ? cell / (uint32_t)kc : cell;
+        r1 = dot_cr + (size_t)h3 * bs;
+        r2 = r1;
+    }
+    const uint8_t *c = codes + (size_t)p * mp;
+    int half = (mode == SCG_IMI) ? (mp >> 1) : mp;
+    float v = 0.0f;
+    for (int k = 0; k < mp; k++) {
+        int bc = k * kp + c[k];
+        v += norm_r[bc] + (k < half ? r1 : r2)[bc];
+    }
+    vterm[p] = v;
+}
+
 }  // namespace
+
+void launch_vterm(int mode, int kc, int mp, int kp, int mc, uint64_t ncells, int64_t N, const uint32_t *off,
+                  const uint8_t *codes, const float *norm_r, const float *dot_cr, float *vterm, cudaStream_t s) {
+    if (N <= 0) return;
+    k_vterm<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(mode, kc, mp, kp, mc, ncells, N, off, codes, norm_r, dot_cr,
+                                                          vterm);
+}
 
 void launch_precompute1(int dim, int mc, int kc, int mp, int kp, const float *cq, const float *pq,
                         float *norm_c, float *norm_r, float *dot_cr, cudaStream_t s) {

@@ -22,7 +22,8 @@ EXPORTS = ["scg_last_error", "scg_index_create", "scg_index_destroy", "scg_load_
            "scg_load_codebooks_file", "scg_load_csr", "scg_load_encoded_file", "scg_load_raw",
            "scg_precompute", "scg_search", "scg_search_device", "scg_set_query_targets",
            "scg_set_cell_budget", "scg_encode", "scg_sc_encode", "scg_encode_device",
-           "scg_index_info", "scg_last_query_stats", "scg_last_timings"]
+           "scg_index_info", "scg_last_query_stats", "scg_last_timings",
+           "scg_cell_counts"]
 
 
 class ScgError(RuntimeError):

@@ -1,0 +1,76 @@
+"""The drop-in C++ headers (second-candidate_b200/cpp) driven the way the
+reference's own test drivers drive the reference classes: results match the
+oracle, the `traversed` invariants hold, and the encoder writes the same
+.edat_ bytes as the reference's layout."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import formats
+import helpers
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "second-candidate_b200")
+
+
+@pytest.fixture(scope="module")
+def driver(tmp_path_factory):
+    import scgpu
+    scgpu.load()
+    exe = str(tmp_path_factory.mktemp("drv") / "dropin_driver")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(PKG, "cpp"), "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "dropin_driver.cpp"), "-L", PKG, "-lscgpu",
+                    "-Wl,-rpath," + PKG, "-o", exe], check=True)
+    return exe
+
+
+def parse(path):
+    rows = []
+    for line in open(path):
+        f = line.split()
+        pairs = [p.split(":") for p in f[2:]]
+        rows.append((int(f[0]), int(f[1]), [int(a) for a, b in pairs], [float(b) for a, b in pairs]))
+    return rows
+
+
+@pytest.mark.parametrize("name,mode,tag", [("imi_d32", O.IMI, "imi"), ("sc_d32", O.SC, "sc"),
+                                           ("ivf_d32", O.IVFADC, "ivf")])
+def test_search_through_dropin(driver, oracle_mod, tmp_path, name, mode, tag):
+    c = helpers.load_case(os.path.join(helpers.GOLDEN, name + ".npz"))
+    D, mc, kc, mp, kp = (int(c[k]) for k in ("D", "mc", "kc", "mp", "kp"))
+    formats.write_ctr(tmp_path / "cq.ctr_", c["cq"], kc, mc, D)
+    formats.write_ctr(tmp_path / "pq.ctr_", c["pq"], kp, mp, D)
+    formats.write_edat(tmp_path / "x.edat_", c["L"], c["pid"], c["icodes"])
+    formats.write_vecs(tmp_path / "q.fvecs", c["Q"])
+    T, w, R = 300, (16 if mode == O.IVFADC else 1 << 16), 20
+    subprocess.run([driver, "search", tag, str(tmp_path / "cq.ctr_"), str(tmp_path / "pq.ctr_"),
+                    str(tmp_path / "x.edat_"), str(tmp_path / "q.fvecs"), str(D), str(R), str(w), str(T),
+                    str(tmp_path / "out.txt")], check=True)
+    rows = parse(tmp_path / "out.txt")
+    ix = helpers.oracle_index(O, c)
+    oi, od, osum = ix.search(mode, c["Q"], R, w, T, order=O.ORDER_EXACT)
+    for i, (s, e, ids, d) in enumerate(rows):
+        assert s == osum[i]
+        m = min(R, s)
+        assert ids == oi[i, :m].tolist()
+        assert np.allclose(d, od[i, :m], rtol=1e-6)
+        if mode == O.IMI:
+            assert e == ix.search_one(mode, c["Q"][i], w, T)["empty"]
+
+
+@pytest.mark.parametrize("name,nc", [("imi_d32", 0), ("sc_d32", 2)])
+def test_encoder_through_dropin(driver, oracle_mod, tmp_path, name, nc):
+    c = helpers.load_case(os.path.join(helpers.GOLDEN, name + ".npz"))
+    D, mc, kc, mp, kp = (int(c[k]) for k in ("D", "mc", "kc", "mp", "kp"))
+    formats.write_ctr(tmp_path / "cq.ctr_", c["cq"], kc, mc, D)
+    formats.write_ctr(tmp_path / "pq.ctr_", c["pq"], kp, mp, D)
+    formats.write_vecs(tmp_path / "x.fvecs", c["X"].astype(np.float32))
+    subprocess.run([driver, "encode", str(nc), str(tmp_path / "cq.ctr_"), str(tmp_path / "pq.ctr_"),
+                    str(tmp_path / "x.fvecs"), str(tmp_path), "d"], check=True)
+    got = open(tmp_path / ("d_mr2_ivf.edat_" if nc else "d_ivf.edat_"), "rb").read()
+    formats.write_edat(tmp_path / "ref.edat_", c["L"], c["pid"], c["icodes"])
+    assert got == open(tmp_path / "ref.edat_", "rb").read()

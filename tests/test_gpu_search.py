@@ -140,3 +140,34 @@ def test_file_loaders(scg, oracle_mod, tmp_path):
         g.load_encoded_file(str(tmp_path / "bad.edat_"), 2)
     assert e.value.code == -3
     g.close()
+
+
+@pytest.mark.parametrize("mode,mc,kc", [(O.IVFADC, 1, 64), (O.IMI, 2, 48), (O.SC, 1, 48)])
+def test_fast_form_tolerance(scg, oracle_mod, mode, mc, kc):
+    """The fast form (FMA tables, per-vector term) reorders the float sums:
+    candidate sets match the exact order except at rare boundary ties, and
+    top-R distances agree with the exact ones within 1e-5 relative."""
+    D, mp, kp = 64, 8, 256
+    mix = W.Mixture(D, 16, 20.0, "u8", seed=31 + mode)
+    X = mix.sample(30000, seed=32)
+    Q = mix.sample(80, seed=33)
+    cq, pq = W.train_codebooks(X[:4000], mc, kc, mp, kp, 4, seed=34)
+    if mode == O.SC:
+        cid, codes = O.sc_encode(D, kc, mp, kp, 2, cq, pq, X)
+        L, pid, co, _ = O.distribution(O.SC, kc, 1, 2, cid, codes)
+    else:
+        cid, codes = O.encode((D, mc, kc, mp, kp), cq, pq, X)
+        L, pid, co, _ = O.distribution(mode, kc, mc, 0, cid, codes)
+    ix = O.Index(D, mc, kc, mp, kp, cq, pq, L, pid, co)
+    g = gpu_index(scg, D, mc, kc, mp, kp, cq, pq, L, pid, co)
+    w = kc if mode == O.IVFADC else 1 << 20
+    R, T = 50, 1500
+    ids, d, sums = g.search(MODES[mode], Q, R, w, T, precision=scg.FAST)
+    oi, od, osum = ix.search(mode, Q, R, w, T, order=O.ORDER_EXACT)
+    same = sums == osum
+    assert same.mean() >= 0.95
+    for i in np.nonzero(same)[0]:
+        m = min(R, int(sums[i]))
+        assert np.allclose(d[i, :m], od[i, :m], rtol=1e-5, atol=1e-2)
+        assert len(set(ids[i, :m].tolist()) & set(oi[i, :m].tolist())) >= m - 2
+    g.close()
