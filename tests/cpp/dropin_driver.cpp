@@ -8,6 +8,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <iomanip>
 #include <iostream>
 
 #include "evaluation.h"
@@ -23,6 +24,7 @@ static int search(int argc, char **argv) {
     float *data = nullptr;
     int N = load_and_convert_data<float, float>(argv[6], data, 4, d, false);
     std::ofstream out(argv[11]);
+    out << std::setprecision(9);
     int sum = 0, bad = 0;
     int *result = nullptr;
     float *dist = nullptr;
