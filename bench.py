@@ -161,6 +161,10 @@ def main():
     ap.add_argument("--cache", default="/tmp/scg_bench_cache")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="fast", choices=["fast", "fp32"])
+    ap.add_argument("--queries", type=int, default=0, help="use only the first N queries")
+    ap.add_argument("--no-plain", action="store_true", help="skip the FP32 plain comparison")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
+    ap.add_argument("--phases", action="store_true", help="report per-phase cycle counters")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -215,6 +219,9 @@ def main():
     mcp = 1 if cfg["mode"] == "sc" else cfg["mc"]
     R, wcap = cfg["R"], cfg["w"]
     T = cfg["T"] if isinstance(cfg["T"], int) else cfg["T"][0]
+    if args.queries:
+        w["Q"] = w["Q"][: args.queries]
+        w["gt"] = w["gt"][: args.queries]
     nq = w["Q"].shape[0]
 
     ix = scgpu.Index(local)
@@ -237,7 +244,7 @@ def main():
 
     # the plain FP32 form (the reference's float order), for comparison
     plain = None
-    if args.precision == "fast":
+    if args.precision == "fast" and not args.no_plain:
         for _ in range(2):
             step(scgpu.FP32_EXACT)
         torch.cuda.synchronize()
@@ -307,17 +314,28 @@ def main():
         except Exception:
             traffic = None
 
+    phases = None
+    if args.phases:
+        ix.set_phase_counters(True)
+        step()
+        phases = ix.last_phase_counters()
+        phases["per_query_cycles"] = {k: phases[k] / nq for k in
+                                      ("sort", "rounds", "cut", "compact", "scan", "final_merge")}
+        ix.set_phase_counters(False)
+
     # end to end through the public host-buffer entry point
-    Qh = torch.from_numpy(w["Q"]).pin_memory().numpy()
-    e2e_times = []
-    for i in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        hid, hd, hs = ix.search(mode, Qh, R, wcap, T, precision=prec)
-        dt = time.perf_counter() - t0
-        if i >= args.warmup:
-            e2e_times.append(dt)
-    e2e_qps = nq * len(e2e_times) / sum(e2e_times) * world
-    same = bool(np.array_equal(hid, ids))
+    e2e_qps, same = None, None
+    if not args.no_e2e:
+        Qh = torch.from_numpy(w["Q"]).pin_memory().numpy()
+        e2e_times = []
+        for i in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            hid, hd, hs = ix.search(mode, Qh, R, wcap, T, precision=prec)
+            dt = time.perf_counter() - t0
+            if i >= args.warmup:
+                e2e_times.append(dt)
+        e2e_qps = nq * len(e2e_times) / sum(e2e_times) * world
+        same = bool(np.array_equal(hid, ids))
 
     line = {
         "metric": METRIC, "value": nq * args.steps * world / (total_ms / 1e3), "unit": "queries/s",
@@ -331,6 +349,7 @@ def main():
                    "timing": "CUDA events per step on the launching stream"},
         "recall@100": recall,
         "fp32_plain": plain,
+        "phases": phases,
         "latency_ms": {"p50": float(np.percentile(times, 50)), "p99": float(np.percentile(times, 99)),
                        "what": "whole batch of %d queries" % nq},
         "kernels_ms": {"tables": tables_ms, "select_scan": search_ms},

@@ -66,7 +66,8 @@ struct scg_index {
     bool have_vterm = false;
     // batch workspace
     DevBuf q, dqc, dqr, qn, qsum, ids, dists, sums, nvis, empty, status, counter;
-    DevBuf rec_key, rec_rank, rec_cnt, vis_cell, vis_pre;
+    DevBuf rec_key, rec_rank, rec_cnt, vis_cell, vis_pre, phase;
+    bool phase_on = false;
     int *h_status = nullptr;  // pinned
     int last_nq = 0;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
@@ -215,6 +216,12 @@ int run_search(scg_index *h, const scg_search_params *p, const float *dQ, int nq
     sa.out_ids = d_ids; sa.out_d = d_d; sa.out_sum = d_sums;
     sa.out_nvis = h->nvis.as<int>(); sa.out_empty = h->empty.as<int>();
     sa.status = h->status.as<int>();
+    sa.phase_cycles = nullptr;
+    if (h->phase_on) {
+        if ((rc = h->phase.ensure(sizeof(long long) * 16))) return rc;
+        SCG_CUDA(cudaMemsetAsync(h->phase.p, 0, sizeof(long long) * 16, s));
+        sa.phase_cycles = h->phase.as<long long>();
+    }
     if (nq > 0 && (rc = search_launch(sa, grid, s))) return rc;
     SCG_CUDA(cudaEventRecord(h->ev[2], s));
     h->last_nq = nq;
@@ -268,7 +275,7 @@ int scg_index_destroy(scg_index *h) {
     DevBuf *all[] = {&h->cq, &h->pq, &h->norm_c, &h->norm_r, &h->dot_cr, &h->off, &h->pid, &h->codes,
                      &h->raw, &h->vterm, &h->q, &h->dqc, &h->dqr, &h->qn, &h->qsum, &h->ids, &h->dists, &h->sums,
                      &h->nvis, &h->empty, &h->status, &h->counter, &h->rec_key, &h->rec_rank,
-                     &h->rec_cnt, &h->vis_cell, &h->vis_pre};
+                     &h->rec_cnt, &h->vis_cell, &h->vis_pre, &h->phase};
     for (DevBuf *b : all) b->release();
     if (h->h_status) cudaFreeHost(h->h_status);
     for (int i = 0; i < 3; i++)
@@ -554,6 +561,24 @@ int scg_cell_counts(scg_index *h, int *L, int64_t ncells) {
     int rc;
     if ((rc = set_device(h))) return rc;
     SCG_CUDA(cudaMemcpy(L, h->off.as<uint32_t>() + 1, sizeof(int) * (size_t)ncells, cudaMemcpyDeviceToHost));
+    return SCG_OK;
+}
+
+int scg_set_phase_counters(scg_index *h, int on) {
+    if (!h) return fail(SCG_ERR_ARG, "null index");
+    h->phase_on = on != 0;
+    return SCG_OK;
+}
+
+int scg_last_phase_counters(scg_index *h, long long *out, int n) {
+    if (!h || !out) return fail(SCG_ERR_ARG, "null argument");
+    if (!h->phase_on || !h->phase.p) return fail(SCG_ERR_STATE, "phase counters are off");
+    std::lock_guard<std::mutex> g(h->mu);
+    int rc;
+    if ((rc = set_device(h))) return rc;
+    long long tmp[16];
+    SCG_CUDA(cudaMemcpy(tmp, h->phase.p, sizeof(tmp), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < n && i < 16; i++) out[i] = tmp[i];
     return SCG_OK;
 }
 

@@ -89,6 +89,7 @@ struct SearchArgs {
     float *out_d;
     int *out_sum, *out_nvis, *out_empty;
     int *status;
+    long long *phase_cycles;  // optional [16] counters
 };
 
 size_t search_smem_bytes(int mode, int kc, int mp, int kp);

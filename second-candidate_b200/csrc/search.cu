@@ -302,6 +302,17 @@ struct CodeWords<0> {
     __device__ __forceinline__ uint32_t code(int k) const { return __ldg(p + k); }
 };
 
+// Optional per-phase cycle counters (thread 0 of each CTA), accumulated
+// into a.phase_cycles[phase] when that pointer is set.
+#define PHASE_MARK(i)                                                        \
+    do {                                                                     \
+        if (a.phase_cycles && tid == 0) {                                    \
+            long long _t = clock64();                                        \
+            atomicAdd((unsigned long long *)&a.phase_cycles[(i)], (unsigned long long)(_t - t_prev)); \
+            t_prev = _t;                                                     \
+        }                                                                    \
+    } while (0)
+
 struct QState {
     int err;
     uint32_t tau;
@@ -353,6 +364,7 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
         __syncthreads();
         const int q = s_q;
         if (q >= a.nq) break;
+        long long t_prev = clock64();
         const int T = a.Tq ? a.Tq[q] : a.T;
         const int w = a.w;
         const int R = a.R;
@@ -393,6 +405,7 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
             needW = 1;
         }
 
+        PHASE_MARK(0);  // lists sorted
         // (2) rounds of staircase enumeration
         for (int h = tid; h < kc; h += NT) S.rowp[h] = (sc && h == 0) ? 1 : 0;
         uint64_t Ssum = 0, Ncell = 0, NEc = 0;  // totals over enumerated cells
@@ -423,11 +436,13 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
                 // bisection for tau: smallest key with staircase count >= target
                 uint32_t lo = round == 0 ? lo_key : tau_prev + 1, hi = hi_key;
                 uint64_t thi = target + target / 4 + 32;
+                if (a.phase_cycles && tid == 0) atomicAdd((unsigned long long *)&a.phase_cycles[8], 1ull);
                 if (lo > hi) lo = hi;
                 int it = 0;
                 while (lo < hi && it < 40) {
                     uint32_t mid = lo + ((hi - lo) >> 1);
                     uint64_t c = staircase_count(L, mid, red);
+                    if (a.phase_cycles && tid == 0) atomicAdd((unsigned long long *)&a.phase_cycles[9], 1ull);
                     if (c >= target) {
                         hi = mid;
                         if (c <= thi) break;
@@ -473,6 +488,7 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
                 }
                 __syncthreads();
                 const int nnew = (int)tot_new;
+                if (a.phase_cycles && tid == 0) atomicAdd((unsigned long long *)&a.phase_cycles[10], (unsigned long long)nnew);
                 uint64_t ls = 0, lne = 0, dummy = 0;
                 for (int idx = tid; idx < nnew; idx += NT) {
                     // row of idx: last h with rowpre[h] <= idx
@@ -525,6 +541,7 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
         __syncthreads();
         const bool qerr = st.err != 0;
 
+        PHASE_MARK(1);  // staircase rounds
         // (3) the cut within the last round
         if (!nothing && !qerr && trig) {
             uint32_t lo = 0xffffffffu, hi = 0;
@@ -630,6 +647,7 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
         }
         __syncthreads();
 
+        PHASE_MARK(2);  // cut
         // (4) visited non-empty cells -> (cell, prefix) list
         int nvis = 0;
         if (!nothing && !st.err) {
@@ -670,6 +688,7 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
         const bool qerr2 = st.err != 0;
         const uint32_t Svis = (nvis > 0) ? (uint32_t)st.sumv : 0u;
 
+        PHASE_MARK(3);  // compaction
         // (5) ADC scan with the fused top-R
         if (tid == 0) {
             st.ncur = 0;
@@ -721,6 +740,7 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
                 }
                 // make room for this round's candidates
                 if (st.ncur + st.npend + NT * CPT > MERGE_N) {
+                    if (a.phase_cycles && tid == 0) atomicAdd((unsigned long long *)&a.phase_cycles[7], 1ull);
                     int n = st.ncur + st.npend;
                     int np2 = next_pow2(n);
                     for (int i = n + tid; i < np2; i += NT) topk[i] = ~0ull;
@@ -810,6 +830,7 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
                 }
                 flat0 += step;
             }
+            PHASE_MARK(4);  // scan rounds
             // final merge
             int n = st.ncur + st.npend;
             int np2 = next_pow2(n > 1 ? n : 2);
@@ -818,6 +839,7 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
             bitonic_sort64(topk, np2);
         }
         __syncthreads();
+        PHASE_MARK(5);  // final merge
         // (6) outputs
         {
             int n = (qerr2 || nvis == 0) ? 0 : st.ncur + st.npend;

@@ -23,7 +23,7 @@ EXPORTS = ["scg_last_error", "scg_index_create", "scg_index_destroy", "scg_load_
            "scg_precompute", "scg_search", "scg_search_device", "scg_set_query_targets",
            "scg_set_cell_budget", "scg_encode", "scg_sc_encode", "scg_encode_device",
            "scg_index_info", "scg_last_query_stats", "scg_last_timings",
-           "scg_cell_counts"]
+           "scg_cell_counts", "scg_set_phase_counters", "scg_last_phase_counters"]
 
 
 class ScgError(RuntimeError):
@@ -158,6 +158,16 @@ class Index:
         empty = np.empty(nq, np.int32)
         _check(_lib.scg_last_query_stats(self._h, _ptr(nvis), _ptr(empty), nq))
         return nvis, empty
+
+    def set_phase_counters(self, on):
+        _check(_lib.scg_set_phase_counters(self._h, 1 if on else 0))
+
+    def last_phase_counters(self):
+        out = np.zeros(16, np.int64)
+        _check(_lib.scg_last_phase_counters(self._h, _ptr(out), 16))
+        names = ["sort", "rounds", "cut", "compact", "scan", "final_merge", "-", "merges", "round_count",
+                 "bisection_steps", "enumerated_cells"]
+        return {n: int(v) for n, v in zip(names, out) if n != "-"}
 
     def last_timings(self):
         ms = np.zeros(2, np.float32)
