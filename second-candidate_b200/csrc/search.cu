@@ -3,8 +3,16 @@
 // time and takes the next query from a global counter, so queries with
 // uneven posting-list totals balance across the persistent grid.
 //
-// Cell selection.  The reference walks the grid of rank pairs (h1, h2) of two
-// sorted coarse lists with a binary heap (multi_query.h:133-205,
+// Coarse ranking.  The reference sorts each coarse list completely
+// (nth_element_id + sort_id with M = kc, multi_query.h:125-128).  Only a
+// prefix of each sorted list is ever reached, so a radix select finds the
+// prefix of the M smallest keys (ties included) and sorts only it.  If the
+// cell selection below then reaches a key at or beyond the smallest key a
+// cell outside the prefix grid can have, the lists are sorted completely and
+// the selection is repeated -- the result is the same as with full sorts.
+//
+// Cell selection.  The reference walks the grid of rank pairs (h1, h2) of the
+// two sorted lists with a binary heap (multi_query.h:133-205,
 // sc_query.h:112-186) and stops after the first cell at which the candidate
 // total reaches T (or the cell cap w).  The visited set is therefore a
 // prefix of the cells sorted by key(h1,h2) = A[h1] + B[h2].  Here the prefix
@@ -19,10 +27,11 @@
 //      cell count for the w rule);
 //   3. cells tied at the cut key are taken in (rank1, rank2) order until the
 //      rule fires -- the order an exact priority queue yields.
-// The ADC scan then walks the visited cells' candidates with one candidate
-// per thread, adds the table entries in the reference's order, and keeps
-// the R smallest (distance, id) pairs: a threshold filter feeds a shared
-// buffer that is merged by a bitonic sort when full.
+// The ADC scan then walks the visited cells' candidates, CPT per thread per
+// round with all loads issued before the sums, adds the table entries in
+// the reference's order, and keeps the R smallest (distance, id) pairs: a
+// threshold filter feeds a pending buffer that is sorted and merged into the
+// sorted top list (merge path) when it fills.
 #include "scg_internal.cuh"
 
 namespace scg {
@@ -30,12 +39,14 @@ namespace scg {
 namespace {
 
 constexpr int NT = 256;
-constexpr int CPT = 4;  // candidates per thread per scan round
 constexpr int NWARP = NT / 32;
+constexpr int CPT = 4;          // candidates per thread per scan round
 constexpr int HBITS = 11;
 constexpr int HBINS = 1 << HBITS;
 constexpr int TIECAP = 64;
-constexpr int MERGE_N = 4096;
+constexpr int RMAX = 1024;      // largest R
+constexpr int PCAP = 2048;      // pending top-R candidates
+constexpr int SBCAP = 2048;     // sorted coarse prefix capacity
 constexpr int MAX_ROUNDS = 64;
 
 struct CellWin {
@@ -60,6 +71,15 @@ struct Smem {
     unsigned char *uni;
 };
 
+__host__ __device__ inline size_t union_bytes(int kc) {
+    size_t trav = (size_t)HBINS * 4 + (size_t)TIECAP * 8;
+    size_t lists = (size_t)SBCAP * 8;
+    size_t scan = (size_t)(RMAX + PCAP + RMAX) * 8 + (size_t)NT * sizeof(CellWin);
+    size_t m = trav > scan ? trav : scan;
+    (void)kc;
+    return m > lists ? m : lists;
+}
+
 __host__ __device__ inline size_t carve(int mode, int kc, int mp, int kp, Smem *s, unsigned char *base) {
     int kcP = next_pow2(kc);
     size_t off = 0;
@@ -78,9 +98,7 @@ __host__ __device__ inline size_t carve(int mode, int kc, int mp, int kp, Smem *
     if (s) s->lut = (float *)(base + off);
     off += align16((size_t)mp * kp * 4);
     if (s) s->uni = base + off;
-    size_t trav = (size_t)HBINS * 4 + (size_t)TIECAP * 8;
-    size_t scan = (size_t)MERGE_N * 8 + (size_t)NT * sizeof(CellWin);
-    off += (trav > scan ? trav : scan);
+    off += union_bytes(kc);
     return off;
 }
 
@@ -124,6 +142,31 @@ __device__ uint64_t block_sum(uint64_t v, uint64_t *red) {
     return v;
 }
 
+// Minimum and maximum of one u64 per thread over the block.
+__device__ void block_minmax(uint64_t &mn, uint64_t &mx, uint64_t *red) {
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        uint64_t a = __shfl_xor_sync(0xffffffffu, mn, o);
+        uint64_t b = __shfl_xor_sync(0xffffffffu, mx, o);
+        mn = a < mn ? a : mn;
+        mx = b > mx ? b : mx;
+    }
+    __syncthreads();
+    if (lane == 0) {
+        red[wid] = mn;
+        red[NWARP + wid] = mx;
+    }
+    __syncthreads();
+    mn = ~0ull;
+    mx = 0;
+    for (int i = 0; i < NWARP; i++) {
+        mn = red[i] < mn ? red[i] : mn;
+        mx = red[NWARP + i] > mx ? red[NWARP + i] : mx;
+    }
+    __syncthreads();
+}
+
 // Exclusive scan of one u64 per thread; returns the exclusive prefix and the
 // block total.
 __device__ uint64_t block_exscan(uint64_t v, uint64_t *red, uint64_t &total) {
@@ -148,6 +191,7 @@ __device__ uint64_t block_exscan(uint64_t v, uint64_t *red, uint64_t &total) {
     return wpre + x - v;
 }
 
+// Ascending bitonic sort of n (a power of two) u64 keys in shared memory.
 __device__ void bitonic_sort64(uint64_t *key, int n) {
     for (int k = 2; k <= n; k <<= 1) {
         for (int j = k >> 1; j > 0; j >>= 1) {
@@ -167,11 +211,87 @@ __device__ void bitonic_sort64(uint64_t *key, int n) {
     }
 }
 
+struct QState {
+    int err;
+    uint32_t s_bin;
+    uint64_t s_acc;
+    uint32_t kappa;
+    uint32_t rank_cut;
+    int take_all;
+    int nties;
+    uint64_t sumv, nv, nev;
+    int nvis;
+    int kA, kB;
+    uint32_t nextA, nextB;  // smallest key outside the sorted prefix (ordered)
+    // scan
+    int ncur, npend;
+    uint64_t thr;
+    int clo, cn;
+    uint32_t wend;
+};
+
+// The prefix of a coarse list: the smallest keys of L[0..n) (u64: ordered
+// key << 32 | centroid id) up to and including every key equal to the m-th
+// smallest, sorted ascending into L[0..c).  Returns c, or -1 when the prefix
+// would exceed SBCAP (the caller then sorts the whole list).  st.nextA/B
+// receives the smallest ordered key left outside.
+__device__ int select_prefix(uint64_t *L, int n, int m, uint64_t *sb, uint32_t *hist, uint64_t *red,
+                             QState &st, uint32_t *next_out) {
+    const int tid = threadIdx.x;
+    // radix select (4 x 8 bits) of the m-th smallest high word
+    uint32_t prefix = 0;
+    uint64_t need = (uint64_t)m;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        hist[tid] = 0;  // NT == 256 bins
+        __syncthreads();
+        for (int i = tid; i < n; i += NT) {
+            uint32_t v = (uint32_t)(L[i] >> 32);
+            if (shift == 24 || (v >> (shift + 8)) == (prefix >> (shift + 8))) atomicAdd(&hist[(v >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        uint64_t cnt = hist[tid], tot;
+        uint64_t ex = block_exscan(cnt, red, tot);
+        if (ex < need && ex + cnt >= need) {
+            st.s_bin = (uint32_t)tid;
+            st.s_acc = ex;
+        }
+        __syncthreads();
+        prefix |= st.s_bin << shift;
+        need -= st.s_acc;
+        __syncthreads();
+    }
+    const uint32_t vm = prefix;
+    // compact every key with high word <= vm; smallest high word above vm
+    uint64_t mine = 0, mn = ~0ull, mx = 0;
+    for (int i = tid; i < n; i += NT) {
+        uint32_t v = (uint32_t)(L[i] >> 32);
+        if (v <= vm) mine++;
+        else if (v < mn) mn = v;
+    }
+    block_minmax(mn, mx, red);
+    uint64_t c;
+    uint64_t pos = block_exscan(mine, red, c);
+    if (c > (uint64_t)SBCAP) return -1;
+    for (int i = tid; i < n; i += NT) {
+        uint64_t k = L[i];
+        if ((uint32_t)(k >> 32) <= vm) sb[pos++] = k;
+    }
+    int c2 = next_pow2((int)c);
+    for (int i = (int)c + tid; i < c2; i += NT) sb[i] = ~0ull;
+    __syncthreads();
+    bitonic_sort64(sb, c2);
+    for (int i = tid; i < (int)c; i += NT) L[i] = sb[i];
+    if (tid == 0) *next_out = mn == ~0ull ? 0xffffffffu : (uint32_t)mn;
+    __syncthreads();
+    return (int)c;
+}
+
 // ---------------------------------------------------------------------------
 
 struct Lists {
     const uint64_t *LA, *LB;
-    int kc, kB;
+    int kA, kB;  // sorted prefix lengths
+    int kc;      // codebook size (cell ids)
     bool ivf;
     __device__ __forceinline__ float a(int h) const { return o2f((uint32_t)(LA[h] >> 32)); }
     __device__ __forceinline__ float b(int h) const { return ivf ? 0.0f : o2f((uint32_t)(LB[h] >> 32)); }
@@ -192,17 +312,20 @@ struct Lists {
 
 __device__ uint64_t staircase_count(const Lists &L, uint32_t tau, uint64_t *red) {
     uint64_t c = 0;
-    for (int h = threadIdx.x; h < L.kc; h += NT) c += (uint64_t)L.row_count(L.a(h), tau);
+    for (int h = threadIdx.x; h < L.kA; h += NT) {
+        float av = L.a(h);
+        if (f2o(__fadd_rn(av, L.b(0))) > tau) continue;
+        c += (uint64_t)L.row_count(av, tau);
+    }
     return block_sum(c, red);
 }
 
 // Radix select over the last round's records [r0, r1): the smallest key x
 // with base + sum_{key <= x} weight >= need.  weight: 0 = length, 1 = one per
-// cell, 2 = one per non-empty cell.  Returns x and sets *below to
-// base + sum_{key < x} weight.
+// cell, 2 = one per non-empty cell.
 __device__ uint32_t radix_cut(const uint32_t *rk, const uint32_t *rc, int r0, int r1, uint32_t lo,
                               uint32_t hi, uint64_t base, uint64_t need, int weight, uint32_t *hist,
-                              uint64_t *red, uint64_t *below, uint32_t *s_bin, uint64_t *s_acc) {
+                              uint64_t *red, QState &st) {
     uint32_t range = hi - lo;
     int nbits = range ? 32 - __clz(range) : 0;
     uint32_t prefix = 0;
@@ -238,27 +361,22 @@ __device__ uint32_t radix_cut(const uint32_t *rk, const uint32_t *rc, int r0, in
             if (bb >= nb) break;
             uint64_t nxt = run + hist[bb];
             if (run < need && nxt >= need) {
-                *s_bin = (uint32_t)bb;
-                *s_acc = run;
+                st.s_bin = (uint32_t)bb;
+                st.s_acc = run;
             }
             run = nxt;
         }
         __syncthreads();
-        prefix |= (*s_bin) << shift;
-        acc = *s_acc;
+        prefix |= st.s_bin << shift;
+        acc = st.s_acc;
         __syncthreads();
     }
-    if (nbits == 0) {
-        // all keys equal lo: everything below is the base
-        acc = base;
-    }
-    *below = acc;
     return lo + prefix;
 }
 
-__device__ __forceinline__ uint32_t cell_of(const Lists &L, bool ivf, uint32_t rank) {
+__device__ __forceinline__ uint32_t cell_of(const Lists &L, uint32_t rank) {
     int h1 = rank >> 16, h2 = rank & 0xffff;
-    return ivf ? L.ta(h1) : L.ta(h1) * (uint32_t)L.kc + L.tb(h2);
+    return L.ivf ? L.ta(h1) : L.ta(h1) * (uint32_t)L.kc + L.tb(h2);
 }
 
 // The mp code bytes of one candidate.  MPC > 0: mp == MPC, loaded with
@@ -293,43 +411,58 @@ struct CodeWords {
 template <>
 struct CodeWords<0> {
     const uint8_t *p;
-    int m;
-    __device__ __forceinline__ void load(const uint8_t *codes, uint32_t pos, int mp) {
-        p = codes + (size_t)pos * mp;
-        m = mp;
-    }
+    __device__ __forceinline__ void load(const uint8_t *codes, uint32_t pos, int mp) { p = codes + (size_t)pos * mp; }
     __device__ __forceinline__ int n(int mp) const { return mp; }
     __device__ __forceinline__ uint32_t code(int k) const { return __ldg(p + k); }
 };
 
 // Optional per-phase cycle counters (thread 0 of each CTA), accumulated
 // into a.phase_cycles[phase] when that pointer is set.
-#define PHASE_MARK(i)                                                        \
-    do {                                                                     \
-        if (a.phase_cycles && tid == 0) {                                    \
-            long long _t = clock64();                                        \
+#define PHASE_MARK(i)                                                                                 \
+    do {                                                                                              \
+        if (a.phase_cycles && tid == 0) {                                                             \
+            long long _t = clock64();                                                                 \
             atomicAdd((unsigned long long *)&a.phase_cycles[(i)], (unsigned long long)(_t - t_prev)); \
-            t_prev = _t;                                                     \
-        }                                                                    \
+            t_prev = _t;                                                                              \
+        }                                                                                             \
+    } while (0)
+#define COUNT(i, v)                                                                                \
+    do {                                                                                           \
+        if (a.phase_cycles && tid == 0)                                                            \
+            atomicAdd((unsigned long long *)&a.phase_cycles[(i)], (unsigned long long)(v));        \
     } while (0)
 
-struct QState {
-    int err;
-    uint32_t tau;
-    uint32_t s_bin;
-    uint64_t s_acc;
-    uint32_t kappa;
-    uint32_t rank_cut;
-    int take_all;
-    int nties;
-    uint64_t sumv, nv, nev;
-    int nvis;
-    // scan
-    int ncur, npend;
-    uint64_t thr;
-    int clo, cn;
-    uint32_t wend;
-};
+// Merges the pending candidates into the sorted top list: sorts the pending
+// part, then each output k < min(R, ncur + npend) is taken by a merge-path
+// search over the two sorted runs.
+__device__ void merge_topk(uint64_t *top, uint64_t *pend, uint64_t *tmp, int R, QState &st) {
+    const int tid = threadIdx.x;
+    const int na = st.ncur, nb = st.npend;
+    const int p2 = next_pow2(nb > 1 ? nb : 2);
+    for (int i = nb + tid; i < p2; i += NT) pend[i] = ~0ull;
+    __syncthreads();
+    bitonic_sort64(pend, p2);
+    const int nout = na + nb < R ? na + nb : R;
+    for (int k = tid; k < nout; k += NT) {
+        int lo = k - nb > 0 ? k - nb : 0, hi = k < na ? k : na;
+        while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (top[mid] < pend[k - 1 - mid]) lo = mid + 1;
+            else hi = mid;
+        }
+        int i = lo, j = k - lo;
+        uint64_t x = i < na ? top[i] : ~0ull, y = j < nb ? pend[j] : ~0ull;
+        tmp[k] = x < y ? x : y;
+    }
+    __syncthreads();
+    for (int k = tid; k < nout; k += NT) top[k] = tmp[k];
+    if (tid == 0) {
+        st.ncur = nout;
+        st.npend = 0;
+        st.thr = nout == R ? tmp[R - 1] : ~0ull;
+    }
+    __syncthreads();
+}
 
 template <int MPC>
 __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
@@ -344,7 +477,7 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
     const int kcP = next_pow2(kc);
     const bool imi = a.mode == SCG_IMI, sc = a.mode == SCG_SC2, ivf = a.mode == SCG_IVFADC;
     const bool fast = a.precision == SCG_FAST;
-    const int kB = ivf ? 1 : kc;
+    const int kBfull = ivf ? 1 : kc;
     const int cap = a.cap_rec;
     uint32_t *rec_key = a.rec_key + (size_t)blockIdx.x * cap;
     uint32_t *rec_rank = a.rec_rank + (size_t)blockIdx.x * cap;
@@ -353,10 +486,12 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
     uint32_t *vis_pre = a.vis_pre + (size_t)blockIdx.x * (cap + 1);
     uint32_t *hist = (uint32_t *)S.uni;
     uint64_t *ties = (uint64_t *)(S.uni + (size_t)HBINS * 4);
-    uint64_t *topk = (uint64_t *)S.uni;
-    CellWin *win = (CellWin *)(S.uni + (size_t)MERGE_N * 8);
+    uint64_t *sb = (uint64_t *)S.uni;  // sorted coarse prefix scratch
+    uint64_t *top = (uint64_t *)S.uni;
+    uint64_t *pend = top + RMAX;
+    uint64_t *tmpk = pend + PCAP;
+    CellWin *win = (CellWin *)(tmpk + RMAX);
     const int bsI = kp * mp / a.mc;  // dot_cr block of one coarse centroid
-    const uint64_t total_cells = (uint64_t)kc * kB - (sc ? 1 : 0);
     const double avg_density = (double)a.N / (double)(a.ncells ? a.ncells : 1);
 
     for (;;) {
@@ -370,29 +505,7 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
         const int R = a.R;
         const float *dqc = a.dqc + (size_t)q * a.mc * kc;
         const float qn0 = a.qn[2 * q], qn1 = a.qn[2 * q + 1], qs = a.qsum[q];
-
-        // (1) sorted coarse lists (sort_id/nth_element_id with M = kc;
-        //     multi_query.h:114-128, sc_query.h:98-106, query.h:230-234):
-        //     key | centroid id, equal keys by id.
-        for (int h = tid; h < kcP; h += NT) {
-            if (h < kc) {
-                float ka = __fadd_rn(imi ? qn0 : qs, dqc[h]);
-                S.LA[h] = ((uint64_t)f2o(ka) << 32) | (uint32_t)h;
-                if (imi) {
-                    float kb = __fadd_rn(qn1, dqc[kc + h]);
-                    S.LB[h] = ((uint64_t)f2o(kb) << 32) | (uint32_t)h;
-                }
-            } else {
-                S.LA[h] = ~0ull;
-                if (imi) S.LB[h] = ~0ull;
-            }
-        }
         for (int i = tid; i < mp * kp; i += NT) S.lut[i] = a.dqr[(size_t)q * mp * kp + i];
-        if (tid == 0) st.err = 0;
-        __syncthreads();
-        bitonic_sort64(S.LA, kcP);
-        if (imi) bitonic_sort64(S.LB, kcP);
-        Lists L{S.LA, S.LB, kc, kB, ivf};
 
         // IMI and SC test the rules before each pop (multi_query.h:151,
         // sc_query.h:130); IVFADC pops first and tests after
@@ -404,250 +517,315 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
             needT = ~0ull;
             needW = 1;
         }
+        const double c0 = (T > 0 ? (double)T : 1.0) / (avg_density > 1e-9 ? avg_density : 1e-9);
+        int M = next_pow2(4 * (int)sqrt(c0) + 1);
+        if (M < 128) M = 128;
+        if (M > SBCAP / 2) M = SBCAP / 2;
 
-        PHASE_MARK(0);  // lists sorted
-        // (2) rounds of staircase enumeration
-        for (int h = tid; h < kc; h += NT) S.rowp[h] = (sc && h == 0) ? 1 : 0;
         uint64_t Ssum = 0, Ncell = 0, NEc = 0;  // totals over enumerated cells
-        uint64_t S0 = 0, N0 = 0, NE0 = 0;
+        uint64_t S0 = 0, N0 = 0, NE0 = 0;       // totals before the last round
         int nrec = 0, r0 = 0;
         bool trig = false;
-        uint32_t tau_prev = 0;
-        const uint32_t lo_key = f2o(__fadd_rn(L.a(0), L.b(0)));
-        const uint32_t hi_key = f2o(__fadd_rn(L.a(kc - 1), L.b(kB - 1)));
-        uint64_t target = 0;
-        {
-            double t0 = (T > 0 ? (double)T : 1.0) / (avg_density > 1e-9 ? avg_density : 1e-9);
-            target = (uint64_t)(t0 * 0.75) + 64;
-            if (sc) target += 1;
-        }
-        __syncthreads();
-        int round = 0;
-        if (!nothing) {
-            for (; round < MAX_ROUNDS; round++) {
-                uint64_t grid_cells = (uint64_t)kc * kB;
-                if (target > grid_cells) target = grid_cells;
-                if (!sc && needW < target) {
-                    // the w rule caps popped cells: never enumerate past w
-                    uint64_t tw = needW;
-                    if (tw < Ncell + 1) tw = Ncell + 1;
-                    if (tw < target) target = tw;
-                }
-                // bisection for tau: smallest key with staircase count >= target
-                uint32_t lo = round == 0 ? lo_key : tau_prev + 1, hi = hi_key;
-                uint64_t thi = target + target / 4 + 32;
-                if (a.phase_cycles && tid == 0) atomicAdd((unsigned long long *)&a.phase_cycles[8], 1ull);
-                if (lo > hi) lo = hi;
-                int it = 0;
-                while (lo < hi && it < 40) {
-                    uint32_t mid = lo + ((hi - lo) >> 1);
-                    uint64_t c = staircase_count(L, mid, red);
-                    if (a.phase_cycles && tid == 0) atomicAdd((unsigned long long *)&a.phase_cycles[9], 1ull);
-                    if (c >= target) {
-                        hi = mid;
-                        if (c <= thi) break;
-                    } else {
-                        lo = mid + 1;
+        Lists L;
+        for (int attempt = 0; attempt < 2; attempt++) {
+            const bool full = attempt == 1 || M >= kc;
+            // (1) coarse lists (sort_id/nth_element_id with M = kc;
+            //     multi_query.h:114-128, sc_query.h:98-106, query.h:230-234):
+            //     ordered key << 32 | centroid id; equal keys by id.
+            for (int h = tid; h < kcP; h += NT) {
+                if (h < kc) {
+                    float ka = __fadd_rn(imi ? qn0 : qs, dqc[h]);
+                    S.LA[h] = ((uint64_t)f2o(ka) << 32) | (uint32_t)h;
+                    if (imi) {
+                        float kb = __fadd_rn(qn1, dqc[kc + h]);
+                        S.LB[h] = ((uint64_t)f2o(kb) << 32) | (uint32_t)h;
                     }
-                    it++;
+                } else {
+                    S.LA[h] = ~0ull;
+                    if (imi) S.LB[h] = ~0ull;
                 }
-                const uint32_t tau = hi;
-                tau_prev = tau;
-                // row counts at tau and the new cells per row
-                uint32_t mycnt = 0;
-                const int per = (kc + NT - 1) / NT;
-                const int hb = tid * per;
-                for (int i = 0; i < per; i++) {
-                    int h = hb + i;
-                    if (h >= kc) break;
-                    int c = L.row_count(L.a(h), tau);
-                    int p0 = S.rowp[h];
-                    if (c < p0) c = p0;
-                    S.rowc[h] = (uint16_t)(c > 65535 ? 65535 : c);
-                    mycnt += (uint32_t)(c - p0);
+            }
+            if (tid == 0) {
+                st.err = 0;
+                st.kA = kc;
+                st.kB = kBfull;
+                st.nextA = 0xffffffffu;
+                st.nextB = 0xffffffffu;
+            }
+            __syncthreads();
+            bool done_a = false, done_b = !imi;
+            if (!full) {
+                int ca = select_prefix(S.LA, kc, M, sb, hist, red, st, &st.nextA);
+                if (ca > 0) {
+                    done_a = true;
+                    if (tid == 0) st.kA = ca;
                 }
-                uint64_t tot_new;
-                uint64_t ex = block_exscan(mycnt, red, tot_new);
-                {
-                    uint32_t run = (uint32_t)ex;
-                    for (int i = 0; i < per; i++) {
-                        int h = hb + i;
-                        if (h >= kc) break;
-                        S.rowpre[h] = run;
-                        run += (uint32_t)(S.rowc[h] - S.rowp[h]);
+                if (imi) {
+                    int cb = select_prefix(S.LB, kc, M, sb, hist, red, st, &st.nextB);
+                    if (cb > 0) {
+                        done_b = true;
+                        if (tid == 0) st.kB = cb;
                     }
-                    if (tid == 0) S.rowpre[kc] = (uint32_t)tot_new;
                 }
-                if ((uint64_t)nrec + tot_new > (uint64_t)cap) {
+                __syncthreads();
+                if (!done_a || !done_b) {
+                    // a prefix beyond SBCAP: sort everything instead
+                    done_a = done_b = false;
+                    for (int h = tid; h < kcP; h += NT) {
+                        if (h < kc) {
+                            S.LA[h] = ((uint64_t)f2o(__fadd_rn(imi ? qn0 : qs, dqc[h])) << 32) | (uint32_t)h;
+                            if (imi) S.LB[h] = ((uint64_t)f2o(__fadd_rn(qn1, dqc[kc + h])) << 32) | (uint32_t)h;
+                        }
+                    }
                     if (tid == 0) {
-                        st.err = 1;
-                        atomicOr(a.status, ST_CELL_BUDGET);
+                        st.kA = kc;
+                        st.kB = kBfull;
+                        st.nextA = st.nextB = 0xffffffffu;
                     }
                     __syncthreads();
-                    break;
                 }
-                __syncthreads();
-                const int nnew = (int)tot_new;
-                if (a.phase_cycles && tid == 0) atomicAdd((unsigned long long *)&a.phase_cycles[10], (unsigned long long)nnew);
-                uint64_t ls = 0, lne = 0, dummy = 0;
-                for (int idx = tid; idx < nnew; idx += NT) {
-                    // row of idx: last h with rowpre[h] <= idx
-                    int lo2 = 0, hi2 = kc - 1;
-                    while (lo2 < hi2) {
-                        int mid = (lo2 + hi2 + 1) >> 1;
-                        if (S.rowpre[mid] <= (uint32_t)idx) lo2 = mid;
-                        else hi2 = mid - 1;
-                    }
-                    int h1 = lo2;
-                    int h2 = S.rowp[h1] + (idx - (int)S.rowpre[h1]);
-                    float key = __fadd_rn(L.a(h1), L.b(h2));
-                    uint32_t rank = ((uint32_t)h1 << 16) | (uint32_t)h2;
-                    uint32_t cell = cell_of(L, ivf, rank);
-                    uint32_t c = a.off[cell + 1] - a.off[cell];
-                    if (sc && cell == 0) c = 0;  // sc_query.h:138-140
-                    rec_key[nrec + idx] = f2o(key);
-                    rec_rank[nrec + idx] = rank;
-                    rec_cnt[nrec + idx] = c;
-                    ls += c;
-                    lne += (c > 0);
-                }
-                block_sum3(ls, lne, dummy, red);
-                S0 = Ssum;
-                N0 = Ncell;
-                NE0 = NEc;
-                r0 = nrec;
-                nrec += nnew;
-                Ssum += ls;
-                Ncell += (uint64_t)nnew;
-                NEc += lne;
-                for (int h = tid; h < kc; h += NT) S.rowp[h] = S.rowc[h];
-                __syncthreads();
-                uint64_t wcnt = sc ? NEc : Ncell;
-                trig = (Ssum >= needT) || (wcnt >= needW);
-                if (trig || Ncell >= total_cells || tau >= hi_key) break;
-                // next target from the density seen so far
-                double dens = Ncell ? (double)Ssum / (double)Ncell : avg_density;
-                if (dens < 1e-6) dens = avg_density > 1e-6 ? avg_density : 1e-6;
-                double need_cells = (double)(needT - Ssum) / dens;
-                uint64_t grow = (uint64_t)(need_cells * 1.25) + 64;
-                uint64_t minimum = Ncell / 4 + 64;
-                target = Ncell + (sc ? 1 : 0) + (grow > minimum ? grow : minimum);
             }
-            if (round >= MAX_ROUNDS && tid == 0) {
-                st.err = 1;
-                atomicOr(a.status, ST_ITER_CAP);
-            }
-        }
-        __syncthreads();
-        const bool qerr = st.err != 0;
-
-        PHASE_MARK(1);  // staircase rounds
-        // (3) the cut within the last round
-        if (!nothing && !qerr && trig) {
-            uint32_t lo = 0xffffffffu, hi = 0;
-            for (int r = r0 + tid; r < nrec; r += NT) {
-                uint32_t k = rec_key[r];
-                lo = min(lo, k);
-                hi = max(hi, k);
-            }
-            // block min / max through the reduction buffer
-            uint64_t mn = lo, mx = hi;
-            {
-                int lane = tid & 31, wid = tid >> 5;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    mn = min(mn, (uint64_t)__shfl_xor_sync(0xffffffffu, mn, o));
-                    mx = max(mx, (uint64_t)__shfl_xor_sync(0xffffffffu, mx, o));
-                }
-                __syncthreads();
-                if (lane == 0) {
-                    red[wid] = mn;
-                    red[NWARP + wid] = mx;
-                }
-                __syncthreads();
-                mn = 0xffffffffu;
-                mx = 0;
-                for (int i = 0; i < NWARP; i++) {
-                    mn = min(mn, red[i]);
-                    mx = max(mx, red[NWARP + i]);
-                }
-                __syncthreads();
-            }
-            uint32_t klo = (uint32_t)mn, khi = (uint32_t)mx;
-            uint32_t kap = 0xffffffffu;
-            uint64_t below;
-            if (Ssum >= needT)
-                kap = radix_cut(rec_key, rec_cnt, r0, nrec, klo, khi, S0, needT, 0, hist, red, &below,
-                                &st.s_bin, &st.s_acc);
-            uint64_t wcnt = sc ? NEc : Ncell;
-            if (wcnt >= needW) {
-                uint32_t kw = radix_cut(rec_key, rec_cnt, r0, nrec, klo, khi, sc ? NE0 : N0, needW,
-                                        sc ? 2 : 1, hist, red, &below, &st.s_bin, &st.s_acc);
-                if (kw < kap) kap = kw;
-            }
-            // totals strictly below kappa, and the ties at kappa
-            uint64_t ls = 0, ln = 0, lne = 0;
-            if (tid == 0) st.nties = 0;
+            if (!done_a) bitonic_sort64(S.LA, kcP);
+            if (imi && !done_b) bitonic_sort64(S.LB, kcP);
             __syncthreads();
-            for (int r = r0 + tid; r < nrec; r += NT) {
-                uint32_t k = rec_key[r];
-                if (k < kap) {
-                    uint32_t c = rec_cnt[r];
-                    ls += c;
-                    ln += 1;
-                    lne += (c > 0);
-                } else if (k == kap) {
-                    int slot = atomicAdd(&st.nties, 1);
-                    if (slot < TIECAP) ties[slot] = ((uint64_t)rec_rank[r] << 32) | rec_cnt[r];
+            L.LA = S.LA;
+            L.LB = S.LB;
+            L.kA = st.kA;
+            L.kB = sc ? st.kA : st.kB;
+            L.kc = kc;
+            L.ivf = ivf;
+            const uint32_t nextB = sc ? st.nextA : st.nextB;
+            // every cell outside the prefix grid has a key >= bound
+            uint32_t bound = 0xffffffffu;
+            if (st.nextA != 0xffffffffu) bound = min(bound, f2o(__fadd_rn(o2f(st.nextA), L.b(0))));
+            if (!ivf && nextB != 0xffffffffu) bound = min(bound, f2o(__fadd_rn(L.a(0), o2f(nextB))));
+            const bool whole = L.kA == kc && (ivf || L.kB == kc);
+            PHASE_MARK(0);  // lists
+
+            // (2) rounds of staircase enumeration over the prefix grid
+            for (int h = tid; h < L.kA; h += NT) S.rowp[h] = (sc && h == 0) ? 1 : 0;
+            Ssum = Ncell = NEc = 0;
+            S0 = N0 = NE0 = 0;
+            nrec = 0;
+            r0 = 0;
+            trig = false;
+            const uint64_t grid_cells = (uint64_t)L.kA * L.kB;
+            const uint64_t total_cells = grid_cells - (sc ? 1 : 0);
+            uint32_t tau_prev = 0;
+            const uint32_t lo_key = f2o(__fadd_rn(L.a(0), L.b(0)));
+            const uint32_t hi_key = f2o(__fadd_rn(L.a(L.kA - 1), L.b(L.kB - 1)));
+            uint64_t target = (uint64_t)(c0 / 8.0);
+            if (target < 64) target = 64;
+            if (target > 1024) target = 1024;
+            if (sc) target += 1;
+            __syncthreads();
+            int round = 0;
+            if (!nothing) {
+                for (; round < MAX_ROUNDS; round++) {
+                    if (target > grid_cells) target = grid_cells;
+                    if (!sc && needW < target) {
+                        // the w rule caps popped cells: never enumerate past w
+                        uint64_t tw = needW;
+                        if (tw < Ncell + 1) tw = Ncell + 1;
+                        if (tw < target) target = tw;
+                    }
+                    // bisection for tau: smallest key with staircase count >= target
+                    uint32_t lo = round == 0 ? lo_key : tau_prev + 1, hi = hi_key;
+                    uint64_t thi = target + target / 4 + 32;
+                    COUNT(8, 1);
+                    if (lo > hi) lo = hi;
+                    int it = 0;
+                    while (lo < hi && it < 40) {
+                        uint32_t mid = lo + ((hi - lo) >> 1);
+                        uint64_t c = staircase_count(L, mid, red);
+                        COUNT(9, 1);
+                        if (c >= target) {
+                            hi = mid;
+                            if (c <= thi) break;
+                        } else {
+                            lo = mid + 1;
+                        }
+                        it++;
+                    }
+                    const uint32_t tau = hi;
+                    tau_prev = tau;
+                    // row counts at tau and the new cells per row
+                    uint32_t mycnt = 0;
+                    const int per = (L.kA + NT - 1) / NT;
+                    const int hb = tid * per;
+                    for (int i = 0; i < per; i++) {
+                        int h = hb + i;
+                        if (h >= L.kA) break;
+                        int c = L.row_count(L.a(h), tau);
+                        int p0 = S.rowp[h];
+                        if (c < p0) c = p0;
+                        S.rowc[h] = (uint16_t)c;
+                        mycnt += (uint32_t)(c - p0);
+                    }
+                    uint64_t tot_new;
+                    uint64_t ex = block_exscan(mycnt, red, tot_new);
+                    {
+                        uint32_t run = (uint32_t)ex;
+                        for (int i = 0; i < per; i++) {
+                            int h = hb + i;
+                            if (h >= L.kA) break;
+                            S.rowpre[h] = run;
+                            run += (uint32_t)(S.rowc[h] - S.rowp[h]);
+                        }
+                    }
+                    if ((uint64_t)nrec + tot_new > (uint64_t)cap) {
+                        if (tid == 0) {
+                            st.err = 1;
+                            atomicOr(a.status, ST_CELL_BUDGET);
+                        }
+                        __syncthreads();
+                        break;
+                    }
+                    __syncthreads();
+                    const int nnew = (int)tot_new;
+                    COUNT(10, nnew);
+                    uint64_t ls = 0, lne = 0, dummy = 0;
+                    int h1 = 0;
+                    for (int idx = tid; idx < nnew; idx += NT) {
+                        // row of idx: last h with rowpre[h] <= idx (rows only grow)
+                        int lo2 = h1, hi2 = L.kA - 1;
+                        while (lo2 < hi2) {
+                            int mid = (lo2 + hi2 + 1) >> 1;
+                            if (S.rowpre[mid] <= (uint32_t)idx) lo2 = mid;
+                            else hi2 = mid - 1;
+                        }
+                        h1 = lo2;
+                        int h2 = S.rowp[h1] + (idx - (int)S.rowpre[h1]);
+                        float key = __fadd_rn(L.a(h1), L.b(h2));
+                        uint32_t rank = ((uint32_t)h1 << 16) | (uint32_t)h2;
+                        uint32_t cell = cell_of(L, rank);
+                        uint32_t c = a.off[cell + 1] - a.off[cell];
+                        if (sc && cell == 0) c = 0;  // sc_query.h:138-140
+                        rec_key[nrec + idx] = f2o(key);
+                        rec_rank[nrec + idx] = rank;
+                        rec_cnt[nrec + idx] = c;
+                        ls += c;
+                        lne += (c > 0);
+                    }
+                    block_sum3(ls, lne, dummy, red);
+                    S0 = Ssum;
+                    N0 = Ncell;
+                    NE0 = NEc;
+                    r0 = nrec;
+                    nrec += nnew;
+                    Ssum += ls;
+                    Ncell += (uint64_t)nnew;
+                    NEc += lne;
+                    for (int h = tid; h < L.kA; h += NT) S.rowp[h] = S.rowc[h];
+                    __syncthreads();
+                    uint64_t wcnt = sc ? NEc : Ncell;
+                    trig = (Ssum >= needT) || (wcnt >= needW);
+                    if (trig || Ncell >= total_cells || tau >= hi_key) break;
+                    // next target from the density seen so far
+                    double dens = Ncell ? (double)Ssum / (double)Ncell : avg_density;
+                    if (dens < 1e-6) dens = avg_density > 1e-6 ? avg_density : 1e-6;
+                    double need_cells = (double)(needT - Ssum) / dens;
+                    uint64_t grow = (uint64_t)(need_cells * 1.25) + 64;
+                    uint64_t minimum = Ncell / 4 + 64;
+                    target = Ncell + (sc ? 1 : 0) + (grow > minimum ? grow : minimum);
                 }
-            }
-            block_sum3(ls, ln, lne, red);
-            if (tid == 0) {
-                uint64_t s = S0 + ls, n = N0 + ln, ne = NE0 + lne;
-                int nt = st.nties;
-                if (nt > TIECAP) {
+                if (round >= MAX_ROUNDS && tid == 0) {
                     st.err = 1;
-                    atomicOr(a.status, ST_TIE_OVERFLOW);
-                    nt = TIECAP;
+                    atomicOr(a.status, ST_ITER_CAP);
                 }
-                // ties in rank order (an exact priority queue's order)
-                for (int i = 1; i < nt; i++) {
-                    uint64_t v = ties[i];
-                    int j = i - 1;
-                    while (j >= 0 && ties[j] > v) {
-                        ties[j + 1] = ties[j];
-                        j--;
-                    }
-                    ties[j + 1] = v;
-                }
-                uint32_t rc_ = 0;
-                for (int i = 0; i < nt; i++) {
-                    uint32_t c = (uint32_t)ties[i];
-                    s += c;
-                    n += 1;
-                    ne += (c > 0);
-                    rc_ = (uint32_t)(ties[i] >> 32);
-                    if (s >= needT || (sc ? ne : n) >= needW) break;
-                }
-                st.kappa = kap;
-                st.rank_cut = rc_;
-                st.take_all = 0;
-                st.sumv = s;
-                st.nv = n;
-                st.nev = ne;
             }
             __syncthreads();
-        } else if (tid == 0) {
-            st.kappa = 0xffffffffu;
-            st.rank_cut = 0xffffffffu;
-            st.take_all = 1;
-            st.sumv = nothing ? 0 : Ssum;
-            st.nv = nothing ? 0 : Ncell;
-            st.nev = nothing ? 0 : NEc;
-        }
-        __syncthreads();
+            const bool qerr = st.err != 0;
+            PHASE_MARK(1);  // staircase rounds
 
-        PHASE_MARK(2);  // cut
+            // (3) the cut within the last round
+            if (!nothing && !qerr && trig) {
+                uint64_t mn = 0xffffffffull, mx = 0;
+                for (int r = r0 + tid; r < nrec; r += NT) {
+                    uint64_t k = rec_key[r];
+                    mn = k < mn ? k : mn;
+                    mx = k > mx ? k : mx;
+                }
+                block_minmax(mn, mx, red);
+                uint32_t klo = (uint32_t)mn, khi = (uint32_t)mx;
+                uint32_t kap = 0xffffffffu;
+                if (Ssum >= needT)
+                    kap = radix_cut(rec_key, rec_cnt, r0, nrec, klo, khi, S0, needT, 0, hist, red, st);
+                uint64_t wcnt = sc ? NEc : Ncell;
+                if (wcnt >= needW) {
+                    uint32_t kw = radix_cut(rec_key, rec_cnt, r0, nrec, klo, khi, sc ? NE0 : N0, needW, sc ? 2 : 1,
+                                            hist, red, st);
+                    if (kw < kap) kap = kw;
+                }
+                // totals strictly below kappa, and the ties at kappa
+                uint64_t ls = 0, ln = 0, lne = 0;
+                if (tid == 0) st.nties = 0;
+                __syncthreads();
+                for (int r = r0 + tid; r < nrec; r += NT) {
+                    uint32_t k = rec_key[r];
+                    if (k < kap) {
+                        uint32_t c = rec_cnt[r];
+                        ls += c;
+                        ln += 1;
+                        lne += (c > 0);
+                    } else if (k == kap) {
+                        int slot = atomicAdd(&st.nties, 1);
+                        if (slot < TIECAP) ties[slot] = ((uint64_t)rec_rank[r] << 32) | rec_cnt[r];
+                    }
+                }
+                block_sum3(ls, ln, lne, red);
+                if (tid == 0) {
+                    uint64_t s = S0 + ls, n = N0 + ln, ne = NE0 + lne;
+                    int nt = st.nties;
+                    if (nt > TIECAP) {
+                        st.err = 1;
+                        atomicOr(a.status, ST_TIE_OVERFLOW);
+                        nt = TIECAP;
+                    }
+                    // ties in rank order (an exact priority queue's order)
+                    for (int i = 1; i < nt; i++) {
+                        uint64_t v = ties[i];
+                        int j = i - 1;
+                        while (j >= 0 && ties[j] > v) {
+                            ties[j + 1] = ties[j];
+                            j--;
+                        }
+                        ties[j + 1] = v;
+                    }
+                    uint32_t rc_ = 0;
+                    for (int i = 0; i < nt; i++) {
+                        uint32_t c = (uint32_t)ties[i];
+                        s += c;
+                        n += 1;
+                        ne += (c > 0);
+                        rc_ = (uint32_t)(ties[i] >> 32);
+                        if (s >= needT || (sc ? ne : n) >= needW) break;
+                    }
+                    st.kappa = kap;
+                    st.rank_cut = rc_;
+                    st.take_all = 0;
+                    st.sumv = s;
+                    st.nv = n;
+                    st.nev = ne;
+                }
+                __syncthreads();
+            } else if (tid == 0) {
+                st.kappa = 0xffffffffu;
+                st.rank_cut = 0xffffffffu;
+                st.take_all = 1;
+                st.sumv = nothing ? 0 : Ssum;
+                st.nv = nothing ? 0 : Ncell;
+                st.nev = nothing ? 0 : NEc;
+            }
+            __syncthreads();
+            PHASE_MARK(2);  // cut
+            // the prefix grid holds every cell with a key <= the cut
+            const bool valid = nothing || st.err || (trig ? st.kappa < bound : whole);
+            if (valid) break;
+            COUNT(11, 1);
+            __syncthreads();
+        }
+
         // (4) visited non-empty cells -> (cell, prefix) list
         int nvis = 0;
         if (!nothing && !st.err) {
@@ -670,7 +848,7 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
                 uint64_t ex = block_exscan(v, red, tot);
                 if (f) {
                     uint64_t p = pos + (ex >> 40);
-                    vis_cell[p] = cell_of(L, ivf, rank);
+                    vis_cell[p] = cell_of(L, rank);
                     vis_pre[p] = (uint32_t)(runc + (ex & 0xffffffffffull));
                 }
                 pos += tot >> 40;
@@ -687,8 +865,8 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
         nvis = st.nvis;
         const bool qerr2 = st.err != 0;
         const uint32_t Svis = (nvis > 0) ? (uint32_t)st.sumv : 0u;
-
         PHASE_MARK(3);  // compaction
+
         // (5) ADC scan with the fused top-R
         if (tid == 0) {
             st.ncur = 0;
@@ -738,21 +916,11 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
                     }
                     __syncthreads();
                 }
-                // make room for this round's candidates
-                if (st.ncur + st.npend + NT * CPT > MERGE_N) {
-                    if (a.phase_cycles && tid == 0) atomicAdd((unsigned long long *)&a.phase_cycles[7], 1ull);
-                    int n = st.ncur + st.npend;
-                    int np2 = next_pow2(n);
-                    for (int i = n + tid; i < np2; i += NT) topk[i] = ~0ull;
-                    __syncthreads();
-                    bitonic_sort64(topk, np2);
-                    if (tid == 0) {
-                        int keep = n < R ? n : R;
-                        st.ncur = keep;
-                        st.npend = 0;
-                        st.thr = keep == R ? topk[R - 1] : ~0ull;
-                    }
-                    __syncthreads();
+                // merge the pending candidates when the top list is not yet
+                // full, or when this round might not fit
+                if ((st.npend > 0 && st.ncur < R) || st.npend + NT * CPT > PCAP) {
+                    COUNT(7, 1);
+                    merge_topk(top, pend, tmpk, R, st);
                 }
                 const uint32_t wend = st.wend;
                 const uint64_t thr = st.thr;
@@ -762,18 +930,28 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
                 float dd[CPT];
                 uint32_t h34[CPT];
                 CodeWords<MPC> cw_[CPT];
+                int ci = 0;
 #pragma unroll
                 for (int j = 0; j < CPT; j++) {
                     const uint32_t flat = flat0 + tid + j * NT;
                     pos[j] = 0xffffffffu;
                     if (flat < wend) {
-                        int lo2 = 0, hi2 = cn - 1;
-                        while (lo2 < hi2) {
-                            int mid = (lo2 + hi2 + 1) >> 1;
-                            if (win[mid].pre <= flat) lo2 = mid;
-                            else hi2 = mid - 1;
+                        // window cell containing flat: advance from the last one
+                        int steps = 0;
+                        while (ci + 1 < cn && win[ci + 1].pre <= flat && steps < 4) {
+                            ci++;
+                            steps++;
                         }
-                        const CellWin cw = win[lo2];
+                        if (ci + 1 < cn && win[ci + 1].pre <= flat) {
+                            int lo2 = ci, hi2 = cn - 1;
+                            while (lo2 < hi2) {
+                                int mid = (lo2 + hi2 + 1) >> 1;
+                                if (win[mid].pre <= flat) lo2 = mid;
+                                else hi2 = mid - 1;
+                            }
+                            ci = lo2;
+                        }
+                        const CellWin cw = win[ci];
                         pos[j] = cw.start + (flat - cw.pre);
                         dd[j] = cw.d0;
                         h34[j] = cw.h34;
@@ -816,7 +994,7 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
                         uint64_t e = ((uint64_t)du << 32) | (uint32_t)a.pid[pos[j]];
                         if (e < thr) {
                             int slot = atomicAdd(&st.npend, 1);
-                            topk[st.ncur + slot] = e;
+                            pend[slot] = e;
                         }
                     }
                 }
@@ -831,23 +1009,17 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
                 flat0 += step;
             }
             PHASE_MARK(4);  // scan rounds
-            // final merge
-            int n = st.ncur + st.npend;
-            int np2 = next_pow2(n > 1 ? n : 2);
-            for (int i = n + tid; i < np2; i += NT) topk[i] = ~0ull;
-            __syncthreads();
-            bitonic_sort64(topk, np2);
+            if (st.npend > 0) merge_topk(top, pend, tmpk, R, st);
         }
         __syncthreads();
         PHASE_MARK(5);  // final merge
-        // (6) outputs
+        // (6) outputs: the top list is sorted by (distance, id)
         {
-            int n = (qerr2 || nvis == 0) ? 0 : st.ncur + st.npend;
-            int keep = n < R ? n : R;
+            int keep = (qerr2 || nvis == 0) ? 0 : st.ncur;
             for (int j = tid; j < R; j += NT) {
                 size_t o = (size_t)q * R + j;
                 if (j < keep) {
-                    uint64_t e = topk[j];
+                    uint64_t e = top[j];
                     a.out_ids[o] = (int)(uint32_t)e;
                     a.out_d[o] = o2f((uint32_t)(e >> 32));
                 } else {

@@ -171,3 +171,29 @@ def test_fast_form_tolerance(scg, oracle_mod, mode, mc, kc):
         assert np.allclose(d[i, :m], od[i, :m], rtol=1e-5, atol=1e-2)
         assert len(set(ids[i, :m].tolist()) & set(oi[i, :m].tolist())) >= m - 2
     g.close()
+
+
+@pytest.mark.parametrize("mode,mc,kc,Ts", [(O.IMI, 2, 512, (50, 500, 3000)), (O.SC, 1, 1024, (200, 2000))])
+def test_sorted_prefix_and_fallback(scg, oracle_mod, mode, mc, kc, Ts):
+    """Coarse lists larger than the sorted prefix: the selection uses the
+    prefix when the cut stays inside it and sorts everything otherwise; both
+    must equal the exact order."""
+    D, mp, kp = 64, 8, 64
+    mix = W.Mixture(D, 16, 20.0, "u8", seed=41 + mode)
+    X = mix.sample(100000, seed=42)
+    Q = mix.sample(12, seed=43)
+    cq, pq = W.train_codebooks(X[:6000], mc, kc, mp, kp, 2, seed=44)
+    g = scg.Index(0)
+    g.load_codebooks(cq, kc, mc, pq, kp, mp, D)
+    if mode == O.SC:
+        cid, codes = g.sc_encode(X, 2)
+        L, pid, co, _ = O.distribution(O.SC, kc, 1, 2, cid, codes)
+    else:
+        cid, codes = g.encode(X)
+        L, pid, co, _ = O.distribution(mode, kc, mc, 0, cid, codes)
+    g.load_csr(L, pid, co)
+    g.precompute()
+    ix = O.Index(D, mc, kc, mp, kp, cq, pq, L, pid, co)
+    for T in Ts:
+        check_against_oracle(ix, g, mode, Q, 30, 1 << 20, T)
+    g.close()
