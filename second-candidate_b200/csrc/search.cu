@@ -40,12 +40,12 @@ namespace {
 
 constexpr int NT = 256;
 constexpr int NWARP = NT / 32;
-constexpr int CPT = 4;          // candidates per thread per scan round
+constexpr int CPT = 8;          // candidates per thread per scan round
 constexpr int HBITS = 11;
 constexpr int HBINS = 1 << HBITS;
 constexpr int TIECAP = 64;
 constexpr int RMAX = 1024;      // largest R
-constexpr int PCAP = 2048;      // pending top-R candidates
+constexpr int PCAP = 4096;      // pending top-R candidates (>= 2 rounds)
 constexpr int SBCAP = 2048;     // sorted coarse prefix capacity
 constexpr int MAX_ROUNDS = 64;
 
@@ -74,7 +74,8 @@ struct Smem {
 __host__ __device__ inline size_t union_bytes(int kc) {
     size_t trav = (size_t)HBINS * 4 + (size_t)TIECAP * 8;
     size_t lists = (size_t)SBCAP * 8;
-    size_t scan = (size_t)(RMAX + PCAP + RMAX) * 8 + (size_t)NT * sizeof(CellWin);
+    size_t scan = (size_t)(RMAX + PCAP + RMAX) * 8 + (size_t)NT * sizeof(CellWin) + (size_t)HBINS * 4 +
+                  (size_t)TIECAP * 8;
     size_t m = trav > scan ? trav : scan;
     (void)kc;
     return m > lists ? m : lists;
@@ -432,35 +433,113 @@ struct CodeWords<0> {
             atomicAdd((unsigned long long *)&a.phase_cycles[(i)], (unsigned long long)(v));        \
     } while (0)
 
-// Merges the pending candidates into the sorted top list: sorts the pending
-// part, then each output k < min(R, ncur + npend) is taken by a merge-path
-// search over the two sorted runs.
-__device__ void merge_topk(uint64_t *top, uint64_t *pend, uint64_t *tmp, int R, QState &st) {
+// Keeps the R smallest of top[0..ncur) and the pending entries.  Pending
+// entries hold (distance, CSR position); they become (distance, id) here,
+// where the id loads of a whole buffer are issued together.  A radix select
+// over the distance words finds the R-th smallest distance v; every entry
+// below v is kept and the entries equal to v are taken in id order.  The top
+// list stays unsorted (the output step sorts it); st.thr becomes the R-th
+// smallest (distance, id) once R entries exist.
+__device__ void merge_topk(uint64_t *top, uint64_t *pend, uint64_t *tmp, uint32_t *hist, uint64_t *ties, int R,
+                           const int *pid, uint64_t *red, QState &st, int *status) {
     const int tid = threadIdx.x;
     const int na = st.ncur, nb = st.npend;
-    const int p2 = next_pow2(nb > 1 ? nb : 2);
-    for (int i = nb + tid; i < p2; i += NT) pend[i] = ~0ull;
+    for (int i = tid; i < nb; i += NT) {
+        uint64_t e = pend[i];
+        pend[i] = (e & 0xffffffff00000000ull) | (uint32_t)__ldg(pid + (uint32_t)e);
+    }
     __syncthreads();
-    bitonic_sort64(pend, p2);
-    const int nout = na + nb < R ? na + nb : R;
-    for (int k = tid; k < nout; k += NT) {
-        int lo = k - nb > 0 ? k - nb : 0, hi = k < na ? k : na;
-        while (lo < hi) {
-            int mid = (lo + hi) >> 1;
-            if (top[mid] < pend[k - 1 - mid]) lo = mid + 1;
-            else hi = mid;
+    const int n = na + nb;
+    if (n <= R) {
+        for (int i = tid; i < nb; i += NT) top[na + i] = pend[i];
+        __syncthreads();
+        if (tid == 0) {
+            st.ncur = n;
+            st.npend = 0;
+            st.thr = ~0ull;
         }
-        int i = lo, j = k - lo;
-        uint64_t x = i < na ? top[i] : ~0ull, y = j < nb ? pend[j] : ~0ull;
-        tmp[k] = x < y ? x : y;
+        __syncthreads();
+        return;
+    }
+    // radix select (11 + 11 + 10 bits) of the R-th smallest distance word
+    uint32_t prefix = 0;
+    uint64_t need = (uint64_t)R;
+    const int shifts[3] = {21, 10, 0}, widths[3] = {11, 11, 10};
+    for (int p = 0; p < 3; p++) {
+        const int sh = shifts[p], bits = widths[p], nbins = 1 << bits, hs = sh + bits;
+        for (int i = tid; i < nbins; i += NT) hist[i] = 0;
+        __syncthreads();
+        for (int i = tid; i < n; i += NT) {
+            uint32_t v = (uint32_t)((i < na ? top[i] : pend[i - na]) >> 32);
+            if (hs < 32 && (v >> hs) != (prefix >> hs)) continue;
+            atomicAdd(&hist[(v >> sh) & (nbins - 1)], 1u);
+        }
+        __syncthreads();
+        const int per = (nbins + NT - 1) / NT;
+        const int b0 = tid * per;
+        uint64_t mine = 0;
+        for (int i = 0; i < per; i++)
+            if (b0 + i < nbins) mine += hist[b0 + i];
+        uint64_t tot;
+        uint64_t run = block_exscan(mine, red, tot);
+        for (int i = 0; i < per; i++) {
+            int bb = b0 + i;
+            if (bb >= nbins) break;
+            uint64_t nxt = run + hist[bb];
+            if (run < need && nxt >= need) {
+                st.s_bin = (uint32_t)bb;
+                st.s_acc = run;
+            }
+            run = nxt;
+        }
+        __syncthreads();
+        prefix |= st.s_bin << sh;
+        need -= st.s_acc;
+        __syncthreads();
+    }
+    const uint32_t v = prefix;
+    // keep everything below v; gather the entries equal to v
+    uint64_t mine = 0;
+    for (int i = tid; i < n; i += NT) mine += ((uint32_t)((i < na ? top[i] : pend[i - na]) >> 32) < v);
+    uint64_t total;
+    uint64_t pos = block_exscan(mine, red, total);
+    if (tid == 0) st.nties = 0;
+    __syncthreads();
+    for (int i = tid; i < n; i += NT) {
+        uint64_t e = i < na ? top[i] : pend[i - na];
+        uint32_t hv = (uint32_t)(e >> 32);
+        if (hv < v) tmp[pos++] = e;
+        else if (hv == v) {
+            int slot = atomicAdd(&st.nties, 1);
+            if (slot < TIECAP) ties[slot] = e;
+        }
     }
     __syncthreads();
-    for (int k = tid; k < nout; k += NT) top[k] = tmp[k];
     if (tid == 0) {
-        st.ncur = nout;
+        // `need` entries equal to v complete the R: the smallest ids
+        int nt = st.nties < TIECAP ? st.nties : TIECAP;
+        for (int i = 1; i < nt; i++) {
+            uint64_t x = ties[i];
+            int j = i - 1;
+            while (j >= 0 && ties[j] > x) {
+                ties[j + 1] = ties[j];
+                j--;
+            }
+            ties[j + 1] = x;
+        }
+        int take = (int)need;
+        if (take > nt) {
+            // more equal distances at the R-th place than the tie buffer holds
+            atomicOr(status, ST_TIE_OVERFLOW);
+            take = nt;
+        }
+        for (int i = 0; i < take; i++) tmp[total + i] = ties[i];
+        st.ncur = (int)total + take;
         st.npend = 0;
-        st.thr = nout == R ? tmp[R - 1] : ~0ull;
+        st.thr = take > 0 ? ties[take - 1] : ~0ull;
     }
+    __syncthreads();
+    for (int i = tid; i < st.ncur; i += NT) top[i] = tmp[i];
     __syncthreads();
 }
 
@@ -491,6 +570,8 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
     uint64_t *pend = top + RMAX;
     uint64_t *tmpk = pend + PCAP;
     CellWin *win = (CellWin *)(tmpk + RMAX);
+    uint32_t *hist2 = (uint32_t *)(win + NT);          // merge radix histogram
+    uint64_t *ties2 = (uint64_t *)(hist2 + HBINS);      // merge ties
     const int bsI = kp * mp / a.mc;  // dot_cr block of one coarse centroid
     const double avg_density = (double)a.N / (double)(a.ncells ? a.ncells : 1);
 
@@ -918,9 +999,9 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
                 }
                 // merge the pending candidates when the top list is not yet
                 // full, or when this round might not fit
-                if ((st.npend > 0 && st.ncur < R) || st.npend + NT * CPT > PCAP) {
+                if ((st.npend > 0 && st.ncur < R) || st.npend > R || st.npend + NT * CPT > PCAP) {
                     COUNT(7, 1);
-                    merge_topk(top, pend, tmpk, R, st);
+                    merge_topk(top, pend, tmpk, hist2, ties2, R, a.pid, red, st, a.status);
                 }
                 const uint32_t wend = st.wend;
                 const uint64_t thr = st.thr;
@@ -989,13 +1070,20 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
                             d = __fadd_rn(d, __fadd_rn(S.lut[bc], __ldg(r1 + bc)));
                         }
                     }
-                    uint32_t du = f2o(d);
-                    if (du <= (uint32_t)(thr >> 32)) {
-                        uint64_t e = ((uint64_t)du << 32) | (uint32_t)a.pid[pos[j]];
-                        if (e < thr) {
-                            int slot = atomicAdd(&st.npend, 1);
-                            pend[slot] = e;
-                        }
+                    // below the threshold (distance, id): the id is only
+                    // needed when the distances are equal
+                    const uint32_t du = f2o(d), tu = (uint32_t)(thr >> 32);
+                    bool pass = du < tu;
+                    if (du == tu) pass = (uint32_t)a.pid[pos[j]] < (uint32_t)thr;
+                    // warp-aggregated append of (distance, position)
+                    const unsigned m = __ballot_sync(__activemask(), pass);
+                    if (pass) {
+                        const int lane = tid & 31;
+                        const int leader = __ffs(m) - 1;
+                        int base = 0;
+                        if (lane == leader) base = atomicAdd(&st.npend, __popc(m));
+                        base = __shfl_sync(m, base, leader);
+                        pend[base + __popc(m & ((1u << lane) - 1))] = ((uint64_t)du << 32) | pos[j];
                     }
                 }
                 uint32_t step = wend > flat0 ? wend - flat0 : 0u;
@@ -1009,13 +1097,19 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
                 flat0 += step;
             }
             PHASE_MARK(4);  // scan rounds
-            if (st.npend > 0) merge_topk(top, pend, tmpk, R, st);
+            if (st.npend > 0) merge_topk(top, pend, tmpk, hist2, ties2, R, a.pid, red, st, a.status);
         }
         __syncthreads();
         PHASE_MARK(5);  // final merge
-        // (6) outputs: the top list is sorted by (distance, id)
+        // (6) outputs: the R best sorted by (distance, id)
         {
             int keep = (qerr2 || nvis == 0) ? 0 : st.ncur;
+            if (keep > 1) {
+                const int k2 = next_pow2(keep);
+                for (int i = keep + tid; i < k2; i += NT) top[i] = ~0ull;
+                __syncthreads();
+                bitonic_sort64(top, k2);
+            }
             for (int j = tid; j < R; j += NT) {
                 size_t o = (size_t)q * R + j;
                 if (j < keep) {
