@@ -45,7 +45,8 @@ constexpr int HBITS = 11;
 constexpr int HBINS = 1 << HBITS;
 constexpr int TIECAP = 64;
 constexpr int RMAX = 1024;      // largest R
-constexpr int PCAP = 4096;      // pending top-R candidates (>= 2 rounds)
+constexpr int PCAP = 2048;      // pending top-R candidates (>= one round + R)
+constexpr int WIN = NT;         // visited cells staged per window
 constexpr int SBCAP = 2048;     // sorted coarse prefix capacity
 constexpr int MAX_ROUNDS = 64;
 
@@ -63,45 +64,107 @@ __host__ __device__ __forceinline__ int next_pow2(int x) {
 }
 __host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
 
+// Candidates staged per scan round: 8 KB of codes per buffer.
+__host__ __device__ __forceinline__ int scan_ncand(int mp) { return mp <= 8 ? 1024 : (mp <= 16 ? 512 : 256); }
+__host__ __device__ __forceinline__ int code_stride(int mp) { return mp <= 4 ? 4 : (mp <= 8 ? 8 : ((mp + 15) & ~15)); }
+
+// Shared memory.  The LUT lives for the whole query; the selection phase
+// (coarse lists, staircase rows, histograms) and the scan phase (cell
+// windows, double-buffered candidate staging, top-R buffers) share the rest.
 struct Smem {
+    float *lut;
+    // selection phase
     uint64_t *LA, *LB;
     uint16_t *rowc, *rowp;
     uint32_t *rowpre;
-    float *lut;
-    unsigned char *uni;
+    uint32_t *hist;   // HBINS
+    uint64_t *ties;   // TIECAP
+    uint64_t *sb;     // SBCAP (aliases hist/ties)
+    // scan phase
+    CellWin *win_[2];
+    unsigned char *scode_[2];
+    float *svt_[2];
+    uint32_t *spos_[2];
+    uint16_t *sci_[2];
+    // buffer b in {0, 1} without indexing a local array (keeps it in registers)
+    __device__ __forceinline__ CellWin *win(int b) const { return b ? win_[1] : win_[0]; }
+    __device__ __forceinline__ unsigned char *scode(int b) const { return b ? scode_[1] : scode_[0]; }
+    __device__ __forceinline__ float *svt(int b) const { return b ? svt_[1] : svt_[0]; }
+    __device__ __forceinline__ uint32_t *spos(int b) const { return b ? spos_[1] : spos_[0]; }
+    __device__ __forceinline__ uint16_t *sci(int b) const { return b ? sci_[1] : sci_[0]; }
+    uint64_t *top, *pend, *tmp;
+    uint32_t *hist2;
+    uint64_t *ties2;
 };
 
-__host__ __device__ inline size_t union_bytes(int kc) {
-    size_t trav = (size_t)HBINS * 4 + (size_t)TIECAP * 8;
-    size_t lists = (size_t)SBCAP * 8;
-    size_t scan = (size_t)(RMAX + PCAP + RMAX) * 8 + (size_t)NT * sizeof(CellWin) + (size_t)HBINS * 4 +
-                  (size_t)TIECAP * 8;
-    size_t m = trav > scan ? trav : scan;
-    (void)kc;
-    return m > lists ? m : lists;
-}
-
 __host__ __device__ inline size_t carve(int mode, int kc, int mp, int kp, Smem *s, unsigned char *base) {
-    int kcP = next_pow2(kc);
+    const int kcP = next_pow2(kc);
     size_t off = 0;
-    size_t la = (size_t)kcP * 8;
-    size_t lb = (mode == SCG_IMI) ? (size_t)kcP * 8 : 0;
+    if (s) s->lut = (float *)(base + off);
+    off += align16((size_t)mp * kp * 4);
+    const size_t phase0 = off;
+    // selection phase
     if (s) s->LA = (uint64_t *)(base + off);
-    off += la;
+    off += (size_t)kcP * 8;
     if (s) s->LB = (mode == SCG_IMI) ? (uint64_t *)(base + off) : s->LA;
-    off += lb;
+    off += (mode == SCG_IMI) ? (size_t)kcP * 8 : 0;
     if (s) s->rowc = (uint16_t *)(base + off);
     off += align16((size_t)kc * 2);
     if (s) s->rowp = (uint16_t *)(base + off);
     off += align16((size_t)kc * 2);
     if (s) s->rowpre = (uint32_t *)(base + off);
     off += align16((size_t)(kc + 1) * 4);
-    if (s) s->lut = (float *)(base + off);
-    off += align16((size_t)mp * kp * 4);
-    if (s) s->uni = base + off;
-    off += union_bytes(kc);
-    return off;
+    if (s) {
+        s->hist = (uint32_t *)(base + off);
+        s->ties = (uint64_t *)(base + off + (size_t)HBINS * 4);
+        s->sb = (uint64_t *)(base + off);
+    }
+    size_t trav = (size_t)HBINS * 4 + (size_t)TIECAP * 8;
+    size_t sbb = (size_t)SBCAP * 8;
+    off += trav > sbb ? trav : sbb;
+    const size_t end1 = off;
+    // scan phase (aliases the selection phase)
+    off = phase0;
+    const int nc = scan_ncand(mp), cs = code_stride(mp);
+    for (int b = 0; b < 2; b++) {
+        if (s) s->win_[b] = (CellWin *)(base + off);
+        off += (size_t)WIN * sizeof(CellWin);
+    }
+    for (int b = 0; b < 2; b++) {
+        if (s) s->scode_[b] = base + off;
+        off += align16((size_t)nc * cs);
+        if (s) s->svt_[b] = (float *)(base + off);
+        off += align16((size_t)nc * 4);
+        if (s) s->spos_[b] = (uint32_t *)(base + off);
+        off += align16((size_t)nc * 4);
+        if (s) s->sci_[b] = (uint16_t *)(base + off);
+        off += align16((size_t)nc * 2);
+    }
+    if (s) s->top = (uint64_t *)(base + off);
+    off += (size_t)RMAX * 8;
+    if (s) s->pend = (uint64_t *)(base + off);
+    off += (size_t)PCAP * 8;
+    if (s) s->tmp = (uint64_t *)(base + off);
+    off += (size_t)RMAX * 8;
+    if (s) s->hist2 = (uint32_t *)(base + off);
+    off += (size_t)HBINS * 4;
+    if (s) s->ties2 = (uint64_t *)(base + off);
+    off += (size_t)TIECAP * 8;
+    return off > end1 ? off : end1;
 }
+
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
+}
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // ---------------------------------------------------------------------------
 // Block-wide helpers (NT threads, all threads must call)
@@ -227,8 +290,10 @@ struct QState {
     // scan
     int ncur, npend;
     uint64_t thr;
-    int clo, cn;
-    uint32_t wend;
+    uint32_t plan_flat, plan_wend;
+    int plan_wb, plan_clo, plan_cn;
+    uint32_t rflat[2];
+    int rcount[2], rwb[2];
 };
 
 // The prefix of a coarse list: the smallest keys of L[0..n) (u64: ordered
@@ -405,6 +470,24 @@ struct CodeWords {
             for (int i = 0; i < MPC / 4; i++) w[i] = __ldg((const uint32_t *)p + i);
         }
     }
+    __device__ __forceinline__ void load_smem(const unsigned char *p, int) {
+        if constexpr (MPC % 16 == 0) {
+#pragma unroll
+            for (int i = 0; i < MPC / 16; i++) {
+                uint4 v = ((const uint4 *)p)[i];
+                w[4 * i] = v.x; w[4 * i + 1] = v.y; w[4 * i + 2] = v.z; w[4 * i + 3] = v.w;
+            }
+        } else if constexpr (MPC % 8 == 0) {
+#pragma unroll
+            for (int i = 0; i < MPC / 8; i++) {
+                uint2 v = ((const uint2 *)p)[i];
+                w[2 * i] = v.x; w[2 * i + 1] = v.y;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < MPC / 4; i++) w[i] = ((const uint32_t *)p)[i];
+        }
+    }
     __device__ __forceinline__ int n(int) const { return MPC; }
     __device__ __forceinline__ uint32_t code(int k) const { return (w[k >> 2] >> ((k & 3) * 8)) & 0xffu; }
 };
@@ -413,8 +496,9 @@ template <>
 struct CodeWords<0> {
     const uint8_t *p;
     __device__ __forceinline__ void load(const uint8_t *codes, uint32_t pos, int mp) { p = codes + (size_t)pos * mp; }
+    __device__ __forceinline__ void load_smem(const unsigned char *q, int) { p = q; }
     __device__ __forceinline__ int n(int mp) const { return mp; }
-    __device__ __forceinline__ uint32_t code(int k) const { return __ldg(p + k); }
+    __device__ __forceinline__ uint32_t code(int k) const { return p[k]; }
 };
 
 // Optional per-phase cycle counters (thread 0 of each CTA), accumulated
@@ -464,9 +548,9 @@ __device__ void merge_topk(uint64_t *top, uint64_t *pend, uint64_t *tmp, uint32_
     // radix select (11 + 11 + 10 bits) of the R-th smallest distance word
     uint32_t prefix = 0;
     uint64_t need = (uint64_t)R;
-    const int shifts[3] = {21, 10, 0}, widths[3] = {11, 11, 10};
+#pragma unroll
     for (int p = 0; p < 3; p++) {
-        const int sh = shifts[p], bits = widths[p], nbins = 1 << bits, hs = sh + bits;
+        const int sh = p == 0 ? 21 : (p == 1 ? 10 : 0), bits = p == 2 ? 10 : 11, nbins = 1 << bits, hs = sh + bits;
         for (int i = tid; i < nbins; i += NT) hist[i] = 0;
         __syncthreads();
         for (int i = tid; i < n; i += NT) {
@@ -543,6 +627,102 @@ __device__ void merge_topk(uint64_t *top, uint64_t *pend, uint64_t *tmp, uint32_
     __syncthreads();
 }
 
+// Plans the next scan round into staging buffer b (restaging the window of
+// visited cells when the round starts past it) and issues the cp.async copies
+// of its codes and per-vector terms.
+template <int MPC>
+__device__ __forceinline__ void plan_round(const SearchArgs &a, Smem &S, QState &st, const uint32_t *vis_cell,
+                                           const uint32_t *vis_pre, int nvis, uint32_t Svis, int kc, bool imi,
+                                           bool sc, float qs, const float *dqc, int mp, bool fast, int NCAND, int CS,
+                                           int cpt, int b) {
+    const int tid = threadIdx.x;
+
+                if (st.plan_flat < Svis && st.plan_flat >= st.plan_wend) {
+                    // stage the next window of visited cells
+                    const int clo = st.plan_clo + st.plan_cn, wb = 1 - st.plan_wb;
+                    const int c = clo + tid;
+                    if (c < nvis) {
+                        uint32_t cell = vis_cell[c];
+                        CellWin cw;
+                        cw.pre = vis_pre[c];
+                        cw.start = a.off[cell];
+                        uint32_t h3, h4;
+                        if (imi) {
+                            h3 = cell / (uint32_t)kc;
+                            h4 = cell - h3 * (uint32_t)kc;
+                            cw.d0 = __fadd_rn(__fadd_rn(qs, dqc[h3]), dqc[kc + h4]);
+                        } else if (sc) {
+                            h3 = cell / (uint32_t)kc;
+                            h4 = 0;
+                            cw.d0 = __fadd_rn(qs, dqc[h3]);
+                        } else {
+                            h3 = cell;
+                            h4 = 0;
+                            cw.d0 = __fadd_rn(qs, dqc[h3]);
+                        }
+                        cw.h34 = h3 | (h4 << 16);
+                        S.win(wb)[tid] = cw;
+                    }
+                    __syncthreads();
+                    if (tid == 0) {
+                        const int cn = min(WIN, nvis - clo);
+                        st.plan_clo = clo;
+                        st.plan_cn = cn;
+                        st.plan_wb = wb;
+                        st.plan_wend = (clo + cn < nvis) ? vis_pre[clo + cn] : Svis;
+                    }
+                    __syncthreads();
+                }
+                const uint32_t f0 = st.plan_flat;
+                const uint32_t cnt = f0 < Svis ? min((uint32_t)NCAND, st.plan_wend - f0) : 0u;
+                const int wb = st.plan_wb, cn = st.plan_cn;
+                const CellWin *W = S.win(wb);
+                int ci = 0;
+                for (int j = 0; j < cpt; j++) {
+                    const int i = tid + j * NT;
+                    if ((uint32_t)i >= cnt) break;
+                    const uint32_t flat = f0 + i;
+                    // window cell containing flat: advance from the last one
+                    int steps = 0;
+                    while (ci + 1 < cn && W[ci + 1].pre <= flat && steps < 4) {
+                        ci++;
+                        steps++;
+                    }
+                    if (ci + 1 < cn && W[ci + 1].pre <= flat) {
+                        int lo2 = ci, hi2 = cn - 1;
+                        while (lo2 < hi2) {
+                            int mid = (lo2 + hi2 + 1) >> 1;
+                            if (W[mid].pre <= flat) lo2 = mid;
+                            else hi2 = mid - 1;
+                        }
+                        ci = lo2;
+                    }
+                    const uint32_t pos = W[ci].start + (flat - W[ci].pre);
+                    S.spos(b)[i] = pos;
+                    S.sci(b)[i] = (uint16_t)ci;
+                    unsigned char *dst = S.scode(b) + (size_t)i * CS;
+                    const uint8_t *src = a.codes + (size_t)pos * mp;
+                    if (MPC == 4) cp_async4(dst, src);
+                    else if (MPC == 8) cp_async8(dst, src);
+                    else if (MPC == 16) cp_async16(dst, src);
+                    else if (MPC == 32) {
+                        cp_async16(dst, src);
+                        cp_async16(dst + 16, src + 16);
+                    } else {
+                        for (int k = 0; k < mp; k++) dst[k] = __ldg(src + k);
+                    }
+                    if (fast) cp_async4(S.svt(b) + i, a.vterm + pos);
+                }
+                cp_async_commit();
+                __syncthreads();
+                if (tid == 0) {
+                    st.rflat[b] = f0;
+                    st.rcount[b] = (int)cnt;
+                    st.rwb[b] = wb;
+                    st.plan_flat = f0 + cnt;
+                }
+            }
+
 template <int MPC>
 __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -563,15 +743,10 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
     uint32_t *rec_cnt = a.rec_cnt + (size_t)blockIdx.x * cap;
     uint32_t *vis_cell = a.vis_cell + (size_t)blockIdx.x * (cap + 1);
     uint32_t *vis_pre = a.vis_pre + (size_t)blockIdx.x * (cap + 1);
-    uint32_t *hist = (uint32_t *)S.uni;
-    uint64_t *ties = (uint64_t *)(S.uni + (size_t)HBINS * 4);
-    uint64_t *sb = (uint64_t *)S.uni;  // sorted coarse prefix scratch
-    uint64_t *top = (uint64_t *)S.uni;
-    uint64_t *pend = top + RMAX;
-    uint64_t *tmpk = pend + PCAP;
-    CellWin *win = (CellWin *)(tmpk + RMAX);
-    uint32_t *hist2 = (uint32_t *)(win + NT);          // merge radix histogram
-    uint64_t *ties2 = (uint64_t *)(hist2 + HBINS);      // merge ties
+    uint32_t *hist = S.hist;
+    uint64_t *ties = S.ties;
+    uint64_t *sb = S.sb;  // sorted coarse prefix scratch
+    const int NCAND = scan_ncand(mp), CS = code_stride(mp);
     const int bsI = kp * mp / a.mc;  // dot_cr block of one coarse centroid
     const double avg_density = (double)a.N / (double)(a.ncells ? a.ncells : 1);
 
@@ -948,125 +1123,69 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
         const uint32_t Svis = (nvis > 0) ? (uint32_t)st.sumv : 0u;
         PHASE_MARK(3);  // compaction
 
-        // (5) ADC scan with the fused top-R
+        // (5) ADC scan with the fused top-R, as a two-stage pipeline: while
+        // one round of candidates is summed, the codes (and per-vector terms)
+        // of the next round land in shared memory through cp.async.
+        uint64_t *top = S.top, *pend = S.pend, *tmpk = S.tmp;
         if (tid == 0) {
             st.ncur = 0;
             st.npend = 0;
             st.thr = ~0ull;
-            st.clo = 0;
-            st.cn = 0;
-            st.wend = 0;
+            st.plan_flat = 0;
+            st.plan_wend = 0;
+            st.plan_wb = 1;
+            st.plan_clo = 0;
+            st.plan_cn = 0;
         }
         __syncthreads();
         if (!qerr2 && nvis > 0) {
-            uint32_t flat0 = 0;
-            while (flat0 < Svis) {
-                // restage the cell window when the current one is consumed
-                if (flat0 >= st.wend) {
-                    int clo = st.clo + st.cn;
-                    __syncthreads();
-                    int c = clo + tid;
-                    if (c < nvis) {
-                        uint32_t cell = vis_cell[c];
-                        CellWin cw;
-                        cw.pre = vis_pre[c];
-                        cw.start = a.off[cell];
-                        uint32_t h3, h4;
-                        if (imi) {
-                            h3 = cell / (uint32_t)kc;
-                            h4 = cell - h3 * (uint32_t)kc;
-                            cw.d0 = __fadd_rn(__fadd_rn(qs, dqc[h3]), dqc[kc + h4]);
-                        } else if (sc) {
-                            h3 = cell / (uint32_t)kc;
-                            h4 = 0;
-                            cw.d0 = __fadd_rn(qs, dqc[h3]);
-                        } else {
-                            h3 = cell;
-                            h4 = 0;
-                            cw.d0 = __fadd_rn(qs, dqc[h3]);
-                        }
-                        cw.h34 = h3 | (h4 << 16);
-                        win[tid] = cw;
-                    }
-                    __syncthreads();
-                    if (tid == 0) {
-                        int cn = min(NT, nvis - clo);
-                        st.clo = clo;
-                        st.cn = cn;
-                        st.wend = (clo + cn < nvis) ? vis_pre[clo + cn] : Svis;
-                    }
-                    __syncthreads();
-                }
+            const int cpt = NCAND / NT;
+            plan_round<MPC>(a, S, st, vis_cell, vis_pre, nvis, Svis, kc, imi, sc, qs, dqc, mp, fast, NCAND, CS, cpt, 0);
+            int b = 0;
+            for (int guard = 0;; guard++) {
+                plan_round<MPC>(a, S, st, vis_cell, vis_pre, nvis, Svis, kc, imi, sc, qs, dqc, mp, fast, NCAND, CS, cpt,
+                                1 - b);
                 // merge the pending candidates when the top list is not yet
-                // full, or when this round might not fit
-                if ((st.npend > 0 && st.ncur < R) || st.npend > R || st.npend + NT * CPT > PCAP) {
+                // full, when they outnumber it, or when a round might not fit
+                __syncthreads();
+                if ((st.npend > 0 && st.ncur < R) || st.npend > R || st.npend + NCAND > PCAP) {
                     COUNT(7, 1);
-                    merge_topk(top, pend, tmpk, hist2, ties2, R, a.pid, red, st, a.status);
+                    merge_topk(top, pend, tmpk, S.hist2, S.ties2, R, a.pid, red, st, a.status);
                 }
-                const uint32_t wend = st.wend;
+                cp_async_wait1();
+                __syncthreads();
+                const int cnt = st.rcount[b];
+                if (cnt == 0 || guard > (int)(Svis / 32u) + 4) break;
+                const CellWin *W = S.win(b ? st.rwb[1] : st.rwb[0]);
                 const uint64_t thr = st.thr;
-                const int cn = st.cn;
-                // CPT candidates per thread, all loads issued before the sums
-                uint32_t pos[CPT];
-                float dd[CPT];
-                uint32_t h34[CPT];
-                CodeWords<MPC> cw_[CPT];
-                int ci = 0;
-#pragma unroll
-                for (int j = 0; j < CPT; j++) {
-                    const uint32_t flat = flat0 + tid + j * NT;
-                    pos[j] = 0xffffffffu;
-                    if (flat < wend) {
-                        // window cell containing flat: advance from the last one
-                        int steps = 0;
-                        while (ci + 1 < cn && win[ci + 1].pre <= flat && steps < 4) {
-                            ci++;
-                            steps++;
-                        }
-                        if (ci + 1 < cn && win[ci + 1].pre <= flat) {
-                            int lo2 = ci, hi2 = cn - 1;
-                            while (lo2 < hi2) {
-                                int mid = (lo2 + hi2 + 1) >> 1;
-                                if (win[mid].pre <= flat) lo2 = mid;
-                                else hi2 = mid - 1;
-                            }
-                            ci = lo2;
-                        }
-                        const CellWin cw = win[ci];
-                        pos[j] = cw.start + (flat - cw.pre);
-                        dd[j] = cw.d0;
-                        h34[j] = cw.h34;
-                        cw_[j].load(a.codes, pos[j], mp);
-                    }
-                }
-                if (fast) {
-#pragma unroll
-                    for (int j = 0; j < CPT; j++)
-                        if (pos[j] != 0xffffffffu) dd[j] = __fadd_rn(dd[j], __ldg(a.vterm + pos[j]));
-                }
-#pragma unroll
-                for (int j = 0; j < CPT; j++) {
-                    if (pos[j] == 0xffffffffu) continue;
-                    float d = dd[j];
-                    const uint32_t h3 = h34[j] & 0xffffu, h4 = h34[j] >> 16;
+                for (int j = 0; j < cpt; j++) {
+                    const int i = tid + j * NT;
+                    if (i >= cnt) break;
+                    const uint32_t pos = S.spos(b)[i];
+                    const CellWin cw = W[S.sci(b)[i]];
+                    float d = cw.d0;
+                    CodeWords<MPC> cwd;
+                    cwd.load_smem(S.scode(b) + (size_t)i * CS, mp);
+                    const uint32_t h3 = cw.h34 & 0xffffu, h4 = cw.h34 >> 16;
                     if (fast) {
                         // d0 + per-vector term + sum_k LUT[k][c_k]
-                        for (int k = 0; k < cw_[j].n(mp); k++) d = __fadd_rn(d, S.lut[k * kp + cw_[j].code(k)]);
+                        d = __fadd_rn(d, S.svt(b)[i]);
+                        for (int k = 0; k < cwd.n(mp); k++) d = __fadd_rn(d, S.lut[k * kp + cwd.code(k)]);
                     } else if (imi) {
                         // multi_query.h:237-254: two adds per subspace
                         const int half = mp >> 1;
                         const float *r1 = a.dot_cr + (size_t)h3 * bsI;
                         const float *r2 = a.dot_cr + (size_t)(h4 + kc - 1) * bsI;
-                        for (int k = 0; k < cw_[j].n(mp); k++) {
-                            int bc = k * kp + cw_[j].code(k);
+                        for (int k = 0; k < cwd.n(mp); k++) {
+                            int bc = k * kp + cwd.code(k);
                             d = __fadd_rn(d, S.lut[bc]);
                             d = __fadd_rn(d, __ldg((k < half ? r1 : r2) + bc));
                         }
                     } else {
                         // query.h:295-306, sc_query.h:222-229: pair sum per subspace
                         const float *r1 = a.dot_cr + (size_t)h3 * bsI;
-                        for (int k = 0; k < cw_[j].n(mp); k++) {
-                            int bc = k * kp + cw_[j].code(k);
+                        for (int k = 0; k < cwd.n(mp); k++) {
+                            int bc = k * kp + cwd.code(k);
                             d = __fadd_rn(d, __fadd_rn(S.lut[bc], __ldg(r1 + bc)));
                         }
                     }
@@ -1074,7 +1193,7 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
                     // needed when the distances are equal
                     const uint32_t du = f2o(d), tu = (uint32_t)(thr >> 32);
                     bool pass = du < tu;
-                    if (du == tu) pass = (uint32_t)a.pid[pos[j]] < (uint32_t)thr;
+                    if (du == tu) pass = (uint32_t)a.pid[pos] < (uint32_t)thr;
                     // warp-aggregated append of (distance, position)
                     const unsigned m = __ballot_sync(__activemask(), pass);
                     if (pass) {
@@ -1083,21 +1202,16 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
                         int base = 0;
                         if (lane == leader) base = atomicAdd(&st.npend, __popc(m));
                         base = __shfl_sync(m, base, leader);
-                        pend[base + __popc(m & ((1u << lane) - 1))] = ((uint64_t)du << 32) | pos[j];
+                        pend[base + __popc(m & ((1u << lane) - 1))] = ((uint64_t)du << 32) | pos;
                     }
                 }
-                uint32_t step = wend > flat0 ? wend - flat0 : 0u;
-                if (step > (uint32_t)(NT * CPT)) step = NT * CPT;
                 __syncthreads();
-                if (step == 0) {
-                    // cannot happen with consistent prefixes; stop instead of spinning
-                    if (tid == 0) atomicOr(a.status, ST_ITER_CAP);
-                    break;
-                }
-                flat0 += step;
+                b = 1 - b;
             }
+            cp_async_wait0();
+            __syncthreads();
             PHASE_MARK(4);  // scan rounds
-            if (st.npend > 0) merge_topk(top, pend, tmpk, hist2, ties2, R, a.pid, red, st, a.status);
+            if (st.npend > 0) merge_topk(top, pend, tmpk, S.hist2, S.ties2, R, a.pid, red, st, a.status);
         }
         __syncthreads();
         PHASE_MARK(5);  // final merge
