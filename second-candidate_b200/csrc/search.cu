@@ -721,6 +721,7 @@ __device__ __forceinline__ void plan_round(const SearchArgs &a, Smem &S, QState 
                     st.rwb[b] = wb;
                     st.plan_flat = f0 + cnt;
                 }
+                __syncthreads();
             }
 
 template <int MPC>
