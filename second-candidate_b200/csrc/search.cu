@@ -47,6 +47,12 @@ constexpr int TIECAP = 64;
 constexpr int RMAX = 1024;      // largest R
 constexpr int PCAP = 2048;      // pending top-R candidates (>= one round + R)
 constexpr int WIN = NT;         // visited cells staged per window
+// warp-centric scan (R <= WRMAX)
+constexpr int WRMAX = 128;      // per-warp top-R queue
+constexpr int WPCAP = 256;      // per-warp pending candidates
+constexpr int WWIN = 32;        // per-warp window of visited cells
+constexpr int UPL = 4;          // candidates per lane per chunk
+constexpr int WCH = 32 * UPL;   // candidates per claimed chunk
 constexpr int SBCAP = 2048;     // sorted coarse prefix capacity
 constexpr int MAX_ROUNDS = 64;
 
@@ -95,6 +101,11 @@ struct Smem {
     uint64_t *top, *pend, *tmp;
     uint32_t *hist2;
     uint64_t *ties2;
+    // warp-centric scan (aliases the staging buffers)
+    CellWin *wwin;    // [NWARP][WWIN]
+    uint64_t *wq;     // [NWARP][WRMAX]
+    uint64_t *wp;     // [NWARP][WPCAP]
+    uint64_t *wt;     // [NWARP][WRMAX]
 };
 
 __host__ __device__ inline size_t carve(int mode, int kc, int mp, int kp, Smem *s, unsigned char *base) {
@@ -139,6 +150,21 @@ __host__ __device__ inline size_t carve(int mode, int kc, int mp, int kp, Smem *
         off += align16((size_t)nc * 4);
         if (s) s->sci_[b] = (uint16_t *)(base + off);
         off += align16((size_t)nc * 2);
+    }
+    {
+        // the warp-centric scan's structures overlay the staging buffers
+        size_t staged = off;
+        size_t w0 = phase0 + 2 * (size_t)WIN * sizeof(CellWin);
+        size_t o = w0;
+        if (s) s->wwin = (CellWin *)(base + o);
+        o += (size_t)NWARP * WWIN * sizeof(CellWin);
+        if (s) s->wq = (uint64_t *)(base + o);
+        o += (size_t)NWARP * WRMAX * 8;
+        if (s) s->wp = (uint64_t *)(base + o);
+        o += (size_t)NWARP * WPCAP * 8;
+        if (s) s->wt = (uint64_t *)(base + o);
+        o += (size_t)NWARP * WRMAX * 8;
+        off = staged > o ? staged : o;
     }
     if (s) s->top = (uint64_t *)(base + off);
     off += (size_t)RMAX * 8;
@@ -294,6 +320,7 @@ struct QState {
     int plan_wb, plan_clo, plan_cn;
     uint32_t rflat[2];
     int rcount[2], rwb[2];
+    uint32_t next_flat;  // warp-centric scan: next unclaimed candidate
 };
 
 // The prefix of a coarse list: the smallest keys of L[0..n) (u64: ordered
@@ -528,9 +555,11 @@ __device__ void merge_topk(uint64_t *top, uint64_t *pend, uint64_t *tmp, uint32_
                            const int *pid, uint64_t *red, QState &st, int *status) {
     const int tid = threadIdx.x;
     const int na = st.ncur, nb = st.npend;
-    for (int i = tid; i < nb; i += NT) {
-        uint64_t e = pend[i];
-        pend[i] = (e & 0xffffffff00000000ull) | (uint32_t)__ldg(pid + (uint32_t)e);
+    if (pid) {
+        for (int i = tid; i < nb; i += NT) {
+            uint64_t e = pend[i];
+            pend[i] = (e & 0xffffffff00000000ull) | (uint32_t)__ldg(pid + (uint32_t)e);
+        }
     }
     __syncthreads();
     const int n = na + nb;
@@ -625,6 +654,60 @@ __device__ void merge_topk(uint64_t *top, uint64_t *pend, uint64_t *tmp, uint32_
     __syncthreads();
     for (int i = tid; i < st.ncur; i += NT) top[i] = tmp[i];
     __syncthreads();
+}
+
+// Warp-synchronous ascending bitonic sort of n (a power of two) u64 keys.
+__device__ __forceinline__ void warp_sort64(uint64_t *key, int n) {
+    const int lane = threadIdx.x & 31;
+    for (int k = 2; k <= n; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = lane; i < n; i += 32) {
+                int ixj = i ^ j;
+                if (ixj > i) {
+                    uint64_t x = key[i], y = key[ixj];
+                    bool up = (i & k) == 0;
+                    if ((x > y) == up) {
+                        key[i] = y;
+                        key[ixj] = x;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// Merges a warp's pending (distance, position) entries into its sorted queue
+// of at most R (distance, id) entries; thr becomes the queue's R-th entry.
+__device__ void warp_merge(uint64_t *wq, int &nq, uint64_t *wp, int &np, uint64_t *wt, int R, const int *pid,
+                           uint64_t &thr) {
+    const int lane = threadIdx.x & 31;
+    for (int i = lane; i < np; i += 32) {
+        uint64_t e = wp[i];
+        wp[i] = (e & 0xffffffff00000000ull) | (uint32_t)__ldg(pid + (uint32_t)e);
+    }
+    const int p2 = next_pow2(np > 1 ? np : 2);
+    for (int i = np + lane; i < p2; i += 32) wp[i] = ~0ull;
+    __syncwarp();
+    warp_sort64(wp, p2);
+    const int nout = nq + np < R ? nq + np : R;
+    for (int k = lane; k < nout; k += 32) {
+        int lo = k - np > 0 ? k - np : 0, hi = k < nq ? k : nq;
+        while (lo < hi) {
+            int mid = (lo + hi) >> 1;
+            if (wq[mid] < wp[k - 1 - mid]) lo = mid + 1;
+            else hi = mid;
+        }
+        int i = lo, j = k - lo;
+        uint64_t x = i < nq ? wq[i] : ~0ull, y = j < np ? wp[j] : ~0ull;
+        wt[k] = x < y ? x : y;
+    }
+    __syncwarp();
+    for (int k = lane; k < nout; k += 32) wq[k] = wt[k];
+    __syncwarp();
+    nq = nout;
+    np = 0;
+    thr = nq == R ? wq[R - 1] : ~0ull;
 }
 
 // Plans the next scan round into staging buffer b (restaging the window of
@@ -1139,7 +1222,141 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
             st.plan_cn = 0;
         }
         __syncthreads();
-        if (!qerr2 && nvis > 0) {
+        if (!qerr2 && nvis > 0 && R <= WRMAX) {
+            // Warp-centric scan: warps claim chunks of WCH candidates, keep
+            // their own window of visited cells and their own top-R queue,
+            // and meet only at the end.
+            const unsigned FULL = 0xffffffffu;
+            const int lane = tid & 31, wid = tid >> 5;
+            CellWin *W = S.wwin + wid * WWIN;
+            uint64_t *wq = S.wq + wid * WRMAX, *wp = S.wp + wid * WPCAP, *wt = S.wt + wid * WRMAX;
+            if (tid == 0) st.next_flat = 0;
+            __syncthreads();
+            int nq = 0, np = 0;
+            uint64_t thr = ~0ull;
+            uint32_t wlo = 1, whi = 0;
+            int wcn = 0;
+            for (;;) {
+                uint32_t base = 0;
+                if (lane == 0) base = atomicAdd(&st.next_flat, (uint32_t)WCH);
+                base = __shfl_sync(FULL, base, 0);
+                if (base >= Svis) break;
+                const uint32_t end = min(base + (uint32_t)WCH, Svis);
+                uint32_t f = base;
+                while (f < end) {
+                    if (f < wlo || f >= whi) {
+                        // window of the visited cells from the one holding f
+                        int ci = 0;
+                        if (lane == 0) {
+                            int lo = 0, hi = nvis - 1;
+                            while (lo < hi) {
+                                int mid = (lo + hi + 1) >> 1;
+                                if (vis_pre[mid] <= f) lo = mid;
+                                else hi = mid - 1;
+                            }
+                            ci = lo;
+                        }
+                        ci = __shfl_sync(FULL, ci, 0);
+                        const int c = ci + lane;
+                        if (c < nvis) {
+                            uint32_t cell = vis_cell[c];
+                            CellWin cw;
+                            cw.pre = vis_pre[c];
+                            cw.start = a.off[cell];
+                            uint32_t h3, h4;
+                            if (imi) {
+                                h3 = cell / (uint32_t)kc;
+                                h4 = cell - h3 * (uint32_t)kc;
+                                cw.d0 = __fadd_rn(__fadd_rn(qs, dqc[h3]), dqc[kc + h4]);
+                            } else if (sc) {
+                                h3 = cell / (uint32_t)kc;
+                                h4 = 0;
+                                cw.d0 = __fadd_rn(qs, dqc[h3]);
+                            } else {
+                                h3 = cell;
+                                h4 = 0;
+                                cw.d0 = __fadd_rn(qs, dqc[h3]);
+                            }
+                            cw.h34 = h3 | (h4 << 16);
+                            W[lane] = cw;
+                        }
+                        wcn = min(WWIN, nvis - ci);
+                        __syncwarp();
+                        wlo = W[0].pre;
+                        whi = (ci + wcn < nvis) ? vis_pre[ci + wcn] : Svis;
+                    }
+                    const uint32_t e2 = min(end, whi);
+                    // loads of UPL candidates per lane, issued together
+                    uint32_t pos[UPL], h34[UPL];
+                    float dd[UPL], vt[UPL];
+                    CodeWords<MPC> cwd[UPL];
+                    int ci = 0;
+#pragma unroll
+                    for (int u = 0; u < UPL; u++) {
+                        const uint32_t ff = f + lane + 32u * u;
+                        pos[u] = 0xffffffffu;
+                        if (ff < e2) {
+                            while (ci + 1 < wcn && W[ci + 1].pre <= ff) ci++;
+                            const CellWin cw = W[ci];
+                            pos[u] = cw.start + (ff - cw.pre);
+                            dd[u] = cw.d0;
+                            h34[u] = cw.h34;
+                            cwd[u].load(a.codes, pos[u], mp);
+                            if (fast) vt[u] = __ldg(a.vterm + pos[u]);
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < UPL; u++) {
+                        bool pass = false;
+                        uint32_t du = 0;
+                        if (pos[u] != 0xffffffffu) {
+                            float d = dd[u];
+                            const uint32_t h3 = h34[u] & 0xffffu, h4 = h34[u] >> 16;
+                            if (fast) {
+                                d = __fadd_rn(d, vt[u]);
+                                for (int k = 0; k < cwd[u].n(mp); k++) d = __fadd_rn(d, S.lut[k * kp + cwd[u].code(k)]);
+                            } else if (imi) {
+                                // multi_query.h:237-254: two adds per subspace
+                                const int half = mp >> 1;
+                                const float *r1 = a.dot_cr + (size_t)h3 * bsI;
+                                const float *r2 = a.dot_cr + (size_t)(h4 + kc - 1) * bsI;
+                                for (int k = 0; k < cwd[u].n(mp); k++) {
+                                    int bc = k * kp + cwd[u].code(k);
+                                    d = __fadd_rn(d, S.lut[bc]);
+                                    d = __fadd_rn(d, __ldg((k < half ? r1 : r2) + bc));
+                                }
+                            } else {
+                                // query.h:295-306, sc_query.h:222-229: pair sum per subspace
+                                const float *r1 = a.dot_cr + (size_t)h3 * bsI;
+                                for (int k = 0; k < cwd[u].n(mp); k++) {
+                                    int bc = k * kp + cwd[u].code(k);
+                                    d = __fadd_rn(d, __fadd_rn(S.lut[bc], __ldg(r1 + bc)));
+                                }
+                            }
+                            du = f2o(d);
+                            const uint32_t tu = (uint32_t)(thr >> 32);
+                            pass = du < tu;
+                            if (du == tu) pass = (uint32_t)a.pid[pos[u]] < (uint32_t)thr;
+                        }
+                        const unsigned m = __ballot_sync(FULL, pass);
+                        if (pass) wp[np + __popc(m & ((1u << lane) - 1))] = ((uint64_t)du << 32) | pos[u];
+                        np += __popc(m);
+                    }
+                    __syncwarp();
+                    if (np > WPCAP - WCH) warp_merge(wq, nq, wp, np, wt, R, a.pid, thr);
+                    f = e2;
+                }
+            }
+            if (np > 0) warp_merge(wq, nq, wp, np, wt, R, a.pid, thr);
+            // the warp queues meet in the pending buffer; one block merge
+            int off0 = 0;
+            if (lane == 0) off0 = atomicAdd(&st.npend, nq);
+            off0 = __shfl_sync(FULL, off0, 0);
+            for (int k = lane; k < nq; k += 32) pend[off0 + k] = wq[k];
+            __syncthreads();
+            PHASE_MARK(4);  // scan
+            if (st.npend > 0) merge_topk(top, pend, tmpk, S.hist2, S.ties2, R, nullptr, red, st, a.status);
+        } else if (!qerr2 && nvis > 0) {
             const int cpt = NCAND / NT;
             plan_round<MPC>(a, S, st, vis_cell, vis_pre, nvis, Svis, kc, imi, sc, qs, dqc, mp, fast, NCAND, CS, cpt, 0);
             int b = 0;
