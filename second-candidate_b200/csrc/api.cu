@@ -66,7 +66,7 @@ struct scg_index {
     bool have_vterm = false;
     // batch workspace
     DevBuf q, dqc, dqr, qn, qsum, ids, dists, sums, nvis, empty, status, counter;
-    DevBuf rec_key, rec_rank, rec_cnt, vis_cell, vis_pre, phase;
+    DevBuf rec_key, rec_rank, rec_cnt, vis_cell, vis_pre, pend, phase;
     bool phase_on = false;
     int *h_status = nullptr;  // pinned
     int last_nq = 0;
@@ -174,6 +174,9 @@ int run_search(scg_index *h, const scg_search_params *p, const float *dQ, int nq
     if ((rc = h->rec_cnt.ensure(4 * slot * grid))) return rc;
     if ((rc = h->vis_cell.ensure(4 * (slot + 1) * grid))) return rc;
     if ((rc = h->vis_pre.ensure(4 * (slot + 1) * grid))) return rc;
+    // survivors of the scan's threshold, per resident CTA
+    const size_t pcap = slot > 65536 ? slot : 65536;
+    if ((rc = h->pend.ensure(8 * pcap * grid))) return rc;
 
     if (p->precision == SCG_FAST && !h->have_vterm) {
         // the fast form's per-vector term (one float per database vector)
@@ -212,6 +215,8 @@ int run_search(scg_index *h, const scg_search_params *p, const float *dQ, int nq
     sa.rec_cnt = h->rec_cnt.as<uint32_t>();
     sa.vis_cell = h->vis_cell.as<uint32_t>(); sa.vis_pre = h->vis_pre.as<uint32_t>();
     sa.cap_rec = h->cap_rec;
+    sa.pend = h->pend.as<uint64_t>();
+    sa.pcap = (uint32_t)pcap;
     sa.qcounter = h->counter.as<int>();
     sa.out_ids = d_ids; sa.out_d = d_d; sa.out_sum = d_sums;
     sa.out_nvis = h->nvis.as<int>(); sa.out_empty = h->empty.as<int>();
@@ -275,7 +280,7 @@ int scg_index_destroy(scg_index *h) {
     DevBuf *all[] = {&h->cq, &h->pq, &h->norm_c, &h->norm_r, &h->dot_cr, &h->off, &h->pid, &h->codes,
                      &h->raw, &h->vterm, &h->q, &h->dqc, &h->dqr, &h->qn, &h->qsum, &h->ids, &h->dists, &h->sums,
                      &h->nvis, &h->empty, &h->status, &h->counter, &h->rec_key, &h->rec_rank,
-                     &h->rec_cnt, &h->vis_cell, &h->vis_pre, &h->phase};
+                     &h->rec_cnt, &h->vis_cell, &h->vis_pre, &h->pend, &h->phase};
     for (DevBuf *b : all) b->release();
     if (h->h_status) cudaFreeHost(h->h_status);
     for (int i = 0; i < 3; i++)

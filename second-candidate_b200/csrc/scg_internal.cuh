@@ -83,6 +83,8 @@ struct SearchArgs {
     uint32_t *rec_key, *rec_rank, *rec_cnt;  // [slots][cap_rec]
     uint32_t *vis_cell, *vis_pre;            // [slots][cap_rec + 1]
     int cap_rec;
+    uint64_t *pend;                          // [slots][pcap] scan survivors
+    uint32_t pcap;
     int *qcounter;                           // dynamic query counter
     // outputs
     int *out_ids;

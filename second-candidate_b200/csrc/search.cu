@@ -45,11 +45,7 @@ constexpr int HBITS = 11;
 constexpr int HBINS = 1 << HBITS;
 constexpr int TIECAP = 64;
 constexpr int RMAX = 1024;      // largest R
-constexpr int PCAP = 2048;      // pending top-R candidates (>= one round + R)
-constexpr int WIN = NT;         // visited cells staged per window
-// warp-centric scan (R <= WRMAX)
-constexpr int WRMAX = 128;      // per-warp top-R queue
-constexpr int WPCAP = 256;      // per-warp pending candidates
+constexpr int WARMN = 4096;     // candidates scored before the threshold is set
 constexpr int WWIN = 32;        // per-warp window of visited cells
 constexpr int UPL = 4;          // candidates per lane per chunk
 constexpr int WCH = 32 * UPL;   // candidates per claimed chunk
@@ -70,10 +66,6 @@ __host__ __device__ __forceinline__ int next_pow2(int x) {
 }
 __host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
 
-// Candidates staged per scan round: 8 KB of codes per buffer.
-__host__ __device__ __forceinline__ int scan_ncand(int mp) { return mp <= 8 ? 1024 : (mp <= 16 ? 512 : 256); }
-__host__ __device__ __forceinline__ int code_stride(int mp) { return mp <= 4 ? 4 : (mp <= 8 ? 8 : ((mp + 15) & ~15)); }
-
 // Shared memory.  The LUT lives for the whole query; the selection phase
 // (coarse lists, staircase rows, histograms) and the scan phase (cell
 // windows, double-buffered candidate staging, top-R buffers) share the rest.
@@ -86,26 +78,12 @@ struct Smem {
     uint32_t *hist;   // HBINS
     uint64_t *ties;   // TIECAP
     uint64_t *sb;     // SBCAP (aliases hist/ties)
-    // scan phase
-    CellWin *win_[2];
-    unsigned char *scode_[2];
-    float *svt_[2];
-    uint32_t *spos_[2];
-    uint16_t *sci_[2];
-    // buffer b in {0, 1} without indexing a local array (keeps it in registers)
-    __device__ __forceinline__ CellWin *win(int b) const { return b ? win_[1] : win_[0]; }
-    __device__ __forceinline__ unsigned char *scode(int b) const { return b ? scode_[1] : scode_[0]; }
-    __device__ __forceinline__ float *svt(int b) const { return b ? svt_[1] : svt_[0]; }
-    __device__ __forceinline__ uint32_t *spos(int b) const { return b ? spos_[1] : spos_[0]; }
-    __device__ __forceinline__ uint16_t *sci(int b) const { return b ? sci_[1] : sci_[0]; }
-    uint64_t *top, *pend, *tmp;
+    // scan phase (aliases the selection phase)
+    CellWin *wwin;    // [NWARP][WWIN]
+    uint64_t *warm;   // [WARMN]
+    uint64_t *top, *tmp;
     uint32_t *hist2;
     uint64_t *ties2;
-    // warp-centric scan (aliases the staging buffers)
-    CellWin *wwin;    // [NWARP][WWIN]
-    uint64_t *wq;     // [NWARP][WRMAX]
-    uint64_t *wp;     // [NWARP][WPCAP]
-    uint64_t *wt;     // [NWARP][WRMAX]
 };
 
 __host__ __device__ inline size_t carve(int mode, int kc, int mp, int kp, Smem *s, unsigned char *base) {
@@ -136,40 +114,12 @@ __host__ __device__ inline size_t carve(int mode, int kc, int mp, int kp, Smem *
     const size_t end1 = off;
     // scan phase (aliases the selection phase)
     off = phase0;
-    const int nc = scan_ncand(mp), cs = code_stride(mp);
-    for (int b = 0; b < 2; b++) {
-        if (s) s->win_[b] = (CellWin *)(base + off);
-        off += (size_t)WIN * sizeof(CellWin);
-    }
-    for (int b = 0; b < 2; b++) {
-        if (s) s->scode_[b] = base + off;
-        off += align16((size_t)nc * cs);
-        if (s) s->svt_[b] = (float *)(base + off);
-        off += align16((size_t)nc * 4);
-        if (s) s->spos_[b] = (uint32_t *)(base + off);
-        off += align16((size_t)nc * 4);
-        if (s) s->sci_[b] = (uint16_t *)(base + off);
-        off += align16((size_t)nc * 2);
-    }
-    {
-        // the warp-centric scan's structures overlay the staging buffers
-        size_t staged = off;
-        size_t w0 = phase0 + 2 * (size_t)WIN * sizeof(CellWin);
-        size_t o = w0;
-        if (s) s->wwin = (CellWin *)(base + o);
-        o += (size_t)NWARP * WWIN * sizeof(CellWin);
-        if (s) s->wq = (uint64_t *)(base + o);
-        o += (size_t)NWARP * WRMAX * 8;
-        if (s) s->wp = (uint64_t *)(base + o);
-        o += (size_t)NWARP * WPCAP * 8;
-        if (s) s->wt = (uint64_t *)(base + o);
-        o += (size_t)NWARP * WRMAX * 8;
-        off = staged > o ? staged : o;
-    }
+    if (s) s->wwin = (CellWin *)(base + off);
+    off += (size_t)NWARP * WWIN * sizeof(CellWin);
+    if (s) s->warm = (uint64_t *)(base + off);
+    off += (size_t)WARMN * 8;
     if (s) s->top = (uint64_t *)(base + off);
     off += (size_t)RMAX * 8;
-    if (s) s->pend = (uint64_t *)(base + off);
-    off += (size_t)PCAP * 8;
     if (s) s->tmp = (uint64_t *)(base + off);
     off += (size_t)RMAX * 8;
     if (s) s->hist2 = (uint32_t *)(base + off);
@@ -178,19 +128,6 @@ __host__ __device__ inline size_t carve(int mode, int kc, int mp, int kp, Smem *
     off += (size_t)TIECAP * 8;
     return off > end1 ? off : end1;
 }
-
-__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
-}
-__device__ __forceinline__ void cp_async8(void *dst, const void *src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
-}
-__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // ---------------------------------------------------------------------------
 // Block-wide helpers (NT threads, all threads must call)
@@ -316,11 +253,7 @@ struct QState {
     // scan
     int ncur, npend;
     uint64_t thr;
-    uint32_t plan_flat, plan_wend;
-    int plan_wb, plan_clo, plan_cn;
-    uint32_t rflat[2];
-    int rcount[2], rwb[2];
-    uint32_t next_flat;  // warp-centric scan: next unclaimed candidate
+    uint32_t next_flat;  // next unclaimed candidate of the scan
 };
 
 // The prefix of a coarse list: the smallest keys of L[0..n) (u64: ordered
@@ -656,156 +589,192 @@ __device__ void merge_topk(uint64_t *top, uint64_t *pend, uint64_t *tmp, uint32_
     __syncthreads();
 }
 
-// Warp-synchronous ascending bitonic sort of n (a power of two) u64 keys.
-__device__ __forceinline__ void warp_sort64(uint64_t *key, int n) {
-    const int lane = threadIdx.x & 31;
-    for (int k = 2; k <= n; k <<= 1) {
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            for (int i = lane; i < n; i += 32) {
-                int ixj = i ^ j;
-                if (ixj > i) {
-                    uint64_t x = key[i], y = key[ixj];
-                    bool up = (i & k) == 0;
-                    if ((x > y) == up) {
-                        key[i] = y;
-                        key[ixj] = x;
-                    }
-                }
-            }
-            __syncwarp();
-        }
-    }
-}
+// Everything the candidate scan needs about one query.
+struct ScanCtx {
+    const uint32_t *vis_cell, *vis_pre;
+    int nvis;
+    uint32_t Svis;
+    int kc, mp, kp, bsI;
+    bool imi, sc, fast;
+    float qs;
+    const float *dqc;
+};
 
-// Merges a warp's pending (distance, position) entries into its sorted queue
-// of at most R (distance, id) entries; thr becomes the queue's R-th entry.
-__device__ void warp_merge(uint64_t *wq, int &nq, uint64_t *wp, int &np, uint64_t *wt, int R, const int *pid,
-                           uint64_t &thr) {
-    const int lane = threadIdx.x & 31;
-    for (int i = lane; i < np; i += 32) {
-        uint64_t e = wp[i];
-        wp[i] = (e & 0xffffffff00000000ull) | (uint32_t)__ldg(pid + (uint32_t)e);
-    }
-    const int p2 = next_pow2(np > 1 ? np : 2);
-    for (int i = np + lane; i < p2; i += 32) wp[i] = ~0ull;
-    __syncwarp();
-    warp_sort64(wp, p2);
-    const int nout = nq + np < R ? nq + np : R;
-    for (int k = lane; k < nout; k += 32) {
-        int lo = k - np > 0 ? k - np : 0, hi = k < nq ? k : nq;
-        while (lo < hi) {
-            int mid = (lo + hi) >> 1;
-            if (wq[mid] < wp[k - 1 - mid]) lo = mid + 1;
-            else hi = mid;
-        }
-        int i = lo, j = k - lo;
-        uint64_t x = i < nq ? wq[i] : ~0ull, y = j < np ? wp[j] : ~0ull;
-        wt[k] = x < y ? x : y;
-    }
-    __syncwarp();
-    for (int k = lane; k < nout; k += 32) wq[k] = wt[k];
-    __syncwarp();
-    nq = nout;
-    np = 0;
-    thr = nq == R ? wq[R - 1] : ~0ull;
-}
-
-// Plans the next scan round into staging buffer b (restaging the window of
-// visited cells when the round starts past it) and issues the cp.async copies
-// of its codes and per-vector terms.
-template <int MPC>
-__device__ __forceinline__ void plan_round(const SearchArgs &a, Smem &S, QState &st, const uint32_t *vis_cell,
-                                           const uint32_t *vis_pre, int nvis, uint32_t Svis, int kc, bool imi,
-                                           bool sc, float qs, const float *dqc, int mp, bool fast, int NCAND, int CS,
-                                           int cpt, int b) {
-    const int tid = threadIdx.x;
-
-                if (st.plan_flat < Svis && st.plan_flat >= st.plan_wend) {
-                    // stage the next window of visited cells
-                    const int clo = st.plan_clo + st.plan_cn, wb = 1 - st.plan_wb;
-                    const int c = clo + tid;
-                    if (c < nvis) {
-                        uint32_t cell = vis_cell[c];
-                        CellWin cw;
-                        cw.pre = vis_pre[c];
-                        cw.start = a.off[cell];
-                        uint32_t h3, h4;
-                        if (imi) {
-                            h3 = cell / (uint32_t)kc;
-                            h4 = cell - h3 * (uint32_t)kc;
-                            cw.d0 = __fadd_rn(__fadd_rn(qs, dqc[h3]), dqc[kc + h4]);
-                        } else if (sc) {
-                            h3 = cell / (uint32_t)kc;
-                            h4 = 0;
-                            cw.d0 = __fadd_rn(qs, dqc[h3]);
-                        } else {
-                            h3 = cell;
-                            h4 = 0;
-                            cw.d0 = __fadd_rn(qs, dqc[h3]);
-                        }
-                        cw.h34 = h3 | (h4 << 16);
-                        S.win(wb)[tid] = cw;
-                    }
-                    __syncthreads();
-                    if (tid == 0) {
-                        const int cn = min(WIN, nvis - clo);
-                        st.plan_clo = clo;
-                        st.plan_cn = cn;
-                        st.plan_wb = wb;
-                        st.plan_wend = (clo + cn < nvis) ? vis_pre[clo + cn] : Svis;
-                    }
-                    __syncthreads();
-                }
-                const uint32_t f0 = st.plan_flat;
-                const uint32_t cnt = f0 < Svis ? min((uint32_t)NCAND, st.plan_wend - f0) : 0u;
-                const int wb = st.plan_wb, cn = st.plan_cn;
-                const CellWin *W = S.win(wb);
+// Warp-centric ADC scan of the candidates [st.next_flat, limit): warps claim
+// chunks of WCH candidates from a shared counter, keep their own window of
+// visited cells, load UPL candidates per lane at once and add the table
+// entries in the reference's order.  WARM == true stores every candidate's
+// (distance, position) at warm[flat]; otherwise candidates with a distance
+// word <= tau are appended to out[] (global, capacity cap) through
+// warp-aggregated atomics on st.npend.
+template <int MPC, bool WARM>
+__device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, QState &st, const ScanCtx &c,
+                                            uint32_t limit, uint32_t tau, uint64_t *warm, uint64_t *out,
+                                            uint32_t cap) {
+    const unsigned FULL = 0xffffffffu;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    CellWin *W = S.wwin + wid * WWIN;
+    uint32_t wlo = 1, whi = 0;
+    int wcn = 0;
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(&st.next_flat, (uint32_t)WCH);
+        base = __shfl_sync(FULL, base, 0);
+        if (base >= limit) break;
+        const uint32_t end = min(base + (uint32_t)WCH, limit);
+        uint32_t f = base;
+        while (f < end) {
+            if (f < wlo || f >= whi) {
+                // window of visited cells from the one holding f
                 int ci = 0;
-                for (int j = 0; j < cpt; j++) {
-                    const int i = tid + j * NT;
-                    if ((uint32_t)i >= cnt) break;
-                    const uint32_t flat = f0 + i;
-                    // window cell containing flat: advance from the last one
-                    int steps = 0;
-                    while (ci + 1 < cn && W[ci + 1].pre <= flat && steps < 4) {
-                        ci++;
-                        steps++;
+                if (lane == 0) {
+                    int lo = 0, hi = c.nvis - 1;
+                    while (lo < hi) {
+                        int mid = (lo + hi + 1) >> 1;
+                        if (c.vis_pre[mid] <= f) lo = mid;
+                        else hi = mid - 1;
                     }
-                    if (ci + 1 < cn && W[ci + 1].pre <= flat) {
-                        int lo2 = ci, hi2 = cn - 1;
-                        while (lo2 < hi2) {
-                            int mid = (lo2 + hi2 + 1) >> 1;
-                            if (W[mid].pre <= flat) lo2 = mid;
-                            else hi2 = mid - 1;
-                        }
-                        ci = lo2;
-                    }
-                    const uint32_t pos = W[ci].start + (flat - W[ci].pre);
-                    S.spos(b)[i] = pos;
-                    S.sci(b)[i] = (uint16_t)ci;
-                    unsigned char *dst = S.scode(b) + (size_t)i * CS;
-                    const uint8_t *src = a.codes + (size_t)pos * mp;
-                    if (MPC == 4) cp_async4(dst, src);
-                    else if (MPC == 8) cp_async8(dst, src);
-                    else if (MPC == 16) cp_async16(dst, src);
-                    else if (MPC == 32) {
-                        cp_async16(dst, src);
-                        cp_async16(dst + 16, src + 16);
+                    ci = lo;
+                }
+                ci = __shfl_sync(FULL, ci, 0);
+                const int cc = ci + lane;
+                if (cc < c.nvis) {
+                    uint32_t cell = c.vis_cell[cc];
+                    CellWin cw;
+                    cw.pre = c.vis_pre[cc];
+                    cw.start = a.off[cell];
+                    uint32_t h3, h4;
+                    if (c.imi) {
+                        h3 = cell / (uint32_t)c.kc;
+                        h4 = cell - h3 * (uint32_t)c.kc;
+                        cw.d0 = __fadd_rn(__fadd_rn(c.qs, c.dqc[h3]), c.dqc[c.kc + h4]);
+                    } else if (c.sc) {
+                        h3 = cell / (uint32_t)c.kc;
+                        h4 = 0;
+                        cw.d0 = __fadd_rn(c.qs, c.dqc[h3]);
                     } else {
-                        for (int k = 0; k < mp; k++) dst[k] = __ldg(src + k);
+                        h3 = cell;
+                        h4 = 0;
+                        cw.d0 = __fadd_rn(c.qs, c.dqc[h3]);
                     }
-                    if (fast) cp_async4(S.svt(b) + i, a.vterm + pos);
+                    cw.h34 = h3 | (h4 << 16);
+                    W[lane] = cw;
                 }
-                cp_async_commit();
-                __syncthreads();
-                if (tid == 0) {
-                    st.rflat[b] = f0;
-                    st.rcount[b] = (int)cnt;
-                    st.rwb[b] = wb;
-                    st.plan_flat = f0 + cnt;
-                }
-                __syncthreads();
+                wcn = min(WWIN, c.nvis - ci);
+                __syncwarp();
+                wlo = W[0].pre;
+                whi = (ci + wcn < c.nvis) ? c.vis_pre[ci + wcn] : c.Svis;
             }
+            const uint32_t e2 = min(end, whi);
+            // loads of UPL candidates per lane, issued together
+            uint32_t pos[UPL], h34[UPL];
+            float dd[UPL], vt[UPL];
+            CodeWords<MPC> cwd[UPL];
+            int ci = 0;
+#pragma unroll
+            for (int u = 0; u < UPL; u++) {
+                const uint32_t ff = f + lane + 32u * u;
+                pos[u] = 0xffffffffu;
+                if (ff < e2) {
+                    while (ci + 1 < wcn && W[ci + 1].pre <= ff) ci++;
+                    const CellWin cw = W[ci];
+                    pos[u] = cw.start + (ff - cw.pre);
+                    dd[u] = cw.d0;
+                    h34[u] = cw.h34;
+                    cwd[u].load(a.codes, pos[u], c.mp);
+                    if (c.fast) vt[u] = __ldg(a.vterm + pos[u]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < UPL; u++) {
+                bool pass = false;
+                uint32_t du = 0;
+                if (pos[u] != 0xffffffffu) {
+                    float d = dd[u];
+                    const uint32_t h3 = h34[u] & 0xffffu, h4 = h34[u] >> 16;
+                    if (c.fast) {
+                        // d0 + per-vector term + sum_k LUT[k][c_k]
+                        d = __fadd_rn(d, vt[u]);
+                        for (int k = 0; k < cwd[u].n(c.mp); k++) d = __fadd_rn(d, S.lut[k * c.kp + cwd[u].code(k)]);
+                    } else if (c.imi) {
+                        // multi_query.h:237-254: two adds per subspace
+                        const int half = c.mp >> 1;
+                        const float *r1 = a.dot_cr + (size_t)h3 * c.bsI;
+                        const float *r2 = a.dot_cr + (size_t)(h4 + c.kc - 1) * c.bsI;
+                        for (int k = 0; k < cwd[u].n(c.mp); k++) {
+                            int bc = k * c.kp + cwd[u].code(k);
+                            d = __fadd_rn(d, S.lut[bc]);
+                            d = __fadd_rn(d, __ldg((k < half ? r1 : r2) + bc));
+                        }
+                    } else {
+                        // query.h:295-306, sc_query.h:222-229: pair sum per subspace
+                        const float *r1 = a.dot_cr + (size_t)h3 * c.bsI;
+                        for (int k = 0; k < cwd[u].n(c.mp); k++) {
+                            int bc = k * c.kp + cwd[u].code(k);
+                            d = __fadd_rn(d, __fadd_rn(S.lut[bc], __ldg(r1 + bc)));
+                        }
+                    }
+                    du = f2o(d);
+                    if (WARM) warm[f + lane + 32u * u] = ((uint64_t)du << 32) | pos[u];
+                    else pass = du <= tau;
+                }
+                if (!WARM) {
+                    const unsigned m = __ballot_sync(FULL, pass);
+                    if (m) {
+                        uint32_t slot0 = 0;
+                        if (lane == __ffs(m) - 1) slot0 = atomicAdd((unsigned *)&st.npend, (unsigned)__popc(m));
+                        slot0 = __shfl_sync(FULL, slot0, __ffs(m) - 1);
+                        const uint32_t slot = slot0 + __popc(m & ((1u << lane) - 1));
+                        if (pass && slot < cap) out[slot] = ((uint64_t)du << 32) | pos[u];
+                    }
+                }
+            }
+            f = e2;
+        }
+    }
+}
+
+// The k-th smallest (1-based) high word of keys[0..n) in shared memory
+// (radix select, 11 + 11 + 10 bits).
+__device__ uint32_t block_kth_hi(const uint64_t *keys, int n, int k, uint32_t *hist, uint64_t *red, QState &st) {
+    const int tid = threadIdx.x;
+    uint32_t prefix = 0;
+    uint64_t need = (uint64_t)k;
+#pragma unroll
+    for (int p = 0; p < 3; p++) {
+        const int sh = p == 0 ? 21 : (p == 1 ? 10 : 0), bits = p == 2 ? 10 : 11, nbins = 1 << bits, hs = sh + bits;
+        for (int i = tid; i < nbins; i += NT) hist[i] = 0;
+        __syncthreads();
+        for (int i = tid; i < n; i += NT) {
+            uint32_t v = (uint32_t)(keys[i] >> 32);
+            if (hs < 32 && (v >> hs) != (prefix >> hs)) continue;
+            atomicAdd(&hist[(v >> sh) & (nbins - 1)], 1u);
+        }
+        __syncthreads();
+        const int per = (nbins + NT - 1) / NT;
+        const int b0 = tid * per;
+        uint64_t mine = 0;
+        for (int i = 0; i < per; i++)
+            if (b0 + i < nbins) mine += hist[b0 + i];
+        uint64_t tot;
+        uint64_t run = block_exscan(mine, red, tot);
+        for (int i = 0; i < per; i++) {
+            int bb = b0 + i;
+            if (bb >= nbins) break;
+            uint64_t nxt = run + hist[bb];
+            if (run < need && nxt >= need) {
+                st.s_bin = (uint32_t)bb;
+                st.s_acc = run;
+            }
+            run = nxt;
+        }
+        __syncthreads();
+        prefix |= st.s_bin << sh;
+        need -= st.s_acc;
+        __syncthreads();
+    }
+    return prefix;
+}
 
 template <int MPC>
 __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
@@ -830,7 +799,6 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
     uint32_t *hist = S.hist;
     uint64_t *ties = S.ties;
     uint64_t *sb = S.sb;  // sorted coarse prefix scratch
-    const int NCAND = scan_ncand(mp), CS = code_stride(mp);
     const int bsI = kp * mp / a.mc;  // dot_cr block of one coarse centroid
     const double avg_density = (double)a.N / (double)(a.ncells ? a.ncells : 1);
 
@@ -1207,235 +1175,74 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
         const uint32_t Svis = (nvis > 0) ? (uint32_t)st.sumv : 0u;
         PHASE_MARK(3);  // compaction
 
-        // (5) ADC scan with the fused top-R, as a two-stage pipeline: while
-        // one round of candidates is summed, the codes (and per-vector terms)
-        // of the next round land in shared memory through cp.async.
-        uint64_t *top = S.top, *pend = S.pend, *tmpk = S.tmp;
+        // (5) ADC scan with the fused top-R.  The first WARMN candidates are
+        // scored into shared memory; their R-th smallest distance bounds the
+        // final R-th distance from above, so the rest of the scan keeps only
+        // candidates at or below it, appended to a per-CTA buffer; one
+        // radix-select merge over that buffer gives the R best.
+        uint64_t *top = S.top, *tmpk = S.tmp;
+        uint64_t *pend_g = a.pend + (size_t)blockIdx.x * a.pcap;
         if (tid == 0) {
             st.ncur = 0;
             st.npend = 0;
-            st.thr = ~0ull;
-            st.plan_flat = 0;
-            st.plan_wend = 0;
-            st.plan_wb = 1;
-            st.plan_clo = 0;
-            st.plan_cn = 0;
+            st.next_flat = 0;
         }
         __syncthreads();
-        if (!qerr2 && nvis > 0 && R <= WRMAX) {
-            // Warp-centric scan: warps claim chunks of WCH candidates, keep
-            // their own window of visited cells and their own top-R queue,
-            // and meet only at the end.
-            const unsigned FULL = 0xffffffffu;
-            const int lane = tid & 31, wid = tid >> 5;
-            CellWin *W = S.wwin + wid * WWIN;
-            uint64_t *wq = S.wq + wid * WRMAX, *wp = S.wp + wid * WPCAP, *wt = S.wt + wid * WRMAX;
-            if (tid == 0) st.next_flat = 0;
+        if (!qerr2 && nvis > 0) {
+            ScanCtx c;
+            c.vis_cell = vis_cell;
+            c.vis_pre = vis_pre;
+            c.nvis = nvis;
+            c.Svis = Svis;
+            c.kc = kc;
+            c.mp = mp;
+            c.kp = kp;
+            c.bsI = bsI;
+            c.imi = imi;
+            c.sc = sc;
+            c.fast = fast;
+            c.qs = qs;
+            c.dqc = dqc;
+            const uint32_t K = Svis < (uint32_t)WARMN ? Svis : (uint32_t)WARMN;
+            scan_chunks<MPC, true>(a, S, st, c, K, 0u, S.warm, nullptr, 0u);
             __syncthreads();
-            int nq = 0, np = 0;
-            uint64_t thr = ~0ull;
-            uint32_t wlo = 1, whi = 0;
-            int wcn = 0;
-            for (;;) {
-                uint32_t base = 0;
-                if (lane == 0) base = atomicAdd(&st.next_flat, (uint32_t)WCH);
-                base = __shfl_sync(FULL, base, 0);
-                if (base >= Svis) break;
-                const uint32_t end = min(base + (uint32_t)WCH, Svis);
-                uint32_t f = base;
-                while (f < end) {
-                    if (f < wlo || f >= whi) {
-                        // window of the visited cells from the one holding f
-                        int ci = 0;
-                        if (lane == 0) {
-                            int lo = 0, hi = nvis - 1;
-                            while (lo < hi) {
-                                int mid = (lo + hi + 1) >> 1;
-                                if (vis_pre[mid] <= f) lo = mid;
-                                else hi = mid - 1;
-                            }
-                            ci = lo;
-                        }
-                        ci = __shfl_sync(FULL, ci, 0);
-                        const int c = ci + lane;
-                        if (c < nvis) {
-                            uint32_t cell = vis_cell[c];
-                            CellWin cw;
-                            cw.pre = vis_pre[c];
-                            cw.start = a.off[cell];
-                            uint32_t h3, h4;
-                            if (imi) {
-                                h3 = cell / (uint32_t)kc;
-                                h4 = cell - h3 * (uint32_t)kc;
-                                cw.d0 = __fadd_rn(__fadd_rn(qs, dqc[h3]), dqc[kc + h4]);
-                            } else if (sc) {
-                                h3 = cell / (uint32_t)kc;
-                                h4 = 0;
-                                cw.d0 = __fadd_rn(qs, dqc[h3]);
-                            } else {
-                                h3 = cell;
-                                h4 = 0;
-                                cw.d0 = __fadd_rn(qs, dqc[h3]);
-                            }
-                            cw.h34 = h3 | (h4 << 16);
-                            W[lane] = cw;
-                        }
-                        wcn = min(WWIN, nvis - ci);
-                        __syncwarp();
-                        wlo = W[0].pre;
-                        whi = (ci + wcn < nvis) ? vis_pre[ci + wcn] : Svis;
-                    }
-                    const uint32_t e2 = min(end, whi);
-                    // loads of UPL candidates per lane, issued together
-                    uint32_t pos[UPL], h34[UPL];
-                    float dd[UPL], vt[UPL];
-                    CodeWords<MPC> cwd[UPL];
-                    int ci = 0;
-#pragma unroll
-                    for (int u = 0; u < UPL; u++) {
-                        const uint32_t ff = f + lane + 32u * u;
-                        pos[u] = 0xffffffffu;
-                        if (ff < e2) {
-                            while (ci + 1 < wcn && W[ci + 1].pre <= ff) ci++;
-                            const CellWin cw = W[ci];
-                            pos[u] = cw.start + (ff - cw.pre);
-                            dd[u] = cw.d0;
-                            h34[u] = cw.h34;
-                            cwd[u].load(a.codes, pos[u], mp);
-                            if (fast) vt[u] = __ldg(a.vterm + pos[u]);
-                        }
-                    }
-#pragma unroll
-                    for (int u = 0; u < UPL; u++) {
-                        bool pass = false;
-                        uint32_t du = 0;
-                        if (pos[u] != 0xffffffffu) {
-                            float d = dd[u];
-                            const uint32_t h3 = h34[u] & 0xffffu, h4 = h34[u] >> 16;
-                            if (fast) {
-                                d = __fadd_rn(d, vt[u]);
-                                for (int k = 0; k < cwd[u].n(mp); k++) d = __fadd_rn(d, S.lut[k * kp + cwd[u].code(k)]);
-                            } else if (imi) {
-                                // multi_query.h:237-254: two adds per subspace
-                                const int half = mp >> 1;
-                                const float *r1 = a.dot_cr + (size_t)h3 * bsI;
-                                const float *r2 = a.dot_cr + (size_t)(h4 + kc - 1) * bsI;
-                                for (int k = 0; k < cwd[u].n(mp); k++) {
-                                    int bc = k * kp + cwd[u].code(k);
-                                    d = __fadd_rn(d, S.lut[bc]);
-                                    d = __fadd_rn(d, __ldg((k < half ? r1 : r2) + bc));
-                                }
-                            } else {
-                                // query.h:295-306, sc_query.h:222-229: pair sum per subspace
-                                const float *r1 = a.dot_cr + (size_t)h3 * bsI;
-                                for (int k = 0; k < cwd[u].n(mp); k++) {
-                                    int bc = k * kp + cwd[u].code(k);
-                                    d = __fadd_rn(d, __fadd_rn(S.lut[bc], __ldg(r1 + bc)));
-                                }
-                            }
-                            du = f2o(d);
-                            const uint32_t tu = (uint32_t)(thr >> 32);
-                            pass = du < tu;
-                            if (du == tu) pass = (uint32_t)a.pid[pos[u]] < (uint32_t)thr;
-                        }
-                        const unsigned m = __ballot_sync(FULL, pass);
-                        if (pass) wp[np + __popc(m & ((1u << lane) - 1))] = ((uint64_t)du << 32) | pos[u];
-                        np += __popc(m);
-                    }
-                    __syncwarp();
-                    if (np > WPCAP - WCH) warp_merge(wq, nq, wp, np, wt, R, a.pid, thr);
-                    f = e2;
+            uint32_t tau = 0xffffffffu;
+            if (K > (uint32_t)R) tau = block_kth_hi(S.warm, (int)K, R, S.hist2, red, st);
+            // the warm entries at or below tau open the pending buffer
+            {
+                uint64_t mine = 0;
+                for (int i = tid; i < (int)K; i += NT) mine += ((uint32_t)(S.warm[i] >> 32) <= tau);
+                uint64_t tot;
+                uint64_t p = block_exscan(mine, red, tot);
+                for (int i = tid; i < (int)K; i += NT) {
+                    uint64_t e = S.warm[i];
+                    if ((uint32_t)(e >> 32) <= tau) pend_g[p++] = e;
                 }
+                if (tid == 0) {
+                    st.npend = (int)tot;
+                    st.next_flat = K;
+                }
+                __syncthreads();
             }
-            if (np > 0) warp_merge(wq, nq, wp, np, wt, R, a.pid, thr);
-            // the warp queues meet in the pending buffer; one block merge
-            int off0 = 0;
-            if (lane == 0) off0 = atomicAdd(&st.npend, nq);
-            off0 = __shfl_sync(FULL, off0, 0);
-            for (int k = lane; k < nq; k += 32) pend[off0 + k] = wq[k];
+            scan_chunks<MPC, false>(a, S, st, c, Svis, tau, nullptr, pend_g, a.pcap);
             __syncthreads();
             PHASE_MARK(4);  // scan
-            if (st.npend > 0) merge_topk(top, pend, tmpk, S.hist2, S.ties2, R, nullptr, red, st, a.status);
-        } else if (!qerr2 && nvis > 0) {
-            const int cpt = NCAND / NT;
-            plan_round<MPC>(a, S, st, vis_cell, vis_pre, nvis, Svis, kc, imi, sc, qs, dqc, mp, fast, NCAND, CS, cpt, 0);
-            int b = 0;
-            for (int guard = 0;; guard++) {
-                plan_round<MPC>(a, S, st, vis_cell, vis_pre, nvis, Svis, kc, imi, sc, qs, dqc, mp, fast, NCAND, CS, cpt,
-                                1 - b);
-                // merge the pending candidates when the top list is not yet
-                // full, when they outnumber it, or when a round might not fit
-                __syncthreads();
-                if ((st.npend > 0 && st.ncur < R) || st.npend > R || st.npend + NCAND > PCAP) {
-                    COUNT(7, 1);
-                    merge_topk(top, pend, tmpk, S.hist2, S.ties2, R, a.pid, red, st, a.status);
-                }
-                cp_async_wait1();
-                __syncthreads();
-                const int cnt = st.rcount[b];
-                if (cnt == 0 || guard > (int)(Svis / 32u) + 4) break;
-                const CellWin *W = S.win(b ? st.rwb[1] : st.rwb[0]);
-                const uint64_t thr = st.thr;
-                for (int j = 0; j < cpt; j++) {
-                    const int i = tid + j * NT;
-                    if (i >= cnt) break;
-                    const uint32_t pos = S.spos(b)[i];
-                    const CellWin cw = W[S.sci(b)[i]];
-                    float d = cw.d0;
-                    CodeWords<MPC> cwd;
-                    cwd.load_smem(S.scode(b) + (size_t)i * CS, mp);
-                    const uint32_t h3 = cw.h34 & 0xffffu, h4 = cw.h34 >> 16;
-                    if (fast) {
-                        // d0 + per-vector term + sum_k LUT[k][c_k]
-                        d = __fadd_rn(d, S.svt(b)[i]);
-                        for (int k = 0; k < cwd.n(mp); k++) d = __fadd_rn(d, S.lut[k * kp + cwd.code(k)]);
-                    } else if (imi) {
-                        // multi_query.h:237-254: two adds per subspace
-                        const int half = mp >> 1;
-                        const float *r1 = a.dot_cr + (size_t)h3 * bsI;
-                        const float *r2 = a.dot_cr + (size_t)(h4 + kc - 1) * bsI;
-                        for (int k = 0; k < cwd.n(mp); k++) {
-                            int bc = k * kp + cwd.code(k);
-                            d = __fadd_rn(d, S.lut[bc]);
-                            d = __fadd_rn(d, __ldg((k < half ? r1 : r2) + bc));
-                        }
-                    } else {
-                        // query.h:295-306, sc_query.h:222-229: pair sum per subspace
-                        const float *r1 = a.dot_cr + (size_t)h3 * bsI;
-                        for (int k = 0; k < cwd.n(mp); k++) {
-                            int bc = k * kp + cwd.code(k);
-                            d = __fadd_rn(d, __fadd_rn(S.lut[bc], __ldg(r1 + bc)));
-                        }
-                    }
-                    // below the threshold (distance, id): the id is only
-                    // needed when the distances are equal
-                    const uint32_t du = f2o(d), tu = (uint32_t)(thr >> 32);
-                    bool pass = du < tu;
-                    if (du == tu) pass = (uint32_t)a.pid[pos] < (uint32_t)thr;
-                    // warp-aggregated append of (distance, position)
-                    const unsigned m = __ballot_sync(__activemask(), pass);
-                    if (pass) {
-                        const int lane = tid & 31;
-                        const int leader = __ffs(m) - 1;
-                        int base = 0;
-                        if (lane == leader) base = atomicAdd(&st.npend, __popc(m));
-                        base = __shfl_sync(m, base, leader);
-                        pend[base + __popc(m & ((1u << lane) - 1))] = ((uint64_t)du << 32) | pos;
-                    }
+            if ((uint32_t)st.npend > a.pcap) {
+                if (tid == 0) {
+                    st.err = 1;
+                    atomicOr(a.status, ST_CELL_BUDGET);
                 }
                 __syncthreads();
-                b = 1 - b;
+            } else if (st.npend > 0) {
+                merge_topk(top, pend_g, tmpk, S.hist2, S.ties2, R, a.pid, red, st, a.status);
             }
-            cp_async_wait0();
-            __syncthreads();
-            PHASE_MARK(4);  // scan rounds
-            if (st.npend > 0) merge_topk(top, pend, tmpk, S.hist2, S.ties2, R, a.pid, red, st, a.status);
         }
         __syncthreads();
         PHASE_MARK(5);  // final merge
         // (6) outputs: the R best sorted by (distance, id)
         {
-            int keep = (qerr2 || nvis == 0) ? 0 : st.ncur;
+            const bool qerr3 = st.err != 0;
+            int keep = (qerr3 || nvis == 0) ? 0 : st.ncur;
             if (keep > 1) {
                 const int k2 = next_pow2(keep);
                 for (int i = keep + tid; i < k2; i += NT) top[i] = ~0ull;
@@ -1454,9 +1261,9 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
                 }
             }
             if (tid == 0) {
-                a.out_sum[q] = qerr2 ? -1 : (int)(nothing ? 0 : st.sumv);
+                a.out_sum[q] = qerr3 ? -1 : (int)(nothing ? 0 : st.sumv);
                 if (a.out_nvis) a.out_nvis[q] = nvis;
-                if (a.out_empty) a.out_empty[q] = qerr2 ? 0 : (int)(st.nv - st.nev);
+                if (a.out_empty) a.out_empty[q] = qerr3 ? 0 : (int)(st.nv - st.nev);
             }
         }
         __syncthreads();
