@@ -109,6 +109,23 @@ int scg_search(scg_index *h, const scg_search_params *p, const float *Q, int nq,
 int scg_search_device(scg_index *h, const scg_search_params *p, const float *dQ, int nq,
                       int *d_ids, float *d_dists, int *d_sums, void *stream);
 
+/* scg_search_device without any device allocation, for callers that cannot
+ * allocate at search time (a memory pool that forbids cudaMalloc, or an
+ * allocator owned by someone else).  No counterpart in the reference.  All
+ * scratch -- per-query tables, cell records, scan survivors -- comes from one
+ * 48 MiB file-scope device array that every GPU loading the library holds
+ * until exit.  Limits: the per-query tables of nq queries must fit beside the
+ * search slots (SCG_ERR_CAP names the largest nq for the index), and each
+ * query may enumerate at most 8192 cells and keep 8192 scan survivors
+ * (SCG_ERR_CAP otherwise).  The first call on a device looks up the array's
+ * device address; make that first call before any stream capture.  Every
+ * call shares the one array: calls that overlap on the GPU (other streams,
+ * other threads, the same device) race and must be serialised by the caller.
+ * The fast form (SCG_FAST) needs its per-vector term, built by an earlier
+ * SCG_FAST call of scg_search or scg_search_device. */
+int scg_search_device_noalloc(scg_index *h, const scg_search_params *p, const float *dQ, int nq,
+                              int *d_ids, float *d_dists, int *d_sums, void *stream);
+
 /* Per-query candidate targets (device pointer to nq ints) for the next
  * scg_search_device call; NULL restores the single T of the parameters. */
 int scg_set_query_targets(scg_index *h, const int *d_T);

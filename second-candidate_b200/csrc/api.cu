@@ -599,3 +599,149 @@ int scg_index_info(scg_index *h, int *dim, int *mc, int *kc, int *mp, int *kp, i
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Search without allocation.
+//
+// Some callers cannot allocate device memory at search time -- code running
+// under a memory pool that forbids cudaMalloc, callers that must not change
+// the device's allocation state while other work runs, or processes whose
+// allocator is owned by someone else.  scg_search_device_noalloc serves them
+// from one file-scope device array of SCG_NOALLOC_SCRATCH_BYTES, which every
+// GPU that loads this library holds until the process exits.
+
+namespace {
+
+constexpr size_t SCG_NOALLOC_SCRATCH_BYTES = 48ull << 20;  // 48 MiB
+constexpr int NOALLOC_CELLS = 8192;                        // cells per query (budget)
+constexpr int NOALLOC_SURVIVORS = 8192;                    // scan survivors per query
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[SCG_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[64] = {nullptr};
+
+// Device address of the scratch array on the current device (the host-side
+// name of the array is only a stand-in).  Looked up once per device.
+int noalloc_scratch(int device, unsigned char **out) {
+    if (device < 0 || device >= 64) return fail(SCG_ERR_ARG, "device index out of range");
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(scratch)");
+        g_noalloc_ptr[device] = ptr;
+    }
+    *out = (unsigned char *)g_noalloc_ptr[device];
+    return SCG_OK;
+}
+
+size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+}  // namespace
+
+extern "C" int scg_search_device_noalloc(scg_index *h, const scg_search_params *p, const float *dQ, int nq,
+                                         int *d_ids, float *d_dists, int *d_sums, void *stream) {
+    int rc;
+    if ((rc = check_ready(h))) return rc;
+    if ((rc = check_params(h, p, nq))) return rc;
+    if (nq > 0 && (!dQ || !d_ids || !d_dists || !d_sums)) return fail(SCG_ERR_ARG, "null buffer");
+    if (p->precision == SCG_FAST && !h->have_vterm)
+        return fail(SCG_ERR_STATE,
+                    "the fast form's per-vector term is built by the first SCG_FAST call of scg_search or "
+                    "scg_search_device; make one before searching without allocation");
+    std::lock_guard<std::mutex> g(h->mu);
+    if ((rc = set_device(h))) return rc;
+    if (nq == 0) return SCG_OK;
+    unsigned char *base = nullptr;
+    if ((rc = noalloc_scratch(h->device, &base))) return rc;
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+
+    // carve the scratch: per-query tables first, then per-CTA slots
+    const size_t per_query = up256(sizeof(float) * (size_t)h->mc * h->kc) + up256(sizeof(float) * (size_t)h->mp * h->kp);
+    const size_t fixed = 4 * up256(sizeof(float) * (size_t)nq * 2) + 2 * 256;  // qn, qsum, nvis, empty; status, counter
+    const size_t slot_bytes = up256(4ull * NOALLOC_CELLS) * 3 + up256(4ull * (NOALLOC_CELLS + 1)) * 2 +
+                              up256(8ull * NOALLOC_SURVIVORS);
+    int per_sm = search_max_blocks_per_sm(p->mode, h->kc, h->mp, h->kp);
+    if (per_sm < 1) return fail(SCG_ERR_ARG, "search kernel does not fit on an SM for this shape");
+    int grid = h->num_sms * per_sm;
+    if (grid > nq) grid = nq;
+    const size_t tables = per_query * (size_t)nq;
+    if (fixed + tables + slot_bytes > SCG_NOALLOC_SCRATCH_BYTES) {
+        size_t maxq = (SCG_NOALLOC_SCRATCH_BYTES - slot_bytes - 4096) / (per_query + 4 * 2 * sizeof(float));
+        return fail(SCG_ERR_CAP, "nq = " + std::to_string(nq) + " exceeds the 48 MiB scratch of the allocation-free "
+                    "search for this index (at most " + std::to_string(maxq) + " queries per call)");
+    }
+    const size_t left = SCG_NOALLOC_SCRATCH_BYTES - fixed - tables;
+    if ((size_t)grid * slot_bytes > left) grid = (int)(left / slot_bytes);
+    if (grid < 1) return fail(SCG_ERR_CAP, "the allocation-free scratch has no room for a search slot");
+
+    unsigned char *cur = base;
+    auto take = [&](size_t bytes) {
+        unsigned char *r = cur;
+        cur += up256(bytes);
+        return r;
+    };
+    float *dqc = (float *)take(sizeof(float) * (size_t)nq * h->mc * h->kc);
+    float *dqr = (float *)take(sizeof(float) * (size_t)nq * h->mp * h->kp);
+    float *qn = (float *)take(sizeof(float) * (size_t)nq * 2);
+    float *qsum = (float *)take(sizeof(float) * (size_t)nq);
+    int *nvis = (int *)take(sizeof(int) * (size_t)nq);
+    int *empty = (int *)take(sizeof(int) * (size_t)nq);
+    int *status = (int *)take(sizeof(int) * 4);
+    int *counter = (int *)take(sizeof(int) * 4);
+    uint32_t *rec_key = (uint32_t *)take(4ull * NOALLOC_CELLS * grid);
+    uint32_t *rec_rank = (uint32_t *)take(4ull * NOALLOC_CELLS * grid);
+    uint32_t *rec_cnt = (uint32_t *)take(4ull * NOALLOC_CELLS * grid);
+    uint32_t *vis_cell = (uint32_t *)take(4ull * (NOALLOC_CELLS + 1) * grid);
+    uint32_t *vis_pre = (uint32_t *)take(4ull * (NOALLOC_CELLS + 1) * grid);
+    uint64_t *pend = (uint64_t *)take(8ull * NOALLOC_SURVIVORS * grid);
+    if ((size_t)(cur - base) > SCG_NOALLOC_SCRATCH_BYTES) return fail(SCG_ERR_CAP, "allocation-free scratch overrun");
+
+    TablesArgs ta;
+    ta.dim = h->dim; ta.mc = h->mc; ta.kc = h->kc; ta.mp = h->mp; ta.kp = h->kp; ta.nq = nq;
+    ta.Q = dQ;
+    ta.cq = h->cq.as<float>(); ta.pq = h->pq.as<float>();
+    ta.norm_c = h->norm_c.as<float>(); ta.norm_r = h->norm_r.as<float>();
+    ta.dqc = dqc; ta.dqr = dqr; ta.qn = qn; ta.qsum = qsum;
+    ta.fast = p->precision == SCG_FAST;
+    launch_tables_exact(ta, s);
+    // the scratch keeps the previous call's contents: clear what starts at zero
+    SCG_CUDA(cudaMemsetAsync(status, 0, sizeof(int) * 4, s));
+    SCG_CUDA(cudaMemsetAsync(counter, 0, sizeof(int) * 4, s));
+    SearchArgs sa;
+    memset(&sa, 0, sizeof(sa));
+    sa.mode = p->mode; sa.dim = h->dim; sa.mc = h->mc; sa.kc = h->kc; sa.mp = h->mp; sa.kp = h->kp;
+    sa.nq = nq; sa.R = p->R; sa.w = p->w; sa.T = p->T; sa.precision = p->precision;
+    sa.Tq = h->d_Tq;
+    sa.dqc = dqc; sa.dqr = dqr; sa.qn = qn; sa.qsum = qsum;
+    sa.off = h->off.as<uint32_t>(); sa.pid = h->pid.as<int>(); sa.codes = h->codes.as<uint8_t>();
+    sa.dot_cr = h->dot_cr.as<float>();
+    sa.vterm = h->vterm.as<float>();
+    sa.ncells = (uint64_t)h->ncells;
+    sa.N = h->N;
+    sa.rec_key = rec_key; sa.rec_rank = rec_rank; sa.rec_cnt = rec_cnt;
+    sa.vis_cell = vis_cell; sa.vis_pre = vis_pre;
+    sa.cap_rec = NOALLOC_CELLS;
+    sa.pend = pend;
+    sa.pcap = NOALLOC_SURVIVORS;
+    sa.qcounter = counter;
+    sa.out_ids = d_ids; sa.out_d = d_dists; sa.out_sum = d_sums;
+    sa.out_nvis = nvis; sa.out_empty = empty;
+    sa.status = status;
+    sa.phase_cycles = nullptr;
+    if ((rc = search_launch(sa, grid, s))) return rc;
+    SCG_CUDA(cudaMemcpyAsync(h->h_status, status, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SCG_CUDA(cudaStreamSynchronize(s));
+    int st = *h->h_status;
+    if (st & ST_CELL_BUDGET)
+        return fail(SCG_ERR_CAP, "a query needs more than the allocation-free search's 8192 cells or survivors");
+    if (st & ST_TIE_OVERFLOW) return fail(SCG_ERR_CAP, "too many cells tie exactly at the cut key");
+    if (st & ST_ITER_CAP) return fail(SCG_ERR_CAP, "cell selection did not converge within its round cap");
+    if (st) return fail(SCG_ERR_CUDA, "search kernel reported status " + std::to_string(st));
+    return SCG_OK;
+}

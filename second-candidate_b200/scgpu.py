@@ -23,7 +23,8 @@ EXPORTS = ["scg_last_error", "scg_index_create", "scg_index_destroy", "scg_load_
            "scg_precompute", "scg_search", "scg_search_device", "scg_set_query_targets",
            "scg_set_cell_budget", "scg_encode", "scg_sc_encode", "scg_encode_device",
            "scg_index_info", "scg_last_query_stats", "scg_last_timings",
-           "scg_cell_counts", "scg_set_phase_counters", "scg_last_phase_counters"]
+           "scg_cell_counts", "scg_set_phase_counters", "scg_last_phase_counters",
+           "scg_search_device_noalloc"]
 
 
 class ScgError(RuntimeError):
@@ -149,6 +150,16 @@ class Index:
                                       ctypes.c_void_p(d_ids), ctypes.c_void_p(d_d),
                                       ctypes.c_void_p(d_sums),
                                       ctypes.c_void_p(stream) if stream else None))
+
+    def search_device_noalloc(self, mode, dQ_ptr, nq, R, w, T, d_ids, d_d, d_sums, stream=None,
+                              precision=FP32_EXACT, rerank=0):
+        """Device-buffer search that allocates nothing (scratch in a static
+        device array); same arguments as search_device."""
+        p = SearchParams(mode, R, w, T, precision, rerank)
+        _check(_lib.scg_search_device_noalloc(self._h, ctypes.byref(p), ctypes.c_void_p(dQ_ptr), nq,
+                                              ctypes.c_void_p(d_ids), ctypes.c_void_p(d_d),
+                                              ctypes.c_void_p(d_sums),
+                                              ctypes.c_void_p(stream) if stream else None))
 
     def set_query_targets(self, d_T_ptr):
         _check(_lib.scg_set_query_targets(self._h, ctypes.c_void_p(d_T_ptr) if d_T_ptr else None))
