@@ -27,11 +27,12 @@
 //      cell count for the w rule);
 //   3. cells tied at the cut key are taken in (rank1, rank2) order until the
 //      rule fires -- the order an exact priority queue yields.
-// The ADC scan then walks the visited cells' candidates, CPT per thread per
-// round with all loads issued before the sums, adds the table entries in
-// the reference's order, and keeps the R smallest (distance, id) pairs: a
-// threshold filter feeds a pending buffer that is sorted and merged into the
-// sorted top list (merge path) when it fills.
+// The ADC scan then scores the first WARMN candidates into shared memory;
+// their R-th smallest distance bounds the final R-th distance, so a
+// barrier-free warp-centric scan of the rest (warps claim chunks of
+// candidates, keep their own window of visited cells, and add the table
+// entries in the reference's order) keeps only candidates at or below that
+// bound, and one radix-select merge over them gives the R best.
 #include "scg_internal.cuh"
 
 namespace scg {
@@ -40,7 +41,6 @@ namespace {
 
 constexpr int NT = 256;
 constexpr int NWARP = NT / 32;
-constexpr int CPT = 8;          // candidates per thread per scan round
 constexpr int HBITS = 11;
 constexpr int HBINS = 1 << HBITS;
 constexpr int TIECAP = 64;
