@@ -25,7 +25,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import time
 
@@ -37,6 +36,13 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 METRIC = "QPS at recall@100 (BF16 batched vs FP32 plain vs CPU); p50/p99 latency"
 MODE_IDS = {"ivfadc": 0, "imi": 1, "sc": 2}
+# name -> (C ABI precision, description)
+PRECISIONS = {
+    "fp32": (0, "fp32-exact: CUDA-core tables in the reference's float order, the reference's ADC adds"),
+    "fast": (1, "bf16x3: tcgen05 BF16 hi/lo split tables (FP32 accumulation), fused per-vector term"),
+    "bf16": (2, "bf16: tcgen05 one-product BF16 tables (FP32 accumulation), fused per-vector term"),
+    "fp16": (3, "fp16: tcgen05 one-product FP16 tables (FP32 accumulation), fused per-vector term"),
+}
 
 
 def log(*a):
@@ -53,52 +59,69 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the
-    timed region."""
+    """SM clock and clock-event (throttle) reasons sampled through NVML every
+    few milliseconds by a thread, so that even a timed region of tens of
+    milliseconds holds samples.  mark() brackets the timed region; stop()
+    summarises the samples inside it (read-only NVML queries)."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
-    def __init__(self, gpu):
-        self.gpu = gpu
-        self.p = None
+    def __init__(self, gpu, period=0.004):
+        self.gpu, self.period = gpu, period
+        self.samples, self.t0, self.t1 = [], None, None
+        self.th, self.run, self.nv, self.err = None, False, None, None
 
     def start(self):
+        import threading
         try:
-            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
-                                       "--format=csv,noheader,nounits", "-lms", "100"],
-                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except Exception:
-            self.p = None
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception as ex:
+            self.err = repr(ex)
+            return
+        self.run = True
+        self.th = threading.Thread(target=self._loop, daemon=True)
+        self.th.start()
+
+    def _loop(self):
+        nv = self.nv
+        while self.run:
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.samples.append((time.perf_counter(), mhz, rs))
+            except Exception as ex:
+                self.err = repr(ex)
+            time.sleep(self.period)
+
+    def mark(self, begin):
+        if begin:
+            self.t0 = time.perf_counter()
+        else:
+            self.t1 = time.perf_counter()
 
     def stop(self):
-        if not self.p:
-            return None
-        self.p.terminate()
-        try:
-            out, _ = self.p.communicate(timeout=5)
-        except Exception:
-            self.p.kill()
-            out, _ = self.p.communicate()
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in out.splitlines():
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx.append(float(f[2]))
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        if not sm:
-            return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
-                "reasons": sorted(reasons)}
+        self.run = False
+        if self.th:
+            self.th.join(timeout=2)
+        if not self.samples:
+            return {"unavailable": self.err or "no samples"} if self.err else None
+        t0 = self.t0 if self.t0 is not None else self.samples[0][0]
+        t1 = self.t1 if self.t1 is not None else self.samples[-1][0]
+        inside = [x for x in self.samples if t0 <= x[0] <= t1] or self.samples
+        reasons = set()
+        for _, _, rs in inside:
+            for name, attr in self.REASONS:
+                if rs & getattr(self.nv, attr, 0):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(x[1] for x in inside), "sm_max_mhz": self.max_mhz,
+                "samples": len(inside), "reasons": sorted(reasons), "source": "NVML, %g ms period" % (1e3 * self.period)}
 
 
 def cpu_reference(w, seconds_target=12.0, threads=None, mode=None):
@@ -140,6 +163,62 @@ def cpu_reference(w, seconds_target=12.0, threads=None, mode=None):
             "seconds": sec, "recall@100": recall_at(ids, w["gt"][:n], min(100, R))}
 
 
+def serve_leg(scgpu, ix, w, mode, wcap, T, prec, batch_qps, seconds, load, seed=7):
+    """A request stream through the server (scg_server_*): Poisson arrivals,
+    each request a batch of 1..4096 queries (log-uniform) drawn from the
+    workload's queries with k in {1, 10, 100}; offered load = `load` x the
+    batch throughput.  Returns QPS (queries completed / span) and request
+    latency percentiles (submit to results on the host)."""
+    import threading
+    rng = np.random.default_rng(seed)
+    Q = w["Q"]
+    mean_batch = (4096 - 1) / np.log(4096)
+    rate = load * batch_qps / mean_batch  # requests per second
+    n = max(8, int(rate * seconds))
+    gaps = rng.exponential(1.0 / rate, n)
+    sizes = np.minimum(4096, np.exp(rng.uniform(0, np.log(4097), n)).astype(int))
+    ks = rng.choice([1, 10, 100], n)
+    starts = rng.integers(0, max(1, Q.shape[0] - 4096), n)
+    srv = scgpu.Server(ix, slots=4, max_batch=4096, max_R=100, arena_bytes=4 << 30)
+    # warm the slots once (first-use costs stay out of the measurement)
+    for t in [srv.submit(mode, Q[:64], 10, wcap, T, precision=prec) for _ in range(8)]:
+        srv.wait(t)
+    tickets = []
+    done = []
+
+    def waiter():
+        i = 0
+        while i < n:
+            if i >= len(tickets):
+                time.sleep(0.0002)
+                continue
+            r = srv.wait(tickets[i])
+            done.append(r[3])
+            i += 1
+
+    th = threading.Thread(target=waiter)
+    th.start()
+    t0 = time.perf_counter()
+    nxt = t0
+    for i in range(n):
+        nxt += gaps[i]
+        d = nxt - time.perf_counter()
+        if d > 0:
+            time.sleep(d)
+        s0 = int(starts[i])
+        tickets.append(srv.submit(mode, Q[s0:s0 + int(sizes[i])], int(ks[i]), wcap, T, precision=prec))
+    th.join()
+    span = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    lat = np.array(done)
+    return {"qps": float(sizes.sum() / span), "requests": int(n), "queries": int(sizes.sum()),
+            "offered_requests_per_s": float(rate), "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "max_inflight": st["max_inflight"], "slots": 4,
+            "what": "Poisson arrivals, batches 1..4096 log-uniform, k in {1,10,100}, continuous batching "
+                    "over 4 streams; latency = submit to results in host memory"}
+
+
 def workload_desc(cfg):
     if cfg["mode"] == "imi":
         idx = "IMI 2x%d, residual PQ %dx%d" % (cfg["kc"], cfg["mp"], cfg["kp"])
@@ -160,11 +239,15 @@ def main():
     ap.add_argument("--workload", default="C2")
     ap.add_argument("--cache", default="/tmp/scg_bench_cache")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--precision", default="fast", choices=["fast", "fp32"])
+    ap.add_argument("--precision", default="fast", choices=list(PRECISIONS))
     ap.add_argument("--queries", type=int, default=0, help="use only the first N queries")
     ap.add_argument("--no-plain", action="store_true", help="skip the FP32 plain comparison")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--phases", action="store_true", help="report per-phase cycle counters")
+    ap.add_argument("--serve-seconds", type=float, default=3.0,
+                    help="length of the serving leg (Poisson request stream); 0 skips it")
+    ap.add_argument("--serve-load", type=float, default=0.5,
+                    help="offered load of the serving leg as a fraction of the batch throughput")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -236,32 +319,37 @@ def main():
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
-    prec = scgpu.FAST if args.precision == "fast" else scgpu.FP32_EXACT
+    prec = PRECISIONS[args.precision][0]
 
     def step(p=None):
         ix.search_device(mode, dQ.data_ptr(), nq, R, wcap, T, d_ids.data_ptr(), d_d.data_ptr(),
                          d_s.data_ptr(), stream=stream.cuda_stream, precision=prec if p is None else p)
 
-    # the plain FP32 form (the reference's float order), for comparison
-    plain = None
-    if args.precision == "fast" and not args.no_plain:
-        for _ in range(2):
-            step(scgpu.FP32_EXACT)
-        torch.cuda.synchronize()
-        pt = []
-        for _ in range(3):
-            flush.zero_()
-            e0p = torch.cuda.Event(enable_timing=True)
-            e1p = torch.cuda.Event(enable_timing=True)
-            e0p.record(stream)
-            step(scgpu.FP32_EXACT)
-            e1p.record(stream)
-            e1p.synchronize()
-            pt.append(e0p.elapsed_time(e1p))
-        pids = d_ids.view(nq, R).cpu().numpy()
-        plain = {"value": nq / (statistics.mean(pt) / 1e3), "unit": "queries/s",
-                 "recall@100": W.recall_at(pids, w["gt"], min(100, R)), "ms_per_step": statistics.mean(pt),
-                 "kernels_ms": dict(zip(("tables", "select_scan"), ix.last_timings()))}
+    # every other arithmetic form on the same queries, for the comparison
+    # (QPS at recall@100): a few timed steps each
+    forms = {}
+    if not args.no_plain:
+        for name, (pv, desc) in PRECISIONS.items():
+            if name == args.precision:
+                continue
+            for _ in range(3):
+                step(pv)
+            torch.cuda.synchronize()
+            pt = []
+            for _ in range(3):
+                flush.zero_()
+                e0p = torch.cuda.Event(enable_timing=True)
+                e1p = torch.cuda.Event(enable_timing=True)
+                e0p.record(stream)
+                step(pv)
+                e1p.record(stream)
+                e1p.synchronize()
+                pt.append(e0p.elapsed_time(e1p))
+            pids = d_ids.view(nq, R).cpu().numpy()
+            forms[name] = {"value": nq / (statistics.mean(pt) / 1e3), "unit": "queries/s",
+                           "recall@100": W.recall_at(pids, w["gt"], min(100, R)),
+                           "ms_per_step": statistics.mean(pt), "what": desc,
+                           "kernels_ms": dict(zip(("tables", "select_scan"), ix.last_timings()))}
 
     for _ in range(args.warmup):
         step()
@@ -272,6 +360,7 @@ def main():
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    clocks.mark(True)
     times, kern = [], []
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -284,6 +373,7 @@ def main():
         times.append(e0.elapsed_time(e1))
         kern.append(ix.last_timings())
     torch.cuda.synchronize()
+    clocks.mark(False)
     if world > 1:
         dist.barrier()
     total_ms = sum(times)
@@ -341,17 +431,19 @@ def main():
         "metric": METRIC, "value": nq * args.steps * world / (total_ms / 1e3), "unit": "queries/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "vs_baseline": None, "dtype": {"fp32": "f32", "fast": "bf16", "bf16": "bf16", "fp16": "f16"}[args.precision],
+        "data": "synthetic",
         "config": {"workload": workload_desc(cfg),
-                   "precision": ("fast: FP32 tables + fused per-vector term" if args.precision == "fast"
-                                 else "fp32-exact (the reference's float order)"),
+                   "precision": PRECISIONS[args.precision][1],
                    "l2": "flushed between steps (256 MB write)", "parallelism": "replicas" if world > 1 else "1 GPU",
                    "timing": "CUDA events per step on the launching stream"},
         "recall@100": recall,
-        "fp32_plain": plain,
+        "fp32_plain": forms.get("fp32"),
+        "other_forms": {k: v for k, v in forms.items() if k != "fp32"},
         "phases": phases,
         "latency_ms": {"p50": float(np.percentile(times, 50)), "p99": float(np.percentile(times, 99)),
                        "what": "whole batch of %d queries" % nq},
+        "batch_ms": {"p50": float(np.percentile(times, 50)), "p99": float(np.percentile(times, 99))},
         "kernels_ms": {"tables": tables_ms, "select_scan": search_ms},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
@@ -363,6 +455,11 @@ def main():
         "clocks": ck,
         "candidates_per_query": float(sums.mean()), "cells_per_query": float(nvis.mean() + empty.mean()),
     }
+    if args.serve_seconds > 0:
+        line["serving"] = serve_leg(scgpu, ix, w, mode, wcap, T, prec, line["value"] / world, args.serve_seconds,
+                                    args.serve_load)
+        line["latency_ms"] = {"p50": line["serving"]["p50_ms"], "p99": line["serving"]["p99_ms"],
+                              "what": "per request of the serving leg"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_reference(w)

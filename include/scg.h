@@ -30,15 +30,20 @@ extern "C" {
 #define SCG_ERR_CUDA (-4)   /* CUDA runtime error                               */
 #define SCG_ERR_CAP (-5)    /* a per-query device budget was exceeded           */
 #define SCG_ERR_STATE (-6)  /* call order (e.g. search before codebooks/index)  */
+#define SCG_PENDING 1       /* scg_server_wait: the request has not finished     */
 
 /* Search modes: the three reference entry points. */
 #define SCG_IVFADC 0  /* PQQuery::search_ivfadc      query.h:202-325        */
 #define SCG_IMI 1     /* MultiQuery::search_multi2   multi_query.h:62-273   */
 #define SCG_SC2 2     /* SCQuery::search_mr_ivf      sc_query.h:60-256      */
 
-/* Arithmetic of the per-query tables and of the ADC sum. */
-#define SCG_FP32_EXACT 0 /* the reference's float operations in its order     */
-#define SCG_FAST 1       /* tensor-core tables, fused per-vector term         */
+/* Arithmetic of the per-query tables and of the ADC sum.  The three
+ * tensor-core forms build the tables as tcgen05 GEMMs with FP32 accumulation
+ * and use the fused per-vector ADC term in the scan. */
+#define SCG_FP32_EXACT 0 /* the reference's float operations in its order      */
+#define SCG_FAST 1       /* BF16 hi/lo split operands, 3 products: ~2^-15 relative */
+#define SCG_BF16 2       /* one BF16 product per term                          */
+#define SCG_FP16 3       /* one FP16 product per term (operands must fit FP16)  */
 
 typedef struct scg_index scg_index;
 
@@ -47,10 +52,12 @@ typedef struct {
     int R;          /* results per query (1..1024)                                 */
     int w;          /* cell cap: popped cells (IVFADC, IMI) or non-empty cells (SC) */
     int T;          /* candidate target: stop after the cell that reaches T         */
-    int precision;  /* SCG_FP32_EXACT or SCG_FAST                                   */
-    int rerank;     /* 0: ADC distances; -1: exact distance for every candidate
-                       (the reference's real_dist branch); L>0: ADC shortlist of L
-                       re-ranked by exact distance                                  */
+    int precision;  /* SCG_FP32_EXACT, SCG_FAST, SCG_BF16 or SCG_FP16                */
+    int rerank;     /* 0: ADC distances.  L > 0 (R <= L <= 1024): the ADC top-L
+                       shortlist re-ranked by the exact distance of the
+                       reference's real_dist branch (query.h:307-312), needs
+                       the raw vectors.  -1 (exact distance for every
+                       candidate) is refused with SCG_ERR_ARG.               */
 } scg_search_params;
 
 /* Message of the last failing call on this thread (always NUL-terminated). */
@@ -84,9 +91,13 @@ int scg_load_csr(scg_index *h, const int *L, const int *pid, const uint8_t *code
  * (query.cpp:82-165) and SCQuery::load_encoded_data (sc_query.cpp:36-123). */
 int scg_load_encoded_file(scg_index *h, const char *path, int nc);
 
-/* Raw vectors [N][dim] (float), for the exact-distance branch and re-rank.
- * Replaces PQQuery::load_data (query.h:82-86). */
+/* Raw vectors [N][dim] (float, row = the vector's id), for the shortlist
+ * re-rank.  Replaces PQQuery::load_data (query.h:82-86). */
 int scg_load_raw(scg_index *h, const float *X, int64_t N);
+
+/* The same for uint8 vectors (e.g. .bvecs data): the exact distances are
+ * those of their float copies, with a quarter of the device memory. */
+int scg_load_raw_u8(scg_index *h, const uint8_t *X, int64_t N);
 
 /* Query-independent tables: ||c||^2, ||r||^2, 2<c,r> and the per-vector ADC
  * term of the fast form.  Replaces PQQuery::pre_compute1 (query.h:91-149). */
@@ -121,10 +132,19 @@ int scg_search_device(scg_index *h, const scg_search_params *p, const float *dQ,
  * device address; make that first call before any stream capture.  Every
  * call shares the one array: calls that overlap on the GPU (other streams,
  * other threads, the same device) race and must be serialised by the caller.
- * The fast form (SCG_FAST) needs its per-vector term, built by an earlier
- * SCG_FAST call of scg_search or scg_search_device. */
+ * The tensor-core forms (SCG_FAST, SCG_BF16, SCG_FP16) need the per-vector
+ * term, built by an earlier call of scg_search or scg_search_device in one of
+ * them. */
 int scg_search_device_noalloc(scg_index *h, const scg_search_params *p, const float *dQ, int nq,
                               int *d_ids, float *d_dists, int *d_sums, void *stream);
+
+/* Batched pre_compute2 (query.h:154-184, with the sequencing of lines 167
+ * and 179 as intended): d_diff_qc[nq][mc*kc] = ||c||^2 - 2<q_part, c> and
+ * d_diff_qr[nq][mp*kp] = ||r||^2 - 2<q_sub, r>, device buffers, in the
+ * arithmetic of `precision` (SCG_FP32_EXACT: bit-identical to the
+ * reference). */
+int scg_query_tables_device(scg_index *h, int precision, const float *dQ, int nq,
+                            float *d_diff_qc, float *d_diff_qr, void *stream);
 
 /* Per-query candidate targets (device pointer to nq ints) for the next
  * scg_search_device call; NULL restores the single T of the parameters. */
@@ -156,7 +176,8 @@ int scg_last_query_stats(scg_index *h, int *nvis, int *empty, int nq);
 
 /* Device time in milliseconds of the kernels of the last search call,
  * measured with CUDA events on its stream: ms[0] the per-query tables,
- * ms[1] the fused selection + scan.  n is the capacity of ms. */
+ * ms[1] the fused selection + scan, ms[2] the shortlist re-rank (0 without
+ * one).  n is the capacity of ms. */
 int scg_last_timings(scg_index *h, float *ms, int n);
 
 /* Copies the cell lengths back as the reference's inclusive prefix L[ncells]
@@ -170,6 +191,43 @@ int scg_cell_counts(scg_index *h, int *L, int64_t ncells);
  * steps, [10] enumerated cells.  n is the capacity of out (<= 16). */
 int scg_set_phase_counters(scg_index *h, int on);
 int scg_last_phase_counters(scg_index *h, long long *out, int n);
+
+/* ------------------------------------------------------------------------
+ * Request loop with continuous batching.  No counterpart in the reference
+ * (its query objects serve one query per call on the calling thread).
+ *
+ * A server holds `slots` CUDA streams, each with its own search workspace,
+ * and a device arena of `arena_bytes` for per-request buffers (queries,
+ * tables, outputs).  Requests -- a batch of 1..max_batch queries with its own
+ * parameters (R <= max_R, T, w, precision, rerank) -- are submitted from any
+ * thread with HOST buffers that must stay valid until the request is waited
+ * for.  A worker thread admits requests in arrival order whenever a slot is
+ * free and the arena has room, runs them concurrently on the device, and
+ * completes them as their streams finish.  A request larger than the arena is
+ * refused at submit (SCG_ERR_CAP).  Results are identical to the same request
+ * alone.  The index must not be reloaded while a server runs on it. */
+typedef struct scg_server scg_server;
+
+int scg_server_create(scg_index *h, int slots, int max_batch, int max_R, size_t arena_bytes,
+                      scg_server **out);
+
+/* Queues a request; *ticket identifies it to scg_server_wait. */
+int scg_server_submit(scg_server *s, const scg_search_params *p, const float *Q, int nq,
+                      int *ids, float *dists, int *sums, uint64_t *ticket);
+
+/* Waits for a request (timeout_s < 0: without limit).  Returns its status,
+ * or SCG_PENDING if the timeout expired first (the ticket stays valid).  On
+ * completion *latency_ms (may be NULL) is the time from submit to the end of
+ * its copy-out, and the ticket is released. */
+int scg_server_wait(scg_server *s, uint64_t ticket, double timeout_s, double *latency_ms);
+
+/* Completed requests, the most requests ever in flight at once, and the
+ * requests waiting for a slot or memory now. */
+int scg_server_stats(scg_server *s, long long *completed, int *max_inflight, int *queued);
+
+/* Finishes every queued and running request, then frees the server.
+ * Tickets not yet waited for are released. */
+int scg_server_destroy(scg_server *s);
 
 /* Index facts: dim, mc, kc, mp, kp, N (any pointer may be NULL). */
 int scg_index_info(scg_index *h, int *dim, int *mc, int *kc, int *mp, int *kp, int64_t *N);

@@ -65,6 +65,7 @@ def lib():
         _lib.orc_search.restype = ctypes.c_int
         _lib.orc_distribution.restype = ctypes.c_int
         _lib.orc_distance_l2_square.restype = ctypes.c_double
+        _lib.orc_rerank.restype = ctypes.c_int
     return _lib
 
 
@@ -156,6 +157,28 @@ class Index:
             out_d[i, :m] = td[:m]
             sums[i] = r["sum"]
         return out_i, out_d, sums
+
+    def rerank(self, Q, ids, R):
+        """Shortlist re-rank (orc_rerank): ids[nq, L] (-1 = none) -> the R
+        smallest exact distances per query, (ids[nq,R] padded with -1,
+        dist[nq,R] padded with +inf)."""
+        if self.raw is None:
+            raise ValueError("raw vectors not given")
+        Q = np.ascontiguousarray(Q, np.float32).reshape(-1, self.dim)
+        ids = np.ascontiguousarray(ids, np.int32)
+        nq, L = ids.shape
+        out_i = np.full((nq, R), -1, np.int32)
+        out_d = np.full((nq, R), np.inf, np.float32)
+        ti = np.zeros(R, np.int32)
+        td = np.zeros(R, np.float32)
+        for i in range(nq):
+            q = np.ascontiguousarray(Q[i])
+            row = np.ascontiguousarray(ids[i])
+            m = lib().orc_rerank(_p(self.raw, _f32p), self.dim, _p(q, _f32p), _p(row, _i32p), L, R,
+                                 _p(ti, _i32p), _p(td, _f32p))
+            out_i[i, :m] = ti[:m]
+            out_d[i, :m] = td[:m]
+        return out_i, out_d
 
 
 def encode(cfg, cq, pq, X):

@@ -450,6 +450,23 @@ void orc_topk(const float *dist, const int *ids, int n, int R, float *out_d, int
     free(t);
 }
 
+int orc_rerank(const float *raw, int dim, const float *q, const int *ids, int L, int R,
+               int *out_ids, float *out_d) {
+    float *d = (float *)malloc(sizeof(float) * (size_t)(L > 0 ? L : 1));
+    int *v = (int *)malloc(sizeof(int) * (size_t)(L > 0 ? L : 1));
+    int n = 0;
+    for (int i = 0; i < L; i++) {
+        if (ids[i] < 0) continue;
+        d[n] = (float)orc_distance_l2_square(q, raw + (size_t)ids[i] * dim, dim);
+        v[n] = ids[i];
+        n++;
+    }
+    orc_topk(d, v, n, R, out_d, out_ids);
+    free(d);
+    free(v);
+    return n < R ? n : R;
+}
+
 /* Encoder::encode<T>, encoder.h:69-192: per part the first nearest coarse
  * centroid (double distances, strict '>'), the float residual, then per
  * subspace the first nearest PQ centroid. */

@@ -73,6 +73,14 @@ int orc_distribution(int mode, int kc, int mc, int nc, int mp, long n,
 
 double orc_distance_l2_square(const float *x, const float *y, int d);
 
+/* Shortlist re-rank: the exact distance of each of the L ids (ids < 0 are
+ * skipped) as the reference's real_dist branch computes it
+ * (query.h:307-312, multi_query.h:255-259, sc_query.h:232-236: the float of
+ * distance_l2_square against raw[id]), then the R smallest in (distance, id)
+ * order.  Returns the number written (<= R). */
+int orc_rerank(const float *raw, int dim, const float *q, const int *ids, int L, int R,
+               int *out_ids, float *out_d);
+
 #ifdef __cplusplus
 }
 #endif

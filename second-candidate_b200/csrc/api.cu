@@ -7,13 +7,14 @@
 #include <string>
 #include <vector>
 
-#include "scg_internal.cuh"
+#include "index.h"
 
 namespace scg {
 
 static thread_local std::string g_err;
 
 void set_error(const std::string &msg) { g_err = msg; }
+std::string last_error_string() { return g_err; }
 int fail(int code, const std::string &msg) {
     g_err = msg;
     return code;
@@ -23,58 +24,11 @@ int cuda_fail(cudaError_t e, const char *what) {
     return e == cudaErrorMemoryAllocation ? SCG_ERR_OOM : SCG_ERR_CUDA;
 }
 
-// Grow-only device buffer.
-struct DevBuf {
-    void *p = nullptr;
-    size_t n = 0;
-    int ensure(size_t bytes) {
-        if (bytes <= n) return SCG_OK;
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-        cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
-        n = bytes;
-        return SCG_OK;
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-    template <class T>
-    T *as() const {
-        return (T *)p;
-    }
-};
-
 }  // namespace scg
 
 using namespace scg;
 
-struct scg_index {
-    int device = 0;
-    int num_sms = 0;
-    cudaStream_t stream = nullptr;
-    int dim = 0, mc = 0, kc = 0, mp = 0, kp = 0;
-    int64_t N = 0;
-    int64_t ncells = 0;
-    bool have_codebooks = false, have_csr = false, precomputed = false;
-    int cap_rec = 131072;
-    const int *d_Tq = nullptr;
-    DevBuf cq, pq, norm_c, norm_r, dot_cr, off, pid, codes, raw, vterm;
-    bool have_vterm = false;
-    // batch workspace
-    DevBuf q, dqc, dqr, qn, qsum, ids, dists, sums, nvis, empty, status, counter;
-    DevBuf rec_key, rec_rank, rec_cnt, vis_cell, vis_pre, pend, phase;
-    bool phase_on = false;
-    int *h_status = nullptr;  // pinned
-    int last_nq = 0;
-    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
-    std::mutex mu;
-};
-
-namespace {
+namespace scg {
 
 int set_device(scg_index *h) {
     cudaError_t e = cudaSetDevice(h->device);
@@ -130,8 +84,14 @@ int check_params(scg_index *h, const scg_search_params *p, int nq) {
     if (!p) return fail(SCG_ERR_ARG, "null params");
     if (nq < 0) return fail(SCG_ERR_ARG, "nq < 0");
     if (p->R < 1 || p->R > 1024) return fail(SCG_ERR_ARG, "R must be in [1, 1024]");
-    if (p->precision != SCG_FP32_EXACT && p->precision != SCG_FAST) return fail(SCG_ERR_ARG, "unknown precision");
-    if (p->rerank != 0) return fail(SCG_ERR_ARG, "rerank not supported by this build");
+    if (p->precision < SCG_FP32_EXACT || p->precision > SCG_FP16) return fail(SCG_ERR_ARG, "unknown precision");
+    if (p->rerank < 0)
+        return fail(SCG_ERR_ARG, "rerank = -1 (exact distance for every candidate) is not served; "
+                                 "use a shortlist rerank = L (R <= L <= 1024)");
+    if (p->rerank > 0) {
+        if (p->rerank < p->R || p->rerank > 1024) return fail(SCG_ERR_ARG, "rerank shortlist L must be in [R, 1024]");
+        if (h->raw_rows < h->N) return fail(SCG_ERR_STATE, "re-rank needs the raw vectors (scg_load_raw)");
+    }
     switch (p->mode) {
         case SCG_IVFADC:
             if (h->mc != 1 || h->ncells != h->kc) return fail(SCG_ERR_ARG, "This search method is for IVFADC only");
@@ -151,97 +111,228 @@ int check_params(scg_index *h, const scg_search_params *p, int nq) {
     return SCG_OK;
 }
 
-int run_search(scg_index *h, const scg_search_params *p, const float *dQ, int nq, int *d_ids, float *d_d,
-               int *d_sums, cudaStream_t s) {
+// Per-query tables in the requested arithmetic: the reference's float order
+// on CUDA cores, or tcgen05 tensor-core GEMMs (BF16 hi/lo split, one BF16 or
+// one FP16 product; FP32 accumulation).
+void launch_tables(const TablesArgs &ta, int precision, cudaStream_t s) {
+    switch (precision) {
+        case SCG_FAST: launch_tables_tc(ta, 3, 1, s); break;
+        case SCG_BF16: launch_tables_tc(ta, 1, 1, s); break;
+        case SCG_FP16: launch_tables_tc(ta, 1, 0, s); break;
+        default: launch_tables_exact(ta, s); break;
+    }
+}
+
+// The scan's form: exact (the reference's adds) or the fast per-vector form.
+int scan_form(int precision) { return precision == SCG_FP32_EXACT ? SCG_FP32_EXACT : SCG_FAST; }
+
+int status_result(int st) {
+    if (st & ST_CELL_BUDGET)
+        return fail(SCG_ERR_CAP, "a query enumerated more cells than the cell budget; raise it with scg_set_cell_budget");
+    if (st & ST_TIE_OVERFLOW) return fail(SCG_ERR_CAP, "too many cells tie exactly at the cut key");
+    if (st & ST_ITER_CAP) return fail(SCG_ERR_CAP, "cell selection did not converge within its round cap");
+    if (st & ST_TC_TIMEOUT) return fail(SCG_ERR_CUDA, "a tensor-core table tile did not complete in time");
+    if (st & ST_BAD_ARG) return fail(SCG_ERR_ARG, "a shortlisted id has no raw vector");
+    if (st) return fail(SCG_ERR_CUDA, "search kernel reported status " + std::to_string(st));
+    return SCG_OK;
+}
+
+int Workspace::init() {
+    cudaError_t e = cudaSuccess;
+    if (!h_status) e = cudaMallocHost((void **)&h_status, sizeof(int) * 4);
+    for (int i = 0; i < 4 && e == cudaSuccess; i++)
+        if (!ev[i]) e = cudaEventCreate(&ev[i]);
+    if (e != cudaSuccess) return cuda_fail(e, "workspace");
+    return SCG_OK;
+}
+
+void Workspace::release() {
+    DevBuf *all[] = {&dqc, &dqr, &qn, &qsum, &nvis, &empty, &status, &counter, &rec_key, &rec_rank,
+                     &rec_cnt, &vis_cell, &vis_pre, &pend, &phase, &sl_ids, &sl_d};
+    for (DevBuf *b : all) b->release();
+    if (h_status) cudaFreeHost(h_status);
+    h_status = nullptr;
+    for (int i = 0; i < 4; i++)
+        if (ev[i]) cudaEventDestroy(ev[i]);
+    for (int i = 0; i < 4; i++) ev[i] = nullptr;
+}
+
+static size_t up256b(size_t x) { return (x + 255) & ~(size_t)255; }
+
+size_t req_bytes(int nq, int dim, int mc, int kc, int mp, int kp, int R, int rerank) {
+    (void)dim;
+    (void)R;
+    size_t b = up256b(4ull * nq * mc * kc) + up256b(4ull * nq * mp * kp) + up256b(8ull * nq) + up256b(4ull * nq) +
+               2 * up256b(4ull * nq);
+    if (rerank > 0) b += 2 * up256b(4ull * nq * rerank);
+    return b;
+}
+
+ReqBufs carve_req(unsigned char *base, int nq, int mc, int kc, int mp, int kp, int rerank) {
+    ReqBufs r;
+    unsigned char *cur = base;
+    auto take = [&](size_t bytes) {
+        unsigned char *p = cur;
+        cur += up256b(bytes);
+        return p;
+    };
+    r.dqc = (float *)take(4ull * nq * mc * kc);
+    r.dqr = (float *)take(4ull * nq * mp * kp);
+    r.qn = (float *)take(8ull * nq);
+    r.qsum = (float *)take(4ull * nq);
+    r.nvis = (int *)take(4ull * nq);
+    r.empty = (int *)take(4ull * nq);
+    r.sl_ids = nullptr;
+    r.sl_d = nullptr;
+    if (rerank > 0) {
+        r.sl_ids = (int *)take(4ull * nq * rerank);
+        r.sl_d = (float *)take(4ull * nq * rerank);
+    }
+    return r;
+}
+
+int ensure_vterm(scg_index *h, cudaStream_t s) {
+    if (h->have_vterm) return SCG_OK;
     int rc;
-    const int R = p->R;
-    if ((rc = h->dqc.ensure(sizeof(float) * (size_t)nq * h->mc * h->kc))) return rc;
-    if ((rc = h->dqr.ensure(sizeof(float) * (size_t)nq * h->mp * h->kp))) return rc;
-    if ((rc = h->qn.ensure(sizeof(float) * (size_t)nq * 2))) return rc;
-    if ((rc = h->qsum.ensure(sizeof(float) * (size_t)nq))) return rc;
-    if ((rc = h->nvis.ensure(sizeof(int) * (size_t)nq))) return rc;
-    if ((rc = h->empty.ensure(sizeof(int) * (size_t)nq))) return rc;
-    if ((rc = h->status.ensure(sizeof(int) * 4))) return rc;
-    if ((rc = h->counter.ensure(sizeof(int) * 4))) return rc;
+    // the fast form's per-vector term (one float per database vector)
+    if ((rc = h->vterm.ensure(sizeof(float) * (size_t)(h->N ? h->N : 1)))) return rc;
+    launch_vterm(index_mode(h), h->kc, h->mp, h->kp, h->mc,
+                 (uint64_t)h->ncells, h->N, h->off.as<uint32_t>(), h->codes.as<uint8_t>(), h->norm_r.as<float>(),
+                 h->dot_cr.as<float>(), h->vterm.as<float>(), s);
+    SCG_CUDA(cudaGetLastError());
+    SCG_CUDA(cudaStreamSynchronize(s));
+    h->have_vterm = true;
+    return SCG_OK;
+}
+
+int reserve_search(scg_index *h, Workspace *ws, int mode, int grid) {
+    int rc;
+    if ((rc = ws->init())) return rc;
+    int per_sm = search_max_blocks_per_sm(mode, h->kc, h->mp, h->kp);
+    if (per_sm < 1) return fail(SCG_ERR_ARG, "search kernel does not fit on an SM for this shape");
+    if (grid <= 0 || grid > h->num_sms * per_sm) grid = h->num_sms * per_sm;
+    const size_t slot = (size_t)h->cap_rec, pcap = slot > 65536 ? slot : 65536;
+    if ((rc = ws->status.ensure(sizeof(int) * 4))) return rc;
+    if ((rc = ws->counter.ensure(sizeof(int) * 4))) return rc;
+    if ((rc = ws->rec_key.ensure(4 * slot * grid))) return rc;
+    if ((rc = ws->rec_rank.ensure(4 * slot * grid))) return rc;
+    if ((rc = ws->rec_cnt.ensure(4 * slot * grid))) return rc;
+    if ((rc = ws->vis_cell.ensure(4 * (slot + 1) * grid))) return rc;
+    if ((rc = ws->vis_pre.ensure(4 * (slot + 1) * grid))) return rc;
+    if ((rc = ws->pend.ensure(8 * pcap * grid))) return rc;
+    return SCG_OK;
+}
+
+int index_mode(const scg_index *h) {
+    return h->mc == 2 ? SCG_IMI : (h->ncells == h->kc ? SCG_IVFADC : SCG_SC2);
+}
+
+int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_params *p, const float *dQ, int nq,
+               int *d_ids, float *d_d, int *d_sums, cudaStream_t s, bool wait) {
+    int rc;
+    if ((rc = ws->init())) return rc;
+    // with a shortlist re-rank the ADC search keeps L candidates per query
+    const bool rr = p->rerank > 0;
+    const int R = rr ? p->rerank : p->R;
+    ReqBufs b;
+    if (rb) {
+        b = *rb;
+    } else {
+        if ((rc = ws->dqc.ensure(sizeof(float) * (size_t)nq * h->mc * h->kc))) return rc;
+        if ((rc = ws->dqr.ensure(sizeof(float) * (size_t)nq * h->mp * h->kp))) return rc;
+        if ((rc = ws->qn.ensure(sizeof(float) * (size_t)nq * 2))) return rc;
+        if ((rc = ws->qsum.ensure(sizeof(float) * (size_t)nq))) return rc;
+        if ((rc = ws->nvis.ensure(sizeof(int) * (size_t)nq))) return rc;
+        if ((rc = ws->empty.ensure(sizeof(int) * (size_t)nq))) return rc;
+        b.dqc = ws->dqc.as<float>(); b.dqr = ws->dqr.as<float>();
+        b.qn = ws->qn.as<float>(); b.qsum = ws->qsum.as<float>();
+        b.nvis = ws->nvis.as<int>(); b.empty = ws->empty.as<int>();
+        b.sl_ids = nullptr; b.sl_d = nullptr;
+        if (rr) {
+            if ((rc = ws->sl_ids.ensure(sizeof(int) * (size_t)nq * R))) return rc;
+            if ((rc = ws->sl_d.ensure(sizeof(float) * (size_t)nq * R))) return rc;
+            b.sl_ids = ws->sl_ids.as<int>(); b.sl_d = ws->sl_d.as<float>();
+        }
+    }
+    int *s_ids = rr ? b.sl_ids : d_ids;
+    float *s_d = rr ? b.sl_d : d_d;
+    if ((rc = ws->status.ensure(sizeof(int) * 4))) return rc;
+    if ((rc = ws->counter.ensure(sizeof(int) * 4))) return rc;
     int per_sm = search_max_blocks_per_sm(p->mode, h->kc, h->mp, h->kp);
     if (per_sm < 1) return fail(SCG_ERR_ARG, "search kernel does not fit on an SM for this shape");
     int grid = h->num_sms * per_sm;
     if (grid > nq) grid = nq;
     if (grid < 1) grid = 1;
     size_t slot = (size_t)h->cap_rec;
-    if ((rc = h->rec_key.ensure(4 * slot * grid))) return rc;
-    if ((rc = h->rec_rank.ensure(4 * slot * grid))) return rc;
-    if ((rc = h->rec_cnt.ensure(4 * slot * grid))) return rc;
-    if ((rc = h->vis_cell.ensure(4 * (slot + 1) * grid))) return rc;
-    if ((rc = h->vis_pre.ensure(4 * (slot + 1) * grid))) return rc;
+    if ((rc = ws->rec_key.ensure(4 * slot * grid))) return rc;
+    if ((rc = ws->rec_rank.ensure(4 * slot * grid))) return rc;
+    if ((rc = ws->rec_cnt.ensure(4 * slot * grid))) return rc;
+    if ((rc = ws->vis_cell.ensure(4 * (slot + 1) * grid))) return rc;
+    if ((rc = ws->vis_pre.ensure(4 * (slot + 1) * grid))) return rc;
     // survivors of the scan's threshold, per resident CTA
     const size_t pcap = slot > 65536 ? slot : 65536;
-    if ((rc = h->pend.ensure(8 * pcap * grid))) return rc;
+    if ((rc = ws->pend.ensure(8 * pcap * grid))) return rc;
 
-    if (p->precision == SCG_FAST && !h->have_vterm) {
-        // the fast form's per-vector term (one float per database vector)
-        if ((rc = h->vterm.ensure(sizeof(float) * (size_t)(h->N ? h->N : 1)))) return rc;
-        launch_vterm(p->mode, h->kc, h->mp, h->kp, h->mc, (uint64_t)h->ncells, h->N, h->off.as<uint32_t>(),
-                     h->codes.as<uint8_t>(), h->norm_r.as<float>(), h->dot_cr.as<float>(), h->vterm.as<float>(), s);
-        SCG_CUDA(cudaGetLastError());
-        h->have_vterm = true;
-    }
+    if (scan_form(p->precision) == SCG_FAST && (rc = ensure_vterm(h, s))) return rc;
     TablesArgs ta;
     ta.dim = h->dim; ta.mc = h->mc; ta.kc = h->kc; ta.mp = h->mp; ta.kp = h->kp; ta.nq = nq;
     ta.Q = dQ;
     ta.cq = h->cq.as<float>(); ta.pq = h->pq.as<float>();
     ta.norm_c = h->norm_c.as<float>(); ta.norm_r = h->norm_r.as<float>();
-    ta.dqc = h->dqc.as<float>(); ta.dqr = h->dqr.as<float>();
-    ta.qn = h->qn.as<float>(); ta.qsum = h->qsum.as<float>();
-    ta.fast = p->precision == SCG_FAST;
-    SCG_CUDA(cudaEventRecord(h->ev[0], s));
-    launch_tables_exact(ta, s);
-    SCG_CUDA(cudaEventRecord(h->ev[1], s));
+    ta.dqc = b.dqc; ta.dqr = b.dqr;
+    ta.qn = b.qn; ta.qsum = b.qsum;
+    ta.lut_only = scan_form(p->precision) == SCG_FAST;
+    ta.status = ws->status.as<int>();
+    SCG_CUDA(cudaMemsetAsync(ws->status.p, 0, sizeof(int) * 4, s));
+    SCG_CUDA(cudaMemsetAsync(ws->counter.p, 0, sizeof(int) * 4, s));
+    SCG_CUDA(cudaEventRecord(ws->ev[0], s));
+    launch_tables(ta, p->precision, s);
+    SCG_CUDA(cudaEventRecord(ws->ev[1], s));
 
-    SCG_CUDA(cudaMemsetAsync(h->status.p, 0, sizeof(int) * 4, s));
-    SCG_CUDA(cudaMemsetAsync(h->counter.p, 0, sizeof(int) * 4, s));
     SearchArgs sa;
     memset(&sa, 0, sizeof(sa));
     sa.mode = p->mode; sa.dim = h->dim; sa.mc = h->mc; sa.kc = h->kc; sa.mp = h->mp; sa.kp = h->kp;
-    sa.nq = nq; sa.R = R; sa.w = p->w; sa.T = p->T; sa.precision = p->precision;
-    sa.Tq = h->d_Tq;
-    sa.dqc = ta.dqc; sa.dqr = ta.dqr; sa.qn = ta.qn; sa.qsum = ta.qsum;
+    sa.nq = nq; sa.R = R; sa.w = p->w; sa.T = p->T; sa.precision = scan_form(p->precision);
+    sa.Tq = rb ? nullptr : h->d_Tq;
+    sa.dqc = b.dqc; sa.dqr = b.dqr; sa.qn = b.qn; sa.qsum = b.qsum;
     sa.off = h->off.as<uint32_t>(); sa.pid = h->pid.as<int>(); sa.codes = h->codes.as<uint8_t>();
     sa.dot_cr = h->dot_cr.as<float>();
     sa.vterm = h->vterm.as<float>();
     sa.ncells = (uint64_t)h->ncells;
     sa.N = h->N;
-    sa.rec_key = h->rec_key.as<uint32_t>(); sa.rec_rank = h->rec_rank.as<uint32_t>();
-    sa.rec_cnt = h->rec_cnt.as<uint32_t>();
-    sa.vis_cell = h->vis_cell.as<uint32_t>(); sa.vis_pre = h->vis_pre.as<uint32_t>();
+    sa.rec_key = ws->rec_key.as<uint32_t>(); sa.rec_rank = ws->rec_rank.as<uint32_t>();
+    sa.rec_cnt = ws->rec_cnt.as<uint32_t>();
+    sa.vis_cell = ws->vis_cell.as<uint32_t>(); sa.vis_pre = ws->vis_pre.as<uint32_t>();
     sa.cap_rec = h->cap_rec;
-    sa.pend = h->pend.as<uint64_t>();
+    sa.pend = ws->pend.as<uint64_t>();
     sa.pcap = (uint32_t)pcap;
-    sa.qcounter = h->counter.as<int>();
-    sa.out_ids = d_ids; sa.out_d = d_d; sa.out_sum = d_sums;
-    sa.out_nvis = h->nvis.as<int>(); sa.out_empty = h->empty.as<int>();
-    sa.status = h->status.as<int>();
+    sa.qcounter = ws->counter.as<int>();
+    sa.out_ids = s_ids; sa.out_d = s_d; sa.out_sum = d_sums;
+    sa.out_nvis = b.nvis; sa.out_empty = b.empty;
+    sa.status = ws->status.as<int>();
     sa.phase_cycles = nullptr;
-    if (h->phase_on) {
-        if ((rc = h->phase.ensure(sizeof(long long) * 16))) return rc;
-        SCG_CUDA(cudaMemsetAsync(h->phase.p, 0, sizeof(long long) * 16, s));
-        sa.phase_cycles = h->phase.as<long long>();
+    if (ws->phase_on) {
+        if ((rc = ws->phase.ensure(sizeof(long long) * 16))) return rc;
+        SCG_CUDA(cudaMemsetAsync(ws->phase.p, 0, sizeof(long long) * 16, s));
+        sa.phase_cycles = ws->phase.as<long long>();
     }
     if (nq > 0 && (rc = search_launch(sa, grid, s))) return rc;
-    SCG_CUDA(cudaEventRecord(h->ev[2], s));
-    h->last_nq = nq;
-    SCG_CUDA(cudaMemcpyAsync(h->h_status, h->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SCG_CUDA(cudaEventRecord(ws->ev[2], s));
+    if (rr && nq > 0) {
+        if (rerank_smem_bytes(R, h->dim) > 227 * 1024) return fail(SCG_ERR_ARG, "dimension too large for the re-rank");
+        launch_rerank(dQ, nq, h->dim, h->raw.p, h->raw_u8 ? 1 : 0, h->raw_rows, s_ids, R, p->R, d_ids, d_d,
+                      ws->status.as<int>(), s);
+        SCG_CUDA(cudaGetLastError());
+    }
+    SCG_CUDA(cudaEventRecord(ws->ev[3], s));
+    ws->last_nq = nq;
+    SCG_CUDA(cudaMemcpyAsync(ws->h_status, ws->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    if (!wait) return SCG_OK;
     SCG_CUDA(cudaStreamSynchronize(s));
-    int st = *h->h_status;
-    if (st & ST_CELL_BUDGET)
-        return fail(SCG_ERR_CAP, "a query enumerated more cells than the cell budget; raise it with scg_set_cell_budget");
-    if (st & ST_TIE_OVERFLOW) return fail(SCG_ERR_CAP, "too many cells tie exactly at the cut key");
-    if (st & ST_ITER_CAP) return fail(SCG_ERR_CAP, "cell selection did not converge within its round cap");
-    if (st) return fail(SCG_ERR_CUDA, "search kernel reported status " + std::to_string(st));
-    return SCG_OK;
+    return status_result(*ws->h_status);
 }
 
-}  // namespace
+}  // namespace scg
 
 extern "C" {
 
@@ -263,11 +354,16 @@ int scg_index_create(scg_index **out, int device) {
     e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_status, sizeof(int) * 4);
-    for (int i = 0; i < 3 && e == cudaSuccess; i++) e = cudaEventCreate(&h->ev[i]);
     if (e != cudaSuccess) {
         delete h;
         return cuda_fail(e, "scg_index_create");
+    }
+    int rc = h->ws.init();
+    if (rc) {
+        h->ws.release();
+        cudaStreamDestroy(h->stream);
+        delete h;
+        return rc;
     }
     *out = h;
     return SCG_OK;
@@ -278,13 +374,9 @@ int scg_index_destroy(scg_index *h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     DevBuf *all[] = {&h->cq, &h->pq, &h->norm_c, &h->norm_r, &h->dot_cr, &h->off, &h->pid, &h->codes,
-                     &h->raw, &h->vterm, &h->q, &h->dqc, &h->dqr, &h->qn, &h->qsum, &h->ids, &h->dists, &h->sums,
-                     &h->nvis, &h->empty, &h->status, &h->counter, &h->rec_key, &h->rec_rank,
-                     &h->rec_cnt, &h->vis_cell, &h->vis_pre, &h->pend, &h->phase};
+                     &h->raw, &h->vterm, &h->q, &h->ids, &h->dists, &h->sums};
     for (DevBuf *b : all) b->release();
-    if (h->h_status) cudaFreeHost(h->h_status);
-    for (int i = 0; i < 3; i++)
-        if (h->ev[i]) cudaEventDestroy(h->ev[i]);
+    h->ws.release();
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return SCG_OK;
@@ -394,16 +486,24 @@ int scg_load_encoded_file(scg_index *h, const char *path, int nc) {
     return scg_load_csr(h, L.data(), pid.data(), codes.data(), N, ncells);
 }
 
-int scg_load_raw(scg_index *h, const float *X, int64_t N) {
-    if (!h || !X) return fail(SCG_ERR_ARG, "null argument");
+static int load_raw(scg_index *h, const void *X, int64_t N, size_t elem, bool u8) {
+    if (!h || (N > 0 && !X)) return fail(SCG_ERR_ARG, "null argument");
+    if (N < 0) return fail(SCG_ERR_ARG, "N < 0");
     if (!h->have_codebooks) return fail(SCG_ERR_STATE, "load codebooks first");
     std::lock_guard<std::mutex> g(h->mu);
     int rc;
     if ((rc = set_device(h))) return rc;
-    if ((rc = h->raw.ensure(sizeof(float) * (size_t)N * h->dim))) return rc;
-    SCG_CUDA(cudaMemcpy(h->raw.p, X, sizeof(float) * (size_t)N * h->dim, cudaMemcpyHostToDevice));
+    const size_t bytes = elem * (size_t)N * h->dim;
+    if ((rc = h->raw.ensure(bytes ? bytes : 16))) return rc;
+    if (bytes) SCG_CUDA(cudaMemcpy(h->raw.p, X, bytes, cudaMemcpyHostToDevice));
+    h->raw_rows = N;
+    h->raw_u8 = u8;
     return SCG_OK;
 }
+
+int scg_load_raw(scg_index *h, const float *X, int64_t N) { return load_raw(h, X, N, sizeof(float), false); }
+
+int scg_load_raw_u8(scg_index *h, const uint8_t *X, int64_t N) { return load_raw(h, X, N, 1, true); }
 
 int scg_precompute(scg_index *h) {
     if (!h) return fail(SCG_ERR_ARG, "null index");
@@ -432,7 +532,7 @@ int scg_search_device(scg_index *h, const scg_search_params *p, const float *dQ,
     std::lock_guard<std::mutex> g(h->mu);
     if ((rc = set_device(h))) return rc;
     cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
-    return run_search(h, p, dQ, nq, d_ids, d_dists, d_sums, s);
+    return run_search(h, &h->ws, nullptr, p, dQ, nq, d_ids, d_dists, d_sums, s, true);
 }
 
 int scg_search(scg_index *h, const scg_search_params *p, const float *Q, int nq, int *ids, float *dists, int *sums) {
@@ -452,13 +552,47 @@ int scg_search(scg_index *h, const scg_search_params *p, const float *Q, int nq,
     SCG_CUDA(cudaMemcpyAsync(h->q.p, Q, sizeof(float) * (size_t)nq * h->dim, cudaMemcpyHostToDevice, s));
     const int *saved = h->d_Tq;
     h->d_Tq = nullptr;
-    rc = run_search(h, p, h->q.as<float>(), nq, h->ids.as<int>(), h->dists.as<float>(), h->sums.as<int>(), s);
+    rc = run_search(h, &h->ws, nullptr, p, h->q.as<float>(), nq, h->ids.as<int>(), h->dists.as<float>(),
+                    h->sums.as<int>(), s, true);
     h->d_Tq = saved;
     if (rc) return rc;
     SCG_CUDA(cudaMemcpyAsync(ids, h->ids.p, sizeof(int) * (size_t)nq * R, cudaMemcpyDeviceToHost, s));
     SCG_CUDA(cudaMemcpyAsync(dists, h->dists.p, sizeof(float) * (size_t)nq * R, cudaMemcpyDeviceToHost, s));
     if (sums) SCG_CUDA(cudaMemcpyAsync(sums, h->sums.p, sizeof(int) * (size_t)nq, cudaMemcpyDeviceToHost, s));
     SCG_CUDA(cudaStreamSynchronize(s));
+    return SCG_OK;
+}
+
+int scg_query_tables_device(scg_index *h, int precision, const float *dQ, int nq, float *d_diff_qc, float *d_diff_qr,
+                            void *stream) {
+    if (!h) return fail(SCG_ERR_ARG, "null index");
+    if (!h->have_codebooks) return fail(SCG_ERR_STATE, "codebooks not loaded");
+    if (!h->precomputed) return fail(SCG_ERR_STATE, "scg_precompute not called");
+    if (precision < SCG_FP32_EXACT || precision > SCG_FP16) return fail(SCG_ERR_ARG, "unknown precision");
+    if (nq < 0) return fail(SCG_ERR_ARG, "nq < 0");
+    if (nq > 0 && (!dQ || !d_diff_qc || !d_diff_qr)) return fail(SCG_ERR_ARG, "null buffer");
+    std::lock_guard<std::mutex> g(h->mu);
+    int rc;
+    if ((rc = set_device(h))) return rc;
+    if (nq == 0) return SCG_OK;
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+    if ((rc = h->ws.status.ensure(sizeof(int) * 4))) return rc;
+    SCG_CUDA(cudaMemsetAsync(h->ws.status.p, 0, sizeof(int) * 4, s));
+    TablesArgs ta;
+    memset(&ta, 0, sizeof(ta));
+    ta.dim = h->dim; ta.mc = h->mc; ta.kc = h->kc; ta.mp = h->mp; ta.kp = h->kp; ta.nq = nq;
+    ta.Q = dQ;
+    ta.cq = h->cq.as<float>(); ta.pq = h->pq.as<float>();
+    ta.norm_c = h->norm_c.as<float>(); ta.norm_r = h->norm_r.as<float>();
+    ta.dqc = d_diff_qc; ta.dqr = d_diff_qr;
+    ta.qn = nullptr; ta.qsum = nullptr;
+    ta.lut_only = 0;
+    ta.status = h->ws.status.as<int>();
+    launch_tables(ta, precision, s);
+    SCG_CUDA(cudaGetLastError());
+    SCG_CUDA(cudaMemcpyAsync(h->ws.h_status, h->ws.status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SCG_CUDA(cudaStreamSynchronize(s));
+    if (*h->ws.h_status) return status_result(*h->ws.h_status);
     return SCG_OK;
 }
 
@@ -536,25 +670,26 @@ int scg_sc_encode(scg_index *h, const float *X, int64_t n, int nc, uint16_t *cid
 
 int scg_last_query_stats(scg_index *h, int *nvis, int *empty, int nq) {
     if (!h) return fail(SCG_ERR_ARG, "null index");
-    if (nq < 0 || nq > h->last_nq) return fail(SCG_ERR_ARG, "nq exceeds the last search's batch");
+    if (nq < 0 || nq > h->ws.last_nq) return fail(SCG_ERR_ARG, "nq exceeds the last search's batch");
     std::lock_guard<std::mutex> g(h->mu);
     int rc;
     if ((rc = set_device(h))) return rc;
-    if (nvis && nq) SCG_CUDA(cudaMemcpy(nvis, h->nvis.p, sizeof(int) * (size_t)nq, cudaMemcpyDeviceToHost));
-    if (empty && nq) SCG_CUDA(cudaMemcpy(empty, h->empty.p, sizeof(int) * (size_t)nq, cudaMemcpyDeviceToHost));
+    if (nvis && nq) SCG_CUDA(cudaMemcpy(nvis, h->ws.nvis.p, sizeof(int) * (size_t)nq, cudaMemcpyDeviceToHost));
+    if (empty && nq) SCG_CUDA(cudaMemcpy(empty, h->ws.empty.p, sizeof(int) * (size_t)nq, cudaMemcpyDeviceToHost));
     return SCG_OK;
 }
 
 int scg_last_timings(scg_index *h, float *ms, int n) {
     if (!h || !ms) return fail(SCG_ERR_ARG, "null argument");
-    if (h->last_nq <= 0) return fail(SCG_ERR_STATE, "no search has run");
+    if (h->ws.last_nq <= 0) return fail(SCG_ERR_STATE, "no search has run");
     std::lock_guard<std::mutex> g(h->mu);
     int rc;
     if ((rc = set_device(h))) return rc;
-    float t[2];
-    SCG_CUDA(cudaEventElapsedTime(&t[0], h->ev[0], h->ev[1]));
-    SCG_CUDA(cudaEventElapsedTime(&t[1], h->ev[1], h->ev[2]));
-    for (int i = 0; i < n && i < 2; i++) ms[i] = t[i];
+    float t[3];
+    SCG_CUDA(cudaEventElapsedTime(&t[0], h->ws.ev[0], h->ws.ev[1]));
+    SCG_CUDA(cudaEventElapsedTime(&t[1], h->ws.ev[1], h->ws.ev[2]));
+    SCG_CUDA(cudaEventElapsedTime(&t[2], h->ws.ev[2], h->ws.ev[3]));
+    for (int i = 0; i < n && i < 3; i++) ms[i] = t[i];
     return SCG_OK;
 }
 
@@ -571,18 +706,18 @@ int scg_cell_counts(scg_index *h, int *L, int64_t ncells) {
 
 int scg_set_phase_counters(scg_index *h, int on) {
     if (!h) return fail(SCG_ERR_ARG, "null index");
-    h->phase_on = on != 0;
+    h->ws.phase_on = on != 0;
     return SCG_OK;
 }
 
 int scg_last_phase_counters(scg_index *h, long long *out, int n) {
     if (!h || !out) return fail(SCG_ERR_ARG, "null argument");
-    if (!h->phase_on || !h->phase.p) return fail(SCG_ERR_STATE, "phase counters are off");
+    if (!h->ws.phase_on || !h->ws.phase.p) return fail(SCG_ERR_STATE, "phase counters are off");
     std::lock_guard<std::mutex> g(h->mu);
     int rc;
     if ((rc = set_device(h))) return rc;
     long long tmp[16];
-    SCG_CUDA(cudaMemcpy(tmp, h->phase.p, sizeof(tmp), cudaMemcpyDeviceToHost));
+    SCG_CUDA(cudaMemcpy(tmp, h->ws.phase.p, sizeof(tmp), cudaMemcpyDeviceToHost));
     for (int i = 0; i < n && i < 16; i++) out[i] = tmp[i];
     return SCG_OK;
 }
@@ -650,9 +785,10 @@ extern "C" int scg_search_device_noalloc(scg_index *h, const scg_search_params *
     if ((rc = check_ready(h))) return rc;
     if ((rc = check_params(h, p, nq))) return rc;
     if (nq > 0 && (!dQ || !d_ids || !d_dists || !d_sums)) return fail(SCG_ERR_ARG, "null buffer");
-    if (p->precision == SCG_FAST && !h->have_vterm)
+    if (p->rerank != 0) return fail(SCG_ERR_ARG, "the allocation-free search does not re-rank (rerank must be 0)");
+    if (scan_form(p->precision) == SCG_FAST && !h->have_vterm)
         return fail(SCG_ERR_STATE,
-                    "the fast form's per-vector term is built by the first SCG_FAST call of scg_search or "
+                    "the per-vector term of the tensor-core forms is built by their first call of scg_search or "
                     "scg_search_device; make one before searching without allocation");
     std::lock_guard<std::mutex> g(h->mu);
     if ((rc = set_device(h))) return rc;
@@ -708,15 +844,16 @@ extern "C" int scg_search_device_noalloc(scg_index *h, const scg_search_params *
     ta.cq = h->cq.as<float>(); ta.pq = h->pq.as<float>();
     ta.norm_c = h->norm_c.as<float>(); ta.norm_r = h->norm_r.as<float>();
     ta.dqc = dqc; ta.dqr = dqr; ta.qn = qn; ta.qsum = qsum;
-    ta.fast = p->precision == SCG_FAST;
-    launch_tables_exact(ta, s);
+    ta.lut_only = scan_form(p->precision) == SCG_FAST;
+    ta.status = status;
     // the scratch keeps the previous call's contents: clear what starts at zero
     SCG_CUDA(cudaMemsetAsync(status, 0, sizeof(int) * 4, s));
     SCG_CUDA(cudaMemsetAsync(counter, 0, sizeof(int) * 4, s));
+    launch_tables(ta, p->precision, s);
     SearchArgs sa;
     memset(&sa, 0, sizeof(sa));
     sa.mode = p->mode; sa.dim = h->dim; sa.mc = h->mc; sa.kc = h->kc; sa.mp = h->mp; sa.kp = h->kp;
-    sa.nq = nq; sa.R = p->R; sa.w = p->w; sa.T = p->T; sa.precision = p->precision;
+    sa.nq = nq; sa.R = p->R; sa.w = p->w; sa.T = p->T; sa.precision = scan_form(p->precision);
     sa.Tq = h->d_Tq;
     sa.dqc = dqc; sa.dqr = dqr; sa.qn = qn; sa.qsum = qsum;
     sa.off = h->off.as<uint32_t>(); sa.pid = h->pid.as<int>(); sa.codes = h->codes.as<uint8_t>();
@@ -735,13 +872,14 @@ extern "C" int scg_search_device_noalloc(scg_index *h, const scg_search_params *
     sa.status = status;
     sa.phase_cycles = nullptr;
     if ((rc = search_launch(sa, grid, s))) return rc;
-    SCG_CUDA(cudaMemcpyAsync(h->h_status, status, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SCG_CUDA(cudaMemcpyAsync(h->ws.h_status, status, sizeof(int), cudaMemcpyDeviceToHost, s));
     SCG_CUDA(cudaStreamSynchronize(s));
-    int st = *h->h_status;
+    int st = *h->ws.h_status;
     if (st & ST_CELL_BUDGET)
         return fail(SCG_ERR_CAP, "a query needs more than the allocation-free search's 8192 cells or survivors");
     if (st & ST_TIE_OVERFLOW) return fail(SCG_ERR_CAP, "too many cells tie exactly at the cut key");
     if (st & ST_ITER_CAP) return fail(SCG_ERR_CAP, "cell selection did not converge within its round cap");
+    if (st & ST_TC_TIMEOUT) return fail(SCG_ERR_CUDA, "a tensor-core table tile did not complete in time");
     if (st) return fail(SCG_ERR_CUDA, "search kernel reported status " + std::to_string(st));
     return SCG_OK;
 }

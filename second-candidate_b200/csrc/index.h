@@ -1,0 +1,106 @@
+// Host-side state of the library: the index handle, per-stream search
+// workspaces, and the internal entry points shared by api.cu (the C ABI) and
+// server.cu (the request loop).
+#pragma once
+
+#include <mutex>
+#include <string>
+
+#include "scg_internal.cuh"
+
+namespace scg {
+
+// Grow-only device buffer.
+struct DevBuf {
+    void *p = nullptr;
+    size_t n = 0;
+    int ensure(size_t bytes) {
+        if (bytes <= n) return SCG_OK;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+        n = bytes;
+        return SCG_OK;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    template <class T>
+    T *as() const {
+        return (T *)p;
+    }
+};
+
+// Everything one in-flight batched search writes besides its outputs: the
+// per-CTA traversal slots, the status word, the query counter, and (unless
+// the caller supplies them) the per-query tables.  One per stream of work.
+struct Workspace {
+    DevBuf dqc, dqr, qn, qsum, nvis, empty, status, counter;
+    DevBuf rec_key, rec_rank, rec_cnt, vis_cell, vis_pre, pend, phase, sl_ids, sl_d;
+    int *h_status = nullptr;  // pinned copy of the status word
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    int last_nq = 0;
+    bool phase_on = false;
+    int init();
+    void release();
+};
+
+// Per-request buffers carved by a caller (the request loop's arena); when
+// given, run_search uses them instead of growing the workspace.
+struct ReqBufs {
+    float *dqc, *dqr, *qn, *qsum;
+    int *nvis, *empty;
+    int *sl_ids;   // [nq][L] when re-ranking
+    float *sl_d;
+};
+
+// Device bytes of the ReqBufs of one request.
+size_t req_bytes(int nq, int dim, int mc, int kc, int mp, int kp, int R, int rerank);
+// Carves ReqBufs for nq queries from base (256-byte aligned pieces).
+ReqBufs carve_req(unsigned char *base, int nq, int mc, int kc, int mp, int kp, int rerank);
+
+}  // namespace scg
+
+struct scg_index {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t stream = nullptr;
+    int dim = 0, mc = 0, kc = 0, mp = 0, kp = 0;
+    int64_t N = 0;
+    int64_t ncells = 0;
+    bool have_codebooks = false, have_csr = false, precomputed = false;
+    int cap_rec = 131072;
+    const int *d_Tq = nullptr;
+    scg::DevBuf cq, pq, norm_c, norm_r, dot_cr, off, pid, codes, raw, vterm;
+    bool have_vterm = false;
+    int64_t raw_rows = 0;   // rows of raw vectors loaded (0: none)
+    bool raw_u8 = false;    // raw vectors held as uint8
+    scg::Workspace ws;      // the workspace of the index's own entry points
+    scg::DevBuf q, ids, dists, sums;  // host-buffer staging of scg_search
+    std::mutex mu;
+};
+
+namespace scg {
+
+int set_device(scg_index *h);
+int check_ready(scg_index *h);
+int check_params(scg_index *h, const scg_search_params *p, int nq);
+// Builds the fast form's per-vector term once (on stream s).
+int ensure_vterm(scg_index *h, cudaStream_t s);
+// Enqueues tables, search and re-rank of nq device queries on stream s.
+// wait = true: synchronises and returns the status; false: returns after
+// enqueueing, the status word lands in ws->h_status when the stream reaches
+// it and is read by status_result(ws).
+int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_params *p, const float *dQ, int nq,
+               int *d_ids, float *d_d, int *d_sums, cudaStream_t s, bool wait);
+int status_result(int st);
+// Grows a workspace to a search grid of `grid` CTAs (<= 0: a full grid).
+int reserve_search(scg_index *h, Workspace *ws, int mode, int grid);
+// The search mode the index's shape implies (IMI, IVFADC or SC).
+int index_mode(const scg_index *h);
+
+}  // namespace scg

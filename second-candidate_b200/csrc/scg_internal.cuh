@@ -44,6 +44,7 @@ enum : int {
     ST_TIE_OVERFLOW = 2,  // more exact key ties at the cut than the tie buffer
     ST_ITER_CAP = 4,      // an iteration cap was reached
     ST_BAD_ARG = 8,
+    ST_TC_TIMEOUT = 16,   // a tensor-core completion wait expired
 };
 
 // ---------------------------------------------------------------------------
@@ -58,12 +59,16 @@ struct TablesArgs {
     float *dqr;            // [nq][mp*kp]
     float *qn;             // [nq][2] half norms (IMI) or [nq][2] = {q_sum, 0}
     float *qsum;           // [nq]
-    int fast;              // 0: the reference's float order; 1: FMA dots, LUT = -2<q,r>
+    int lut_only;          // 1: dqr holds -2<q,r> (the fast form keeps ||r||^2 per vector)
+    int *status;           // optional status word (ST_* bits)
 };
 
 void launch_precompute1(int dim, int mc, int kc, int mp, int kp, const float *cq, const float *pq,
                         float *norm_c, float *norm_r, float *dot_cr, cudaStream_t s);
 void launch_tables_exact(const TablesArgs &a, cudaStream_t s);
+// Tensor-core tables: nsplit 3 (hi/lo split, FP32-accurate) or 1; fmt 1 = bf16, 0 = f16.
+void launch_tables_tc(const TablesArgs &a, int nsplit, int fmt, cudaStream_t s);
+void launch_query_norms(const TablesArgs &a, cudaStream_t s);
 void launch_vterm(int mode, int kc, int mp, int kp, int mc, uint64_t ncells, int64_t N, const uint32_t *off,
                   const uint8_t *codes, const float *norm_r, const float *dot_cr, float *vterm, cudaStream_t s);
 
@@ -106,5 +111,9 @@ struct EncodeArgs {
     uint8_t *codes;
 };
 void launch_encode(const EncodeArgs &a, cudaStream_t s);
+
+size_t rerank_smem_bytes(int L, int dim);
+int launch_rerank(const float *Q, int nq, int dim, const void *raw, int raw_u8, int64_t N, const int *sl_ids, int L,
+                  int R, int *out_ids, float *out_d, int *status, cudaStream_t s);
 
 }  // namespace scg

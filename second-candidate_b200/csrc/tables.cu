@@ -112,24 +112,16 @@ __global__ void __launch_bounds__(ET) k_tables_exact(TablesArgs a, int ctiles, i
             cs[kk][ee] = (eg < seglen && kk < kn) ? cent[(size_t)eg * len + k0 + kk] : 0.0f;
         }
         __syncthreads();
-        if (a.fast) {
-            for (int kk = 0; kk < kn; kk++) {
-                float c = cs[kk][t];
+        for (int kk = 0; kk < kn; kk++) {
+            float c = cs[kk][t];
 #pragma unroll
-                for (int i = 0; i < QT; i++) acc[i] = fmaf(qs[i][kk], c, acc[i]);
-            }
-        } else {
-            for (int kk = 0; kk < kn; kk++) {
-                float c = cs[kk][t];
-#pragma unroll
-                for (int i = 0; i < QT; i++) acc[i] = __fadd_rn(acc[i], __fmul_rn(qs[i][kk], c));
-            }
+            for (int i = 0; i < QT; i++) acc[i] = __fadd_rn(acc[i], __fmul_rn(qs[i][kk], c));
         }
         __syncthreads();
     }
     if (e < seglen) {
         // the fast form keeps ||r||^2 in the per-vector term: its LUT is -2<q,r>
-        const bool lut_only = a.fast && out == a.dqr;
+        const bool lut_only = a.lut_only && out == a.dqr;
         float nv = lut_only ? 0.0f : norm[e];
 #pragma unroll
         for (int i = 0; i < QT; i++) {
@@ -223,6 +215,11 @@ void launch_tables_exact(const TablesArgs &a, cudaStream_t s) {
     int ctiles = (a.kc + ET - 1) / ET, ptiles = (a.kp + ET - 1) / ET;
     dim3 grid(a.mc * ctiles + a.mp * ptiles, (a.nq + QT - 1) / QT);
     k_tables_exact<<<grid, ET, 0, s>>>(a, ctiles, ptiles);
+    launch_query_norms(a, s);
+}
+
+void launch_query_norms(const TablesArgs &a, cudaStream_t s) {
+    if (a.nq <= 0 || !a.qn) return;
     k_query_norms<<<(a.nq + 127) / 128, 128, 0, s>>>(a.Q, a.nq, a.dim, a.mc, a.qn, a.qsum);
 }
 

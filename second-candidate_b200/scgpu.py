@@ -13,7 +13,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libscgpu.so")
 
 IVFADC, IMI, SC2 = 0, 1, 2
-FP32_EXACT, FAST = 0, 1
+FP32_EXACT, FAST, BF16, FP16 = 0, 1, 2, 3
+
+PENDING = 1
 
 ERRORS = {-1: "SCG_ERR_ARG", -2: "SCG_ERR_OOM", -3: "SCG_ERR_IO", -4: "SCG_ERR_CUDA",
           -5: "SCG_ERR_CAP", -6: "SCG_ERR_STATE"}
@@ -24,7 +26,9 @@ EXPORTS = ["scg_last_error", "scg_index_create", "scg_index_destroy", "scg_load_
            "scg_set_cell_budget", "scg_encode", "scg_sc_encode", "scg_encode_device",
            "scg_index_info", "scg_last_query_stats", "scg_last_timings",
            "scg_cell_counts", "scg_set_phase_counters", "scg_last_phase_counters",
-           "scg_search_device_noalloc"]
+           "scg_search_device_noalloc", "scg_query_tables_device", "scg_load_raw_u8",
+           "scg_server_create", "scg_server_submit", "scg_server_wait", "scg_server_stats",
+           "scg_server_destroy"]
 
 
 class ScgError(RuntimeError):
@@ -122,8 +126,13 @@ class Index:
         self._refresh_info()
 
     def load_raw(self, X):
-        X = np.ascontiguousarray(X, np.float32)
-        _check(_lib.scg_load_raw(self._h, _ptr(X), ctypes.c_int64(X.shape[0])))
+        """Raw vectors for the shortlist re-rank: float32, or uint8 kept as uint8."""
+        if X.dtype == np.uint8:
+            X = np.ascontiguousarray(X)
+            _check(_lib.scg_load_raw_u8(self._h, _ptr(X), ctypes.c_int64(X.shape[0])))
+        else:
+            X = np.ascontiguousarray(X, np.float32)
+            _check(_lib.scg_load_raw(self._h, _ptr(X), ctypes.c_int64(X.shape[0])))
 
     def precompute(self):
         _check(_lib.scg_precompute(self._h))
@@ -161,6 +170,12 @@ class Index:
                                               ctypes.c_void_p(d_sums),
                                               ctypes.c_void_p(stream) if stream else None))
 
+    def query_tables_device(self, precision, dQ_ptr, nq, d_dqc, d_dqr, stream=None):
+        """Batched per-query tables (diff_qc, diff_qr) into device buffers."""
+        _check(_lib.scg_query_tables_device(self._h, precision, ctypes.c_void_p(dQ_ptr), nq,
+                                            ctypes.c_void_p(d_dqc), ctypes.c_void_p(d_dqr),
+                                            ctypes.c_void_p(stream) if stream else None))
+
     def set_query_targets(self, d_T_ptr):
         _check(_lib.scg_set_query_targets(self._h, ctypes.c_void_p(d_T_ptr) if d_T_ptr else None))
 
@@ -181,9 +196,10 @@ class Index:
         return {n: int(v) for n, v in zip(names, out) if n != "-"}
 
     def last_timings(self):
-        ms = np.zeros(2, np.float32)
-        _check(_lib.scg_last_timings(self._h, _ptr(ms), 2))
-        return float(ms[0]), float(ms[1])
+        """Device ms of the last search: (tables, selection + scan, re-rank)."""
+        ms = np.zeros(3, np.float32)
+        _check(_lib.scg_last_timings(self._h, _ptr(ms), 3))
+        return float(ms[0]), float(ms[1]), float(ms[2])
 
     def encode(self, X):
         X = np.ascontiguousarray(X, np.float32)
@@ -205,3 +221,59 @@ class Index:
         _check(_lib.scg_encode_device(self._h, ctypes.c_void_p(dX_ptr), ctypes.c_int64(n), nc,
                                       ctypes.c_void_p(d_cid), ctypes.c_void_p(d_codes),
                                       ctypes.c_void_p(stream) if stream else None))
+
+
+class Server:
+    """Request loop with continuous batching over one Index (scg_server_*).
+
+    submit() takes host arrays and returns a ticket; the arrays are kept
+    alive here until wait() returns the results."""
+
+    def __init__(self, index, slots=4, max_batch=4096, max_R=100, arena_bytes=1 << 30):
+        self.index = index
+        self._s = ctypes.c_void_p()
+        _check(_lib.scg_server_create(index.handle, slots, max_batch, max_R, ctypes.c_size_t(arena_bytes),
+                                      ctypes.byref(self._s)))
+        self._live = {}
+
+    def submit(self, mode, Q, R, w, T, precision=FP32_EXACT, rerank=0):
+        Q = np.ascontiguousarray(Q, np.float32).reshape(-1, self.index.dim)
+        nq = Q.shape[0]
+        ids = np.empty((nq, R), np.int32)
+        d = np.empty((nq, R), np.float32)
+        sums = np.empty(nq, np.int32)
+        p = SearchParams(mode, R, w, T, precision, rerank)
+        t = ctypes.c_uint64()
+        _check(_lib.scg_server_submit(self._s, ctypes.byref(p), _ptr(Q), nq, _ptr(ids), _ptr(d), _ptr(sums),
+                                      ctypes.byref(t)))
+        self._live[t.value] = (Q, ids, d, sums)
+        return t.value
+
+    def wait(self, ticket, timeout=-1.0):
+        """(ids, dists, sums, latency_ms), or None if the timeout expired."""
+        lat = ctypes.c_double()
+        rc = _lib.scg_server_wait(self._s, ctypes.c_uint64(ticket), ctypes.c_double(timeout), ctypes.byref(lat))
+        if rc == PENDING:
+            return None
+        Q, ids, d, sums = self._live.pop(ticket)
+        _check(rc)
+        return ids, d, sums, lat.value
+
+    def stats(self):
+        c = ctypes.c_longlong()
+        m = ctypes.c_int()
+        q = ctypes.c_int()
+        _check(_lib.scg_server_stats(self._s, ctypes.byref(c), ctypes.byref(m), ctypes.byref(q)))
+        return {"completed": c.value, "max_inflight": m.value, "queued": q.value}
+
+    def close(self):
+        if self._s:
+            _lib.scg_server_destroy(self._s)
+            self._s = ctypes.c_void_p()
+            self._live.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

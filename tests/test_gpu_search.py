@@ -143,10 +143,15 @@ def test_file_loaders(scg, oracle_mod, tmp_path):
 
 
 @pytest.mark.parametrize("mode,mc,kc", [(O.IVFADC, 1, 64), (O.IMI, 2, 48), (O.SC, 1, 48)])
-def test_fast_form_tolerance(scg, oracle_mod, mode, mc, kc):
-    """The fast form (FMA tables, per-vector term) reorders the float sums:
-    candidate sets match the exact order except at rare boundary ties, and
-    top-R distances agree with the exact ones within 1e-5 relative."""
+@pytest.mark.parametrize("form", ["FAST", "BF16"])
+def test_tensor_core_forms(scg, oracle_mod, mode, mc, kc, form):
+    """The tensor-core forms reorder and round the float sums.  SCG_FAST
+    (split BF16 tables, within 3 * 2^-16 of the dot-product scale): candidate
+    sets match the exact order except at rare boundary ties, top-R distances
+    agree within 1e-4 relative and at most two ids of a top-R differ.
+    SCG_BF16 (one BF16 product, 2^-7 of the scale; uint8-valued data near 255
+    lose half a unit per coordinate): each returned distance is within 5% of
+    the exact ADC distance of the same id, and most of each top-R agrees."""
     D, mp, kp = 64, 8, 256
     mix = W.Mixture(D, 16, 20.0, "u8", seed=31 + mode)
     X = mix.sample(30000, seed=32)
@@ -162,14 +167,26 @@ def test_fast_form_tolerance(scg, oracle_mod, mode, mc, kc):
     g = gpu_index(scg, D, mc, kc, mp, kp, cq, pq, L, pid, co)
     w = kc if mode == O.IVFADC else 1 << 20
     R, T = 50, 1500
-    ids, d, sums = g.search(MODES[mode], Q, R, w, T, precision=scg.FAST)
+    ids, d, sums = g.search(MODES[mode], Q, R, w, T, precision=getattr(scg, form))
     oi, od, osum = ix.search(mode, Q, R, w, T, order=O.ORDER_EXACT)
     same = sums == osum
-    assert same.mean() >= 0.95
+    overlap = []
     for i in np.nonzero(same)[0]:
         m = min(R, int(sums[i]))
-        assert np.allclose(d[i, :m], od[i, :m], rtol=1e-5, atol=1e-2)
-        assert len(set(ids[i, :m].tolist()) & set(oi[i, :m].tolist())) >= m - 2
+        overlap.append(len(set(ids[i, :m].tolist()) & set(oi[i, :m].tolist())) / max(m, 1))
+        if form == "FAST":
+            assert np.allclose(d[i, :m], od[i, :m], rtol=1e-4, atol=1e-2)
+            assert overlap[-1] * m >= m - 2
+        else:
+            cand = ix.search_one(mode, Q[i], w, T)
+            exact = dict(zip(cand["ids"].tolist(), cand["dist"].tolist()))
+            for j in range(m):
+                e = exact[int(ids[i, j])]
+                assert abs(float(d[i, j]) - e) <= 0.05 * abs(e) + 1.0, (i, j, d[i, j], e)
+    if form == "FAST":
+        assert same.mean() >= 0.95
+    else:
+        assert same.mean() >= 0.5 and np.mean(overlap) >= 0.6, (same.mean(), np.mean(overlap))
     g.close()
 
 
