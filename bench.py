@@ -321,6 +321,14 @@ def main():
 
     prec = PRECISIONS[args.precision][0]
 
+    # the scan's chunking picked by the library's autotuner on this batch, for
+    # both scan forms (exact and fast)
+    tuning = {}
+    for name, pv in (("fast", prec), ("fp32", 0)):
+        choice, ms = ix.autotune(mode, dQ.data_ptr(), nq, R, wcap, T, d_ids.data_ptr(), d_d.data_ptr(),
+                                 d_s.data_ptr(), precision=pv)
+        tuning[name] = {"candidates_per_lane": choice, "ms_by_choice": dict(zip((2, 4, 8), ms))}
+
     def step(p=None):
         ix.search_device(mode, dQ.data_ptr(), nq, R, wcap, T, d_ids.data_ptr(), d_d.data_ptr(),
                          d_s.data_ptr(), stream=stream.cuda_stream, precision=prec if p is None else p)
@@ -452,6 +460,7 @@ def main():
         "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": int(nq * cfg["D"] * 4),
                 "d2h_bytes_per_step": int(nq * R * 8 + nq * 4), "same_ids_as_device_path": same},
         "gpu_launches": 3 * args.steps,
+        "autotune": tuning,
         "clocks": ck,
         "candidates_per_query": float(sums.mean()), "cells_per_query": float(nvis.mean() + empty.mean()),
     }

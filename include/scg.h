@@ -146,6 +146,19 @@ int scg_search_device_noalloc(scg_index *h, const scg_search_params *p, const fl
 int scg_query_tables_device(scg_index *h, int precision, const float *dQ, int nq,
                             float *d_diff_qc, float *d_diff_qr, void *stream);
 
+/* Autotuner of the scan's chunking: times the fused search kernel on the
+ * given device batch with 2, 4 and 8 candidates per lane per claimed chunk
+ * (64, 128, 256 candidates per warp claim), keeps the fastest for this
+ * index and the scan form of p->precision, and reports it (*choice; ms[3]
+ * the best time of each, may be NULL).  Outputs are written as by
+ * scg_search_device.  No counterpart in the reference. */
+int scg_autotune(scg_index *h, const scg_search_params *p, const float *dQ, int nq, int *d_ids,
+                 float *d_dists, int *d_sums, int *choice, float *ms);
+
+/* Sets the scan's candidates per lane (2, 4 or 8) for the scan form of
+ * `precision` without timing. */
+int scg_set_scan_tuning(scg_index *h, int precision, int upl);
+
 /* Per-query candidate targets (device pointer to nq ints) for the next
  * scg_search_device call; NULL restores the single T of the parameters. */
 int scg_set_query_targets(scg_index *h, const int *d_T);

@@ -7,7 +7,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libscgpu.so")
-SOURCES = ["api.cu", "tables.cu", "tables_tc.cu", "search.cu", "encode.cu", "rerank.cu", "server.cu"]
+SOURCES = ["api.cu", "tables.cu", "tables_tc.cu", "search.cu", "encode.cu", "rerank.cu", "server.cu", "coarse.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]

@@ -148,7 +148,7 @@ int Workspace::init() {
 
 void Workspace::release() {
     DevBuf *all[] = {&dqc, &dqr, &qn, &qsum, &nvis, &empty, &status, &counter, &rec_key, &rec_rank,
-                     &rec_cnt, &vis_cell, &vis_pre, &pend, &phase, &sl_ids, &sl_d};
+                     &rec_cnt, &vis_cell, &vis_pre, &pend, &phase, &sl_ids, &sl_d, &slist, &smeta};
     for (DevBuf *b : all) b->release();
     if (h_status) cudaFreeHost(h_status);
     h_status = nullptr;
@@ -159,11 +159,17 @@ void Workspace::release() {
 
 static size_t up256b(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Bytes of the sorted coarse lists of nq queries (0 when kc is too large
+// for the ahead-of-time sort).
+static size_t slist_bytes(int nq, int mc, int kc) {
+    return 8ull * nq * (mc == 2 ? 2 : 1) * (size_t)coarse_sort_width(kc);
+}
+
 size_t req_bytes(int nq, int dim, int mc, int kc, int mp, int kp, int R, int rerank) {
     (void)dim;
     (void)R;
     size_t b = up256b(4ull * nq * mc * kc) + up256b(4ull * nq * mp * kp) + up256b(8ull * nq) + up256b(4ull * nq) +
-               2 * up256b(4ull * nq);
+               2 * up256b(4ull * nq) + up256b(slist_bytes(nq, mc, kc)) + up256b(8ull * nq * 2);
     if (rerank > 0) b += 2 * up256b(4ull * nq * rerank);
     return b;
 }
@@ -184,6 +190,8 @@ ReqBufs carve_req(unsigned char *base, int nq, int mc, int kc, int mp, int kp, i
     r.empty = (int *)take(4ull * nq);
     r.sl_ids = nullptr;
     r.sl_d = nullptr;
+    r.slist = coarse_sort_width(kc) ? (uint64_t *)take(slist_bytes(nq, mc, kc)) : nullptr;
+    r.smeta = (uint32_t *)take(8ull * nq * 2);
     if (rerank > 0) {
         r.sl_ids = (int *)take(4ull * nq * rerank);
         r.sl_d = (float *)take(4ull * nq * rerank);
@@ -208,7 +216,11 @@ int ensure_vterm(scg_index *h, cudaStream_t s) {
 int reserve_search(scg_index *h, Workspace *ws, int mode, int grid) {
     int rc;
     if ((rc = ws->init())) return rc;
-    int per_sm = search_max_blocks_per_sm(mode, h->kc, h->mp, h->kp);
+    int per_sm = 0;
+    for (int u : {2, 4, 8}) {
+        const int b = search_max_blocks_per_sm(mode, h->kc, h->mp, h->kp, u);
+        per_sm = b > per_sm ? b : per_sm;
+    }
     if (per_sm < 1) return fail(SCG_ERR_ARG, "search kernel does not fit on an SM for this shape");
     if (grid <= 0 || grid > h->num_sms * per_sm) grid = h->num_sms * per_sm;
     const size_t slot = (size_t)h->cap_rec, pcap = slot > 65536 ? slot : 65536;
@@ -248,6 +260,14 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
         b.qn = ws->qn.as<float>(); b.qsum = ws->qsum.as<float>();
         b.nvis = ws->nvis.as<int>(); b.empty = ws->empty.as<int>();
         b.sl_ids = nullptr; b.sl_d = nullptr;
+        b.slist = nullptr;
+        b.smeta = nullptr;
+        if (coarse_sort_width(h->kc)) {
+            if ((rc = ws->slist.ensure(slist_bytes(nq, h->mc, h->kc)))) return rc;
+            if ((rc = ws->smeta.ensure(8ull * nq * 2))) return rc;
+            b.slist = ws->slist.as<uint64_t>();
+            b.smeta = ws->smeta.as<uint32_t>();
+        }
         if (rr) {
             if ((rc = ws->sl_ids.ensure(sizeof(int) * (size_t)nq * R))) return rc;
             if ((rc = ws->sl_d.ensure(sizeof(float) * (size_t)nq * R))) return rc;
@@ -258,7 +278,8 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     float *s_d = rr ? b.sl_d : d_d;
     if ((rc = ws->status.ensure(sizeof(int) * 4))) return rc;
     if ((rc = ws->counter.ensure(sizeof(int) * 4))) return rc;
-    int per_sm = search_max_blocks_per_sm(p->mode, h->kc, h->mp, h->kp);
+    const int upl = h->tuned_upl[scan_form(p->precision) == SCG_FAST ? 1 : 0];
+    int per_sm = search_max_blocks_per_sm(p->mode, h->kc, h->mp, h->kp, upl);
     if (per_sm < 1) return fail(SCG_ERR_ARG, "search kernel does not fit on an SM for this shape");
     int grid = h->num_sms * per_sm;
     if (grid > nq) grid = nq;
@@ -287,12 +308,29 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     SCG_CUDA(cudaMemsetAsync(ws->counter.p, 0, sizeof(int) * 4, s));
     SCG_CUDA(cudaEventRecord(ws->ev[0], s));
     launch_tables(ta, p->precision, s);
+    if (b.slist) {
+        CoarseArgs ca;
+        ca.dqc = b.dqc; ca.qn = b.qn; ca.qsum = b.qsum;
+        ca.nq = nq; ca.kc = h->kc; ca.mc = h->mc; ca.imi = h->mc == 2 ? 1 : 0;
+        ca.Tq = rb ? nullptr : h->d_Tq;
+        ca.T = p->T;
+        ca.avg_density = (double)h->N / (double)(h->ncells ? h->ncells : 1);
+        ca.max_prefix = 1024;
+        ca.width = coarse_sort_width(h->kc);
+        ca.out = b.slist;
+        ca.meta = b.smeta;
+        launch_coarse_prefix(ca, s);
+    }
     SCG_CUDA(cudaEventRecord(ws->ev[1], s));
 
     SearchArgs sa;
     memset(&sa, 0, sizeof(sa));
     sa.mode = p->mode; sa.dim = h->dim; sa.mc = h->mc; sa.kc = h->kc; sa.mp = h->mp; sa.kp = h->kp;
     sa.nq = nq; sa.R = R; sa.w = p->w; sa.T = p->T; sa.precision = scan_form(p->precision);
+    sa.upl = upl;
+    sa.slist = b.slist;
+    sa.smeta = b.smeta;
+    sa.slist_w = coarse_sort_width(h->kc);
     sa.Tq = rb ? nullptr : h->d_Tq;
     sa.dqc = b.dqc; sa.dqr = b.dqr; sa.qn = b.qn; sa.qsum = b.qsum;
     sa.off = h->off.as<uint32_t>(); sa.pid = h->pid.as<int>(); sa.codes = h->codes.as<uint8_t>();
@@ -596,6 +634,52 @@ int scg_query_tables_device(scg_index *h, int precision, const float *dQ, int nq
     return SCG_OK;
 }
 
+int scg_set_scan_tuning(scg_index *h, int precision, int upl) {
+    if (!h) return fail(SCG_ERR_ARG, "null index");
+    if (precision < SCG_FP32_EXACT || precision > SCG_FP16) return fail(SCG_ERR_ARG, "unknown precision");
+    if (upl != 2 && upl != 4 && upl != 8) return fail(SCG_ERR_ARG, "candidates per lane must be 2, 4 or 8");
+    std::lock_guard<std::mutex> g(h->mu);
+    h->tuned_upl[scan_form(precision) == SCG_FAST ? 1 : 0] = upl;
+    return SCG_OK;
+}
+
+int scg_autotune(scg_index *h, const scg_search_params *p, const float *dQ, int nq, int *d_ids, float *d_dists,
+                 int *d_sums, int *choice, float *ms) {
+    int rc;
+    if ((rc = check_ready(h))) return rc;
+    if ((rc = check_params(h, p, nq))) return rc;
+    if (nq < 1 || !dQ || !d_ids || !d_dists || !d_sums) return fail(SCG_ERR_ARG, "autotune needs a non-empty batch");
+    std::lock_guard<std::mutex> g(h->mu);
+    if ((rc = set_device(h))) return rc;
+    cudaStream_t s = h->stream;
+    const int form = scan_form(p->precision) == SCG_FAST ? 1 : 0;
+    const int saved = h->tuned_upl[form];
+    const int cand[3] = {2, 4, 8};
+    float best = 3.4e38f;
+    int pick = saved;
+    for (int i = 0; i < 3; i++) {
+        h->tuned_upl[form] = cand[i];
+        float t = 3.4e38f;
+        for (int rep = 0; rep < 3; rep++) {  // first run warms up
+            if ((rc = run_search(h, &h->ws, nullptr, p, dQ, nq, d_ids, d_dists, d_sums, s, true))) {
+                h->tuned_upl[form] = saved;
+                return rc;
+            }
+            float k = 0;
+            SCG_CUDA(cudaEventElapsedTime(&k, h->ws.ev[1], h->ws.ev[2]));
+            if (rep > 0 && k < t) t = k;
+        }
+        if (ms) ms[i] = t;
+        if (t < best) {
+            best = t;
+            pick = cand[i];
+        }
+    }
+    h->tuned_upl[form] = pick;
+    if (choice) *choice = pick;
+    return SCG_OK;
+}
+
 int scg_set_query_targets(scg_index *h, const int *d_T) {
     if (!h) return fail(SCG_ERR_ARG, "null index");
     h->d_Tq = d_T;
@@ -802,7 +886,8 @@ extern "C" int scg_search_device_noalloc(scg_index *h, const scg_search_params *
     const size_t fixed = 4 * up256(sizeof(float) * (size_t)nq * 2) + 2 * 256;  // qn, qsum, nvis, empty; status, counter
     const size_t slot_bytes = up256(4ull * NOALLOC_CELLS) * 3 + up256(4ull * (NOALLOC_CELLS + 1)) * 2 +
                               up256(8ull * NOALLOC_SURVIVORS);
-    int per_sm = search_max_blocks_per_sm(p->mode, h->kc, h->mp, h->kp);
+    const int upl = h->tuned_upl[scan_form(p->precision) == SCG_FAST ? 1 : 0];
+    int per_sm = search_max_blocks_per_sm(p->mode, h->kc, h->mp, h->kp, upl);
     if (per_sm < 1) return fail(SCG_ERR_ARG, "search kernel does not fit on an SM for this shape");
     int grid = h->num_sms * per_sm;
     if (grid > nq) grid = nq;
@@ -854,6 +939,7 @@ extern "C" int scg_search_device_noalloc(scg_index *h, const scg_search_params *
     memset(&sa, 0, sizeof(sa));
     sa.mode = p->mode; sa.dim = h->dim; sa.mc = h->mc; sa.kc = h->kc; sa.mp = h->mp; sa.kp = h->kp;
     sa.nq = nq; sa.R = p->R; sa.w = p->w; sa.T = p->T; sa.precision = scan_form(p->precision);
+    sa.upl = upl;
     sa.Tq = h->d_Tq;
     sa.dqc = dqc; sa.dqr = dqr; sa.qn = qn; sa.qsum = qsum;
     sa.off = h->off.as<uint32_t>(); sa.pid = h->pid.as<int>(); sa.codes = h->codes.as<uint8_t>();

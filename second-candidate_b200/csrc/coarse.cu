@@ -1,0 +1,178 @@
+// Coarse ranking of a whole batch ahead of the fused search.
+//
+// The reference sorts each coarse list of a query completely
+// (nth_element_id + sort_id with M = kc, multi_query.h:114-128,
+// sc_query.h:98-106, query.h:230-234), but the multi-sequence walk only
+// reaches a prefix.  For kc <= 1024 one warp handles one list: the keys
+// (ordered float of q_part + diff_qc, << 32 | centroid id, so equal keys go
+// by id) sit 32 per lane at most; a binary search over the high words finds
+// vm, the M-th smallest (M from the query's candidate target, the same rule
+// the fused kernel uses), every key with high word <= vm is compacted through
+// shared memory and sorted by a register bitonic network (register swaps for
+// partner distances >= 32, warp shuffles below).  Per list the kernel writes
+// the sorted prefix, its length and the smallest high word after it; the
+// fused kernel then treats the prefix exactly as its own radix-selected
+// prefix (and still sorts everything itself if the walk leaves the prefix).
+#include "scg_internal.cuh"
+
+namespace scg {
+
+namespace {
+
+constexpr int CS_THREADS = 128;  // 4 warps, one list each
+constexpr int CS_CAP = 1024;     // keys per list
+
+__device__ __forceinline__ uint64_t shfl_xor64(uint64_t v, int m) {
+    const uint32_t lo = __shfl_xor_sync(0xffffffffu, (uint32_t)v, m);
+    const uint32_t hi = __shfl_xor_sync(0xffffffffu, (uint32_t)(v >> 32), m);
+    return ((uint64_t)hi << 32) | lo;
+}
+
+// Ascending bitonic sort of 32 * P keys held striped (element r * 32 + lane).
+template <int P>
+__device__ __forceinline__ void warp_sort(uint64_t (&v)[P], int lane) {
+    constexpr int n = 32 * P;
+#pragma unroll
+    for (int k = 2; k <= n; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            if (j >= 32) {
+                const int rj = j >> 5;
+#pragma unroll
+                for (int r = 0; r < P; r++) {
+                    const int pr = r ^ rj;
+                    if (pr > r) {
+                        const bool asc = ((r * 32) & k) == 0;
+                        const uint64_t x = v[r], y = v[pr];
+                        if ((x > y) == asc) {
+                            v[r] = y;
+                            v[pr] = x;
+                        }
+                    }
+                }
+            } else {
+                const bool lower = (lane & j) == 0;
+#pragma unroll
+                for (int r = 0; r < P; r++) {
+                    const bool asc = ((r * 32 + lane) & k) == 0;
+                    const uint64_t o = shfl_xor64(v[r], j);
+                    const uint64_t mn = v[r] < o ? v[r] : o, mx = v[r] < o ? o : v[r];
+                    v[r] = (lower == asc) ? mn : mx;
+                }
+            }
+        }
+    }
+}
+
+// Sorts buf[0, 32 * P) (padding already ~0) and writes it to dst.
+template <int P>
+__device__ __forceinline__ void sort_out(const uint64_t *buf, uint64_t *dst, int lane) {
+    uint64_t v[P];
+#pragma unroll
+    for (int r = 0; r < P; r++) v[r] = buf[r * 32 + lane];
+    warp_sort<P>(v, lane);
+#pragma unroll
+    for (int r = 0; r < P; r++) dst[r * 32 + lane] = v[r];
+}
+
+template <int P>
+__global__ void __launch_bounds__(CS_THREADS) k_coarse_prefix(CoarseArgs a) {
+    __shared__ uint64_t buf[CS_THREADS / 32][CS_CAP];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int list = blockIdx.x * (CS_THREADS / 32) + wid;
+    const int nlists = a.imi ? 2 : 1;
+    if (list >= a.nq * nlists) return;  // whole warps leave together
+    const int q = list / nlists, part = list - q * nlists;
+    const float base = a.imi ? a.qn[2 * q + part] : a.qsum[q];
+    const float *row = a.dqc + (size_t)q * a.mc * a.kc + (size_t)part * a.kc;
+    uint64_t v[P];
+#pragma unroll
+    for (int r = 0; r < P; r++) {
+        const int i = r * 32 + lane;
+        v[r] = i < a.kc ? (((uint64_t)f2o(__fadd_rn(base, row[i])) << 32) | (uint32_t)i) : ~0ull;
+    }
+    // prefix length rule of the fused kernel
+    const int T = a.Tq ? a.Tq[q] : a.T;
+    const double c0 = (T > 0 ? (double)T : 1.0) / (a.avg_density > 1e-9 ? a.avg_density : 1e-9);
+    int M = 1;
+    while (M < 4 * (int)sqrt(c0) + 1) M <<= 1;
+    if (M < 128) M = 128;
+    if (M > a.max_prefix) M = a.max_prefix;
+    uint32_t vm = 0xffffffffu;
+    if (M < a.kc) {
+        // vm = the M-th smallest high word (binary search on the value)
+        uint32_t lo = 0, hi = 0xffffffffu;
+        while (lo < hi) {
+            const uint32_t mid = lo + ((hi - lo) >> 1);
+            int cnt = 0;
+#pragma unroll
+            for (int r = 0; r < P; r++) cnt += (uint32_t)(v[r] >> 32) <= mid;
+            cnt = __reduce_add_sync(FULL, cnt);
+            if (cnt >= M) hi = mid;
+            else lo = mid + 1;
+        }
+        vm = lo;
+    }
+    // compact the keys with high word <= vm; the smallest high word above vm
+    uint64_t *b = buf[wid];
+    int c = 0;
+    uint32_t nxt = 0xffffffffu;
+#pragma unroll
+    for (int r = 0; r < P; r++) {
+        const uint32_t hw = (uint32_t)(v[r] >> 32);
+        const bool in = v[r] != ~0ull && hw <= vm;
+        if (!in && v[r] != ~0ull && hw < nxt) nxt = hw;
+        const unsigned m = __ballot_sync(FULL, in);
+        if (in) b[c + __popc(m & ((1u << lane) - 1))] = v[r];
+        c += __popc(m);
+    }
+    nxt = __reduce_min_sync(FULL, nxt);
+    int c2 = 32;
+    while (c2 < c) c2 <<= 1;
+    for (int i = c + lane; i < c2; i += 32) b[i] = ~0ull;
+    __syncwarp();
+    uint64_t *dst = a.out + (size_t)list * a.width;
+    switch (c2) {
+        case 32: sort_out<1>(b, dst, lane); break;
+        case 64: sort_out<2>(b, dst, lane); break;
+        case 128: sort_out<4>(b, dst, lane); break;
+        case 256: sort_out<8>(b, dst, lane); break;
+        case 512: sort_out<16>(b, dst, lane); break;
+        default: sort_out<32>(b, dst, lane); break;
+    }
+    if (lane == 0) {
+        a.meta[2 * list] = (uint32_t)c;
+        a.meta[2 * list + 1] = nxt;
+    }
+}
+
+template <int P>
+void launch_p(const CoarseArgs &a, cudaStream_t s) {
+    const int lists = a.nq * (a.imi ? 2 : 1);
+    const int grid = (lists + CS_THREADS / 32 - 1) / (CS_THREADS / 32);
+    k_coarse_prefix<P><<<grid, CS_THREADS, 0, s>>>(a);
+}
+
+}  // namespace
+
+int coarse_sort_width(int kc) {
+    int p = 32;
+    while (p < kc) p <<= 1;
+    return p <= CS_CAP ? p : 0;
+}
+
+void launch_coarse_prefix(const CoarseArgs &a, cudaStream_t s) {
+    if (a.nq <= 0) return;
+    switch (coarse_sort_width(a.kc)) {
+        case 32: launch_p<1>(a, s); break;
+        case 64: launch_p<2>(a, s); break;
+        case 128: launch_p<4>(a, s); break;
+        case 256: launch_p<8>(a, s); break;
+        case 512: launch_p<16>(a, s); break;
+        case 1024: launch_p<32>(a, s); break;
+        default: break;
+    }
+}
+
+}  // namespace scg

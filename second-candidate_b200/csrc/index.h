@@ -40,7 +40,7 @@ struct DevBuf {
 // the caller supplies them) the per-query tables.  One per stream of work.
 struct Workspace {
     DevBuf dqc, dqr, qn, qsum, nvis, empty, status, counter;
-    DevBuf rec_key, rec_rank, rec_cnt, vis_cell, vis_pre, pend, phase, sl_ids, sl_d;
+    DevBuf rec_key, rec_rank, rec_cnt, vis_cell, vis_pre, pend, phase, sl_ids, sl_d, slist, smeta;
     int *h_status = nullptr;  // pinned copy of the status word
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     int last_nq = 0;
@@ -56,6 +56,8 @@ struct ReqBufs {
     int *nvis, *empty;
     int *sl_ids;   // [nq][L] when re-ranking
     float *sl_d;
+    uint64_t *slist;  // [nq][lists][width] sorted coarse-list prefixes (kc <= 1024)
+    uint32_t *smeta;  // [nq][lists][2] their lengths and next high words
 };
 
 // Device bytes of the ReqBufs of one request.
@@ -79,6 +81,7 @@ struct scg_index {
     bool have_vterm = false;
     int64_t raw_rows = 0;   // rows of raw vectors loaded (0: none)
     bool raw_u8 = false;    // raw vectors held as uint8
+    int tuned_upl[2] = {4, 4};  // scan candidates per lane, per scan form (exact, fast)
     scg::Workspace ws;      // the workspace of the index's own entry points
     scg::DevBuf q, ids, dists, sums;  // host-buffer staging of scg_search
     std::mutex mu;
@@ -102,5 +105,7 @@ int status_result(int st);
 int reserve_search(scg_index *h, Workspace *ws, int mode, int grid);
 // The search mode the index's shape implies (IMI, IVFADC or SC).
 int index_mode(const scg_index *h);
+// The scan form of an arithmetic precision: SCG_FP32_EXACT or SCG_FAST.
+int scan_form(int precision);
 
 }  // namespace scg

@@ -75,7 +75,11 @@ void launch_vterm(int mode, int kc, int mp, int kp, int mc, uint64_t ncells, int
 struct SearchArgs {
     int mode, dim, mc, kc, mp, kp, nq, R, w, T;
     int precision;
+    int upl;                // candidates per lane per scan chunk: 2, 4 or 8
     const int *Tq;          // optional per-query T
+    const uint64_t *slist;  // optional coarse-list prefixes sorted ahead: [nq][lists][slist_w]
+    const uint32_t *smeta;  // their lengths and next high words: [nq][lists][2]
+    int slist_w;
     const float *dqc, *dqr, *qn, *qsum;
     const uint32_t *off;    // [ncells+1] exclusive offsets
     const int *pid;
@@ -101,7 +105,7 @@ struct SearchArgs {
 
 size_t search_smem_bytes(int mode, int kc, int mp, int kp);
 int search_launch(const SearchArgs &a, int grid, cudaStream_t s);
-int search_max_blocks_per_sm(int mode, int kc, int mp, int kp);
+int search_max_blocks_per_sm(int mode, int kc, int mp, int kp, int upl);
 
 struct EncodeArgs {
     int dim, mc, kc, mp, kp, nc;  // nc = 0: IVF/IMI encoder; nc >= 2: SC encoder
@@ -111,6 +115,22 @@ struct EncodeArgs {
     uint8_t *codes;
 };
 void launch_encode(const EncodeArgs &a, cudaStream_t s);
+
+// Sorted coarse-list prefixes of a batch, ahead of the fused search
+// (kc <= 1024; width = coarse_sort_width(kc), 0 when kc is larger).
+struct CoarseArgs {
+    const float *dqc, *qn, *qsum;
+    int nq, kc, mc, imi;
+    const int *Tq;       // optional per-query T
+    int T;
+    double avg_density;  // N / cells, for the prefix length rule
+    int max_prefix;
+    int width;           // stride of a list in out
+    uint64_t *out;       // [nq][lists][width] sorted prefix keys
+    uint32_t *meta;      // [nq][lists][2]: prefix length, smallest high word after it
+};
+int coarse_sort_width(int kc);
+void launch_coarse_prefix(const CoarseArgs &a, cudaStream_t s);
 
 size_t rerank_smem_bytes(int L, int dim);
 int launch_rerank(const float *Q, int nq, int dim, const void *raw, int raw_u8, int64_t N, const int *sl_ids, int L,

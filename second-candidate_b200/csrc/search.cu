@@ -47,8 +47,8 @@ constexpr int TIECAP = 64;
 constexpr int RMAX = 1024;      // largest R
 constexpr int WARMN = 4096;     // candidates scored before the threshold is set
 constexpr int WWIN = 32;        // per-warp window of visited cells
-constexpr int UPL = 4;          // candidates per lane per chunk
-constexpr int WCH = 32 * UPL;   // candidates per claimed chunk
+// Candidates per lane per claimed chunk (U, a template parameter of the
+// scan: 2, 4 or 8); a warp claims 32 * U candidates at a time.
 constexpr int SBCAP = 2048;     // sorted coarse prefix capacity
 constexpr int MAX_ROUNDS = 64;
 
@@ -601,13 +601,13 @@ struct ScanCtx {
 };
 
 // Warp-centric ADC scan of the candidates [st.next_flat, limit): warps claim
-// chunks of WCH candidates from a shared counter, keep their own window of
-// visited cells, load UPL candidates per lane at once and add the table
+// chunks of 32 * U candidates from a shared counter, keep their own window of
+// visited cells, load U candidates per lane at once and add the table
 // entries in the reference's order.  WARM == true stores every candidate's
 // (distance, position) at warm[flat]; otherwise candidates with a distance
 // word <= tau are appended to out[] (global, capacity cap) through
 // warp-aggregated atomics on st.npend.
-template <int MPC, bool WARM>
+template <int MPC, bool WARM, int U>
 __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, QState &st, const ScanCtx &c,
                                             uint32_t limit, uint32_t tau, uint64_t *warm, uint64_t *out,
                                             uint32_t cap) {
@@ -618,10 +618,11 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
     int wcn = 0;
     for (;;) {
         uint32_t base = 0;
-        if (lane == 0) base = atomicAdd(&st.next_flat, (uint32_t)WCH);
+        constexpr uint32_t WCH = 32u * U;
+        if (lane == 0) base = atomicAdd(&st.next_flat, WCH);
         base = __shfl_sync(FULL, base, 0);
         if (base >= limit) break;
-        const uint32_t end = min(base + (uint32_t)WCH, limit);
+        const uint32_t end = min(base + WCH, limit);
         uint32_t f = base;
         while (f < end) {
             if (f < wlo || f >= whi) {
@@ -666,13 +667,13 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
                 whi = (ci + wcn < c.nvis) ? c.vis_pre[ci + wcn] : c.Svis;
             }
             const uint32_t e2 = min(end, whi);
-            // loads of UPL candidates per lane, issued together
-            uint32_t pos[UPL], h34[UPL];
-            float dd[UPL], vt[UPL];
-            CodeWords<MPC> cwd[UPL];
+            // loads of U candidates per lane, issued together
+            uint32_t pos[U], h34[U];
+            float dd[U], vt[U];
+            CodeWords<MPC> cwd[U];
             int ci = 0;
 #pragma unroll
-            for (int u = 0; u < UPL; u++) {
+            for (int u = 0; u < U; u++) {
                 const uint32_t ff = f + lane + 32u * u;
                 pos[u] = 0xffffffffu;
                 if (ff < e2) {
@@ -686,16 +687,28 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
                 }
             }
 #pragma unroll
-            for (int u = 0; u < UPL; u++) {
+            for (int u = 0; u < U; u++) {
                 bool pass = false;
                 uint32_t du = 0;
                 if (pos[u] != 0xffffffffu) {
                     float d = dd[u];
                     const uint32_t h3 = h34[u] & 0xffffu, h4 = h34[u] >> 16;
                     if (c.fast) {
-                        // d0 + per-vector term + sum_k LUT[k][c_k]
+                        // d0 + per-vector term + sum_k LUT[k][c_k], the LUT
+                        // entries summed as a tree (independent adds)
                         d = __fadd_rn(d, vt[u]);
-                        for (int k = 0; k < cwd[u].n(c.mp); k++) d = __fadd_rn(d, S.lut[k * c.kp + cwd[u].code(k)]);
+                        if constexpr (MPC > 0) {
+                            float v[MPC];
+#pragma unroll
+                            for (int k = 0; k < MPC; k++) v[k] = S.lut[k * c.kp + cwd[u].code(k)];
+#pragma unroll
+                            for (int s2 = 1; s2 < MPC; s2 <<= 1)
+#pragma unroll
+                                for (int k = 0; k + s2 < MPC; k += 2 * s2) v[k] = __fadd_rn(v[k], v[k + s2]);
+                            d = __fadd_rn(d, v[0]);
+                        } else {
+                            for (int k = 0; k < cwd[u].n(c.mp); k++) d = __fadd_rn(d, S.lut[k * c.kp + cwd[u].code(k)]);
+                        }
                     } else if (c.imi) {
                         // multi_query.h:237-254: two adds per subspace
                         const int half = c.mp >> 1;
@@ -776,7 +789,7 @@ __device__ uint32_t block_kth_hi(const uint64_t *keys, int n, int k, uint32_t *h
     return prefix;
 }
 
-template <int MPC>
+template <int MPC, int U>
 __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint64_t red[3 * NWARP];
@@ -837,60 +850,79 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
         Lists L;
         for (int attempt = 0; attempt < 2; attempt++) {
             const bool full = attempt == 1 || M >= kc;
-            // (1) coarse lists (sort_id/nth_element_id with M = kc;
-            //     multi_query.h:114-128, sc_query.h:98-106, query.h:230-234):
-            //     ordered key << 32 | centroid id; equal keys by id.
-            for (int h = tid; h < kcP; h += NT) {
-                if (h < kc) {
-                    float ka = __fadd_rn(imi ? qn0 : qs, dqc[h]);
-                    S.LA[h] = ((uint64_t)f2o(ka) << 32) | (uint32_t)h;
-                    if (imi) {
-                        float kb = __fadd_rn(qn1, dqc[kc + h]);
-                        S.LB[h] = ((uint64_t)f2o(kb) << 32) | (uint32_t)h;
-                    }
-                } else {
-                    S.LA[h] = ~0ull;
-                    if (imi) S.LB[h] = ~0ull;
-                }
-            }
-            if (tid == 0) {
-                st.err = 0;
-                st.kA = kc;
-                st.kB = kBfull;
-                st.nextA = 0xffffffffu;
-                st.nextB = 0xffffffffu;
-            }
-            __syncthreads();
             bool done_a = false, done_b = !imi;
-            if (!full) {
-                int ca = select_prefix(S.LA, kc, M, sb, hist, red, st, &st.nextA);
-                if (ca > 0) {
-                    done_a = true;
-                    if (tid == 0) st.kA = ca;
+            if (a.slist && attempt == 0) {
+                // prefixes sorted ahead by k_coarse_prefix (same prefix rule)
+                const int nl = imi ? 2 : 1;
+                const uint64_t *src = a.slist + (size_t)q * nl * a.slist_w;
+                const uint32_t *meta = a.smeta + (size_t)q * nl * 2;
+                const int ca = (int)meta[0], cb = imi ? (int)meta[2] : 0;
+                for (int h = tid; h < ca; h += NT) S.LA[h] = src[h];
+                for (int h = tid; h < cb; h += NT) S.LB[h] = src[a.slist_w + h];
+                if (tid == 0) {
+                    st.err = 0;
+                    st.kA = ca;
+                    st.kB = imi ? cb : kBfull;
+                    st.nextA = meta[1];
+                    st.nextB = imi ? meta[3] : 0xffffffffu;
                 }
-                if (imi) {
-                    int cb = select_prefix(S.LB, kc, M, sb, hist, red, st, &st.nextB);
-                    if (cb > 0) {
-                        done_b = true;
-                        if (tid == 0) st.kB = cb;
+                done_a = done_b = true;
+                __syncthreads();
+            } else {
+                // (1) coarse lists (sort_id/nth_element_id with M = kc;
+                //     multi_query.h:114-128, sc_query.h:98-106, query.h:230-234):
+                //     ordered key << 32 | centroid id; equal keys by id.
+                for (int h = tid; h < kcP; h += NT) {
+                    if (h < kc) {
+                        float ka = __fadd_rn(imi ? qn0 : qs, dqc[h]);
+                        S.LA[h] = ((uint64_t)f2o(ka) << 32) | (uint32_t)h;
+                        if (imi) {
+                            float kb = __fadd_rn(qn1, dqc[kc + h]);
+                            S.LB[h] = ((uint64_t)f2o(kb) << 32) | (uint32_t)h;
+                        }
+                    } else {
+                        S.LA[h] = ~0ull;
+                        if (imi) S.LB[h] = ~0ull;
                     }
+                }
+                if (tid == 0) {
+                    st.err = 0;
+                    st.kA = kc;
+                    st.kB = kBfull;
+                    st.nextA = 0xffffffffu;
+                    st.nextB = 0xffffffffu;
                 }
                 __syncthreads();
-                if (!done_a || !done_b) {
-                    // a prefix beyond SBCAP: sort everything instead
-                    done_a = done_b = false;
-                    for (int h = tid; h < kcP; h += NT) {
-                        if (h < kc) {
-                            S.LA[h] = ((uint64_t)f2o(__fadd_rn(imi ? qn0 : qs, dqc[h])) << 32) | (uint32_t)h;
-                            if (imi) S.LB[h] = ((uint64_t)f2o(__fadd_rn(qn1, dqc[kc + h])) << 32) | (uint32_t)h;
+                if (!full) {
+                    int ca = select_prefix(S.LA, kc, M, sb, hist, red, st, &st.nextA);
+                    if (ca > 0) {
+                        done_a = true;
+                        if (tid == 0) st.kA = ca;
+                    }
+                    if (imi) {
+                        int cb = select_prefix(S.LB, kc, M, sb, hist, red, st, &st.nextB);
+                        if (cb > 0) {
+                            done_b = true;
+                            if (tid == 0) st.kB = cb;
                         }
                     }
-                    if (tid == 0) {
-                        st.kA = kc;
-                        st.kB = kBfull;
-                        st.nextA = st.nextB = 0xffffffffu;
-                    }
                     __syncthreads();
+                    if (!done_a || !done_b) {
+                        // a prefix beyond SBCAP: sort everything instead
+                        done_a = done_b = false;
+                        for (int h = tid; h < kcP; h += NT) {
+                            if (h < kc) {
+                                S.LA[h] = ((uint64_t)f2o(__fadd_rn(imi ? qn0 : qs, dqc[h])) << 32) | (uint32_t)h;
+                                if (imi) S.LB[h] = ((uint64_t)f2o(__fadd_rn(qn1, dqc[kc + h])) << 32) | (uint32_t)h;
+                            }
+                        }
+                        if (tid == 0) {
+                            st.kA = kc;
+                            st.kB = kBfull;
+                            st.nextA = st.nextB = 0xffffffffu;
+                        }
+                        __syncthreads();
+                    }
                 }
             }
             if (!done_a) bitonic_sort64(S.LA, kcP);
@@ -1204,7 +1236,7 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
             c.qs = qs;
             c.dqc = dqc;
             const uint32_t K = Svis < (uint32_t)WARMN ? Svis : (uint32_t)WARMN;
-            scan_chunks<MPC, true>(a, S, st, c, K, 0u, S.warm, nullptr, 0u);
+            scan_chunks<MPC, true, U>(a, S, st, c, K, 0u, S.warm, nullptr, 0u);
             __syncthreads();
             uint32_t tau = 0xffffffffu;
             if (K > (uint32_t)R) tau = block_kth_hi(S.warm, (int)K, R, S.hist2, red, st);
@@ -1224,7 +1256,7 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
                 }
                 __syncthreads();
             }
-            scan_chunks<MPC, false>(a, S, st, c, Svis, tau, nullptr, pend_g, a.pcap);
+            scan_chunks<MPC, false, U>(a, S, st, c, Svis, tau, nullptr, pend_g, a.pcap);
             __syncthreads();
             PHASE_MARK(4);  // scan
             if ((uint32_t)st.npend > a.pcap) {
@@ -1274,43 +1306,61 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
 
 size_t search_smem_bytes(int mode, int kc, int mp, int kp) { return carve(mode, kc, mp, kp, nullptr, nullptr); }
 
-template <int MPC>
+template <int MPC, int U>
 static int occupancy(size_t smem) {
-    cudaFuncSetAttribute(k_search<MPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_search<MPC, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<MPC>, NT, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<MPC, U>, NT, smem);
     return nb;
 }
 
-int search_max_blocks_per_sm(int mode, int kc, int mp, int kp) {
-    size_t smem = search_smem_bytes(mode, kc, mp, kp);
+template <int U>
+static int occupancy_mp(int mp, size_t smem) {
     switch (mp) {
-        case 4: return occupancy<4>(smem);
-        case 8: return occupancy<8>(smem);
-        case 16: return occupancy<16>(smem);
-        case 32: return occupancy<32>(smem);
-        default: return occupancy<0>(smem);
+        case 4: return occupancy<4, U>(smem);
+        case 8: return occupancy<8, U>(smem);
+        case 16: return occupancy<16, U>(smem);
+        case 32: return occupancy<32, U>(smem);
+        default: return occupancy<0, U>(smem);
     }
 }
 
-template <int MPC>
+int search_max_blocks_per_sm(int mode, int kc, int mp, int kp, int upl) {
+    const size_t smem = search_smem_bytes(mode, kc, mp, kp);
+    switch (upl) {
+        case 2: return occupancy_mp<2>(mp, smem);
+        case 8: return occupancy_mp<8>(mp, smem);
+        default: return occupancy_mp<4>(mp, smem);
+    }
+}
+
+template <int MPC, int U>
 static int launch(const SearchArgs &a, int grid, size_t smem, cudaStream_t s) {
-    cudaError_t e = cudaFuncSetAttribute(k_search<MPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_search<MPC, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_search)");
-    k_search<MPC><<<grid, NT, smem, s>>>(a);
+    k_search<MPC, U><<<grid, NT, smem, s>>>(a);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "k_search launch");
     return SCG_OK;
 }
 
-int search_launch(const SearchArgs &a, int grid, cudaStream_t s) {
-    size_t smem = search_smem_bytes(a.mode, a.kc, a.mp, a.kp);
+template <int U>
+static int launch_mp(const SearchArgs &a, int grid, size_t smem, cudaStream_t s) {
     switch (a.mp) {
-        case 4: return launch<4>(a, grid, smem, s);
-        case 8: return launch<8>(a, grid, smem, s);
-        case 16: return launch<16>(a, grid, smem, s);
-        case 32: return launch<32>(a, grid, smem, s);
-        default: return launch<0>(a, grid, smem, s);
+        case 4: return launch<4, U>(a, grid, smem, s);
+        case 8: return launch<8, U>(a, grid, smem, s);
+        case 16: return launch<16, U>(a, grid, smem, s);
+        case 32: return launch<32, U>(a, grid, smem, s);
+        default: return launch<0, U>(a, grid, smem, s);
+    }
+}
+
+int search_launch(const SearchArgs &a, int grid, cudaStream_t s) {
+    const size_t smem = search_smem_bytes(a.mode, a.kc, a.mp, a.kp);
+    switch (a.upl) {
+        case 2: return launch_mp<2>(a, grid, smem, s);
+        case 8: return launch_mp<8>(a, grid, smem, s);
+        default: return launch_mp<4>(a, grid, smem, s);
     }
 }
 

@@ -28,7 +28,7 @@ EXPORTS = ["scg_last_error", "scg_index_create", "scg_index_destroy", "scg_load_
            "scg_cell_counts", "scg_set_phase_counters", "scg_last_phase_counters",
            "scg_search_device_noalloc", "scg_query_tables_device", "scg_load_raw_u8",
            "scg_server_create", "scg_server_submit", "scg_server_wait", "scg_server_stats",
-           "scg_server_destroy"]
+           "scg_server_destroy", "scg_autotune", "scg_set_scan_tuning"]
 
 
 class ScgError(RuntimeError):
@@ -175,6 +175,18 @@ class Index:
         _check(_lib.scg_query_tables_device(self._h, precision, ctypes.c_void_p(dQ_ptr), nq,
                                             ctypes.c_void_p(d_dqc), ctypes.c_void_p(d_dqr),
                                             ctypes.c_void_p(stream) if stream else None))
+
+    def autotune(self, mode, dQ_ptr, nq, R, w, T, d_ids, d_d, d_sums, precision=FP32_EXACT, rerank=0):
+        """Times the scan variants on a device batch; returns (choice, ms[3])."""
+        p = SearchParams(mode, R, w, T, precision, rerank)
+        c = ctypes.c_int()
+        ms = np.zeros(3, np.float32)
+        _check(_lib.scg_autotune(self._h, ctypes.byref(p), ctypes.c_void_p(dQ_ptr), nq, ctypes.c_void_p(d_ids),
+                                 ctypes.c_void_p(d_d), ctypes.c_void_p(d_sums), ctypes.byref(c), _ptr(ms)))
+        return c.value, ms.tolist()
+
+    def set_scan_tuning(self, precision, upl):
+        _check(_lib.scg_set_scan_tuning(self._h, precision, upl))
 
     def set_query_targets(self, d_T_ptr):
         _check(_lib.scg_set_query_targets(self._h, ctypes.c_void_p(d_T_ptr) if d_T_ptr else None))
