@@ -103,7 +103,9 @@ int scg_load_raw_u8(scg_index *h, const uint8_t *X, int64_t N);
  * term of the fast form.  Replaces PQQuery::pre_compute1 (query.h:91-149). */
 int scg_precompute(scg_index *h);
 
-/* Batched search with HOST buffers: Q[nq][dim] in, ids[nq][R], dists[nq][R],
+/* Batched search with HOST buffers (batches of 1024 or more queries run in
+ * 2 or 4 chunks over two streams, so that copies overlap the search):
+ * Q[nq][dim] in, ids[nq][R], dists[nq][R],
  * sums[nq] out (sums may be NULL).  Each query returns its top min(R, sum)
  * candidates in ascending distance (equal distances by id); unused slots hold
  * id -1 and distance +inf.  `sum` is the candidate count the reference
@@ -188,9 +190,11 @@ int scg_encode_device(scg_index *h, const float *dX, int64_t n, int nc, uint16_t
 int scg_last_query_stats(scg_index *h, int *nvis, int *empty, int nq);
 
 /* Device time in milliseconds of the kernels of the last search call,
- * measured with CUDA events on its stream: ms[0] the per-query tables,
- * ms[1] the fused selection + scan, ms[2] the shortlist re-rank (0 without
- * one).  n is the capacity of ms. */
+ * measured with CUDA events on its stream: ms[0] the per-query tables and
+ * coarse-list prefixes, ms[1] the fused selection + scan, ms[2] the
+ * shortlist re-rank (0 without one).  After scg_search (host buffers), which
+ * runs large batches in chunks over two streams, the figures are those of
+ * the last chunk on the index's own stream.  n is the capacity of ms. */
 int scg_last_timings(scg_index *h, float *ms, int n);
 
 /* Copies the cell lengths back as the reference's inclusive prefix L[ncells]

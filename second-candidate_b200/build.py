@@ -7,7 +7,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libscgpu.so")
-SOURCES = ["api.cu", "tables.cu", "tables_tc.cu", "search.cu", "encode.cu", "rerank.cu", "server.cu", "coarse.cu"]
+SOURCES = ["search_u4.cu", "search_u2.cu", "search_u8.cu", "api.cu", "tables.cu", "tables_tc.cu", "search.cu",
+           "encode.cu", "rerank.cu", "server.cu", "coarse.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
@@ -22,17 +23,25 @@ def _stale():
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force=False, verbose=False):
+def build(force=False, verbose=False, jobs=None):
+    """Compiles every source for sm_100a (in parallel) and links libscgpu.so
+    in-tree; does nothing when the library is newer than every source."""
     if not force and not _stale():
         return LIB
-    objs = []
-    for src in SOURCES:
-        obj = os.path.join(CSRC, src.replace(".cu", ".o"))
-        cmd = [NVCC] + FLAGS + ["-I", os.path.join(ROOT, "include"), "-c", os.path.join(CSRC, src), "-o", obj]
-        if verbose:
-            print(" ".join(cmd), file=sys.stderr)
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
+    from concurrent.futures import ThreadPoolExecutor
+    objs = [os.path.join(CSRC, src.replace(".cu", ".o")) for src in SOURCES]
+    cmds = [[NVCC] + FLAGS + ["-I", os.path.join(ROOT, "include"), "-c", os.path.join(CSRC, src), "-o", obj]
+            for src, obj in zip(SOURCES, objs)]
+    if verbose:
+        for c in cmds:
+            print(" ".join(c), file=sys.stderr)
+    jobs = jobs or min(len(cmds), max(1, os.cpu_count() or 1))
+    with ThreadPoolExecutor(jobs) as ex:
+        results = list(ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds))
+    for c, r in zip(cmds, results):
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise subprocess.CalledProcessError(r.returncode, c)
     tmp = LIB + ".tmp"
     subprocess.run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp] + objs + ["-lcudart"], check=True)
     os.replace(tmp, LIB)

@@ -1,5 +1,6 @@
 // C ABI of libscgpu.so (include/scg.h): the index handle, loaders, and the
 // host orchestration of the batched search and the encoders.
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -240,7 +241,7 @@ int index_mode(const scg_index *h) {
 }
 
 int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_params *p, const float *dQ, int nq,
-               int *d_ids, float *d_d, int *d_sums, cudaStream_t s, bool wait) {
+               int *d_ids, float *d_d, int *d_sums, cudaStream_t s, bool wait, int *h_stat) {
     int rc;
     if ((rc = ws->init())) return rc;
     // with a shortlist re-rank the ADC search keeps L candidates per query
@@ -364,10 +365,11 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     }
     SCG_CUDA(cudaEventRecord(ws->ev[3], s));
     ws->last_nq = nq;
-    SCG_CUDA(cudaMemcpyAsync(ws->h_status, ws->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    int *dst = h_stat ? h_stat : ws->h_status;
+    SCG_CUDA(cudaMemcpyAsync(dst, ws->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     if (!wait) return SCG_OK;
     SCG_CUDA(cudaStreamSynchronize(s));
-    return status_result(*ws->h_status);
+    return status_result(*dst);
 }
 
 }  // namespace scg
@@ -396,9 +398,15 @@ int scg_index_create(scg_index **out, int device) {
         delete h;
         return cuda_fail(e, "scg_index_create");
     }
-    int rc = h->ws.init();
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->stream2, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&h->h_chunk_status, sizeof(int) * 8);
+    int rc = e == cudaSuccess ? h->ws.init() : cuda_fail(e, "scg_index_create");
+    if (rc == SCG_OK) rc = h->ws2.init();
     if (rc) {
         h->ws.release();
+        h->ws2.release();
+        if (h->h_chunk_status) cudaFreeHost(h->h_chunk_status);
+        if (h->stream2) cudaStreamDestroy(h->stream2);
         cudaStreamDestroy(h->stream);
         delete h;
         return rc;
@@ -412,9 +420,13 @@ int scg_index_destroy(scg_index *h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     DevBuf *all[] = {&h->cq, &h->pq, &h->norm_c, &h->norm_r, &h->dot_cr, &h->off, &h->pid, &h->codes,
-                     &h->raw, &h->vterm, &h->q, &h->ids, &h->dists, &h->sums};
+                     &h->raw, &h->vterm, &h->q, &h->ids, &h->dists, &h->sums, &h->reqbuf};
     for (DevBuf *b : all) b->release();
+    if (h->stream2) cudaStreamSynchronize(h->stream2);
     h->ws.release();
+    h->ws2.release();
+    if (h->h_chunk_status) cudaFreeHost(h->h_chunk_status);
+    if (h->stream2) cudaStreamDestroy(h->stream2);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return SCG_OK;
@@ -581,23 +593,66 @@ int scg_search(scg_index *h, const scg_search_params *p, const float *Q, int nq,
     std::lock_guard<std::mutex> g(h->mu);
     if ((rc = set_device(h))) return rc;
     if (nq == 0) return SCG_OK;
-    cudaStream_t s = h->stream;
     const int R = p->R;
     if ((rc = h->q.ensure(sizeof(float) * (size_t)nq * h->dim))) return rc;
     if ((rc = h->ids.ensure(sizeof(int) * (size_t)nq * R))) return rc;
     if ((rc = h->dists.ensure(sizeof(float) * (size_t)nq * R))) return rc;
     if ((rc = h->sums.ensure(sizeof(int) * (size_t)nq))) return rc;
-    SCG_CUDA(cudaMemcpyAsync(h->q.p, Q, sizeof(float) * (size_t)nq * h->dim, cudaMemcpyHostToDevice, s));
-    const int *saved = h->d_Tq;
-    h->d_Tq = nullptr;
-    rc = run_search(h, &h->ws, nullptr, p, h->q.as<float>(), nq, h->ids.as<int>(), h->dists.as<float>(),
-                    h->sums.as<int>(), s, true);
-    h->d_Tq = saved;
-    if (rc) return rc;
-    SCG_CUDA(cudaMemcpyAsync(ids, h->ids.p, sizeof(int) * (size_t)nq * R, cudaMemcpyDeviceToHost, s));
-    SCG_CUDA(cudaMemcpyAsync(dists, h->dists.p, sizeof(float) * (size_t)nq * R, cudaMemcpyDeviceToHost, s));
-    if (sums) SCG_CUDA(cudaMemcpyAsync(sums, h->sums.p, sizeof(int) * (size_t)nq, cudaMemcpyDeviceToHost, s));
-    SCG_CUDA(cudaStreamSynchronize(s));
+    if ((rc = h->ws.nvis.ensure(sizeof(int) * (size_t)nq))) return rc;
+    if ((rc = h->ws.empty.ensure(sizeof(int) * (size_t)nq))) return rc;
+    // The batch runs in chunks alternating over two streams, so that the
+    // copies of one chunk overlap the search of another.  All chunks are
+    // enqueued before the first copy-out (a copy into pageable memory waits
+    // for its stream).
+    const int nch = nq >= 4096 ? 4 : (nq >= 1024 ? 2 : 1);
+    const int per = (nq + nch - 1) / nch;
+    size_t off_b[8];
+    size_t total = 0;
+    for (int c = 0; c < nch; c++) {
+        const int n = std::min(per, nq - c * per);
+        off_b[c] = total;
+        total += req_bytes(n, h->dim, h->mc, h->kc, h->mp, h->kp, R, p->rerank);
+    }
+    if ((rc = h->reqbuf.ensure(total))) return rc;
+    cudaStream_t ss[2] = {h->stream, h->stream2};
+    Workspace *ww[2] = {&h->ws, &h->ws2};
+    for (int c = 0; c < nch; c++) {
+        const int q0 = c * per, n = std::min(per, nq - q0);
+        cudaStream_t s = ss[c & 1];
+        ReqBufs rb = carve_req(h->reqbuf.as<unsigned char>() + off_b[c], n, h->mc, h->kc, h->mp, h->kp, p->rerank);
+        float *dq = h->q.as<float>() + (size_t)q0 * h->dim;
+        SCG_CUDA(cudaMemcpyAsync(dq, Q + (size_t)q0 * h->dim, sizeof(float) * (size_t)n * h->dim,
+                                 cudaMemcpyHostToDevice, s));
+        h->h_chunk_status[c] = 0;
+        rc = run_search(h, ww[c & 1], &rb, p, dq, n, h->ids.as<int>() + (size_t)q0 * R,
+                        h->dists.as<float>() + (size_t)q0 * R, h->sums.as<int>() + q0, s, false,
+                        &h->h_chunk_status[c]);
+        if (rc) {
+            cudaStreamSynchronize(h->stream);
+            cudaStreamSynchronize(h->stream2);
+            return rc;
+        }
+        // per-query facts for scg_last_query_stats, in batch order
+        SCG_CUDA(cudaMemcpyAsync(h->ws.nvis.as<int>() + q0, rb.nvis, sizeof(int) * (size_t)n,
+                                 cudaMemcpyDeviceToDevice, s));
+        SCG_CUDA(cudaMemcpyAsync(h->ws.empty.as<int>() + q0, rb.empty, sizeof(int) * (size_t)n,
+                                 cudaMemcpyDeviceToDevice, s));
+    }
+    for (int c = 0; c < nch; c++) {
+        const int q0 = c * per, n = std::min(per, nq - q0);
+        cudaStream_t s = ss[c & 1];
+        SCG_CUDA(cudaMemcpyAsync(ids + (size_t)q0 * R, h->ids.as<int>() + (size_t)q0 * R, sizeof(int) * (size_t)n * R,
+                                 cudaMemcpyDeviceToHost, s));
+        SCG_CUDA(cudaMemcpyAsync(dists + (size_t)q0 * R, h->dists.as<float>() + (size_t)q0 * R,
+                                 sizeof(float) * (size_t)n * R, cudaMemcpyDeviceToHost, s));
+        if (sums)
+            SCG_CUDA(cudaMemcpyAsync(sums + q0, h->sums.as<int>() + q0, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    }
+    SCG_CUDA(cudaStreamSynchronize(h->stream));
+    SCG_CUDA(cudaStreamSynchronize(h->stream2));
+    h->ws.last_nq = nq;
+    for (int c = 0; c < nch; c++)
+        if (h->h_chunk_status[c]) return status_result(h->h_chunk_status[c]);
     return SCG_OK;
 }
 

@@ -83,7 +83,11 @@ struct scg_index {
     bool raw_u8 = false;    // raw vectors held as uint8
     int tuned_upl[2] = {4, 4};  // scan candidates per lane, per scan form (exact, fast)
     scg::Workspace ws;      // the workspace of the index's own entry points
-    scg::DevBuf q, ids, dists, sums;  // host-buffer staging of scg_search
+    // scg_search (host buffers) pipelines a batch in chunks over two streams
+    cudaStream_t stream2 = nullptr;
+    scg::Workspace ws2;
+    int *h_chunk_status = nullptr;  // pinned [8]
+    scg::DevBuf q, ids, dists, sums, reqbuf;  // device staging of scg_search
     std::mutex mu;
 };
 
@@ -98,8 +102,10 @@ int ensure_vterm(scg_index *h, cudaStream_t s);
 // wait = true: synchronises and returns the status; false: returns after
 // enqueueing, the status word lands in ws->h_status when the stream reaches
 // it and is read by status_result(ws).
+// h_stat (optional): pinned int that receives the status word instead of
+// ws->h_status.
 int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_params *p, const float *dQ, int nq,
-               int *d_ids, float *d_d, int *d_sums, cudaStream_t s, bool wait);
+               int *d_ids, float *d_d, int *d_sums, cudaStream_t s, bool wait, int *h_stat = nullptr);
 int status_result(int st);
 // Grows a workspace to a search grid of `grid` CTAs (<= 0: a full grid).
 int reserve_search(scg_index *h, Workspace *ws, int mode, int grid);

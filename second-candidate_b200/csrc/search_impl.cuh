@@ -1,0 +1,1350 @@
+// Fused batched search (the kernel template; search_u2/u4/u8.cu instantiate it): per query, coarse ranking -> multi-sequence cell
+// selection -> ADC scan with a fused top-R.  One CTA works on one query at a
+// time and takes the next query from a global counter, so queries with
+// uneven posting-list totals balance across the persistent grid.
+//
+// Coarse ranking.  The reference sorts each coarse list completely
+// (nth_element_id + sort_id with M = kc, multi_query.h:125-128).  Only a
+// prefix of each sorted list is ever reached, so a radix select finds the
+// prefix of the M smallest keys (ties included) and sorts only it.  If the
+// cell selection below then reaches a key at or beyond the smallest key a
+// cell outside the prefix grid can have, the lists are sorted completely and
+// the selection is repeated -- the result is the same as with full sorts.
+//
+// Cell selection.  The reference walks the grid of rank pairs (h1, h2) of the
+// two sorted lists with a binary heap (multi_query.h:133-205,
+// sc_query.h:112-186) and stops after the first cell at which the candidate
+// total reaches T (or the cell cap w).  The visited set is therefore a
+// prefix of the cells sorted by key(h1,h2) = A[h1] + B[h2].  Here the prefix
+// is found without a serial heap:
+//   1. rounds of "all cells with key <= tau": tau is bisected so that the
+//      staircase {key <= tau} holds about a target number of cells (one
+//      binary search per row, all rows in parallel); the new cells of the
+//      round are enumerated, their lengths read from the CSR offsets and
+//      kept as records (key, rank pair, length) in a per-CTA scratch slot;
+//   2. once the totals reach T (or w), the exact cut key is found by a radix
+//      select over the last round's records, weighted by length (or by
+//      cell count for the w rule);
+//   3. cells tied at the cut key are taken in (rank1, rank2) order until the
+//      rule fires -- the order an exact priority queue yields.
+// The ADC scan then scores the first WARMN candidates into shared memory;
+// their R-th smallest distance bounds the final R-th distance, so a
+// barrier-free warp-centric scan of the rest (warps claim chunks of
+// candidates, keep their own window of visited cells, and add the table
+// entries in the reference's order) keeps only candidates at or below that
+// bound, and one radix-select merge over them gives the R best.
+#pragma once
+
+#include "scg_internal.cuh"
+
+namespace scg {
+
+namespace {
+
+constexpr int NT = 256;
+constexpr int NWARP = NT / 32;
+constexpr int HBITS = 11;
+constexpr int HBINS = 1 << HBITS;
+constexpr int TIECAP = 64;
+constexpr int RMAX = 1024;      // largest R
+constexpr int WARMN = 4096;     // candidates scored before the threshold is set
+constexpr int WWIN = 32;        // per-warp window of visited cells
+// Candidates per lane per claimed chunk (U, a template parameter of the
+// scan: 2, 4 or 8); a warp claims 32 * U candidates at a time.
+constexpr int SBCAP = 2048;     // sorted coarse prefix capacity
+constexpr int MAX_ROUNDS = 64;
+
+struct CellWin {
+    uint32_t pre;    // candidates before this cell (flat index)
+    uint32_t start;  // CSR start
+    float d0;        // per-cell constant of the ADC sum
+    uint32_t h34;    // h3 | h4 << 16
+};
+
+__host__ __device__ __forceinline__ int next_pow2(int x) {
+    int p = 1;
+    while (p < x) p <<= 1;
+    return p;
+}
+__host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) & ~(size_t)15; }
+
+// Shared memory.  The LUT lives for the whole query; the selection phase
+// (coarse lists, staircase rows, histograms) and the scan phase (cell
+// windows, double-buffered candidate staging, top-R buffers) share the rest.
+struct Smem {
+    float *lut;
+    // selection phase
+    uint64_t *LA, *LB;
+    uint16_t *rowc, *rowp;
+    uint32_t *rowpre;
+    uint32_t *hist;   // HBINS
+    uint64_t *ties;   // TIECAP
+    uint64_t *sb;     // SBCAP (aliases hist/ties)
+    // scan phase (aliases the selection phase)
+    CellWin *wwin;    // [NWARP][WWIN]
+    uint64_t *warm;   // [WARMN]
+    uint64_t *top, *tmp;
+    uint32_t *hist2;
+    uint64_t *ties2;
+};
+
+__host__ __device__ inline size_t carve(int mode, int kc, int mp, int kp, Smem *s, unsigned char *base) {
+    const int kcP = next_pow2(kc);
+    size_t off = 0;
+    if (s) s->lut = (float *)(base + off);
+    off += align16((size_t)mp * kp * 4);
+    const size_t phase0 = off;
+    // selection phase
+    if (s) s->LA = (uint64_t *)(base + off);
+    off += (size_t)kcP * 8;
+    if (s) s->LB = (mode == SCG_IMI) ? (uint64_t *)(base + off) : s->LA;
+    off += (mode == SCG_IMI) ? (size_t)kcP * 8 : 0;
+    if (s) s->rowc = (uint16_t *)(base + off);
+    off += align16((size_t)kc * 2);
+    if (s) s->rowp = (uint16_t *)(base + off);
+    off += align16((size_t)kc * 2);
+    if (s) s->rowpre = (uint32_t *)(base + off);
+    off += align16((size_t)(kc + 1) * 4);
+    if (s) {
+        s->hist = (uint32_t *)(base + off);
+        s->ties = (uint64_t *)(base + off + (size_t)HBINS * 4);
+        s->sb = (uint64_t *)(base + off);
+    }
+    size_t trav = (size_t)HBINS * 4 + (size_t)TIECAP * 8;
+    size_t sbb = (size_t)SBCAP * 8;
+    off += trav > sbb ? trav : sbb;
+    const size_t end1 = off;
+    // scan phase (aliases the selection phase)
+    off = phase0;
+    if (s) s->wwin = (CellWin *)(base + off);
+    off += (size_t)NWARP * WWIN * sizeof(CellWin);
+    if (s) s->warm = (uint64_t *)(base + off);
+    off += (size_t)WARMN * 8;
+    if (s) s->top = (uint64_t *)(base + off);
+    off += (size_t)RMAX * 8;
+    if (s) s->tmp = (uint64_t *)(base + off);
+    off += (size_t)RMAX * 8;
+    if (s) s->hist2 = (uint32_t *)(base + off);
+    off += (size_t)HBINS * 4;
+    if (s) s->ties2 = (uint64_t *)(base + off);
+    off += (size_t)TIECAP * 8;
+    return off > end1 ? off : end1;
+}
+
+// ---------------------------------------------------------------------------
+// Block-wide helpers (NT threads, all threads must call)
+
+__device__ __forceinline__ uint64_t warp_sum64(uint64_t v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sums three values over the block.
+__device__ void block_sum3(uint64_t &a, uint64_t &b, uint64_t &c, uint64_t *red) {
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    a = warp_sum64(a);
+    b = warp_sum64(b);
+    c = warp_sum64(c);
+    __syncthreads();
+    if (lane == 0) {
+        red[wid] = a;
+        red[NWARP + wid] = b;
+        red[2 * NWARP + wid] = c;
+    }
+    __syncthreads();
+    uint64_t x = 0, y = 0, z = 0;
+    for (int i = 0; i < NWARP; i++) {
+        x += red[i];
+        y += red[NWARP + i];
+        z += red[2 * NWARP + i];
+    }
+    a = x;
+    b = y;
+    c = z;
+    __syncthreads();
+}
+
+__device__ uint64_t block_sum(uint64_t v, uint64_t *red) {
+    uint64_t b = 0, c = 0;
+    block_sum3(v, b, c, red);
+    return v;
+}
+
+// Minimum and maximum of one u64 per thread over the block.
+__device__ void block_minmax(uint64_t &mn, uint64_t &mx, uint64_t *red) {
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        uint64_t a = __shfl_xor_sync(0xffffffffu, mn, o);
+        uint64_t b = __shfl_xor_sync(0xffffffffu, mx, o);
+        mn = a < mn ? a : mn;
+        mx = b > mx ? b : mx;
+    }
+    __syncthreads();
+    if (lane == 0) {
+        red[wid] = mn;
+        red[NWARP + wid] = mx;
+    }
+    __syncthreads();
+    mn = ~0ull;
+    mx = 0;
+    for (int i = 0; i < NWARP; i++) {
+        mn = red[i] < mn ? red[i] : mn;
+        mx = red[NWARP + i] > mx ? red[NWARP + i] : mx;
+    }
+    __syncthreads();
+}
+
+// Exclusive scan of one u64 per thread; returns the exclusive prefix and the
+// block total.
+__device__ uint64_t block_exscan(uint64_t v, uint64_t *red, uint64_t &total) {
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    uint64_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint64_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    __syncthreads();
+    if (lane == 31) red[wid] = x;
+    __syncthreads();
+    uint64_t wpre = 0, tot = 0;
+    for (int i = 0; i < NWARP; i++) {
+        uint64_t r = red[i];
+        if (i < wid) wpre += r;
+        tot += r;
+    }
+    total = tot;
+    __syncthreads();
+    return wpre + x - v;
+}
+
+// Ascending bitonic sort of n (a power of two) u64 keys in shared memory.
+__device__ void bitonic_sort64(uint64_t *key, int n) {
+    for (int k = 2; k <= n; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < n; i += NT) {
+                int ixj = i ^ j;
+                if (ixj > i) {
+                    uint64_t x = key[i], y = key[ixj];
+                    bool up = (i & k) == 0;
+                    if ((x > y) == up) {
+                        key[i] = y;
+                        key[ixj] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+struct QState {
+    int err;
+    uint32_t s_bin;
+    uint64_t s_acc;
+    uint32_t kappa;
+    uint32_t rank_cut;
+    int take_all;
+    int nties;
+    uint64_t sumv, nv, nev;
+    int nvis;
+    int kA, kB;
+    uint32_t nextA, nextB;  // smallest key outside the sorted prefix (ordered)
+    // scan
+    int ncur, npend;
+    uint64_t thr;
+    uint32_t next_flat;  // next unclaimed candidate of the scan
+};
+
+// The prefix of a coarse list: the smallest keys of L[0..n) (u64: ordered
+// key << 32 | centroid id) up to and including every key equal to the m-th
+// smallest, sorted ascending into L[0..c).  Returns c, or -1 when the prefix
+// would exceed SBCAP (the caller then sorts the whole list).  st.nextA/B
+// receives the smallest ordered key left outside.
+__device__ int select_prefix(uint64_t *L, int n, int m, uint64_t *sb, uint32_t *hist, uint64_t *red,
+                             QState &st, uint32_t *next_out) {
+    const int tid = threadIdx.x;
+    // radix select (4 x 8 bits) of the m-th smallest high word
+    uint32_t prefix = 0;
+    uint64_t need = (uint64_t)m;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        hist[tid] = 0;  // NT == 256 bins
+        __syncthreads();
+        for (int i = tid; i < n; i += NT) {
+            uint32_t v = (uint32_t)(L[i] >> 32);
+            if (shift == 24 || (v >> (shift + 8)) == (prefix >> (shift + 8))) atomicAdd(&hist[(v >> shift) & 255u], 1u);
+        }
+        __syncthreads();
+        uint64_t cnt = hist[tid], tot;
+        uint64_t ex = block_exscan(cnt, red, tot);
+        if (ex < need && ex + cnt >= need) {
+            st.s_bin = (uint32_t)tid;
+            st.s_acc = ex;
+        }
+        __syncthreads();
+        prefix |= st.s_bin << shift;
+        need -= st.s_acc;
+        __syncthreads();
+    }
+    const uint32_t vm = prefix;
+    // compact every key with high word <= vm; smallest high word above vm
+    uint64_t mine = 0, mn = ~0ull, mx = 0;
+    for (int i = tid; i < n; i += NT) {
+        uint32_t v = (uint32_t)(L[i] >> 32);
+        if (v <= vm) mine++;
+        else if (v < mn) mn = v;
+    }
+    block_minmax(mn, mx, red);
+    uint64_t c;
+    uint64_t pos = block_exscan(mine, red, c);
+    if (c > (uint64_t)SBCAP) return -1;
+    for (int i = tid; i < n; i += NT) {
+        uint64_t k = L[i];
+        if ((uint32_t)(k >> 32) <= vm) sb[pos++] = k;
+    }
+    int c2 = next_pow2((int)c);
+    for (int i = (int)c + tid; i < c2; i += NT) sb[i] = ~0ull;
+    __syncthreads();
+    bitonic_sort64(sb, c2);
+    for (int i = tid; i < (int)c; i += NT) L[i] = sb[i];
+    if (tid == 0) *next_out = mn == ~0ull ? 0xffffffffu : (uint32_t)mn;
+    __syncthreads();
+    return (int)c;
+}
+
+// ---------------------------------------------------------------------------
+
+struct Lists {
+    const uint64_t *LA, *LB;
+    int kA, kB;  // sorted prefix lengths
+    int kc;      // codebook size (cell ids)
+    bool ivf;
+    __device__ __forceinline__ float a(int h) const { return o2f((uint32_t)(LA[h] >> 32)); }
+    __device__ __forceinline__ float b(int h) const { return ivf ? 0.0f : o2f((uint32_t)(LB[h] >> 32)); }
+    __device__ __forceinline__ uint32_t ta(int h) const { return (uint32_t)LA[h]; }
+    __device__ __forceinline__ uint32_t tb(int h) const { return (uint32_t)LB[h]; }
+    // number of h2 in [0, kB) with f2o(a + B[h2]) <= tau
+    __device__ __forceinline__ int row_count(float av, uint32_t tau) const {
+        if (f2o(__fadd_rn(av, b(0))) > tau) return 0;
+        int lo = 1, hi = kB;  // answer in [1, kB]
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (f2o(__fadd_rn(av, b(mid - 1))) <= tau) lo = mid;
+            else hi = mid - 1;
+        }
+        return lo;
+    }
+};
+
+__device__ uint64_t staircase_count(const Lists &L, uint32_t tau, uint64_t *red) {
+    uint64_t c = 0;
+    for (int h = threadIdx.x; h < L.kA; h += NT) {
+        float av = L.a(h);
+        if (f2o(__fadd_rn(av, L.b(0))) > tau) continue;
+        c += (uint64_t)L.row_count(av, tau);
+    }
+    return block_sum(c, red);
+}
+
+// Radix select over the last round's records [r0, r1): the smallest key x
+// with base + sum_{key <= x} weight >= need.  weight: 0 = length, 1 = one per
+// cell, 2 = one per non-empty cell.
+__device__ uint32_t radix_cut(const uint32_t *rk, const uint32_t *rc, int r0, int r1, uint32_t lo,
+                              uint32_t hi, uint64_t base, uint64_t need, int weight, uint32_t *hist,
+                              uint64_t *red, QState &st) {
+    uint32_t range = hi - lo;
+    int nbits = range ? 32 - __clz(range) : 0;
+    uint32_t prefix = 0;
+    uint64_t acc = base;
+    int shift = nbits;
+    while (shift > 0) {
+        int db = shift < HBITS ? shift : HBITS;
+        shift -= db;
+        int nb = 1 << db;
+        for (int i = threadIdx.x; i < nb; i += NT) hist[i] = 0;
+        __syncthreads();
+        int hs = shift + db;
+        for (int r = r0 + threadIdx.x; r < r1; r += NT) {
+            uint32_t rel = rk[r] - lo;
+            if (hs < 32 && (rel >> hs) != (prefix >> hs)) continue;
+            uint32_t dg = (rel >> shift) & (nb - 1);
+            uint32_t c = rc[r];
+            uint32_t wt = weight == 0 ? c : (weight == 1 ? 1u : (c > 0 ? 1u : 0u));
+            if (wt) atomicAdd(&hist[dg], wt);
+        }
+        __syncthreads();
+        // first bin at which acc + inclusive prefix >= need
+        int per = (nb + NT - 1) / NT;
+        int b0 = threadIdx.x * per;
+        uint64_t mine = 0;
+        for (int i = 0; i < per; i++)
+            if (b0 + i < nb) mine += hist[b0 + i];
+        uint64_t tot;
+        uint64_t ex = block_exscan(mine, red, tot);
+        uint64_t run = acc + ex;
+        for (int i = 0; i < per; i++) {
+            int bb = b0 + i;
+            if (bb >= nb) break;
+            uint64_t nxt = run + hist[bb];
+            if (run < need && nxt >= need) {
+                st.s_bin = (uint32_t)bb;
+                st.s_acc = run;
+            }
+            run = nxt;
+        }
+        __syncthreads();
+        prefix |= st.s_bin << shift;
+        acc = st.s_acc;
+        __syncthreads();
+    }
+    return lo + prefix;
+}
+
+__device__ __forceinline__ uint32_t cell_of(const Lists &L, uint32_t rank) {
+    int h1 = rank >> 16, h2 = rank & 0xffff;
+    return L.ivf ? L.ta(h1) : L.ta(h1) * (uint32_t)L.kc + L.tb(h2);
+}
+
+// The mp code bytes of one candidate.  MPC > 0: mp == MPC, loaded with
+// 16/8/4-byte vector loads (rows are MPC-byte aligned); MPC == 0: any mp,
+// byte loads on demand.
+template <int MPC>
+struct CodeWords {
+    uint32_t w[(MPC + 3) / 4];
+    __device__ __forceinline__ void load(const uint8_t *codes, uint32_t pos, int) {
+        const uint8_t *p = codes + (size_t)pos * MPC;
+        if constexpr (MPC % 16 == 0) {
+#pragma unroll
+            for (int i = 0; i < MPC / 16; i++) {
+                uint4 v = __ldg((const uint4 *)p + i);
+                w[4 * i] = v.x; w[4 * i + 1] = v.y; w[4 * i + 2] = v.z; w[4 * i + 3] = v.w;
+            }
+        } else if constexpr (MPC % 8 == 0) {
+#pragma unroll
+            for (int i = 0; i < MPC / 8; i++) {
+                uint2 v = __ldg((const uint2 *)p + i);
+                w[2 * i] = v.x; w[2 * i + 1] = v.y;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < MPC / 4; i++) w[i] = __ldg((const uint32_t *)p + i);
+        }
+    }
+    __device__ __forceinline__ void load_smem(const unsigned char *p, int) {
+        if constexpr (MPC % 16 == 0) {
+#pragma unroll
+            for (int i = 0; i < MPC / 16; i++) {
+                uint4 v = ((const uint4 *)p)[i];
+                w[4 * i] = v.x; w[4 * i + 1] = v.y; w[4 * i + 2] = v.z; w[4 * i + 3] = v.w;
+            }
+        } else if constexpr (MPC % 8 == 0) {
+#pragma unroll
+            for (int i = 0; i < MPC / 8; i++) {
+                uint2 v = ((const uint2 *)p)[i];
+                w[2 * i] = v.x; w[2 * i + 1] = v.y;
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < MPC / 4; i++) w[i] = ((const uint32_t *)p)[i];
+        }
+    }
+    __device__ __forceinline__ int n(int) const { return MPC; }
+    __device__ __forceinline__ uint32_t code(int k) const { return (w[k >> 2] >> ((k & 3) * 8)) & 0xffu; }
+};
+
+template <>
+struct CodeWords<0> {
+    const uint8_t *p;
+    __device__ __forceinline__ void load(const uint8_t *codes, uint32_t pos, int mp) { p = codes + (size_t)pos * mp; }
+    __device__ __forceinline__ void load_smem(const unsigned char *q, int) { p = q; }
+    __device__ __forceinline__ int n(int mp) const { return mp; }
+    __device__ __forceinline__ uint32_t code(int k) const { return p[k]; }
+};
+
+// Optional per-phase cycle counters (thread 0 of each CTA), accumulated
+// into a.phase_cycles[phase] when that pointer is set.
+#define PHASE_MARK(i)                                                                                 \
+    do {                                                                                              \
+        if (a.phase_cycles && tid == 0) {                                                             \
+            long long _t = clock64();                                                                 \
+            atomicAdd((unsigned long long *)&a.phase_cycles[(i)], (unsigned long long)(_t - t_prev)); \
+            t_prev = _t;                                                                              \
+        }                                                                                             \
+    } while (0)
+#define COUNT(i, v)                                                                                \
+    do {                                                                                           \
+        if (a.phase_cycles && tid == 0)                                                            \
+            atomicAdd((unsigned long long *)&a.phase_cycles[(i)], (unsigned long long)(v));        \
+    } while (0)
+
+// Keeps the R smallest of top[0..ncur) and the pending entries.  Pending
+// entries hold (distance, CSR position); they become (distance, id) here,
+// where the id loads of a whole buffer are issued together.  A radix select
+// over the distance words finds the R-th smallest distance v; every entry
+// below v is kept and the entries equal to v are taken in id order.  The top
+// list stays unsorted (the output step sorts it); st.thr becomes the R-th
+// smallest (distance, id) once R entries exist.
+__device__ void merge_topk(uint64_t *top, uint64_t *pend, uint64_t *tmp, uint32_t *hist, uint64_t *ties, int R,
+                           const int *pid, uint64_t *red, QState &st, int *status) {
+    const int tid = threadIdx.x;
+    const int na = st.ncur, nb = st.npend;
+    if (pid) {
+        for (int i = tid; i < nb; i += NT) {
+            uint64_t e = pend[i];
+            pend[i] = (e & 0xffffffff00000000ull) | (uint32_t)__ldg(pid + (uint32_t)e);
+        }
+    }
+    __syncthreads();
+    const int n = na + nb;
+    if (n <= R) {
+        for (int i = tid; i < nb; i += NT) top[na + i] = pend[i];
+        __syncthreads();
+        if (tid == 0) {
+            st.ncur = n;
+            st.npend = 0;
+            st.thr = ~0ull;
+        }
+        __syncthreads();
+        return;
+    }
+    // radix select (11 + 11 + 10 bits) of the R-th smallest distance word
+    uint32_t prefix = 0;
+    uint64_t need = (uint64_t)R;
+#pragma unroll
+    for (int p = 0; p < 3; p++) {
+        const int sh = p == 0 ? 21 : (p == 1 ? 10 : 0), bits = p == 2 ? 10 : 11, nbins = 1 << bits, hs = sh + bits;
+        for (int i = tid; i < nbins; i += NT) hist[i] = 0;
+        __syncthreads();
+        for (int i = tid; i < n; i += NT) {
+            uint32_t v = (uint32_t)((i < na ? top[i] : pend[i - na]) >> 32);
+            if (hs < 32 && (v >> hs) != (prefix >> hs)) continue;
+            atomicAdd(&hist[(v >> sh) & (nbins - 1)], 1u);
+        }
+        __syncthreads();
+        const int per = (nbins + NT - 1) / NT;
+        const int b0 = tid * per;
+        uint64_t mine = 0;
+        for (int i = 0; i < per; i++)
+            if (b0 + i < nbins) mine += hist[b0 + i];
+        uint64_t tot;
+        uint64_t run = block_exscan(mine, red, tot);
+        for (int i = 0; i < per; i++) {
+            int bb = b0 + i;
+            if (bb >= nbins) break;
+            uint64_t nxt = run + hist[bb];
+            if (run < need && nxt >= need) {
+                st.s_bin = (uint32_t)bb;
+                st.s_acc = run;
+            }
+            run = nxt;
+        }
+        __syncthreads();
+        prefix |= st.s_bin << sh;
+        need -= st.s_acc;
+        __syncthreads();
+    }
+    const uint32_t v = prefix;
+    // keep everything below v; gather the entries equal to v
+    uint64_t mine = 0;
+    for (int i = tid; i < n; i += NT) mine += ((uint32_t)((i < na ? top[i] : pend[i - na]) >> 32) < v);
+    uint64_t total;
+    uint64_t pos = block_exscan(mine, red, total);
+    if (tid == 0) st.nties = 0;
+    __syncthreads();
+    for (int i = tid; i < n; i += NT) {
+        uint64_t e = i < na ? top[i] : pend[i - na];
+        uint32_t hv = (uint32_t)(e >> 32);
+        if (hv < v) tmp[pos++] = e;
+        else if (hv == v) {
+            int slot = atomicAdd(&st.nties, 1);
+            if (slot < TIECAP) ties[slot] = e;
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        // `need` entries equal to v complete the R: the smallest ids
+        int nt = st.nties < TIECAP ? st.nties : TIECAP;
+        for (int i = 1; i < nt; i++) {
+            uint64_t x = ties[i];
+            int j = i - 1;
+            while (j >= 0 && ties[j] > x) {
+                ties[j + 1] = ties[j];
+                j--;
+            }
+            ties[j + 1] = x;
+        }
+        int take = (int)need;
+        if (take > nt) {
+            // more equal distances at the R-th place than the tie buffer holds
+            atomicOr(status, ST_TIE_OVERFLOW);
+            take = nt;
+        }
+        for (int i = 0; i < take; i++) tmp[total + i] = ties[i];
+        st.ncur = (int)total + take;
+        st.npend = 0;
+        st.thr = take > 0 ? ties[take - 1] : ~0ull;
+    }
+    __syncthreads();
+    for (int i = tid; i < st.ncur; i += NT) top[i] = tmp[i];
+    __syncthreads();
+}
+
+// Everything the candidate scan needs about one query.
+struct ScanCtx {
+    const uint32_t *vis_cell, *vis_pre;
+    int nvis;
+    uint32_t Svis;
+    int kc, mp, kp, bsI;
+    bool imi, sc, fast;
+    float qs;
+    const float *dqc;
+};
+
+// Warp-centric ADC scan of the candidates [st.next_flat, limit): warps claim
+// chunks of 32 * U candidates from a shared counter, keep their own window of
+// visited cells, load U candidates per lane at once and add the table
+// entries in the reference's order.  WARM == true stores every candidate's
+// (distance, position) at warm[flat]; otherwise candidates with a distance
+// word <= tau are appended to out[] (global, capacity cap) through
+// warp-aggregated atomics on st.npend.
+template <int MPC, bool WARM, int U>
+__device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, QState &st, const ScanCtx &c,
+                                            uint32_t limit, uint32_t tau, uint64_t *warm, uint64_t *out,
+                                            uint32_t cap) {
+    const unsigned FULL = 0xffffffffu;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    CellWin *W = S.wwin + wid * WWIN;
+    uint32_t wlo = 1, whi = 0;
+    int wcn = 0;
+    for (;;) {
+        uint32_t base = 0;
+        constexpr uint32_t WCH = 32u * U;
+        if (lane == 0) base = atomicAdd(&st.next_flat, WCH);
+        base = __shfl_sync(FULL, base, 0);
+        if (base >= limit) break;
+        const uint32_t end = min(base + WCH, limit);
+        uint32_t f = base;
+        while (f < end) {
+            if (f < wlo || f >= whi) {
+                // window of visited cells from the one holding f
+                int ci = 0;
+                if (lane == 0) {
+                    int lo = 0, hi = c.nvis - 1;
+                    while (lo < hi) {
+                        int mid = (lo + hi + 1) >> 1;
+                        if (c.vis_pre[mid] <= f) lo = mid;
+                        else hi = mid - 1;
+                    }
+                    ci = lo;
+                }
+                ci = __shfl_sync(FULL, ci, 0);
+                const int cc = ci + lane;
+                if (cc < c.nvis) {
+                    uint32_t cell = c.vis_cell[cc];
+                    CellWin cw;
+                    cw.pre = c.vis_pre[cc];
+                    cw.start = a.off[cell];
+                    uint32_t h3, h4;
+                    if (c.imi) {
+                        h3 = cell / (uint32_t)c.kc;
+                        h4 = cell - h3 * (uint32_t)c.kc;
+                        cw.d0 = __fadd_rn(__fadd_rn(c.qs, c.dqc[h3]), c.dqc[c.kc + h4]);
+                    } else if (c.sc) {
+                        h3 = cell / (uint32_t)c.kc;
+                        h4 = 0;
+                        cw.d0 = __fadd_rn(c.qs, c.dqc[h3]);
+                    } else {
+                        h3 = cell;
+                        h4 = 0;
+                        cw.d0 = __fadd_rn(c.qs, c.dqc[h3]);
+                    }
+                    cw.h34 = h3 | (h4 << 16);
+                    W[lane] = cw;
+                }
+                wcn = min(WWIN, c.nvis - ci);
+                __syncwarp();
+                wlo = W[0].pre;
+                whi = (ci + wcn < c.nvis) ? c.vis_pre[ci + wcn] : c.Svis;
+            }
+            const uint32_t e2 = min(end, whi);
+            // loads of U candidates per lane, issued together
+            uint32_t pos[U], h34[U];
+            float dd[U], vt[U];
+            CodeWords<MPC> cwd[U];
+            int ci = 0;
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const uint32_t ff = f + lane + 32u * u;
+                pos[u] = 0xffffffffu;
+                if (ff < e2) {
+                    while (ci + 1 < wcn && W[ci + 1].pre <= ff) ci++;
+                    const CellWin cw = W[ci];
+                    pos[u] = cw.start + (ff - cw.pre);
+                    dd[u] = cw.d0;
+                    h34[u] = cw.h34;
+                    cwd[u].load(a.codes, pos[u], c.mp);
+                    if (c.fast) vt[u] = __ldg(a.vterm + pos[u]);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                bool pass = false;
+                uint32_t du = 0;
+                if (pos[u] != 0xffffffffu) {
+                    float d = dd[u];
+                    const uint32_t h3 = h34[u] & 0xffffu, h4 = h34[u] >> 16;
+                    if (c.fast) {
+                        // d0 + per-vector term + sum_k LUT[k][c_k], the LUT
+                        // entries summed as a tree (independent adds)
+                        d = __fadd_rn(d, vt[u]);
+                        if constexpr (MPC > 0) {
+                            float v[MPC];
+#pragma unroll
+                            for (int k = 0; k < MPC; k++) v[k] = S.lut[k * c.kp + cwd[u].code(k)];
+#pragma unroll
+                            for (int s2 = 1; s2 < MPC; s2 <<= 1)
+#pragma unroll
+                                for (int k = 0; k + s2 < MPC; k += 2 * s2) v[k] = __fadd_rn(v[k], v[k + s2]);
+                            d = __fadd_rn(d, v[0]);
+                        } else {
+                            for (int k = 0; k < cwd[u].n(c.mp); k++) d = __fadd_rn(d, S.lut[k * c.kp + cwd[u].code(k)]);
+                        }
+                    } else if (c.imi) {
+                        // multi_query.h:237-254: two adds per subspace
+                        const int half = c.mp >> 1;
+                        const float *r1 = a.dot_cr + (size_t)h3 * c.bsI;
+                        const float *r2 = a.dot_cr + (size_t)(h4 + c.kc - 1) * c.bsI;
+                        for (int k = 0; k < cwd[u].n(c.mp); k++) {
+                            int bc = k * c.kp + cwd[u].code(k);
+                            d = __fadd_rn(d, S.lut[bc]);
+                            d = __fadd_rn(d, __ldg((k < half ? r1 : r2) + bc));
+                        }
+                    } else {
+                        // query.h:295-306, sc_query.h:222-229: pair sum per subspace
+                        const float *r1 = a.dot_cr + (size_t)h3 * c.bsI;
+                        for (int k = 0; k < cwd[u].n(c.mp); k++) {
+                            int bc = k * c.kp + cwd[u].code(k);
+                            d = __fadd_rn(d, __fadd_rn(S.lut[bc], __ldg(r1 + bc)));
+                        }
+                    }
+                    du = f2o(d);
+                    if (WARM) warm[f + lane + 32u * u] = ((uint64_t)du << 32) | pos[u];
+                    else pass = du <= tau;
+                }
+                if (!WARM) {
+                    const unsigned m = __ballot_sync(FULL, pass);
+                    if (m) {
+                        uint32_t slot0 = 0;
+                        if (lane == __ffs(m) - 1) slot0 = atomicAdd((unsigned *)&st.npend, (unsigned)__popc(m));
+                        slot0 = __shfl_sync(FULL, slot0, __ffs(m) - 1);
+                        const uint32_t slot = slot0 + __popc(m & ((1u << lane) - 1));
+                        if (pass && slot < cap) out[slot] = ((uint64_t)du << 32) | pos[u];
+                    }
+                }
+            }
+            f = e2;
+        }
+    }
+}
+
+// The k-th smallest (1-based) high word of keys[0..n) in shared memory
+// (radix select, 11 + 11 + 10 bits).
+__device__ uint32_t block_kth_hi(const uint64_t *keys, int n, int k, uint32_t *hist, uint64_t *red, QState &st) {
+    const int tid = threadIdx.x;
+    uint32_t prefix = 0;
+    uint64_t need = (uint64_t)k;
+#pragma unroll
+    for (int p = 0; p < 3; p++) {
+        const int sh = p == 0 ? 21 : (p == 1 ? 10 : 0), bits = p == 2 ? 10 : 11, nbins = 1 << bits, hs = sh + bits;
+        for (int i = tid; i < nbins; i += NT) hist[i] = 0;
+        __syncthreads();
+        for (int i = tid; i < n; i += NT) {
+            uint32_t v = (uint32_t)(keys[i] >> 32);
+            if (hs < 32 && (v >> hs) != (prefix >> hs)) continue;
+            atomicAdd(&hist[(v >> sh) & (nbins - 1)], 1u);
+        }
+        __syncthreads();
+        const int per = (nbins + NT - 1) / NT;
+        const int b0 = tid * per;
+        uint64_t mine = 0;
+        for (int i = 0; i < per; i++)
+            if (b0 + i < nbins) mine += hist[b0 + i];
+        uint64_t tot;
+        uint64_t run = block_exscan(mine, red, tot);
+        for (int i = 0; i < per; i++) {
+            int bb = b0 + i;
+            if (bb >= nbins) break;
+            uint64_t nxt = run + hist[bb];
+            if (run < need && nxt >= need) {
+                st.s_bin = (uint32_t)bb;
+                st.s_acc = run;
+            }
+            run = nxt;
+        }
+        __syncthreads();
+        prefix |= st.s_bin << sh;
+        need -= st.s_acc;
+        __syncthreads();
+    }
+    return prefix;
+}
+
+template <int MPC, int U>
+__global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint64_t red[3 * NWARP];
+    __shared__ QState st;
+    __shared__ int s_q;
+    Smem S;
+    carve(a.mode, a.kc, a.mp, a.kp, &S, smem);
+    const int tid = threadIdx.x;
+    const int kc = a.kc, mp = a.mp, kp = a.kp;
+    const int kcP = next_pow2(kc);
+    const bool imi = a.mode == SCG_IMI, sc = a.mode == SCG_SC2, ivf = a.mode == SCG_IVFADC;
+    const bool fast = a.precision == SCG_FAST;
+    const int kBfull = ivf ? 1 : kc;
+    const int cap = a.cap_rec;
+    uint32_t *rec_key = a.rec_key + (size_t)blockIdx.x * cap;
+    uint32_t *rec_rank = a.rec_rank + (size_t)blockIdx.x * cap;
+    uint32_t *rec_cnt = a.rec_cnt + (size_t)blockIdx.x * cap;
+    uint32_t *vis_cell = a.vis_cell + (size_t)blockIdx.x * (cap + 1);
+    uint32_t *vis_pre = a.vis_pre + (size_t)blockIdx.x * (cap + 1);
+    uint32_t *hist = S.hist;
+    uint64_t *ties = S.ties;
+    uint64_t *sb = S.sb;  // sorted coarse prefix scratch
+    const int bsI = kp * mp / a.mc;  // dot_cr block of one coarse centroid
+    const double avg_density = (double)a.N / (double)(a.ncells ? a.ncells : 1);
+
+    for (;;) {
+        if (tid == 0) s_q = atomicAdd(a.qcounter, 1);
+        __syncthreads();
+        const int q = s_q;
+        if (q >= a.nq) break;
+        long long t_prev = clock64();
+        const int T = a.Tq ? a.Tq[q] : a.T;
+        const int w = a.w;
+        const int R = a.R;
+        const float *dqc = a.dqc + (size_t)q * a.mc * kc;
+        const float qn0 = a.qn[2 * q], qn1 = a.qn[2 * q + 1], qs = a.qsum[q];
+        for (int i = tid; i < mp * kp; i += NT) S.lut[i] = a.dqr[(size_t)q * mp * kp + i];
+
+        // IMI and SC test the rules before each pop (multi_query.h:151,
+        // sc_query.h:130); IVFADC pops first and tests after
+        // (query.h:249-259), so T <= 0 still visits one cell there.
+        const bool nothing = (w <= 0) || (!ivf && T <= 0);
+        uint64_t needT = (uint64_t)(T > 0 ? T : 0);
+        uint64_t needW = (uint64_t)(w > 0 ? w : 0);
+        if (ivf && T <= 0) {
+            needT = ~0ull;
+            needW = 1;
+        }
+        const double c0 = (T > 0 ? (double)T : 1.0) / (avg_density > 1e-9 ? avg_density : 1e-9);
+        int M = next_pow2(4 * (int)sqrt(c0) + 1);
+        if (M < 128) M = 128;
+        if (M > SBCAP / 2) M = SBCAP / 2;
+
+        uint64_t Ssum = 0, Ncell = 0, NEc = 0;  // totals over enumerated cells
+        uint64_t S0 = 0, N0 = 0, NE0 = 0;       // totals before the last round
+        int nrec = 0, r0 = 0;
+        bool trig = false;
+        Lists L;
+        for (int attempt = 0; attempt < 2; attempt++) {
+            const bool full = attempt == 1 || M >= kc;
+            bool done_a = false, done_b = !imi;
+            if (a.slist && attempt == 0) {
+                // prefixes sorted ahead by k_coarse_prefix (same prefix rule)
+                const int nl = imi ? 2 : 1;
+                const uint64_t *src = a.slist + (size_t)q * nl * a.slist_w;
+                const uint32_t *meta = a.smeta + (size_t)q * nl * 2;
+                const int ca = (int)meta[0], cb = imi ? (int)meta[2] : 0;
+                for (int h = tid; h < ca; h += NT) S.LA[h] = src[h];
+                for (int h = tid; h < cb; h += NT) S.LB[h] = src[a.slist_w + h];
+                if (tid == 0) {
+                    st.err = 0;
+                    st.kA = ca;
+                    st.kB = imi ? cb : kBfull;
+                    st.nextA = meta[1];
+                    st.nextB = imi ? meta[3] : 0xffffffffu;
+                }
+                done_a = done_b = true;
+                __syncthreads();
+            } else {
+                // (1) coarse lists (sort_id/nth_element_id with M = kc;
+                //     multi_query.h:114-128, sc_query.h:98-106, query.h:230-234):
+                //     ordered key << 32 | centroid id; equal keys by id.
+                for (int h = tid; h < kcP; h += NT) {
+                    if (h < kc) {
+                        float ka = __fadd_rn(imi ? qn0 : qs, dqc[h]);
+                        S.LA[h] = ((uint64_t)f2o(ka) << 32) | (uint32_t)h;
+                        if (imi) {
+                            float kb = __fadd_rn(qn1, dqc[kc + h]);
+                            S.LB[h] = ((uint64_t)f2o(kb) << 32) | (uint32_t)h;
+                        }
+                    } else {
+                        S.LA[h] = ~0ull;
+                        if (imi) S.LB[h] = ~0ull;
+                    }
+                }
+                if (tid == 0) {
+                    st.err = 0;
+                    st.kA = kc;
+                    st.kB = kBfull;
+                    st.nextA = 0xffffffffu;
+                    st.nextB = 0xffffffffu;
+                }
+                __syncthreads();
+                if (!full) {
+                    int ca = select_prefix(S.LA, kc, M, sb, hist, red, st, &st.nextA);
+                    if (ca > 0) {
+                        done_a = true;
+                        if (tid == 0) st.kA = ca;
+                    }
+                    if (imi) {
+                        int cb = select_prefix(S.LB, kc, M, sb, hist, red, st, &st.nextB);
+                        if (cb > 0) {
+                            done_b = true;
+                            if (tid == 0) st.kB = cb;
+                        }
+                    }
+                    __syncthreads();
+                    if (!done_a || !done_b) {
+                        // a prefix beyond SBCAP: sort everything instead
+                        done_a = done_b = false;
+                        for (int h = tid; h < kcP; h += NT) {
+                            if (h < kc) {
+                                S.LA[h] = ((uint64_t)f2o(__fadd_rn(imi ? qn0 : qs, dqc[h])) << 32) | (uint32_t)h;
+                                if (imi) S.LB[h] = ((uint64_t)f2o(__fadd_rn(qn1, dqc[kc + h])) << 32) | (uint32_t)h;
+                            }
+                        }
+                        if (tid == 0) {
+                            st.kA = kc;
+                            st.kB = kBfull;
+                            st.nextA = st.nextB = 0xffffffffu;
+                        }
+                        __syncthreads();
+                    }
+                }
+            }
+            if (!done_a) bitonic_sort64(S.LA, kcP);
+            if (imi && !done_b) bitonic_sort64(S.LB, kcP);
+            __syncthreads();
+            L.LA = S.LA;
+            L.LB = S.LB;
+            L.kA = st.kA;
+            L.kB = sc ? st.kA : st.kB;
+            L.kc = kc;
+            L.ivf = ivf;
+            const uint32_t nextB = sc ? st.nextA : st.nextB;
+            // every cell outside the prefix grid has a key >= bound
+            uint32_t bound = 0xffffffffu;
+            if (st.nextA != 0xffffffffu) bound = min(bound, f2o(__fadd_rn(o2f(st.nextA), L.b(0))));
+            if (!ivf && nextB != 0xffffffffu) bound = min(bound, f2o(__fadd_rn(L.a(0), o2f(nextB))));
+            const bool whole = L.kA == kc && (ivf || L.kB == kc);
+            PHASE_MARK(0);  // lists
+
+            // (2) rounds of staircase enumeration over the prefix grid
+            for (int h = tid; h < L.kA; h += NT) S.rowp[h] = (sc && h == 0) ? 1 : 0;
+            Ssum = Ncell = NEc = 0;
+            S0 = N0 = NE0 = 0;
+            nrec = 0;
+            r0 = 0;
+            trig = false;
+            const uint64_t grid_cells = (uint64_t)L.kA * L.kB;
+            const uint64_t total_cells = grid_cells - (sc ? 1 : 0);
+            uint32_t tau_prev = 0;
+            const uint32_t lo_key = f2o(__fadd_rn(L.a(0), L.b(0)));
+            const uint32_t hi_key = f2o(__fadd_rn(L.a(L.kA - 1), L.b(L.kB - 1)));
+            uint64_t target = (uint64_t)(c0 / 8.0);
+            if (target < 64) target = 64;
+            if (target > 1024) target = 1024;
+            if (sc) target += 1;
+            __syncthreads();
+            int round = 0;
+            if (!nothing) {
+                for (; round < MAX_ROUNDS; round++) {
+                    if (target > grid_cells) target = grid_cells;
+                    if (!sc && needW < target) {
+                        // the w rule caps popped cells: never enumerate past w
+                        uint64_t tw = needW;
+                        if (tw < Ncell + 1) tw = Ncell + 1;
+                        if (tw < target) target = tw;
+                    }
+                    // bisection for tau: smallest key with staircase count >= target
+                    uint32_t lo = round == 0 ? lo_key : tau_prev + 1, hi = hi_key;
+                    uint64_t thi = target + target / 4 + 32;
+                    COUNT(8, 1);
+                    if (lo > hi) lo = hi;
+                    int it = 0;
+                    while (lo < hi && it < 40) {
+                        uint32_t mid = lo + ((hi - lo) >> 1);
+                        uint64_t c = staircase_count(L, mid, red);
+                        COUNT(9, 1);
+                        if (c >= target) {
+                            hi = mid;
+                            if (c <= thi) break;
+                        } else {
+                            lo = mid + 1;
+                        }
+                        it++;
+                    }
+                    const uint32_t tau = hi;
+                    tau_prev = tau;
+                    // row counts at tau and the new cells per row
+                    uint32_t mycnt = 0;
+                    const int per = (L.kA + NT - 1) / NT;
+                    const int hb = tid * per;
+                    for (int i = 0; i < per; i++) {
+                        int h = hb + i;
+                        if (h >= L.kA) break;
+                        int c = L.row_count(L.a(h), tau);
+                        int p0 = S.rowp[h];
+                        if (c < p0) c = p0;
+                        S.rowc[h] = (uint16_t)c;
+                        mycnt += (uint32_t)(c - p0);
+                    }
+                    uint64_t tot_new;
+                    uint64_t ex = block_exscan(mycnt, red, tot_new);
+                    {
+                        uint32_t run = (uint32_t)ex;
+                        for (int i = 0; i < per; i++) {
+                            int h = hb + i;
+                            if (h >= L.kA) break;
+                            S.rowpre[h] = run;
+                            run += (uint32_t)(S.rowc[h] - S.rowp[h]);
+                        }
+                    }
+                    if ((uint64_t)nrec + tot_new > (uint64_t)cap) {
+                        if (tid == 0) {
+                            st.err = 1;
+                            atomicOr(a.status, ST_CELL_BUDGET);
+                        }
+                        __syncthreads();
+                        break;
+                    }
+                    __syncthreads();
+                    const int nnew = (int)tot_new;
+                    COUNT(10, nnew);
+                    uint64_t ls = 0, lne = 0, dummy = 0;
+                    int h1 = 0;
+                    for (int idx = tid; idx < nnew; idx += NT) {
+                        // row of idx: last h with rowpre[h] <= idx (rows only grow)
+                        int lo2 = h1, hi2 = L.kA - 1;
+                        while (lo2 < hi2) {
+                            int mid = (lo2 + hi2 + 1) >> 1;
+                            if (S.rowpre[mid] <= (uint32_t)idx) lo2 = mid;
+                            else hi2 = mid - 1;
+                        }
+                        h1 = lo2;
+                        int h2 = S.rowp[h1] + (idx - (int)S.rowpre[h1]);
+                        float key = __fadd_rn(L.a(h1), L.b(h2));
+                        uint32_t rank = ((uint32_t)h1 << 16) | (uint32_t)h2;
+                        uint32_t cell = cell_of(L, rank);
+                        uint32_t c = a.off[cell + 1] - a.off[cell];
+                        if (sc && cell == 0) c = 0;  // sc_query.h:138-140
+                        rec_key[nrec + idx] = f2o(key);
+                        rec_rank[nrec + idx] = rank;
+                        rec_cnt[nrec + idx] = c;
+                        ls += c;
+                        lne += (c > 0);
+                    }
+                    block_sum3(ls, lne, dummy, red);
+                    S0 = Ssum;
+                    N0 = Ncell;
+                    NE0 = NEc;
+                    r0 = nrec;
+                    nrec += nnew;
+                    Ssum += ls;
+                    Ncell += (uint64_t)nnew;
+                    NEc += lne;
+                    for (int h = tid; h < L.kA; h += NT) S.rowp[h] = S.rowc[h];
+                    __syncthreads();
+                    uint64_t wcnt = sc ? NEc : Ncell;
+                    trig = (Ssum >= needT) || (wcnt >= needW);
+                    if (trig || Ncell >= total_cells || tau >= hi_key) break;
+                    // next target from the density seen so far
+                    double dens = Ncell ? (double)Ssum / (double)Ncell : avg_density;
+                    if (dens < 1e-6) dens = avg_density > 1e-6 ? avg_density : 1e-6;
+                    double need_cells = (double)(needT - Ssum) / dens;
+                    uint64_t grow = (uint64_t)(need_cells * 1.25) + 64;
+                    uint64_t minimum = Ncell / 4 + 64;
+                    target = Ncell + (sc ? 1 : 0) + (grow > minimum ? grow : minimum);
+                }
+                if (round >= MAX_ROUNDS && tid == 0) {
+                    st.err = 1;
+                    atomicOr(a.status, ST_ITER_CAP);
+                }
+            }
+            __syncthreads();
+            const bool qerr = st.err != 0;
+            PHASE_MARK(1);  // staircase rounds
+
+            // (3) the cut within the last round
+            if (!nothing && !qerr && trig) {
+                uint64_t mn = 0xffffffffull, mx = 0;
+                for (int r = r0 + tid; r < nrec; r += NT) {
+                    uint64_t k = rec_key[r];
+                    mn = k < mn ? k : mn;
+                    mx = k > mx ? k : mx;
+                }
+                block_minmax(mn, mx, red);
+                uint32_t klo = (uint32_t)mn, khi = (uint32_t)mx;
+                uint32_t kap = 0xffffffffu;
+                if (Ssum >= needT)
+                    kap = radix_cut(rec_key, rec_cnt, r0, nrec, klo, khi, S0, needT, 0, hist, red, st);
+                uint64_t wcnt = sc ? NEc : Ncell;
+                if (wcnt >= needW) {
+                    uint32_t kw = radix_cut(rec_key, rec_cnt, r0, nrec, klo, khi, sc ? NE0 : N0, needW, sc ? 2 : 1,
+                                            hist, red, st);
+                    if (kw < kap) kap = kw;
+                }
+                // totals strictly below kappa, and the ties at kappa
+                uint64_t ls = 0, ln = 0, lne = 0;
+                if (tid == 0) st.nties = 0;
+                __syncthreads();
+                for (int r = r0 + tid; r < nrec; r += NT) {
+                    uint32_t k = rec_key[r];
+                    if (k < kap) {
+                        uint32_t c = rec_cnt[r];
+                        ls += c;
+                        ln += 1;
+                        lne += (c > 0);
+                    } else if (k == kap) {
+                        int slot = atomicAdd(&st.nties, 1);
+                        if (slot < TIECAP) ties[slot] = ((uint64_t)rec_rank[r] << 32) | rec_cnt[r];
+                    }
+                }
+                block_sum3(ls, ln, lne, red);
+                if (tid == 0) {
+                    uint64_t s = S0 + ls, n = N0 + ln, ne = NE0 + lne;
+                    int nt = st.nties;
+                    if (nt > TIECAP) {
+                        st.err = 1;
+                        atomicOr(a.status, ST_TIE_OVERFLOW);
+                        nt = TIECAP;
+                    }
+                    // ties in rank order (an exact priority queue's order)
+                    for (int i = 1; i < nt; i++) {
+                        uint64_t v = ties[i];
+                        int j = i - 1;
+                        while (j >= 0 && ties[j] > v) {
+                            ties[j + 1] = ties[j];
+                            j--;
+                        }
+                        ties[j + 1] = v;
+                    }
+                    uint32_t rc_ = 0;
+                    for (int i = 0; i < nt; i++) {
+                        uint32_t c = (uint32_t)ties[i];
+                        s += c;
+                        n += 1;
+                        ne += (c > 0);
+                        rc_ = (uint32_t)(ties[i] >> 32);
+                        if (s >= needT || (sc ? ne : n) >= needW) break;
+                    }
+                    st.kappa = kap;
+                    st.rank_cut = rc_;
+                    st.take_all = 0;
+                    st.sumv = s;
+                    st.nv = n;
+                    st.nev = ne;
+                }
+                __syncthreads();
+            } else if (tid == 0) {
+                st.kappa = 0xffffffffu;
+                st.rank_cut = 0xffffffffu;
+                st.take_all = 1;
+                st.sumv = nothing ? 0 : Ssum;
+                st.nv = nothing ? 0 : Ncell;
+                st.nev = nothing ? 0 : NEc;
+            }
+            __syncthreads();
+            PHASE_MARK(2);  // cut
+            // the prefix grid holds every cell with a key <= the cut
+            const bool valid = nothing || st.err || (trig ? st.kappa < bound : whole);
+            if (valid) break;
+            COUNT(11, 1);
+            __syncthreads();
+        }
+
+        // (4) visited non-empty cells -> (cell, prefix) list
+        int nvis = 0;
+        if (!nothing && !st.err) {
+            const uint32_t kap = st.kappa, rcut = st.rank_cut;
+            const bool all = st.take_all != 0;
+            uint64_t pos = 0, runc = 0;
+            for (int base = 0; base < nrec; base += NT) {
+                int r = base + tid;
+                bool f = false;
+                uint32_t c = 0, rank = 0;
+                if (r < nrec) {
+                    c = rec_cnt[r];
+                    rank = rec_rank[r];
+                    uint32_t k = rec_key[r];
+                    bool inc = all || r < r0 || k < kap || (k == kap && rank <= rcut);
+                    f = inc && c > 0;
+                }
+                uint64_t v = f ? ((1ull << 40) | c) : 0ull;
+                uint64_t tot;
+                uint64_t ex = block_exscan(v, red, tot);
+                if (f) {
+                    uint64_t p = pos + (ex >> 40);
+                    vis_cell[p] = cell_of(L, rank);
+                    vis_pre[p] = (uint32_t)(runc + (ex & 0xffffffffffull));
+                }
+                pos += tot >> 40;
+                runc += tot & 0xffffffffffull;
+            }
+            nvis = (int)pos;
+            if (tid == 0) {
+                vis_pre[nvis] = (uint32_t)runc;
+                st.sumv = runc;  // the candidates of the visited cells
+            }
+        }
+        if (tid == 0) st.nvis = nvis;
+        __syncthreads();
+        nvis = st.nvis;
+        const bool qerr2 = st.err != 0;
+        const uint32_t Svis = (nvis > 0) ? (uint32_t)st.sumv : 0u;
+        PHASE_MARK(3);  // compaction
+
+        // (5) ADC scan with the fused top-R.  The first WARMN candidates are
+        // scored into shared memory; their R-th smallest distance bounds the
+        // final R-th distance from above, so the rest of the scan keeps only
+        // candidates at or below it, appended to a per-CTA buffer; one
+        // radix-select merge over that buffer gives the R best.
+        uint64_t *top = S.top, *tmpk = S.tmp;
+        uint64_t *pend_g = a.pend + (size_t)blockIdx.x * a.pcap;
+        if (tid == 0) {
+            st.ncur = 0;
+            st.npend = 0;
+            st.next_flat = 0;
+        }
+        __syncthreads();
+        if (!qerr2 && nvis > 0) {
+            ScanCtx c;
+            c.vis_cell = vis_cell;
+            c.vis_pre = vis_pre;
+            c.nvis = nvis;
+            c.Svis = Svis;
+            c.kc = kc;
+            c.mp = mp;
+            c.kp = kp;
+            c.bsI = bsI;
+            c.imi = imi;
+            c.sc = sc;
+            c.fast = fast;
+            c.qs = qs;
+            c.dqc = dqc;
+            const uint32_t K = Svis < (uint32_t)WARMN ? Svis : (uint32_t)WARMN;
+            scan_chunks<MPC, true, U>(a, S, st, c, K, 0u, S.warm, nullptr, 0u);
+            __syncthreads();
+            uint32_t tau = 0xffffffffu;
+            if (K > (uint32_t)R) tau = block_kth_hi(S.warm, (int)K, R, S.hist2, red, st);
+            // the warm entries at or below tau open the pending buffer
+            {
+                uint64_t mine = 0;
+                for (int i = tid; i < (int)K; i += NT) mine += ((uint32_t)(S.warm[i] >> 32) <= tau);
+                uint64_t tot;
+                uint64_t p = block_exscan(mine, red, tot);
+                for (int i = tid; i < (int)K; i += NT) {
+                    uint64_t e = S.warm[i];
+                    if ((uint32_t)(e >> 32) <= tau) pend_g[p++] = e;
+                }
+                if (tid == 0) {
+                    st.npend = (int)tot;
+                    st.next_flat = K;
+                }
+                __syncthreads();
+            }
+            scan_chunks<MPC, false, U>(a, S, st, c, Svis, tau, nullptr, pend_g, a.pcap);
+            __syncthreads();
+            PHASE_MARK(4);  // scan
+            if ((uint32_t)st.npend > a.pcap) {
+                if (tid == 0) {
+                    st.err = 1;
+                    atomicOr(a.status, ST_CELL_BUDGET);
+                }
+                __syncthreads();
+            } else if (st.npend > 0) {
+                merge_topk(top, pend_g, tmpk, S.hist2, S.ties2, R, a.pid, red, st, a.status);
+            }
+        }
+        __syncthreads();
+        PHASE_MARK(5);  // final merge
+        // (6) outputs: the R best sorted by (distance, id)
+        {
+            const bool qerr3 = st.err != 0;
+            int keep = (qerr3 || nvis == 0) ? 0 : st.ncur;
+            if (keep > 1) {
+                const int k2 = next_pow2(keep);
+                for (int i = keep + tid; i < k2; i += NT) top[i] = ~0ull;
+                __syncthreads();
+                bitonic_sort64(top, k2);
+            }
+            for (int j = tid; j < R; j += NT) {
+                size_t o = (size_t)q * R + j;
+                if (j < keep) {
+                    uint64_t e = top[j];
+                    a.out_ids[o] = (int)(uint32_t)e;
+                    a.out_d[o] = o2f((uint32_t)(e >> 32));
+                } else {
+                    a.out_ids[o] = -1;
+                    a.out_d[o] = __int_as_float(0x7f800000);
+                }
+            }
+            if (tid == 0) {
+                a.out_sum[q] = qerr3 ? -1 : (int)(nothing ? 0 : st.sumv);
+                if (a.out_nvis) a.out_nvis[q] = nvis;
+                if (a.out_empty) a.out_empty[q] = qerr3 ? 0 : (int)(st.nv - st.nev);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+
+template <int MPC, int U>
+int occupancy(size_t smem) {
+    cudaFuncSetAttribute(k_search<MPC, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int nb = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<MPC, U>, NT, smem);
+    return nb;
+}
+
+template <int U>
+int occupancy_mp(int mp, size_t smem) {
+    switch (mp) {
+        case 4: return occupancy<4, U>(smem);
+        case 8: return occupancy<8, U>(smem);
+        case 16: return occupancy<16, U>(smem);
+        case 32: return occupancy<32, U>(smem);
+        default: return occupancy<0, U>(smem);
+    }
+}
+
+template <int MPC, int U>
+int launch(const SearchArgs &a, int grid, size_t smem, cudaStream_t s) {
+    cudaError_t e = cudaFuncSetAttribute(k_search<MPC, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_search)");
+    k_search<MPC, U><<<grid, NT, smem, s>>>(a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "k_search launch");
+    return SCG_OK;
+}
+
+template <int U>
+int launch_mp(const SearchArgs &a, int grid, size_t smem, cudaStream_t s) {
+    switch (a.mp) {
+        case 4: return launch<4, U>(a, grid, smem, s);
+        case 8: return launch<8, U>(a, grid, smem, s);
+        case 16: return launch<16, U>(a, grid, smem, s);
+        case 32: return launch<32, U>(a, grid, smem, s);
+        default: return launch<0, U>(a, grid, smem, s);
+    }
+}
+
+}  // namespace
+
+}  // namespace scg

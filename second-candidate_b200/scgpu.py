@@ -140,13 +140,20 @@ class Index:
     def set_cell_budget(self, n):
         _check(_lib.scg_set_cell_budget(self._h, n))
 
-    def search(self, mode, Q, R, w, T, precision=FP32_EXACT, rerank=0):
-        """Host-buffer search: returns (ids[nq,R], dists[nq,R], sums[nq])."""
+    def search(self, mode, Q, R, w, T, precision=FP32_EXACT, rerank=0, out=None):
+        """Host-buffer search: returns (ids[nq,R], dists[nq,R], sums[nq]).
+        `out` may hold caller-owned (ids, dists, sums) arrays to fill (e.g.
+        in pinned memory)."""
         Q = np.ascontiguousarray(Q, np.float32).reshape(-1, self.dim)
         nq = Q.shape[0]
-        ids = np.empty((nq, R), np.int32)
-        d = np.empty((nq, R), np.float32)
-        sums = np.empty(nq, np.int32)
+        if out is not None:
+            ids, d, sums = out
+            assert ids.shape == (nq, R) and d.shape == (nq, R) and sums.shape == (nq,)
+            assert ids.flags.c_contiguous and d.flags.c_contiguous and sums.flags.c_contiguous
+        else:
+            ids = np.empty((nq, R), np.int32)
+            d = np.empty((nq, R), np.float32)
+            sums = np.empty(nq, np.int32)
         p = SearchParams(mode, R, w, T, precision, rerank)
         _check(_lib.scg_search(self._h, ctypes.byref(p), _ptr(Q), nq, _ptr(ids), _ptr(d), _ptr(sums)))
         return ids, d, sums

@@ -214,3 +214,34 @@ def test_sorted_prefix_and_fallback(scg, oracle_mod, mode, mc, kc, Ts):
     for T in Ts:
         check_against_oracle(ix, g, mode, Q, 30, 1 << 20, T)
     g.close()
+
+
+def test_host_path_chunks_equal_device_path(scg, oracle_mod):
+    """scg_search runs batches of >= 1024 queries in chunks over two streams;
+    results and per-query facts must equal the one-launch device path."""
+    import torch
+    D, mc, kc, mp, kp = 64, 2, 64, 8, 256
+    mix = W.Mixture(D, 16, 20.0, "u8", seed=51)
+    X = mix.sample(60000, seed=52)
+    cq, pq = W.train_codebooks(X[:5000], mc, kc, mp, kp, 3, seed=53)
+    cid, codes = O.encode((D, mc, kc, mp, kp), cq, pq, X)
+    L, pid, co, _ = O.distribution(O.IMI, kc, mc, 0, cid, codes)
+    g = gpu_index(scg, D, mc, kc, mp, kp, cq, pq, L, pid, co)
+    for nq in (4500, 1500):
+        Q = mix.sample(nq, seed=54 + nq)
+        for prec in (scg.FP32_EXACT, scg.FAST):
+            ids, d, sums = g.search(1, Q, 20, 1 << 20, 1500, precision=prec)
+            nvis, empty = g.last_query_stats(nq)
+            dQ = torch.from_numpy(Q).cuda()
+            di = torch.empty(nq * 20, dtype=torch.int32, device="cuda")
+            dd = torch.empty(nq * 20, dtype=torch.float32, device="cuda")
+            ds = torch.empty(nq, dtype=torch.int32, device="cuda")
+            torch.cuda.synchronize()
+            g.search_device(1, dQ.data_ptr(), nq, 20, 1 << 20, 1500, di.data_ptr(), dd.data_ptr(), ds.data_ptr(),
+                            precision=prec)
+            torch.cuda.synchronize()
+            assert np.array_equal(ids.ravel(), di.cpu().numpy()) and np.array_equal(d.ravel(), dd.cpu().numpy())
+            assert np.array_equal(sums, ds.cpu().numpy())
+            nv2, em2 = g.last_query_stats(nq)
+            assert np.array_equal(nvis, nv2) and np.array_equal(empty, em2)
+    g.close()
