@@ -161,6 +161,12 @@ int scg_autotune(scg_index *h, const scg_search_params *p, const float *dQ, int 
  * `precision` without timing. */
 int scg_set_scan_tuning(scg_index *h, int precision, int upl);
 
+/* Kernel organisation of the search: on (the default), cell selection and
+ * the ADC scan run as two persistent kernels (the scan kernel holds more
+ * resident warps per SM); off, as one fused kernel.  Both give identical
+ * results; searches with per-query targets always use the fused kernel. */
+int scg_set_kernel_split(scg_index *h, int on);
+
 /* Per-query candidate targets (device pointer to nq ints) for the next
  * scg_search_device call; NULL restores the single T of the parameters. */
 int scg_set_query_targets(scg_index *h, const int *d_T);

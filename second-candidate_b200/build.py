@@ -7,7 +7,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libscgpu.so")
-SOURCES = ["search_u4.cu", "search_u2.cu", "search_u8.cu", "api.cu", "tables.cu", "tables_tc.cu", "search.cu",
+SOURCES = ["search_u4.cu", "search_u2.cu", "search_u8.cu", "search_sel.cu", "api.cu", "tables.cu", "tables_tc.cu", "search.cu",
            "encode.cu", "rerank.cu", "server.cu", "coarse.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
@@ -23,14 +23,18 @@ def _stale():
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force=False, verbose=False, jobs=None):
+def build(force=False, verbose=False, jobs=None, out=None, defines=()):
     """Compiles every source for sm_100a (in parallel) and links libscgpu.so
-    in-tree; does nothing when the library is newer than every source."""
-    if not force and not _stale():
+    in-tree (or at `out`, with extra -D `defines`); does nothing when the
+    in-tree library is newer than every source."""
+    lib = out or LIB
+    if out is None and not force and not _stale():
         return LIB
     from concurrent.futures import ThreadPoolExecutor
-    objs = [os.path.join(CSRC, src.replace(".cu", ".o")) for src in SOURCES]
-    cmds = [[NVCC] + FLAGS + ["-I", os.path.join(ROOT, "include"), "-c", os.path.join(CSRC, src), "-o", obj]
+    objdir = os.path.dirname(lib) if out else CSRC
+    objs = [os.path.join(objdir, src.replace(".cu", ".o")) for src in SOURCES]
+    dflags = ["-D" + d for d in defines]
+    cmds = [[NVCC] + FLAGS + dflags + ["-I", os.path.join(ROOT, "include"), "-c", os.path.join(CSRC, src), "-o", obj]
             for src, obj in zip(SOURCES, objs)]
     if verbose:
         for c in cmds:
@@ -42,12 +46,12 @@ def build(force=False, verbose=False, jobs=None):
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise subprocess.CalledProcessError(r.returncode, c)
-    tmp = LIB + ".tmp"
+    tmp = lib + ".tmp"
     subprocess.run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", tmp] + objs + ["-lcudart"], check=True)
-    os.replace(tmp, LIB)
+    os.replace(tmp, lib)
     for o in objs:
         os.remove(o)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":

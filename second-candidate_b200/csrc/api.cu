@@ -149,7 +149,7 @@ int Workspace::init() {
 
 void Workspace::release() {
     DevBuf *all[] = {&dqc, &dqr, &qn, &qsum, &nvis, &empty, &status, &counter, &rec_key, &rec_rank,
-                     &rec_cnt, &vis_cell, &vis_pre, &pend, &phase, &sl_ids, &sl_d, &slist, &smeta};
+                     &rec_cnt, &vis_cell, &vis_pre, &pend, &phase, &sl_ids, &sl_d, &slist, &smeta, &qmeta, &pool_cell, &pool_pre};
     for (DevBuf *b : all) b->release();
     if (h_status) cudaFreeHost(h_status);
     h_status = nullptr;
@@ -217,23 +217,43 @@ int ensure_vterm(scg_index *h, cudaStream_t s) {
 int reserve_search(scg_index *h, Workspace *ws, int mode, int grid) {
     int rc;
     if ((rc = ws->init())) return rc;
-    int per_sm = 0;
+    // the largest grid of each slot kind over the kernel variants
+    int g_rec = 0, g_vis = 0, g_pend = 0;
     for (int u : {2, 4, 8}) {
-        const int b = search_max_blocks_per_sm(mode, h->kc, h->mp, h->kp, u);
-        per_sm = b > per_sm ? b : per_sm;
+        const int f = h->num_sms * search_max_blocks_per_sm(mode, h->kc, h->mp, h->kp, u, 0);
+        const int c = h->num_sms * search_max_blocks_per_sm(mode, h->kc, h->mp, h->kp, u, 2);
+        g_rec = std::max(g_rec, f);
+        g_vis = std::max(g_vis, f);
+        g_pend = std::max(g_pend, std::max(f, c));
     }
-    if (per_sm < 1) return fail(SCG_ERR_ARG, "search kernel does not fit on an SM for this shape");
-    if (grid <= 0 || grid > h->num_sms * per_sm) grid = h->num_sms * per_sm;
+    g_rec = std::max(g_rec, h->num_sms * search_max_blocks_per_sm(mode, h->kc, h->mp, h->kp, 4, 1));
+    if (g_rec < 1) return fail(SCG_ERR_ARG, "search kernel does not fit on an SM for this shape");
+    if (grid > 0) {
+        g_rec = std::min(g_rec, grid);
+        g_vis = std::min(g_vis, grid);
+        g_pend = std::min(g_pend, grid);
+    }
     const size_t slot = (size_t)h->cap_rec, pcap = slot > 65536 ? slot : 65536;
     if ((rc = ws->status.ensure(sizeof(int) * 4))) return rc;
     if ((rc = ws->counter.ensure(sizeof(int) * 4))) return rc;
-    if ((rc = ws->rec_key.ensure(4 * slot * grid))) return rc;
-    if ((rc = ws->rec_rank.ensure(4 * slot * grid))) return rc;
-    if ((rc = ws->rec_cnt.ensure(4 * slot * grid))) return rc;
-    if ((rc = ws->vis_cell.ensure(4 * (slot + 1) * grid))) return rc;
-    if ((rc = ws->vis_pre.ensure(4 * (slot + 1) * grid))) return rc;
-    if ((rc = ws->pend.ensure(8 * pcap * grid))) return rc;
+    if ((rc = ws->rec_key.ensure(4 * slot * g_rec))) return rc;
+    if ((rc = ws->rec_rank.ensure(4 * slot * g_rec))) return rc;
+    if ((rc = ws->rec_cnt.ensure(4 * slot * g_rec))) return rc;
+    if ((rc = ws->vis_cell.ensure(4 * (slot + 1) * g_vis))) return rc;
+    if ((rc = ws->vis_pre.ensure(4 * (slot + 1) * g_vis))) return rc;
+    if ((rc = ws->pend.ensure(8 * pcap * g_pend))) return rc;
     return SCG_OK;
+}
+
+// Entries of one query's visited list in the split kernels' pool: a bound on
+// the visited non-empty cells (each holds a candidate, so at most T of them;
+// at most w; at most N; at most the cell budget) plus the closing prefix.
+static int64_t pool_stride(const scg_index *h, const scg_search_params *p) {
+    int64_t b = h->cap_rec;
+    b = std::min<int64_t>(b, p->T > 0 ? (int64_t)p->T : 1);
+    b = std::min<int64_t>(b, p->w > 0 ? (int64_t)p->w : 1);
+    b = std::min<int64_t>(b, h->N > 0 ? h->N : 1);
+    return b + 1;
 }
 
 int index_mode(const scg_index *h) {
@@ -280,20 +300,35 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     if ((rc = ws->status.ensure(sizeof(int) * 4))) return rc;
     if ((rc = ws->counter.ensure(sizeof(int) * 4))) return rc;
     const int upl = h->tuned_upl[scan_form(p->precision) == SCG_FAST ? 1 : 0];
-    int per_sm = search_max_blocks_per_sm(p->mode, h->kc, h->mp, h->kp, upl);
-    if (per_sm < 1) return fail(SCG_ERR_ARG, "search kernel does not fit on an SM for this shape");
-    int grid = h->num_sms * per_sm;
-    if (grid > nq) grid = nq;
-    if (grid < 1) grid = 1;
+    const int *Tq = rb ? nullptr : h->d_Tq;
+    // split kernels (selection, then a lighter scan at higher occupancy)
+    // unless per-query targets make the visited-list bound unknown here
+    const int64_t stride = pool_stride(h, p);
+    const bool split = h->split && !Tq && (uint64_t)stride * (uint64_t)nq * 8 <= (8ull << 30);
+    auto grid_of = [&](int part) {
+        int g = h->num_sms * search_max_blocks_per_sm(p->mode, h->kc, h->mp, h->kp, upl, part);
+        return std::max(1, std::min(g, nq));
+    };
+    const int g_fused = split ? 0 : grid_of(0);
+    const int g_sel = split ? grid_of(1) : 0, g_scan = split ? grid_of(2) : 0;
+    if (std::max(g_fused, std::max(g_sel, g_scan)) < 1)
+        return fail(SCG_ERR_ARG, "search kernel does not fit on an SM for this shape");
     size_t slot = (size_t)h->cap_rec;
-    if ((rc = ws->rec_key.ensure(4 * slot * grid))) return rc;
-    if ((rc = ws->rec_rank.ensure(4 * slot * grid))) return rc;
-    if ((rc = ws->rec_cnt.ensure(4 * slot * grid))) return rc;
-    if ((rc = ws->vis_cell.ensure(4 * (slot + 1) * grid))) return rc;
-    if ((rc = ws->vis_pre.ensure(4 * (slot + 1) * grid))) return rc;
+    const int g_rec = std::max(g_fused, g_sel), g_pend = std::max(g_fused, g_scan);
+    if ((rc = ws->rec_key.ensure(4 * slot * g_rec))) return rc;
+    if ((rc = ws->rec_rank.ensure(4 * slot * g_rec))) return rc;
+    if ((rc = ws->rec_cnt.ensure(4 * slot * g_rec))) return rc;
+    if (!split) {
+        if ((rc = ws->vis_cell.ensure(4 * (slot + 1) * g_fused))) return rc;
+        if ((rc = ws->vis_pre.ensure(4 * (slot + 1) * g_fused))) return rc;
+    } else {
+        if ((rc = ws->qmeta.ensure(sizeof(QMeta) * (size_t)nq))) return rc;
+        if ((rc = ws->pool_cell.ensure(4 * (size_t)stride * nq))) return rc;
+        if ((rc = ws->pool_pre.ensure(4 * (size_t)stride * nq))) return rc;
+    }
     // survivors of the scan's threshold, per resident CTA
     const size_t pcap = slot > 65536 ? slot : 65536;
-    if ((rc = ws->pend.ensure(8 * pcap * grid))) return rc;
+    if ((rc = ws->pend.ensure(8 * pcap * g_pend))) return rc;
 
     if (scan_form(p->precision) == SCG_FAST && (rc = ensure_vterm(h, s))) return rc;
     TablesArgs ta;
@@ -332,7 +367,7 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     sa.slist = b.slist;
     sa.smeta = b.smeta;
     sa.slist_w = coarse_sort_width(h->kc);
-    sa.Tq = rb ? nullptr : h->d_Tq;
+    sa.Tq = Tq;
     sa.dqc = b.dqc; sa.dqr = b.dqr; sa.qn = b.qn; sa.qsum = b.qsum;
     sa.off = h->off.as<uint32_t>(); sa.pid = h->pid.as<int>(); sa.codes = h->codes.as<uint8_t>();
     sa.dot_cr = h->dot_cr.as<float>();
@@ -341,7 +376,12 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     sa.N = h->N;
     sa.rec_key = ws->rec_key.as<uint32_t>(); sa.rec_rank = ws->rec_rank.as<uint32_t>();
     sa.rec_cnt = ws->rec_cnt.as<uint32_t>();
-    sa.vis_cell = ws->vis_cell.as<uint32_t>(); sa.vis_pre = ws->vis_pre.as<uint32_t>();
+    sa.vis_cell = split ? nullptr : ws->vis_cell.as<uint32_t>();
+    sa.vis_pre = split ? nullptr : ws->vis_pre.as<uint32_t>();
+    sa.qmeta = split ? ws->qmeta.as<QMeta>() : nullptr;
+    sa.pool_cell = split ? ws->pool_cell.as<uint32_t>() : nullptr;
+    sa.pool_pre = split ? ws->pool_pre.as<uint32_t>() : nullptr;
+    sa.pool_stride = split ? (uint32_t)stride : 0u;
     sa.cap_rec = h->cap_rec;
     sa.pend = ws->pend.as<uint64_t>();
     sa.pcap = (uint32_t)pcap;
@@ -355,7 +395,17 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
         SCG_CUDA(cudaMemsetAsync(ws->phase.p, 0, sizeof(long long) * 16, s));
         sa.phase_cycles = ws->phase.as<long long>();
     }
-    if (nq > 0 && (rc = search_launch(sa, grid, s))) return rc;
+    if (nq > 0) {
+        if (split) {
+            // two persistent launches, each with its own query counter
+            sa.qcounter = ws->counter.as<int>();
+            if ((rc = search_launch(sa, 1, g_sel, s))) return rc;
+            sa.qcounter = ws->counter.as<int>() + 1;
+            if ((rc = search_launch(sa, 2, g_scan, s))) return rc;
+        } else if ((rc = search_launch(sa, 0, g_fused, s))) {
+            return rc;
+        }
+    }
     SCG_CUDA(cudaEventRecord(ws->ev[2], s));
     if (rr && nq > 0) {
         if (rerank_smem_bytes(R, h->dim) > 227 * 1024) return fail(SCG_ERR_ARG, "dimension too large for the re-rank");
@@ -735,6 +785,13 @@ int scg_autotune(scg_index *h, const scg_search_params *p, const float *dQ, int 
     return SCG_OK;
 }
 
+int scg_set_kernel_split(scg_index *h, int on) {
+    if (!h) return fail(SCG_ERR_ARG, "null index");
+    std::lock_guard<std::mutex> g(h->mu);
+    h->split = on != 0;
+    return SCG_OK;
+}
+
 int scg_set_query_targets(scg_index *h, const int *d_T) {
     if (!h) return fail(SCG_ERR_ARG, "null index");
     h->d_Tq = d_T;
@@ -942,7 +999,7 @@ extern "C" int scg_search_device_noalloc(scg_index *h, const scg_search_params *
     const size_t slot_bytes = up256(4ull * NOALLOC_CELLS) * 3 + up256(4ull * (NOALLOC_CELLS + 1)) * 2 +
                               up256(8ull * NOALLOC_SURVIVORS);
     const int upl = h->tuned_upl[scan_form(p->precision) == SCG_FAST ? 1 : 0];
-    int per_sm = search_max_blocks_per_sm(p->mode, h->kc, h->mp, h->kp, upl);
+    int per_sm = search_max_blocks_per_sm(p->mode, h->kc, h->mp, h->kp, upl, 0);
     if (per_sm < 1) return fail(SCG_ERR_ARG, "search kernel does not fit on an SM for this shape");
     int grid = h->num_sms * per_sm;
     if (grid > nq) grid = nq;
@@ -1012,7 +1069,7 @@ extern "C" int scg_search_device_noalloc(scg_index *h, const scg_search_params *
     sa.out_nvis = nvis; sa.out_empty = empty;
     sa.status = status;
     sa.phase_cycles = nullptr;
-    if ((rc = search_launch(sa, grid, s))) return rc;
+    if ((rc = search_launch(sa, 0, grid, s))) return rc;
     SCG_CUDA(cudaMemcpyAsync(h->ws.h_status, status, sizeof(int), cudaMemcpyDeviceToHost, s));
     SCG_CUDA(cudaStreamSynchronize(s));
     int st = *h->ws.h_status;

@@ -41,6 +41,7 @@ struct DevBuf {
 struct Workspace {
     DevBuf dqc, dqr, qn, qsum, nvis, empty, status, counter;
     DevBuf rec_key, rec_rank, rec_cnt, vis_cell, vis_pre, pend, phase, sl_ids, sl_d, slist, smeta;
+    DevBuf qmeta, pool_cell, pool_pre;  // selection -> scan hand-off of the split kernels
     int *h_status = nullptr;  // pinned copy of the status word
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     int last_nq = 0;
@@ -82,6 +83,7 @@ struct scg_index {
     int64_t raw_rows = 0;   // rows of raw vectors loaded (0: none)
     bool raw_u8 = false;    // raw vectors held as uint8
     int tuned_upl[2] = {4, 4};  // scan candidates per lane, per scan form (exact, fast)
+    bool split = true;          // selection and scan as two kernels where possible
     scg::Workspace ws;      // the workspace of the index's own entry points
     // scg_search (host buffers) pipelines a batch in chunks over two streams
     cudaStream_t stream2 = nullptr;

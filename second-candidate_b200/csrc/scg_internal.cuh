@@ -72,6 +72,14 @@ void launch_query_norms(const TablesArgs &a, cudaStream_t s);
 void launch_vterm(int mode, int kc, int mp, int kp, int mc, uint64_t ncells, int64_t N, const uint32_t *off,
                   const uint8_t *codes, const float *norm_r, const float *dot_cr, float *vterm, cudaStream_t s);
 
+// One query's visited-cell list as the selection kernel leaves it.
+struct QMeta {
+    int nvis;       // visited non-empty cells
+    uint32_t svis;  // their candidates
+    int err;        // the selection failed (outputs void)
+    int pad;
+};
+
 struct SearchArgs {
     int mode, dim, mc, kc, mp, kp, nq, R, w, T;
     int precision;
@@ -94,6 +102,10 @@ struct SearchArgs {
     int cap_rec;
     uint64_t *pend;                          // [slots][pcap] scan survivors
     uint32_t pcap;
+    // selection -> scan hand-off of the split kernels (parts 1 and 2)
+    QMeta *qmeta;                            // [nq]
+    uint32_t *pool_cell, *pool_pre;          // [nq][pool_stride] visited lists
+    uint32_t pool_stride;
     int *qcounter;                           // dynamic query counter
     // outputs
     int *out_ids;
@@ -103,9 +115,10 @@ struct SearchArgs {
     long long *phase_cycles;  // optional [16] counters
 };
 
-size_t search_smem_bytes(int mode, int kc, int mp, int kp);
-int search_launch(const SearchArgs &a, int grid, cudaStream_t s);
-int search_max_blocks_per_sm(int mode, int kc, int mp, int kp, int upl);
+// part 0: fused selection + scan; 1: selection only; 2: scan only.
+size_t search_smem_bytes(int mode, int kc, int mp, int kp, int part);
+int search_launch(const SearchArgs &a, int part, int grid, cudaStream_t s);
+int search_max_blocks_per_sm(int mode, int kc, int mp, int kp, int upl, int part);
 
 struct EncodeArgs {
     int dim, mc, kc, mp, kp, nc;  // nc = 0: IVF/IMI encoder; nc >= 2: SC encoder

@@ -70,7 +70,11 @@ __host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) &
 
 // Shared memory.  The LUT lives for the whole query; the selection phase
 // (coarse lists, staircase rows, histograms) and the scan phase (cell
-// windows, double-buffered candidate staging, top-R buffers) share the rest.
+// windows, warm-up scores, top-R buffers) share the rest.  Inside the scan
+// phase the top-R buffers alias the warm-up scores, which are dead once the
+// threshold and the survivor buffer are set.  The selection-only kernel
+// (part 1) has no LUT and no scan phase, the scan-only kernel (part 2) no
+// selection phase.
 struct Smem {
     float *lut;
     // selection phase
@@ -83,53 +87,61 @@ struct Smem {
     // scan phase (aliases the selection phase)
     CellWin *wwin;    // [NWARP][WWIN]
     uint64_t *warm;   // [WARMN]
-    uint64_t *top, *tmp;
+    uint64_t *top, *tmp;  // [RMAX] each, inside warm
     uint32_t *hist2;
     uint64_t *ties2;
 };
 
-__host__ __device__ inline size_t carve(int mode, int kc, int mp, int kp, Smem *s, unsigned char *base) {
+__host__ __device__ inline size_t carve(int mode, int kc, int mp, int kp, int part, Smem *s, unsigned char *base) {
     const int kcP = next_pow2(kc);
     size_t off = 0;
     if (s) s->lut = (float *)(base + off);
-    off += align16((size_t)mp * kp * 4);
+    if (part != 1) off += align16((size_t)mp * kp * 4);
     const size_t phase0 = off;
-    // selection phase
-    if (s) s->LA = (uint64_t *)(base + off);
-    off += (size_t)kcP * 8;
-    if (s) s->LB = (mode == SCG_IMI) ? (uint64_t *)(base + off) : s->LA;
-    off += (mode == SCG_IMI) ? (size_t)kcP * 8 : 0;
-    if (s) s->rowc = (uint16_t *)(base + off);
-    off += align16((size_t)kc * 2);
-    if (s) s->rowp = (uint16_t *)(base + off);
-    off += align16((size_t)kc * 2);
-    if (s) s->rowpre = (uint32_t *)(base + off);
-    off += align16((size_t)(kc + 1) * 4);
-    if (s) {
-        s->hist = (uint32_t *)(base + off);
-        s->ties = (uint64_t *)(base + off + (size_t)HBINS * 4);
-        s->sb = (uint64_t *)(base + off);
+    size_t end1 = phase0, end2 = phase0;
+    if (part != 2) {
+        // selection phase
+        if (s) s->LA = (uint64_t *)(base + off);
+        off += (size_t)kcP * 8;
+        if (s) s->LB = (mode == SCG_IMI) ? (uint64_t *)(base + off) : s->LA;
+        off += (mode == SCG_IMI) ? (size_t)kcP * 8 : 0;
+        if (s) s->rowc = (uint16_t *)(base + off);
+        off += align16((size_t)kc * 2);
+        if (s) s->rowp = (uint16_t *)(base + off);
+        off += align16((size_t)kc * 2);
+        if (s) s->rowpre = (uint32_t *)(base + off);
+        off += align16((size_t)(kc + 1) * 4);
+        if (s) {
+            s->hist = (uint32_t *)(base + off);
+            s->ties = (uint64_t *)(base + off + (size_t)HBINS * 4);
+            s->sb = (uint64_t *)(base + off);
+        }
+        size_t trav = (size_t)HBINS * 4 + (size_t)TIECAP * 8;
+        size_t sbb = (size_t)SBCAP * 8;
+        off += trav > sbb ? trav : sbb;
+        end1 = off;
     }
-    size_t trav = (size_t)HBINS * 4 + (size_t)TIECAP * 8;
-    size_t sbb = (size_t)SBCAP * 8;
-    off += trav > sbb ? trav : sbb;
-    const size_t end1 = off;
-    // scan phase (aliases the selection phase)
-    off = phase0;
-    if (s) s->wwin = (CellWin *)(base + off);
-    off += (size_t)NWARP * WWIN * sizeof(CellWin);
-    if (s) s->warm = (uint64_t *)(base + off);
-    off += (size_t)WARMN * 8;
-    if (s) s->top = (uint64_t *)(base + off);
-    off += (size_t)RMAX * 8;
-    if (s) s->tmp = (uint64_t *)(base + off);
-    off += (size_t)RMAX * 8;
-    if (s) s->hist2 = (uint32_t *)(base + off);
-    off += (size_t)HBINS * 4;
-    if (s) s->ties2 = (uint64_t *)(base + off);
-    off += (size_t)TIECAP * 8;
-    return off > end1 ? off : end1;
+    if (part != 1) {
+        // scan phase (aliases the selection phase)
+        off = phase0;
+        if (s) s->wwin = (CellWin *)(base + off);
+        off += (size_t)NWARP * WWIN * sizeof(CellWin);
+        if (s) {
+            s->warm = (uint64_t *)(base + off);
+            s->top = s->warm;
+            s->tmp = s->warm + RMAX;
+        }
+        off += (size_t)WARMN * 8;
+        if (s) s->hist2 = (uint32_t *)(base + off);
+        off += (size_t)HBINS * 4;
+        if (s) s->ties2 = (uint64_t *)(base + off);
+        off += (size_t)TIECAP * 8;
+        end2 = off;
+    }
+    return end1 > end2 ? end1 : end2;
 }
+
+static_assert(2 * RMAX <= WARMN, "top-R buffers live inside the warm-up scores");
 
 // ---------------------------------------------------------------------------
 // Block-wide helpers (NT threads, all threads must call)
@@ -791,14 +803,25 @@ __device__ uint32_t block_kth_hi(const uint64_t *keys, int n, int k, uint32_t *h
     return prefix;
 }
 
-template <int MPC, int U>
-__global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
+// Resident CTAs per SM the register allocation is sized for.
+#ifndef SCG_SEARCH_MIN_BLOCKS
+#define SCG_SEARCH_MIN_BLOCKS 2
+#endif
+// ... and of the scan-only kernel (part 2).
+#ifndef SCG_SCAN_MIN_BLOCKS
+#define SCG_SCAN_MIN_BLOCKS 4
+#endif
+
+// PART 0: selection and scan fused; 1: selection only, publishing each
+// query's visited cells (a.qmeta, a.pool_*); 2: scan only, from them.
+template <int MPC, int U, int PART>
+__global__ void __launch_bounds__(NT, PART == 2 ? SCG_SCAN_MIN_BLOCKS : SCG_SEARCH_MIN_BLOCKS) k_search(SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint64_t red[3 * NWARP];
     __shared__ QState st;
     __shared__ int s_q;
     Smem S;
-    carve(a.mode, a.kc, a.mp, a.kp, &S, smem);
+    carve(a.mode, a.kc, a.mp, a.kp, PART, &S, smem);
     const int tid = threadIdx.x;
     const int kc = a.kc, mp = a.mp, kp = a.kp;
     const int kcP = next_pow2(kc);
@@ -809,8 +832,8 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
     uint32_t *rec_key = a.rec_key + (size_t)blockIdx.x * cap;
     uint32_t *rec_rank = a.rec_rank + (size_t)blockIdx.x * cap;
     uint32_t *rec_cnt = a.rec_cnt + (size_t)blockIdx.x * cap;
-    uint32_t *vis_cell = a.vis_cell + (size_t)blockIdx.x * (cap + 1);
-    uint32_t *vis_pre = a.vis_pre + (size_t)blockIdx.x * (cap + 1);
+    uint32_t *vis_cell = a.vis_cell ? a.vis_cell + (size_t)blockIdx.x * (cap + 1) : nullptr;
+    uint32_t *vis_pre = a.vis_pre ? a.vis_pre + (size_t)blockIdx.x * (cap + 1) : nullptr;
     uint32_t *hist = S.hist;
     uint64_t *ties = S.ties;
     uint64_t *sb = S.sb;  // sorted coarse prefix scratch
@@ -828,7 +851,33 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
         const int R = a.R;
         const float *dqc = a.dqc + (size_t)q * a.mc * kc;
         const float qn0 = a.qn[2 * q], qn1 = a.qn[2 * q + 1], qs = a.qsum[q];
-        for (int i = tid; i < mp * kp; i += NT) S.lut[i] = a.dqr[(size_t)q * mp * kp + i];
+        if constexpr (PART != 1)
+            for (int i = tid; i < mp * kp; i += NT) S.lut[i] = a.dqr[(size_t)q * mp * kp + i];
+
+        bool nothing_q = false;  // the query visits nothing (T <= 0 or w <= 0)
+        int nvis = 0;
+        bool qerr2 = false;
+        uint32_t Svis = 0;
+        const uint32_t *vcell = vis_cell, *vpre = vis_pre;
+        if constexpr (PART == 2) {
+            // the selection kernel's result for this query
+            const QMeta m = a.qmeta[q];
+            nvis = m.nvis;
+            Svis = m.svis;
+            qerr2 = m.err != 0;
+            vcell = a.pool_cell + (size_t)q * a.pool_stride;
+            vpre = a.pool_pre + (size_t)q * a.pool_stride;
+            if (tid == 0) st.err = qerr2 ? 1 : 0;
+            __syncthreads();
+        } else {
+            // PART 1 compacts straight into the query's pool region
+            if constexpr (PART == 1) {
+                vcell = a.pool_cell + (size_t)q * a.pool_stride;
+                vpre = a.pool_pre + (size_t)q * a.pool_stride;
+            }
+            uint32_t *vis_cell_w = (uint32_t *)vcell, *vis_pre_w = (uint32_t *)vpre;
+            // entries a visited list holds (the last is the closing prefix)
+            const uint64_t vcap = PART == 1 ? (uint64_t)a.pool_stride - 1 : (uint64_t)cap;
 
         // IMI and SC test the rules before each pop (multi_query.h:151,
         // sc_query.h:130); IVFADC pops first and tests after
@@ -1169,7 +1218,6 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
         }
 
         // (4) visited non-empty cells -> (cell, prefix) list
-        int nvis = 0;
         if (!nothing && !st.err) {
             const uint32_t kap = st.kappa, rcut = st.rank_cut;
             const bool all = st.take_all != 0;
@@ -1190,24 +1238,49 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
                 uint64_t ex = block_exscan(v, red, tot);
                 if (f) {
                     uint64_t p = pos + (ex >> 40);
-                    vis_cell[p] = cell_of(L, rank);
-                    vis_pre[p] = (uint32_t)(runc + (ex & 0xffffffffffull));
+                    if (p < vcap) {
+                        vis_cell_w[p] = cell_of(L, rank);
+                        vis_pre_w[p] = (uint32_t)(runc + (ex & 0xffffffffffull));
+                    }
                 }
                 pos += tot >> 40;
                 runc += tot & 0xffffffffffull;
             }
             nvis = (int)pos;
             if (tid == 0) {
-                vis_pre[nvis] = (uint32_t)runc;
+                if (pos <= vcap) {
+                    vis_pre_w[nvis] = (uint32_t)runc;
+                } else {
+                    // more visited cells than the list holds: an error, never a truncation
+                    st.err = 1;
+                    atomicOr(a.status, ST_CELL_BUDGET);
+                }
                 st.sumv = runc;  // the candidates of the visited cells
             }
         }
         if (tid == 0) st.nvis = nvis;
         __syncthreads();
         nvis = st.nvis;
-        const bool qerr2 = st.err != 0;
-        const uint32_t Svis = (nvis > 0) ? (uint32_t)st.sumv : 0u;
+        qerr2 = st.err != 0;
+        Svis = (nvis > 0) ? (uint32_t)st.sumv : 0u;
+        nothing_q = nothing;
         PHASE_MARK(3);  // compaction
+            if constexpr (PART == 1) {
+                if (tid == 0) {
+                    QMeta m;
+                    m.nvis = qerr2 ? 0 : nvis;
+                    m.svis = Svis;
+                    m.err = qerr2 ? 1 : 0;
+                    m.pad = 0;
+                    a.qmeta[q] = m;
+                    a.out_sum[q] = qerr2 ? -1 : (int)(nothing ? 0 : st.sumv);
+                    if (a.out_nvis) a.out_nvis[q] = nvis;
+                    if (a.out_empty) a.out_empty[q] = qerr2 ? 0 : (int)(st.nv - st.nev);
+                }
+                __syncthreads();
+                continue;
+            }
+        }
 
         // (5) ADC scan with the fused top-R.  The first WARMN candidates are
         // scored into shared memory; their R-th smallest distance bounds the
@@ -1224,8 +1297,8 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
         __syncthreads();
         if (!qerr2 && nvis > 0) {
             ScanCtx c;
-            c.vis_cell = vis_cell;
-            c.vis_pre = vis_pre;
+            c.vis_cell = vcell;
+            c.vis_pre = vpre;
             c.nvis = nvis;
             c.Svis = Svis;
             c.kc = kc;
@@ -1295,9 +1368,15 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
                 }
             }
             if (tid == 0) {
-                a.out_sum[q] = qerr3 ? -1 : (int)(nothing ? 0 : st.sumv);
-                if (a.out_nvis) a.out_nvis[q] = nvis;
-                if (a.out_empty) a.out_empty[q] = qerr3 ? 0 : (int)(st.nv - st.nev);
+                if constexpr (PART == 0) {
+                    a.out_sum[q] = qerr3 ? -1 : (int)(nothing_q ? 0 : st.sumv);
+                    if (a.out_nvis) a.out_nvis[q] = nvis;
+                    if (a.out_empty) a.out_empty[q] = qerr3 ? 0 : (int)(st.nv - st.nev);
+                } else if (qerr3 && !qerr2) {
+                    // the selection kernel wrote the facts; a scan failure voids them
+                    a.out_sum[q] = -1;
+                    if (a.out_empty) a.out_empty[q] = 0;
+                }
             }
         }
         __syncthreads();
@@ -1305,43 +1384,44 @@ __global__ void __launch_bounds__(NT, 2) k_search(SearchArgs a) {
 }
 
 
-template <int MPC, int U>
+template <int MPC, int U, int PART>
 int occupancy(size_t smem) {
-    cudaFuncSetAttribute(k_search<MPC, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_search<MPC, U, PART>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<MPC, U>, NT, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<MPC, U, PART>, NT, smem);
     return nb;
 }
 
-template <int U>
+template <int U, int PART>
 int occupancy_mp(int mp, size_t smem) {
     switch (mp) {
-        case 4: return occupancy<4, U>(smem);
-        case 8: return occupancy<8, U>(smem);
-        case 16: return occupancy<16, U>(smem);
-        case 32: return occupancy<32, U>(smem);
-        default: return occupancy<0, U>(smem);
+        case 4: return occupancy<4, U, PART>(smem);
+        case 8: return occupancy<8, U, PART>(smem);
+        case 16: return occupancy<16, U, PART>(smem);
+        case 32: return occupancy<32, U, PART>(smem);
+        default: return occupancy<0, U, PART>(smem);
     }
 }
 
-template <int MPC, int U>
+template <int MPC, int U, int PART>
 int launch(const SearchArgs &a, int grid, size_t smem, cudaStream_t s) {
-    cudaError_t e = cudaFuncSetAttribute(k_search<MPC, U>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e =
+        cudaFuncSetAttribute(k_search<MPC, U, PART>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_search)");
-    k_search<MPC, U><<<grid, NT, smem, s>>>(a);
+    k_search<MPC, U, PART><<<grid, NT, smem, s>>>(a);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "k_search launch");
     return SCG_OK;
 }
 
-template <int U>
+template <int U, int PART>
 int launch_mp(const SearchArgs &a, int grid, size_t smem, cudaStream_t s) {
     switch (a.mp) {
-        case 4: return launch<4, U>(a, grid, smem, s);
-        case 8: return launch<8, U>(a, grid, smem, s);
-        case 16: return launch<16, U>(a, grid, smem, s);
-        case 32: return launch<32, U>(a, grid, smem, s);
-        default: return launch<0, U>(a, grid, smem, s);
+        case 4: return launch<4, U, PART>(a, grid, smem, s);
+        case 8: return launch<8, U, PART>(a, grid, smem, s);
+        case 16: return launch<16, U, PART>(a, grid, smem, s);
+        case 32: return launch<32, U, PART>(a, grid, smem, s);
+        default: return launch<0, U, PART>(a, grid, smem, s);
     }
 }
 

@@ -1,10 +1,15 @@
-// Instantiations of the fused search kernel with 4 candidates per lane per
-// scan chunk (one translation unit per variant, so they compile in parallel).
+// Instantiations of the fused (part 0) and scan-only (part 2) search kernels
+// with 4 candidates per lane per scan chunk (one translation unit per
+// variant, so that they compile in parallel).
 #include "search_impl.cuh"
 
 namespace scg {
 
-int search_launch_u4(const SearchArgs &a, int grid, size_t smem, cudaStream_t s) { return launch_mp<4>(a, grid, smem, s); }
-int search_occupancy_u4(int mp, size_t smem) { return occupancy_mp<4>(mp, smem); }
+int search_launch_u4(const SearchArgs &a, int part, int grid, size_t smem, cudaStream_t s) {
+    return part == 2 ? launch_mp<4, 2>(a, grid, smem, s) : launch_mp<4, 0>(a, grid, smem, s);
+}
+int search_occupancy_u4(int mp, int part, size_t smem) {
+    return part == 2 ? occupancy_mp<4, 2>(mp, smem) : occupancy_mp<4, 0>(mp, smem);
+}
 
 }  // namespace scg

@@ -10,7 +10,9 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libscgpu.so")
+# SCG_LIBRARY points at another build of the library (e.g. one compiled with
+# different tuning defines); the default is the in-tree build.
+LIB_PATH = os.environ.get("SCG_LIBRARY") or os.path.join(HERE, "libscgpu.so")
 
 IVFADC, IMI, SC2 = 0, 1, 2
 FP32_EXACT, FAST, BF16, FP16 = 0, 1, 2, 3
@@ -28,7 +30,8 @@ EXPORTS = ["scg_last_error", "scg_index_create", "scg_index_destroy", "scg_load_
            "scg_cell_counts", "scg_set_phase_counters", "scg_last_phase_counters",
            "scg_search_device_noalloc", "scg_query_tables_device", "scg_load_raw_u8",
            "scg_server_create", "scg_server_submit", "scg_server_wait", "scg_server_stats",
-           "scg_server_destroy", "scg_autotune", "scg_set_scan_tuning"]
+           "scg_server_destroy", "scg_autotune", "scg_set_scan_tuning",
+           "scg_set_kernel_split"]
 
 
 class ScgError(RuntimeError):
@@ -50,7 +53,7 @@ def load(build_if_missing=True):
     global _lib
     if _lib is not None:
         return _lib
-    if build_if_missing:
+    if build_if_missing and LIB_PATH == os.path.join(HERE, "libscgpu.so"):
         import importlib.util
         spec = importlib.util.spec_from_file_location("scg_build", os.path.join(HERE, "build.py"))
         mod = importlib.util.module_from_spec(spec)
@@ -191,6 +194,9 @@ class Index:
         _check(_lib.scg_autotune(self._h, ctypes.byref(p), ctypes.c_void_p(dQ_ptr), nq, ctypes.c_void_p(d_ids),
                                  ctypes.c_void_p(d_d), ctypes.c_void_p(d_sums), ctypes.byref(c), _ptr(ms)))
         return c.value, ms.tolist()
+
+    def set_kernel_split(self, on):
+        _check(_lib.scg_set_kernel_split(self._h, 1 if on else 0))
 
     def set_scan_tuning(self, precision, upl):
         _check(_lib.scg_set_scan_tuning(self._h, precision, upl))

@@ -245,3 +245,55 @@ def test_host_path_chunks_equal_device_path(scg, oracle_mod):
             nv2, em2 = g.last_query_stats(nq)
             assert np.array_equal(nvis, nv2) and np.array_equal(empty, em2)
     g.close()
+
+
+@pytest.mark.parametrize("mode,mc,kc", [(O.IVFADC, 1, 64), (O.IMI, 2, 48), (O.SC, 1, 48)])
+def test_split_kernels_and_per_query_targets(scg, oracle_mod, mode, mc, kc):
+    """Selection and scan as two kernels (the default) give exactly the fused
+    kernel's results; per-query candidate targets (device array, fused
+    kernel) give, for each query, the result of a call with that T."""
+    import torch
+    D, mp, kp = 64, 8, 256
+    mix = W.Mixture(D, 16, 20.0, "u8", seed=61 + mode)
+    X = mix.sample(40000, seed=62)
+    Q = mix.sample(90, seed=63)
+    cq, pq = W.train_codebooks(X[:5000], mc, kc, mp, kp, 3, seed=64)
+    if mode == O.SC:
+        cid, codes = O.sc_encode(D, kc, mp, kp, 2, cq, pq, X)
+        L, pid, co, _ = O.distribution(O.SC, kc, 1, 2, cid, codes)
+    else:
+        cid, codes = O.encode((D, mc, kc, mp, kp), cq, pq, X)
+        L, pid, co, _ = O.distribution(mode, kc, mc, 0, cid, codes)
+    g = gpu_index(scg, D, mc, kc, mp, kp, cq, pq, L, pid, co)
+    w = kc if mode == O.IVFADC else 1 << 20
+    m = MODES[mode]
+    for prec in (scg.FP32_EXACT, scg.FAST):
+        for R, T, ww in ((50, 1500, w), (10, 1, w), (100, 6000, 7)):
+            g.set_kernel_split(True)
+            a = g.search(m, Q, R, ww, T, precision=prec)
+            na = g.last_query_stats(Q.shape[0])
+            g.set_kernel_split(False)
+            b = g.search(m, Q, R, ww, T, precision=prec)
+            nb = g.last_query_stats(Q.shape[0])
+            g.set_kernel_split(True)
+            for x, y in zip(a + na, b + nb):
+                assert np.array_equal(x, y), (prec, R, T, ww)
+    rng = np.random.default_rng(65)
+    Ts = rng.choice([300, 1500, 4000], Q.shape[0]).astype(np.int32)
+    nq, R = Q.shape[0], 30
+    dQ = torch.from_numpy(Q).cuda()
+    dT = torch.from_numpy(Ts).cuda()
+    di = torch.empty(nq * R, dtype=torch.int32, device="cuda")
+    dd = torch.empty(nq * R, dtype=torch.float32, device="cuda")
+    ds = torch.empty(nq, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    g.set_query_targets(dT.data_ptr())
+    g.search_device(m, dQ.data_ptr(), nq, R, w, 999, di.data_ptr(), dd.data_ptr(), ds.data_ptr(), precision=scg.FAST)
+    g.set_query_targets(None)
+    torch.cuda.synchronize()
+    ids, d, sums = di.cpu().numpy().reshape(nq, R), dd.cpu().numpy().reshape(nq, R), ds.cpu().numpy()
+    for T in np.unique(Ts):
+        rows = np.nonzero(Ts == T)[0]
+        ai, ad, asum = g.search(m, Q[rows], R, w, int(T), precision=scg.FAST)
+        assert np.array_equal(ids[rows], ai) and np.array_equal(d[rows], ad) and np.array_equal(sums[rows], asum)
+    g.close()
