@@ -630,6 +630,9 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
     CellWin *W = S.wwin + wid * WWIN;
     uint32_t wlo = 1, whi = 0;
     int wcn = 0;
+    // this lane's window index: candidates only move forward within a window,
+    // so the cell lookup resumes where the last one stopped
+    int ci_l = 0;
     for (;;) {
         uint32_t base = 0;
         constexpr uint32_t WCH = 32u * U;
@@ -679,13 +682,14 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
                 __syncwarp();
                 wlo = W[0].pre;
                 whi = (ci + wcn < c.nvis) ? c.vis_pre[ci + wcn] : c.Svis;
+                ci_l = 0;
             }
             const uint32_t e2 = min(end, whi);
             // loads of U candidates per lane, issued together
             uint32_t pos[U], h34[U];
             float dd[U], vt[U];
             CodeWords<MPC> cwd[U];
-            int ci = 0;
+            int ci = ci_l;
 #pragma unroll
             for (int u = 0; u < U; u++) {
                 const uint32_t ff = f + lane + 32u * u;
@@ -700,6 +704,7 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
                     if (c.fast) vt[u] = __ldg(a.vterm + pos[u]);
                 }
             }
+            ci_l = ci;
 #pragma unroll
             for (int u = 0; u < U; u++) {
                 bool pass = false;
