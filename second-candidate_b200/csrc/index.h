@@ -82,7 +82,7 @@ struct scg_index {
     bool have_vterm = false;
     int64_t raw_rows = 0;   // rows of raw vectors loaded (0: none)
     bool raw_u8 = false;    // raw vectors held as uint8
-    int tuned_upl[2] = {4, 4};  // scan candidates per lane, per scan form (exact, fast)
+    int tuned_upl[2] = {2, 2};  // scan candidates per lane, per scan form (exact, fast)
     bool split = true;          // selection and scan as two kernels where possible
     scg::Workspace ws;      // the workspace of the index's own entry points
     // scg_search (host buffers) pipelines a batch in chunks over two streams

@@ -812,7 +812,10 @@ __device__ uint32_t block_kth_hi(const uint64_t *keys, int n, int k, uint32_t *h
 #ifndef SCG_SEARCH_MIN_BLOCKS
 #define SCG_SEARCH_MIN_BLOCKS 2
 #endif
-// ... and of the scan-only kernel (part 2).
+// ... of the selection-only kernel (part 1) and of the scan-only kernel (part 2).
+#ifndef SCG_SELECT_MIN_BLOCKS
+#define SCG_SELECT_MIN_BLOCKS 3
+#endif
 #ifndef SCG_SCAN_MIN_BLOCKS
 #define SCG_SCAN_MIN_BLOCKS 4
 #endif
@@ -820,7 +823,9 @@ __device__ uint32_t block_kth_hi(const uint64_t *keys, int n, int k, uint32_t *h
 // PART 0: selection and scan fused; 1: selection only, publishing each
 // query's visited cells (a.qmeta, a.pool_*); 2: scan only, from them.
 template <int MPC, int U, int PART>
-__global__ void __launch_bounds__(NT, PART == 2 ? SCG_SCAN_MIN_BLOCKS : SCG_SEARCH_MIN_BLOCKS) k_search(SearchArgs a) {
+__global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
+                                      : PART == 1 ? SCG_SELECT_MIN_BLOCKS
+                                                  : SCG_SEARCH_MIN_BLOCKS) k_search(SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint64_t red[3 * NWARP];
     __shared__ QState st;
