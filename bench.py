@@ -163,28 +163,45 @@ def cpu_reference(w, seconds_target=12.0, threads=None, mode=None):
             "seconds": sec, "recall@100": recall_at(ids, w["gt"][:n], min(100, R))}
 
 
-def serve_leg(scgpu, ix, w, mode, wcap, T, prec, batch_qps, seconds, load, seed=7):
-    """A request stream through the server (scg_server_*): Poisson arrivals,
-    each request a batch of 1..4096 queries (log-uniform) drawn from the
-    workload's queries with k in {1, 10, 100}; offered load = `load` x the
-    batch throughput.  Returns QPS (queries completed / span) and request
-    latency percentiles (submit to results on the host)."""
+def serve_leg(scgpu, ix, w, mode, wcap, T, prec, seconds, load, seed=7):
+    """A request stream through the server (scg_server_*): each request a
+    batch of 1..4096 queries (log-uniform) drawn from the workload's queries,
+    k in {1, 10, 100}.  First the server's capacity for this mix (requests
+    kept 16 deep, as fast as it completes them), then Poisson arrivals at
+    `load` x that capacity for `seconds`.  Latency = submit to results in
+    host memory, per request."""
     import threading
     rng = np.random.default_rng(seed)
     Q = w["Q"]
-    mean_batch = (4096 - 1) / np.log(4096)
-    rate = load * batch_qps / mean_batch  # requests per second
-    n = max(8, int(rate * seconds))
-    gaps = rng.exponential(1.0 / rate, n)
-    sizes = np.minimum(4096, np.exp(rng.uniform(0, np.log(4097), n)).astype(int))
-    ks = rng.choice([1, 10, 100], n)
-    starts = rng.integers(0, max(1, Q.shape[0] - 4096), n)
+
+    def mix(n):
+        sizes = np.minimum(4096, np.exp(rng.uniform(0, np.log(4097), n)).astype(int))
+        ks = rng.choice([1, 10, 100], n)
+        starts = rng.integers(0, max(1, Q.shape[0] - 4096), n)
+        return sizes, ks, starts
+
     srv = scgpu.Server(ix, slots=4, max_batch=4096, max_R=100, arena_bytes=4 << 30)
-    # warm the slots once (first-use costs stay out of the measurement)
     for t in [srv.submit(mode, Q[:64], 10, wcap, T, precision=prec) for _ in range(8)]:
         srv.wait(t)
-    tickets = []
-    done = []
+    # capacity (closed loop, 16 outstanding)
+    n_cap = 600
+    sizes, ks, starts = mix(n_cap)
+    pending = []
+    t0 = time.perf_counter()
+    for i in range(n_cap):
+        if len(pending) >= 16:
+            srv.wait(pending.pop(0))
+        pending.append(srv.submit(mode, Q[starts[i]:starts[i] + sizes[i]], int(ks[i]), wcap, T, precision=prec))
+    for t in pending:
+        srv.wait(t)
+    capacity = float(sizes.sum() / (time.perf_counter() - t0))
+    # open loop at `load` x capacity
+    mean_batch = (4096 - 1) / np.log(4096)
+    rate = load * capacity / mean_batch
+    n = max(8, int(rate * seconds))
+    gaps = rng.exponential(1.0 / rate, n)
+    sizes, ks, starts = mix(n)
+    tickets, done = [], []
 
     def waiter():
         i = 0
@@ -192,8 +209,7 @@ def serve_leg(scgpu, ix, w, mode, wcap, T, prec, batch_qps, seconds, load, seed=
             if i >= len(tickets):
                 time.sleep(0.0002)
                 continue
-            r = srv.wait(tickets[i])
-            done.append(r[3])
+            done.append(srv.wait(tickets[i], times=True)[3])
             i += 1
 
     th = threading.Thread(target=waiter)
@@ -211,12 +227,21 @@ def serve_leg(scgpu, ix, w, mode, wcap, T, prec, batch_qps, seconds, load, seed=
     span = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
-    lat = np.array(done)
-    return {"qps": float(sizes.sum() / span), "requests": int(n), "queries": int(sizes.sum()),
-            "offered_requests_per_s": float(rate), "p50_ms": float(np.percentile(lat, 50)),
-            "p99_ms": float(np.percentile(lat, 99)), "max_inflight": st["max_inflight"], "slots": 4,
-            "what": "Poisson arrivals, batches 1..4096 log-uniform, k in {1,10,100}, continuous batching "
-                    "over 4 streams; latency = submit to results in host memory"}
+    lat = np.array([x[0] for x in done])
+    qd = np.array([x[1] for x in done])
+    svc = np.array([x[2] for x in done])
+    worst = np.argsort(lat)[-5:][::-1]
+    return {"capacity_qps": capacity,
+            "queued_ms": {"p50": float(np.percentile(qd, 50)), "p99": float(np.percentile(qd, 99))},
+            "service_ms": {"p50": float(np.percentile(svc, 50)), "p99": float(np.percentile(svc, 99))},
+            "slowest": [{"nq": int(sizes[i]), "k": int(ks[i]), "total_ms": float(lat[i]), "queued_ms": float(qd[i]),
+                         "service_ms": float(svc[i])} for i in worst], "load": load, "qps": float(sizes.sum() / span), "requests": int(n),
+            "queries": int(sizes.sum()), "offered_requests_per_s": float(rate),
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "max_inflight": st["max_inflight"], "slots": 4,
+            "what": "batches 1..4096 log-uniform, k in {1,10,100}; capacity = closed loop 16 deep; then Poisson "
+                    "arrivals at load x capacity; continuous batching over 4 streams; latency = submit to "
+                    "results in host memory"}
 
 
 def workload_desc(cfg):
@@ -247,7 +272,7 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=3.0,
                     help="length of the serving leg (Poisson request stream); 0 skips it")
     ap.add_argument("--serve-load", type=float, default=0.5,
-                    help="offered load of the serving leg as a fraction of the batch throughput")
+                    help="offered load of the serving leg as a fraction of the server's measured capacity")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -472,8 +497,7 @@ def main():
         "candidates_per_query": float(sums.mean()), "cells_per_query": float(nvis.mean() + empty.mean()),
     }
     if args.serve_seconds > 0:
-        line["serving"] = serve_leg(scgpu, ix, w, mode, wcap, T, prec, line["value"] / world, args.serve_seconds,
-                                    args.serve_load)
+        line["serving"] = serve_leg(scgpu, ix, w, mode, wcap, T, prec, args.serve_seconds, args.serve_load)
         line["latency_ms"] = {"p50": line["serving"]["p50_ms"], "p99": line["serving"]["p99_ms"],
                               "what": "per request of the serving leg"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

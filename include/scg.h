@@ -244,6 +244,10 @@ int scg_server_submit(scg_server *s, const scg_search_params *p, const float *Q,
  * its copy-out, and the ticket is released. */
 int scg_server_wait(scg_server *s, uint64_t ticket, double timeout_s, double *latency_ms);
 
+/* The same with times_ms[3] (may be NULL): submit to completion, submit to
+ * admission (time queued for a slot or memory), admission to completion. */
+int scg_server_wait_times(scg_server *s, uint64_t ticket, double timeout_s, double *times_ms);
+
 /* Completed requests, the most requests ever in flight at once, and the
  * requests waiting for a slot or memory now. */
 int scg_server_stats(scg_server *s, long long *completed, int *max_inflight, int *queued);

@@ -134,6 +134,7 @@ int status_result(int st) {
     if (st & ST_ITER_CAP) return fail(SCG_ERR_CAP, "cell selection did not converge within its round cap");
     if (st & ST_TC_TIMEOUT) return fail(SCG_ERR_CUDA, "a tensor-core table tile did not complete in time");
     if (st & ST_BAD_ARG) return fail(SCG_ERR_ARG, "a shortlisted id has no raw vector");
+    if (st & ST_POOL) return fail(SCG_ERR_CAP, "the visited-cell pool of the split kernels ran out");
     if (st) return fail(SCG_ERR_CUDA, "search kernel reported status " + std::to_string(st));
     return SCG_OK;
 }
@@ -245,15 +246,33 @@ int reserve_search(scg_index *h, Workspace *ws, int mode, int grid) {
     return SCG_OK;
 }
 
-// Entries of one query's visited list in the split kernels' pool: a bound on
-// the visited non-empty cells (each holds a candidate, so at most T of them;
-// at most w; at most N; at most the cell budget) plus the closing prefix.
-static int64_t pool_stride(const scg_index *h, const scg_search_params *p) {
-    int64_t b = h->cap_rec;
-    b = std::min<int64_t>(b, p->T > 0 ? (int64_t)p->T : 1);
-    b = std::min<int64_t>(b, p->w > 0 ? (int64_t)p->w : 1);
+// Pool of the split kernels' visited lists: each query owns POOL_SLOT
+// entries (or fewer when T, w or N bound its list below that: each visited
+// non-empty cell holds a candidate, so a list has at most min(T, w, N) cells
+// plus its closing prefix); longer lists take a range of a shared overflow
+// area.  Should that run out, the batch is searched again by the fused
+// kernel.
+constexpr int64_t POOL_SLOT = 128;
+
+static void pool_dims(const scg_index *h, const scg_search_params *p, int nq, int64_t *stride, int64_t *over) {
+    int64_t b = POOL_SLOT - 1;
+    if (p) {
+        b = std::min<int64_t>(b, p->T > 0 ? (int64_t)p->T : 1);
+        b = std::min<int64_t>(b, p->w > 0 ? (int64_t)p->w : 1);
+    }
     b = std::min<int64_t>(b, h->N > 0 ? h->N : 1);
-    return b + 1;
+    *stride = b + 1;
+    *over = std::max<int64_t>(65536, 16 * (int64_t)nq);
+}
+
+int reserve_pool(scg_index *h, Workspace *ws, int nq) {
+    int64_t stride, over;
+    pool_dims(h, nullptr, nq, &stride, &over);
+    int rc;
+    if ((rc = ws->qmeta.ensure(sizeof(QMeta) * (size_t)nq))) return rc;
+    if ((rc = ws->pool_cell.ensure(4 * (size_t)(stride * nq + over)))) return rc;
+    if ((rc = ws->pool_pre.ensure(4 * (size_t)(stride * nq + over)))) return rc;
+    return SCG_OK;
 }
 
 int index_mode(const scg_index *h) {
@@ -261,7 +280,7 @@ int index_mode(const scg_index *h) {
 }
 
 int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_params *p, const float *dQ, int nq,
-               int *d_ids, float *d_d, int *d_sums, cudaStream_t s, bool wait, int *h_stat) {
+               int *d_ids, float *d_d, int *d_sums, cudaStream_t s, bool wait, int *h_stat, bool allow_split) {
     int rc;
     if ((rc = ws->init())) return rc;
     // with a shortlist re-rank the ADC search keeps L candidates per query
@@ -303,8 +322,9 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     const int *Tq = rb ? nullptr : h->d_Tq;
     // split kernels (selection, then a lighter scan at higher occupancy)
     // unless per-query targets make the visited-list bound unknown here
-    const int64_t stride = pool_stride(h, p);
-    const bool split = h->split && !Tq && (uint64_t)stride * (uint64_t)nq * 8 <= (8ull << 30);
+    int64_t stride = 0, over = 0;
+    pool_dims(h, p, nq, &stride, &over);
+    const bool split = allow_split && h->split && !Tq && stride * (int64_t)nq + over < (1ll << 32);
     auto grid_of = [&](int part) {
         int g = h->num_sms * search_max_blocks_per_sm(p->mode, h->kc, h->mp, h->kp, upl, part);
         return std::max(1, std::min(g, nq));
@@ -323,8 +343,8 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
         if ((rc = ws->vis_pre.ensure(4 * (slot + 1) * g_fused))) return rc;
     } else {
         if ((rc = ws->qmeta.ensure(sizeof(QMeta) * (size_t)nq))) return rc;
-        if ((rc = ws->pool_cell.ensure(4 * (size_t)stride * nq))) return rc;
-        if ((rc = ws->pool_pre.ensure(4 * (size_t)stride * nq))) return rc;
+        if ((rc = ws->pool_cell.ensure(4 * (size_t)(stride * nq + over)))) return rc;
+        if ((rc = ws->pool_pre.ensure(4 * (size_t)(stride * nq + over)))) return rc;
     }
     // survivors of the scan's threshold, per resident CTA
     const size_t pcap = slot > 65536 ? slot : 65536;
@@ -382,6 +402,8 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     sa.pool_cell = split ? ws->pool_cell.as<uint32_t>() : nullptr;
     sa.pool_pre = split ? ws->pool_pre.as<uint32_t>() : nullptr;
     sa.pool_stride = split ? (uint32_t)stride : 0u;
+    sa.pool_over = ws->counter.as<uint32_t>() + 2;
+    sa.pool_over_cap = split ? (uint32_t)over : 0u;
     sa.cap_rec = h->cap_rec;
     sa.pend = ws->pend.as<uint64_t>();
     sa.pcap = (uint32_t)pcap;
@@ -419,6 +441,8 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     SCG_CUDA(cudaMemcpyAsync(dst, ws->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     if (!wait) return SCG_OK;
     SCG_CUDA(cudaStreamSynchronize(s));
+    if (split && (*dst & ST_POOL))  // the visited lists outgrew the pool
+        return run_search(h, ws, rb, p, dQ, nq, d_ids, d_d, d_sums, s, true, h_stat, false);
     return status_result(*dst);
 }
 
@@ -701,8 +725,27 @@ int scg_search(scg_index *h, const scg_search_params *p, const float *Q, int nq,
     SCG_CUDA(cudaStreamSynchronize(h->stream));
     SCG_CUDA(cudaStreamSynchronize(h->stream2));
     h->ws.last_nq = nq;
-    for (int c = 0; c < nch; c++)
-        if (h->h_chunk_status[c]) return status_result(h->h_chunk_status[c]);
+    for (int c = 0; c < nch; c++) {
+        if (h->h_chunk_status[c] == ST_POOL) {
+            // this chunk's visited lists outgrew the pool: search it again fused
+            const int q0 = c * per, n = std::min(per, nq - q0);
+            cudaStream_t s = h->stream;
+            ReqBufs rb = carve_req(h->reqbuf.as<unsigned char>() + off_b[c], n, h->mc, h->kc, h->mp, h->kp, p->rerank);
+            rc = run_search(h, &h->ws, &rb, p, h->q.as<float>() + (size_t)q0 * h->dim, n,
+                            h->ids.as<int>() + (size_t)q0 * R, h->dists.as<float>() + (size_t)q0 * R,
+                            h->sums.as<int>() + q0, s, true, &h->h_chunk_status[c], false);
+            if (rc) return rc;
+            SCG_CUDA(cudaMemcpy(ids + (size_t)q0 * R, h->ids.as<int>() + (size_t)q0 * R, sizeof(int) * (size_t)n * R,
+                                cudaMemcpyDeviceToHost));
+            SCG_CUDA(cudaMemcpy(dists + (size_t)q0 * R, h->dists.as<float>() + (size_t)q0 * R,
+                                sizeof(float) * (size_t)n * R, cudaMemcpyDeviceToHost));
+            if (sums) SCG_CUDA(cudaMemcpy(sums + q0, h->sums.as<int>() + q0, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost));
+            SCG_CUDA(cudaMemcpy(h->ws.nvis.as<int>() + q0, rb.nvis, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice));
+            SCG_CUDA(cudaMemcpy(h->ws.empty.as<int>() + q0, rb.empty, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice));
+        } else if (h->h_chunk_status[c]) {
+            return status_result(h->h_chunk_status[c]);
+        }
+    }
     return SCG_OK;
 }
 

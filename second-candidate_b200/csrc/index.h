@@ -106,8 +106,13 @@ int ensure_vterm(scg_index *h, cudaStream_t s);
 // it and is read by status_result(ws).
 // h_stat (optional): pinned int that receives the status word instead of
 // ws->h_status.
+// allow_split = false forces the fused kernel.  With wait = true a batch
+// whose visited lists outgrew the split kernels' pool is searched again fused.
 int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_params *p, const float *dQ, int nq,
-               int *d_ids, float *d_d, int *d_sums, cudaStream_t s, bool wait, int *h_stat = nullptr);
+               int *d_ids, float *d_d, int *d_sums, cudaStream_t s, bool wait, int *h_stat = nullptr,
+               bool allow_split = true);
+// Sizes a workspace's visited-list pool for batches of nq queries.
+int reserve_pool(scg_index *h, Workspace *ws, int nq);
 int status_result(int st);
 // Grows a workspace to a search grid of `grid` CTAs (<= 0: a full grid).
 int reserve_search(scg_index *h, Workspace *ws, int mode, int grid);

@@ -45,6 +45,7 @@ enum : int {
     ST_ITER_CAP = 4,      // an iteration cap was reached
     ST_BAD_ARG = 8,
     ST_TC_TIMEOUT = 16,   // a tensor-core completion wait expired
+    ST_POOL = 32,         // the split kernels' visited-list pool ran out (the batch reruns fused)
 };
 
 // ---------------------------------------------------------------------------
@@ -74,10 +75,10 @@ void launch_vterm(int mode, int kc, int mp, int kp, int mc, uint64_t ncells, int
 
 // One query's visited-cell list as the selection kernel leaves it.
 struct QMeta {
+    uint32_t off;   // start of the list in the pool
     int nvis;       // visited non-empty cells
     uint32_t svis;  // their candidates
     int err;        // the selection failed (outputs void)
-    int pad;
 };
 
 struct SearchArgs {
@@ -104,8 +105,10 @@ struct SearchArgs {
     uint32_t pcap;
     // selection -> scan hand-off of the split kernels (parts 1 and 2)
     QMeta *qmeta;                            // [nq]
-    uint32_t *pool_cell, *pool_pre;          // [nq][pool_stride] visited lists
-    uint32_t pool_stride;
+    uint32_t *pool_cell, *pool_pre;          // [nq * pool_stride + pool_over_cap] visited lists
+    uint32_t pool_stride;                    // each query's own region
+    uint32_t *pool_over;                     // allocation counter of the overflow area
+    uint32_t pool_over_cap;
     int *qcounter;                           // dynamic query counter
     // outputs
     int *out_ids;

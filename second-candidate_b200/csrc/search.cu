@@ -3,6 +3,10 @@
 // the scan-only kernel (part 2) with the requested candidates per lane (the
 // variants are compiled in search_u2.cu, search_u4.cu, search_u8.cu and
 // search_sel.cu).
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "search_impl.cuh"
 
 namespace scg {
@@ -20,7 +24,7 @@ size_t search_smem_bytes(int mode, int kc, int mp, int kp, int part) {
     return carve(mode, kc, mp, kp, part, nullptr, nullptr);
 }
 
-int search_max_blocks_per_sm(int mode, int kc, int mp, int kp, int upl, int part) {
+static int occupancy_query(int mode, int kc, int mp, int kp, int upl, int part) {
     const size_t smem = search_smem_bytes(mode, kc, mp, kp, part);
     if (part == 1) return search_occupancy_select(smem);
     switch (upl) {
@@ -28,6 +32,24 @@ int search_max_blocks_per_sm(int mode, int kc, int mp, int kp, int upl, int part
         case 8: return search_occupancy_u8(mp, part, smem);
         default: return search_occupancy_u4(mp, part, smem);
     }
+}
+
+// Resident CTAs per SM, asked of the runtime once per device and shape.
+int search_max_blocks_per_sm(int mode, int kc, int mp, int kp, int upl, int part) {
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int, int, int, int, int>, int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const auto key = std::make_tuple(dev, mode, kc, mp, kp, upl, part);
+    {
+        std::lock_guard<std::mutex> g(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
+    const int nb = occupancy_query(mode, kc, mp, kp, upl, part);
+    std::lock_guard<std::mutex> g(mu);
+    if (nb > 0) cache[key] = nb;
+    return nb;
 }
 
 int search_launch(const SearchArgs &a, int part, int grid, cudaStream_t s) {

@@ -268,6 +268,7 @@ struct QState {
     int ncur, npend;
     uint64_t thr;
     uint32_t next_flat;  // next unclaimed candidate of the scan
+    uint32_t pool_off, pool_cap;  // the query's visited-list region (selection kernel)
 };
 
 // The prefix of a coarse list: the smallest keys of L[0..n) (u64: ordered
@@ -875,19 +876,16 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
             nvis = m.nvis;
             Svis = m.svis;
             qerr2 = m.err != 0;
-            vcell = a.pool_cell + (size_t)q * a.pool_stride;
-            vpre = a.pool_pre + (size_t)q * a.pool_stride;
+            vcell = a.pool_cell + m.off;
+            vpre = a.pool_pre + m.off;
             if (tid == 0) st.err = qerr2 ? 1 : 0;
             __syncthreads();
         } else {
-            // PART 1 compacts straight into the query's pool region
-            if constexpr (PART == 1) {
-                vcell = a.pool_cell + (size_t)q * a.pool_stride;
-                vpre = a.pool_pre + (size_t)q * a.pool_stride;
-            }
+            // PART 1 compacts straight into the query's pool region (set
+            // after the cut, when the list's length is known)
             uint32_t *vis_cell_w = (uint32_t *)vcell, *vis_pre_w = (uint32_t *)vpre;
             // entries a visited list holds (the last is the closing prefix)
-            const uint64_t vcap = PART == 1 ? (uint64_t)a.pool_stride - 1 : (uint64_t)cap;
+            uint64_t vcap = (uint64_t)cap;
 
         // IMI and SC test the rules before each pop (multi_query.h:151,
         // sc_query.h:130); IVFADC pops first and tests after
@@ -1226,6 +1224,32 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
             COUNT(11, 1);
             __syncthreads();
         }
+        if constexpr (PART == 1) {
+            // the query's region of the pool: its own stride-sized slot, or a
+            // range of the shared overflow area for a longer list
+            if (tid == 0) {
+                const uint32_t need = (!nothing && !st.err) ? (uint32_t)st.nev + 1u : 1u;
+                uint32_t off = (uint32_t)q * a.pool_stride, capv = a.pool_stride;
+                if (need > a.pool_stride) {
+                    const uint32_t o = atomicAdd(a.pool_over, need);
+                    if ((uint64_t)o + need <= (uint64_t)a.pool_over_cap) {
+                        off = (uint32_t)a.nq * a.pool_stride + o;
+                        capv = need;
+                    } else {
+                        st.err = 1;
+                        atomicOr(a.status, ST_POOL);
+                    }
+                }
+                st.pool_off = off;
+                st.pool_cap = capv;
+            }
+            __syncthreads();
+            vcell = a.pool_cell + st.pool_off;
+            vpre = a.pool_pre + st.pool_off;
+            vis_cell_w = (uint32_t *)vcell;
+            vis_pre_w = (uint32_t *)vpre;
+            vcap = (uint64_t)st.pool_cap - 1;
+        }
 
         // (4) visited non-empty cells -> (cell, prefix) list
         if (!nothing && !st.err) {
@@ -1278,10 +1302,10 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
             if constexpr (PART == 1) {
                 if (tid == 0) {
                     QMeta m;
+                    m.off = st.pool_off;
                     m.nvis = qerr2 ? 0 : nvis;
                     m.svis = Svis;
                     m.err = qerr2 ? 1 : 0;
-                    m.pad = 0;
                     a.qmeta[q] = m;
                     a.out_sum[q] = qerr2 ? -1 : (int)(nothing ? 0 : st.sumv);
                     if (a.out_nvis) a.out_nvis[q] = nvis;
@@ -1394,9 +1418,25 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
 }
 
 
+// Dynamic shared memory already granted to a kernel variant, per device
+// (the attribute is set once, not on every launch).
+template <int MPC, int U, int PART>
+int grant_smem(size_t smem) {
+    static int granted[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || granted[dev] < (int)smem) {
+        cudaError_t e =
+            cudaFuncSetAttribute(k_search<MPC, U, PART>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_search)");
+        if (dev >= 0 && dev < 64) granted[dev] = (int)smem;
+    }
+    return SCG_OK;
+}
+
 template <int MPC, int U, int PART>
 int occupancy(size_t smem) {
-    cudaFuncSetAttribute(k_search<MPC, U, PART>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (grant_smem<MPC, U, PART>(smem)) return 0;
     int nb = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<MPC, U, PART>, NT, smem);
     return nb;
@@ -1415,11 +1455,10 @@ int occupancy_mp(int mp, size_t smem) {
 
 template <int MPC, int U, int PART>
 int launch(const SearchArgs &a, int grid, size_t smem, cudaStream_t s) {
-    cudaError_t e =
-        cudaFuncSetAttribute(k_search<MPC, U, PART>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_search)");
+    int rc = grant_smem<MPC, U, PART>(smem);
+    if (rc) return rc;
     k_search<MPC, U, PART><<<grid, NT, smem, s>>>(a);
-    e = cudaGetLastError();
+    cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "k_search launch");
     return SCG_OK;
 }

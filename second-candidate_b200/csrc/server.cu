@@ -119,13 +119,45 @@ size_t request_bytes(const scg_index *h, const scg_search_params *p, int nq) {
            req_bytes(nq, h->dim, h->mc, h->kc, h->mp, h->kp, p->R, p->rerank);
 }
 
+// Re-searches a request whose visited lists outgrew the split kernels' pool
+// with the fused kernel, on its slot, synchronously; results land in the
+// slot's pinned staging like a normal completion.
+int rerun_fused(scg_server *s, Slot &sl, Request *r) {
+    scg_index *h = s->h;
+    const int nq = r->nq, R = r->p.R;
+    unsigned char *cur = s->arena.as<unsigned char>() + sl.off;
+    auto take = [&](size_t bytes) {
+        unsigned char *p = cur;
+        cur += up256(bytes);
+        return p;
+    };
+    float *dQ = (float *)take(4ull * nq * h->dim);
+    int *d_ids = (int *)take(4ull * nq * R);
+    float *d_d = (float *)take(4ull * nq * R);
+    int *d_s = (int *)take(4ull * nq);
+    ReqBufs rb = carve_req(cur, nq, h->mc, h->kc, h->mp, h->kp, r->p.rerank);
+    int rc = run_search(h, &sl.ws, &rb, &r->p, dQ, nq, d_ids, d_d, d_s, sl.stream, true, nullptr, false);
+    if (rc) return rc;
+    cudaError_t e = cudaMemcpy(sl.hids, d_ids, 4ull * nq * R, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(sl.hd, d_d, 4ull * nq * R, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(sl.hs, d_s, 4ull * nq, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "result copy");
+    return SCG_OK;
+}
+
 void finish(scg_server *s, Slot &sl, cudaError_t q) {
     Request *r = sl.req;
+    int st = q == cudaSuccess ? *sl.ws.h_status : 0;
+    int rc = SCG_OK;
     if (q != cudaSuccess) {
-        r->rc = cuda_fail(q, "request stream");
-        r->err = last_error_string();
-    } else if (*sl.ws.h_status) {
-        r->rc = status_result(*sl.ws.h_status);
+        rc = cuda_fail(q, "request stream");
+    } else if (st == ST_POOL) {
+        rc = rerun_fused(s, sl, r);
+    } else if (st) {
+        rc = status_result(st);
+    }
+    if (rc) {
+        r->rc = rc;
         r->err = last_error_string();
     } else {
         const size_t n = (size_t)r->nq * r->p.R;
@@ -262,6 +294,7 @@ int scg_server_create(scg_index *h, int nslots, int max_batch, int max_R, size_t
         if (e == cudaSuccess) e = cudaMallocHost((void **)&sl.hd, 4ull * max_batch * max_R);
         if (e == cudaSuccess) e = cudaMallocHost((void **)&sl.hs, 4ull * max_batch);
         if (e == cudaSuccess) rc = reserve_search(h, &sl.ws, index_mode(h), 0);
+        if (rc == SCG_OK) rc = reserve_pool(h, &sl.ws, max_batch);
     }
     if (!rc && e != cudaSuccess) rc = cuda_fail(e, "scg_server_create");
     if (rc) {
@@ -310,7 +343,7 @@ int scg_server_submit(scg_server *s, const scg_search_params *p, const float *Q,
     return SCG_OK;
 }
 
-int scg_server_wait(scg_server *s, uint64_t ticket, double timeout_s, double *latency_ms) {
+int scg_server_wait_times(scg_server *s, uint64_t ticket, double timeout_s, double *times_ms) {
     if (!s) return fail(SCG_ERR_ARG, "null server");
     std::unique_lock<std::mutex> lk(s->mu);
     auto it = s->reqs.find(ticket);
@@ -322,11 +355,23 @@ int scg_server_wait(scg_server *s, uint64_t ticket, double timeout_s, double *la
     } else if (!s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), ready)) {
         return SCG_PENDING;
     }
-    if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+    if (times_ms) {
+        using ms = std::chrono::duration<double, std::milli>;
+        times_ms[0] = ms(r->t_done - r->t_submit).count();
+        times_ms[1] = ms(r->t_start - r->t_submit).count();
+        times_ms[2] = ms(r->t_done - r->t_start).count();
+    }
     const int rc = r->rc;
     if (rc) set_error(r->err);
     s->reqs.erase(it);
     delete r;
+    return rc;
+}
+
+int scg_server_wait(scg_server *s, uint64_t ticket, double timeout_s, double *latency_ms) {
+    double t[3];
+    const int rc = scg_server_wait_times(s, ticket, timeout_s, t);
+    if (rc != SCG_PENDING && latency_ms) *latency_ms = t[0];
     return rc;
 }
 

@@ -31,7 +31,7 @@ EXPORTS = ["scg_last_error", "scg_index_create", "scg_index_destroy", "scg_load_
            "scg_search_device_noalloc", "scg_query_tables_device", "scg_load_raw_u8",
            "scg_server_create", "scg_server_submit", "scg_server_wait", "scg_server_stats",
            "scg_server_destroy", "scg_autotune", "scg_set_scan_tuning",
-           "scg_set_kernel_split"]
+           "scg_set_kernel_split", "scg_server_wait_times"]
 
 
 class ScgError(RuntimeError):
@@ -274,15 +274,16 @@ class Server:
         self._live[t.value] = (Q, ids, d, sums)
         return t.value
 
-    def wait(self, ticket, timeout=-1.0):
-        """(ids, dists, sums, latency_ms), or None if the timeout expired."""
-        lat = ctypes.c_double()
-        rc = _lib.scg_server_wait(self._s, ctypes.c_uint64(ticket), ctypes.c_double(timeout), ctypes.byref(lat))
+    def wait(self, ticket, timeout=-1.0, times=False):
+        """(ids, dists, sums, latency_ms), or None if the timeout expired.
+        With times=True the last item is (total, queued, service) in ms."""
+        t = np.zeros(3, np.float64)
+        rc = _lib.scg_server_wait_times(self._s, ctypes.c_uint64(ticket), ctypes.c_double(timeout), _ptr(t))
         if rc == PENDING:
             return None
         Q, ids, d, sums = self._live.pop(ticket)
         _check(rc)
-        return ids, d, sums, lat.value
+        return ids, d, sums, (tuple(t.tolist()) if times else float(t[0]))
 
     def stats(self):
         c = ctypes.c_longlong()

@@ -297,3 +297,46 @@ def test_split_kernels_and_per_query_targets(scg, oracle_mod, mode, mc, kc):
         ai, ad, asum = g.search(m, Q[rows], R, w, int(T), precision=scg.FAST)
         assert np.array_equal(ids[rows], ai) and np.array_equal(d[rows], ad) and np.array_equal(sums[rows], asum)
     g.close()
+
+
+def test_pool_overflow_reruns_fused(scg, oracle_mod):
+    """Long visited lists (hundreds of cells per query) overflow the split
+    kernels' shared pool area; the batch is then searched by the fused
+    kernel, so results never change: host path, device path and server."""
+    import torch
+    D, mc, kc, mp, kp = 64, 2, 256, 8, 256
+    mix = W.Mixture(D, 16, 20.0, "u8", seed=71)
+    X = mix.sample(60000, seed=72)
+    Q = mix.sample(700, seed=73)
+    cq, pq = W.train_codebooks(X[:8000], mc, kc, mp, kp, 3, seed=74)
+    g = scg.Index(0)
+    g.load_codebooks(cq, kc, mc, pq, kp, mp, D)
+    cid, codes = g.encode(X)
+    L, pid, co, _ = O.distribution(O.IMI, kc, mc, 0, cid, codes)
+    g.load_csr(L, pid, co)
+    g.precompute()
+    R, T = 20, 4000
+    g.set_kernel_split(False)
+    ref = g.search(1, Q, R, 1 << 20, T, precision=scg.FAST)
+    nv, _ = g.last_query_stats(Q.shape[0])
+    # lists longer than a query's own pool slot, more than the overflow area holds
+    assert (nv >= 128).mean() > 0.5 and nv.sum() > 65536 + 16 * Q.shape[0] + 128 * Q.shape[0], nv.mean()
+    g.set_kernel_split(True)
+    got = g.search(1, Q, R, 1 << 20, T, precision=scg.FAST)
+    for x, y in zip(ref, got):
+        assert np.array_equal(x, y)
+    nq = Q.shape[0]
+    dQ = torch.from_numpy(Q).cuda()
+    di = torch.empty(nq * R, dtype=torch.int32, device="cuda")
+    dd = torch.empty(nq * R, dtype=torch.float32, device="cuda")
+    ds = torch.empty(nq, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    g.search_device(1, dQ.data_ptr(), nq, R, 1 << 20, T, di.data_ptr(), dd.data_ptr(), ds.data_ptr(),
+                    precision=scg.FAST)
+    torch.cuda.synchronize()
+    assert np.array_equal(di.cpu().numpy(), ref[0].ravel()) and np.array_equal(dd.cpu().numpy(), ref[1].ravel())
+    srv = scg.Server(g, slots=2, max_batch=1024, max_R=R, arena_bytes=512 << 20)
+    ids, d, sums, _ = srv.wait(srv.submit(1, Q, R, 1 << 20, T, precision=scg.FAST))
+    srv.close()
+    assert np.array_equal(ids, ref[0]) and np.array_equal(d, ref[1]) and np.array_equal(sums, ref[2])
+    g.close()
