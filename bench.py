@@ -269,6 +269,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the FP32 plain comparison")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--phases", action="store_true", help="report per-phase cycle counters")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the library's default scan chunking")
     ap.add_argument("--serve-seconds", type=float, default=3.0,
                     help="length of the serving leg (Poisson request stream); 0 skips it")
     ap.add_argument("--serve-load", type=float, default=0.5,
@@ -349,7 +350,7 @@ def main():
     # the scan's chunking picked by the library's autotuner on this batch, for
     # both scan forms (exact and fast)
     tuning = {}
-    for name, pv in (("fast", prec), ("fp32", 0)):
+    for name, pv in ((("fast", prec), ("fp32", 0)) if not args.no_autotune else ()):
         choice, ms = ix.autotune(mode, dQ.data_ptr(), nq, R, wcap, T, d_ids.data_ptr(), d_d.data_ptr(),
                                  d_s.data_ptr(), precision=pv)
         tuning[name] = {"candidates_per_lane": choice, "ms_by_choice": dict(zip((2, 4, 8), ms))}
@@ -382,7 +383,8 @@ def main():
             forms[name] = {"value": nq / (statistics.mean(pt) / 1e3), "unit": "queries/s",
                            "recall@100": W.recall_at(pids, w["gt"], min(100, R)),
                            "ms_per_step": statistics.mean(pt), "what": desc,
-                           "kernels_ms": dict(zip(("tables", "select_scan"), ix.last_timings()))}
+                           "kernels_ms": dict(zip(("tables_and_prefix", "select_scan", "rerank", "select", "scan"),
+                                                  ix.last_timings()))}
 
     for _ in range(args.warmup):
         step()
@@ -421,19 +423,23 @@ def main():
     nvis, empty = ix.last_query_stats(nq)
     recall = W.recall_at(ids, w["gt"], min(100, R))
 
-    # roofline of the fused selection + scan kernel: algorithmic bytes = the
-    # codes of every scanned candidate + 8 bytes of CSR offsets per visited
-    # cell + 4 bytes per returned id
+    # roofline of the dominant kernel, the ADC scan (the scan-only kernel when
+    # selection and scan run as two kernels): algorithmic bytes = the codes of
+    # every scanned candidate + 8 bytes of CSR offsets per visited cell + 4
+    # bytes per returned id
     search_ms = statistics.mean(k[1] for k in kern)
     tables_ms = statistics.mean(k[0] for k in kern)
+    select_ms = statistics.mean(k[3] for k in kern)
+    scan_ms = statistics.mean(k[4] for k in kern)
+    split = scan_ms > 0
     alg_bytes = float(sums.astype(np.int64).sum() * cfg["mp"] + 8 * nvis.astype(np.int64).sum() + 4 * nq * R)
     hbm, _, peak_kind = peaks()
-    achieved = alg_bytes / (search_ms / 1e3) / 1e9
+    achieved = alg_bytes / ((scan_ms if split else search_ms) / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get("k_search:" + args.workload)
+            traffic = json.load(open(tpath)).get(("k_search_scan:" if split else "k_search:") + args.workload)
         except Exception:
             traffic = None
 
@@ -484,14 +490,18 @@ def main():
         "latency_ms": {"p50": float(np.percentile(times, 50)), "p99": float(np.percentile(times, 99)),
                        "what": "whole batch of %d queries" % nq},
         "batch_ms": {"p50": float(np.percentile(times, 50)), "p99": float(np.percentile(times, 99))},
-        "kernels_ms": {"tables": tables_ms, "select_scan": search_ms},
+        "kernels_ms": {"tables_and_prefix": tables_ms, "select_scan": search_ms, "select": select_ms,
+                       "scan": scan_ms},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
-                     "kernel": "k_search (selection + ADC scan + top-R)",
+                     "kernel": ("k_search<.., 2> (ADC scan + top-R; selection runs as its own kernel)" if split
+                                else "k_search (fused selection + ADC scan + top-R)"),
                      "alg_bytes_per_launch": alg_bytes},
         "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": int(nq * cfg["D"] * 4),
                 "d2h_bytes_per_step": int(nq * R * 8 + nq * 4), "same_ids_as_device_path": same},
-        "gpu_launches": 3 * args.steps,
+        # per step: tensor-core tables, query norms, coarse prefixes,
+        # selection, scan (the fused kernel replaces the last two)
+        "gpu_launches": (5 if split else 4) * args.steps,
         "autotune": tuning,
         "clocks": ck,
         "candidates_per_query": float(sums.mean()), "cells_per_query": float(nvis.mean() + empty.mean()),

@@ -197,8 +197,9 @@ int scg_last_query_stats(scg_index *h, int *nvis, int *empty, int nq);
 
 /* Device time in milliseconds of the kernels of the last search call,
  * measured with CUDA events on its stream: ms[0] the per-query tables and
- * coarse-list prefixes, ms[1] the fused selection + scan, ms[2] the
- * shortlist re-rank (0 without one).  After scg_search (host buffers), which
+ * coarse-list prefixes, ms[1] cell selection + scan, ms[2] the shortlist
+ * re-rank (0 without one), ms[3] and ms[4] the selection kernel and the scan
+ * kernel alone when they ran as two kernels (0 otherwise).  After scg_search (host buffers), which
  * runs large batches in chunks over two streams, the figures are those of
  * the last chunk on the index's own stream.  n is the capacity of ms. */
 int scg_last_timings(scg_index *h, float *ms, int n);

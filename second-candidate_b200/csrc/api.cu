@@ -142,7 +142,7 @@ int status_result(int st) {
 int Workspace::init() {
     cudaError_t e = cudaSuccess;
     if (!h_status) e = cudaMallocHost((void **)&h_status, sizeof(int) * 4);
-    for (int i = 0; i < 4 && e == cudaSuccess; i++)
+    for (int i = 0; i < 5 && e == cudaSuccess; i++)
         if (!ev[i]) e = cudaEventCreate(&ev[i]);
     if (e != cudaSuccess) return cuda_fail(e, "workspace");
     return SCG_OK;
@@ -154,9 +154,9 @@ void Workspace::release() {
     for (DevBuf *b : all) b->release();
     if (h_status) cudaFreeHost(h_status);
     h_status = nullptr;
-    for (int i = 0; i < 4; i++)
+    for (int i = 0; i < 5; i++)
         if (ev[i]) cudaEventDestroy(ev[i]);
-    for (int i = 0; i < 4; i++) ev[i] = nullptr;
+    for (int i = 0; i < 5; i++) ev[i] = nullptr;
 }
 
 static size_t up256b(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -422,6 +422,7 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
             // two persistent launches, each with its own query counter
             sa.qcounter = ws->counter.as<int>();
             if ((rc = search_launch(sa, 1, g_sel, s))) return rc;
+            SCG_CUDA(cudaEventRecord(ws->ev[4], s));
             sa.qcounter = ws->counter.as<int>() + 1;
             if ((rc = search_launch(sa, 2, g_scan, s))) return rc;
         } else if ((rc = search_launch(sa, 0, g_fused, s))) {
@@ -437,6 +438,7 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     }
     SCG_CUDA(cudaEventRecord(ws->ev[3], s));
     ws->last_nq = nq;
+    ws->last_split = split && nq > 0;
     int *dst = h_stat ? h_stat : ws->h_status;
     SCG_CUDA(cudaMemcpyAsync(dst, ws->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     if (!wait) return SCG_OK;
@@ -924,11 +926,15 @@ int scg_last_timings(scg_index *h, float *ms, int n) {
     std::lock_guard<std::mutex> g(h->mu);
     int rc;
     if ((rc = set_device(h))) return rc;
-    float t[3];
+    float t[5] = {0, 0, 0, 0, 0};
     SCG_CUDA(cudaEventElapsedTime(&t[0], h->ws.ev[0], h->ws.ev[1]));
     SCG_CUDA(cudaEventElapsedTime(&t[1], h->ws.ev[1], h->ws.ev[2]));
     SCG_CUDA(cudaEventElapsedTime(&t[2], h->ws.ev[2], h->ws.ev[3]));
-    for (int i = 0; i < n && i < 3; i++) ms[i] = t[i];
+    if (h->ws.last_split) {
+        SCG_CUDA(cudaEventElapsedTime(&t[3], h->ws.ev[1], h->ws.ev[4]));
+        SCG_CUDA(cudaEventElapsedTime(&t[4], h->ws.ev[4], h->ws.ev[2]));
+    }
+    for (int i = 0; i < n && i < 5; i++) ms[i] = t[i];
     return SCG_OK;
 }
 

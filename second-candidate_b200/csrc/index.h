@@ -43,7 +43,10 @@ struct Workspace {
     DevBuf rec_key, rec_rank, rec_cnt, vis_cell, vis_pre, pend, phase, sl_ids, sl_d, slist, smeta;
     DevBuf qmeta, pool_cell, pool_pre;  // selection -> scan hand-off of the split kernels
     int *h_status = nullptr;  // pinned copy of the status word
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // events: before tables, after tables, after selection + scan, after
+    // re-rank, between the selection and scan kernels (split launches)
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    bool last_split = false;
     int last_nq = 0;
     bool phase_on = false;
     int init();

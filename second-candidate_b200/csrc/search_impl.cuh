@@ -632,8 +632,11 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
     uint32_t wlo = 1, whi = 0;
     int wcn = 0;
     // this lane's window index: candidates only move forward within a window,
-    // so the cell lookup resumes where the last one stopped
+    // so the cell lookup resumes where the last one stopped; the current cell
+    // is cached in registers ([r_pre, r_next) of the flat candidate index)
     int ci_l = 0;
+    uint32_t r_pre = 0, r_next = 0, r_start = 0, r_h34 = 0;
+    float r_d0 = 0.0f;
     for (;;) {
         uint32_t base = 0;
         constexpr uint32_t WCH = 32u * U;
@@ -684,6 +687,7 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
                 wlo = W[0].pre;
                 whi = (ci + wcn < c.nvis) ? c.vis_pre[ci + wcn] : c.Svis;
                 ci_l = 0;
+                r_next = 0;  // the cached cell belongs to the old window
             }
             const uint32_t e2 = min(end, whi);
             // loads of U candidates per lane, issued together
@@ -696,11 +700,18 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
                 const uint32_t ff = f + lane + 32u * u;
                 pos[u] = 0xffffffffu;
                 if (ff < e2) {
-                    while (ci + 1 < wcn && W[ci + 1].pre <= ff) ci++;
-                    const CellWin cw = W[ci];
-                    pos[u] = cw.start + (ff - cw.pre);
-                    dd[u] = cw.d0;
-                    h34[u] = cw.h34;
+                    if (ff >= r_next || ff < r_pre) {
+                        while (ci + 1 < wcn && W[ci + 1].pre <= ff) ci++;
+                        const CellWin cw = W[ci];
+                        r_pre = cw.pre;
+                        r_start = cw.start;
+                        r_d0 = cw.d0;
+                        r_h34 = cw.h34;
+                        r_next = (ci + 1 < wcn) ? W[ci + 1].pre : whi;
+                    }
+                    pos[u] = r_start + (ff - r_pre);
+                    dd[u] = r_d0;
+                    h34[u] = r_h34;
                     cwd[u].load(a.codes, pos[u], c.mp);
                     if (c.fast) vt[u] = __ldg(a.vterm + pos[u]);
                 }

@@ -221,10 +221,11 @@ class Index:
         return {n: int(v) for n, v in zip(names, out) if n != "-"}
 
     def last_timings(self):
-        """Device ms of the last search: (tables, selection + scan, re-rank)."""
-        ms = np.zeros(3, np.float32)
-        _check(_lib.scg_last_timings(self._h, _ptr(ms), 3))
-        return float(ms[0]), float(ms[1]), float(ms[2])
+        """Device ms of the last search: (tables, selection + scan, re-rank,
+        selection kernel, scan kernel) -- the last two 0 for the fused kernel."""
+        ms = np.zeros(5, np.float32)
+        _check(_lib.scg_last_timings(self._h, _ptr(ms), 5))
+        return tuple(float(x) for x in ms)
 
     def encode(self, X):
         X = np.ascontiguousarray(X, np.float32)
