@@ -244,6 +244,41 @@ def serve_leg(scgpu, ix, w, mode, wcap, T, prec, seconds, load, seed=7):
                     "results in host memory"}
 
 
+def encode_leg(scgpu, ix, cfg, rows, dev):
+    """Encoder throughput on rows drawn like the workload's base (device
+    buffers): the tensor-core encoder (tcgen05 distance tables + exact
+    re-check) against the all-double kernel; both must give the same codes."""
+    import torch
+    g = torch.Generator(device=dev).manual_seed(99)
+    D = cfg["D"]
+    means = torch.rand(cfg["comps"], D, generator=g, device=dev) * 128.0
+    comp = torch.randint(0, cfg["comps"], (rows,), generator=g, device=dev)
+    X = (means[comp] + cfg["sigma"] * torch.randn(rows, D, generator=g, device=dev)).round_().clamp_(0, 255)
+    mcp = 1 if cfg["mode"] == "sc" else cfg["mc"]
+    out = {}
+    codes = {}
+    for name, method in (("tensor", scgpu.ENC_TENSOR), ("exact", scgpu.ENC_EXACT)):
+        ix.set_encoder(method)
+        cid = torch.empty(rows, mcp, dtype=torch.int16, device=dev)
+        cod = torch.empty(rows, cfg["mp"], dtype=torch.uint8, device=dev)
+        ix.encode_device(X[:65536].data_ptr(), 65536, 0, cid.data_ptr(), cod.data_ptr())  # warm-up
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        ix.encode_device(X.data_ptr(), rows, 0, cid.data_ptr(), cod.data_ptr())
+        e1.record()
+        e1.synchronize()
+        out[name + "_rows_per_s"] = rows / (e0.elapsed_time(e1) / 1e3)
+        codes[name] = (cid.cpu().numpy(), cod.cpu().numpy())
+    ix.set_encoder(scgpu.ENC_TENSOR)
+    out["same_codes"] = bool(np.array_equal(codes["tensor"][0], codes["exact"][0]) and
+                             np.array_equal(codes["tensor"][1], codes["exact"][1]))
+    out["rows"] = rows
+    out["what"] = ("Encoder::encode<T> codes (IVF/IMI) of rows drawn from the workload's mixture: tcgen05 "
+                   "split-BF16 distance tables + exact double re-check vs the all-double kernel")
+    return out
+
+
 def workload_desc(cfg):
     if cfg["mode"] == "imi":
         idx = "IMI 2x%d, residual PQ %dx%d" % (cfg["kc"], cfg["mp"], cfg["kp"])
@@ -270,6 +305,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--phases", action="store_true", help="report per-phase cycle counters")
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default scan chunking")
+    ap.add_argument("--encode-rows", type=int, default=2_000_000,
+                    help="rows of the encoder leg (tensor-core vs exact encoder); 0 skips it")
     ap.add_argument("--serve-seconds", type=float, default=3.0,
                     help="length of the serving leg (Poisson request stream); 0 skips it")
     ap.add_argument("--serve-load", type=float, default=0.5,
@@ -506,6 +543,8 @@ def main():
         "clocks": ck,
         "candidates_per_query": float(sums.mean()), "cells_per_query": float(nvis.mean() + empty.mean()),
     }
+    if args.encode_rows > 0:
+        line["encode"] = encode_leg(scgpu, ix, cfg, args.encode_rows, dev)
     if args.serve_seconds > 0:
         line["serving"] = serve_leg(scgpu, ix, w, mode, wcap, T, prec, args.serve_seconds, args.serve_load)
         line["latency_ms"] = {"p50": line["serving"]["p50_ms"], "p99": line["serving"]["p99_ms"],

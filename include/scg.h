@@ -186,6 +186,16 @@ int scg_encode(scg_index *h, const float *X, int64_t n, uint16_t *cid, uint8_t *
 int scg_sc_encode(scg_index *h, const float *X, int64_t n, int nc, uint16_t *cid,
                   uint8_t *codes);
 
+/* Encoder arithmetic for IVF/IMI codes (scg_encode, scg_encode_device with
+ * nc = 0).  SCG_ENC_TENSOR (the default): distances ranked by tcgen05
+ * split-BF16 GEMM tiles, every centroid within the tiles' error margin of the
+ * minimum re-scored with the reference's double arithmetic -- the codes are
+ * the reference's.  SCG_ENC_EXACT: every distance in double (one thread per
+ * row).  The second-candidate encoder always uses the exact kernel. */
+#define SCG_ENC_EXACT 0
+#define SCG_ENC_TENSOR 1
+int scg_set_encoder(scg_index *h, int method);
+
 /* Device-buffer form of the two encoders (X, cid, codes on the device). */
 int scg_encode_device(scg_index *h, const float *dX, int64_t n, int nc, uint16_t *d_cid,
                       uint8_t *d_codes, void *stream);

@@ -352,6 +352,7 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
 
     if (scan_form(p->precision) == SCG_FAST && (rc = ensure_vterm(h, s))) return rc;
     TablesArgs ta;
+    memset(&ta, 0, sizeof(ta));
     ta.dim = h->dim; ta.mc = h->mc; ta.kc = h->kc; ta.mp = h->mp; ta.kp = h->kp; ta.nq = nq;
     ta.Q = dQ;
     ta.cq = h->cq.as<float>(); ta.pq = h->pq.as<float>();
@@ -496,7 +497,9 @@ int scg_index_destroy(scg_index *h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     DevBuf *all[] = {&h->cq, &h->pq, &h->norm_c, &h->norm_r, &h->dot_cr, &h->off, &h->pid, &h->codes,
-                     &h->raw, &h->vterm, &h->q, &h->ids, &h->dists, &h->sums, &h->reqbuf};
+                     &h->raw, &h->vterm, &h->q, &h->ids, &h->dists, &h->sums, &h->reqbuf,
+                     &h->enc_nc, &h->enc_nr, &h->enc_cmax, &h->enc_rmax, &h->enc_tab, &h->enc_res,
+                     &h->enc_status};
     for (DevBuf *b : all) b->release();
     if (h->stream2) cudaStreamSynchronize(h->stream2);
     h->ws.release();
@@ -523,6 +526,7 @@ int scg_load_codebooks(scg_index *h, const float *cq, int kc, int mc, const floa
     SCG_CUDA(cudaMemcpy(h->pq.p, pq, sizeof(float) * (size_t)kp * dim, cudaMemcpyHostToDevice));
     h->dim = dim; h->mc = mc; h->kc = kc; h->mp = mp; h->kp = kp;
     h->have_codebooks = true;
+    h->enc_ready = false;
     h->precomputed = false;
     h->have_vterm = false;
     return SCG_OK;
@@ -850,6 +854,72 @@ int scg_set_cell_budget(scg_index *h, int max_cells) {
     return SCG_OK;
 }
 
+// IVF/IMI codes through tensor-core distance tables and exact re-checks
+// (encode_tc.cu), a chunk of rows at a time.
+static int encode_tc(scg_index *h, const float *dX, int64_t n, uint16_t *d_cid, uint8_t *d_codes, cudaStream_t s) {
+    int rc;
+    const int bsc = h->dim / h->mc, bsp = h->dim / h->mp;
+    if (!h->enc_ready) {
+        if ((rc = h->enc_nc.ensure(4ull * h->mc * h->kc))) return rc;
+        if ((rc = h->enc_nr.ensure(4ull * h->mp * h->kp))) return rc;
+        if ((rc = h->enc_cmax.ensure(4ull * h->mc))) return rc;
+        if ((rc = h->enc_rmax.ensure(4ull * h->mp))) return rc;
+        launch_norms(h->cq.as<float>(), h->mc * h->kc, bsc, h->enc_nc.as<float>(), s);
+        launch_norms(h->pq.as<float>(), h->mp * h->kp, bsp, h->enc_nr.as<float>(), s);
+        launch_segmax(h->enc_nc.as<float>(), h->mc, h->kc, h->enc_cmax.as<float>(), s);
+        launch_segmax(h->enc_nr.as<float>(), h->mp, h->kp, h->enc_rmax.as<float>(), s);
+        SCG_CUDA(cudaGetLastError());
+        h->enc_ready = true;
+    }
+    const int64_t RC = 32768;
+    const int64_t width = std::max<int64_t>((int64_t)h->mc * h->kc, (int64_t)h->mp * h->kp);
+    if ((rc = h->enc_tab.ensure(4ull * RC * width))) return rc;
+    if ((rc = h->enc_res.ensure(4ull * RC * h->dim))) return rc;
+    if ((rc = h->enc_status.ensure(16))) return rc;
+    SCG_CUDA(cudaMemsetAsync(h->enc_status.p, 0, 16, s));
+    for (int64_t r0 = 0; r0 < n; r0 += RC) {
+        const int nr = (int)std::min<int64_t>(RC, n - r0);
+        TablesArgs ta;
+        memset(&ta, 0, sizeof(ta));
+        ta.dim = h->dim; ta.mc = h->mc; ta.kc = h->kc; ta.mp = h->mp; ta.kp = h->kp; ta.nq = nr;
+        ta.Q = dX + (size_t)r0 * h->dim;
+        ta.cq = h->cq.as<float>(); ta.pq = h->pq.as<float>();
+        ta.norm_c = h->enc_nc.as<float>(); ta.norm_r = h->enc_nr.as<float>();
+        ta.dqc = h->enc_tab.as<float>(); ta.dqr = h->enc_tab.as<float>();
+        ta.status = h->enc_status.as<int>();
+        ta.segs = 1;
+        launch_tables_tc(ta, 3, 1, s);
+        PickArgs pa;
+        pa.X = ta.Q; pa.n = nr; pa.dim = h->dim; pa.nseg = h->mc; pa.kseg = h->kc; pa.len = bsc;
+        pa.C = h->cq.as<float>(); pa.tab = h->enc_tab.as<float>(); pa.segmax = h->enc_cmax.as<float>();
+        pa.cid = d_cid + (size_t)r0 * h->mc; pa.code = nullptr; pa.resid = h->enc_res.as<float>();
+        pa.status = h->enc_status.as<int>();
+        launch_pick(pa, s);
+        ta.Q = h->enc_res.as<float>();
+        ta.segs = 2;
+        launch_tables_tc(ta, 3, 1, s);
+        pa.X = h->enc_res.as<float>(); pa.nseg = h->mp; pa.kseg = h->kp; pa.len = bsp;
+        pa.C = h->pq.as<float>(); pa.segmax = h->enc_rmax.as<float>();
+        pa.cid = nullptr; pa.code = d_codes + (size_t)r0 * h->mp; pa.resid = nullptr;
+        launch_pick(pa, s);
+        SCG_CUDA(cudaGetLastError());
+    }
+    int st = 0;
+    SCG_CUDA(cudaMemcpyAsync(&st, h->enc_status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    SCG_CUDA(cudaStreamSynchronize(s));
+    if (st & ST_TC_TIMEOUT) return fail(SCG_ERR_CUDA, "a tensor-core distance tile did not complete in time");
+    if (st & ST_BAD_ARG) return fail(SCG_ERR_ARG, "a row has no finite distance (NaN or infinite input)");
+    return SCG_OK;
+}
+
+int scg_set_encoder(scg_index *h, int method) {
+    if (!h) return fail(SCG_ERR_ARG, "null index");
+    if (method != SCG_ENC_EXACT && method != SCG_ENC_TENSOR) return fail(SCG_ERR_ARG, "unknown encoder");
+    std::lock_guard<std::mutex> g(h->mu);
+    h->encoder = method;
+    return SCG_OK;
+}
+
 int scg_encode_device(scg_index *h, const float *dX, int64_t n, int nc, uint16_t *d_cid, uint8_t *d_codes,
                       void *stream) {
     if (!h) return fail(SCG_ERR_ARG, "null index");
@@ -860,12 +930,13 @@ int scg_encode_device(scg_index *h, const float *dX, int64_t n, int nc, uint16_t
     if (nc && h->mc != 1) return fail(SCG_ERR_ARG, "the second-candidate encoder needs mc = 1");
     if (nc > h->kc) return fail(SCG_ERR_ARG, "nc > kc");
     int mcp = nc ? 1 : h->mc;
-    size_t smem = sizeof(float) * (8192 + (size_t)(h->dim / mcp) * 64 + (size_t)h->dim * 64);
-    if (smem > 227 * 1024) return fail(SCG_ERR_ARG, "dimension too large for the encoder's shared-memory tile");
     std::lock_guard<std::mutex> g(h->mu);
     int rc;
     if ((rc = set_device(h))) return rc;
     cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+    if (nc == 0 && h->encoder == SCG_ENC_TENSOR) return n > 0 ? encode_tc(h, dX, n, d_cid, d_codes, s) : SCG_OK;
+    if (encode_smem_bytes(h->dim, mcp) > 227 * 1024)
+        return fail(SCG_ERR_ARG, "dimension too large for the exact encoder's shared-memory tile");
     EncodeArgs a;
     a.dim = h->dim; a.mc = h->mc; a.kc = h->kc; a.mp = h->mp; a.kp = h->kp; a.nc = nc; a.n = n;
     a.X = dX; a.cq = h->cq.as<float>(); a.pq = h->pq.as<float>(); a.cid = d_cid; a.codes = d_codes;
@@ -1085,6 +1156,7 @@ extern "C" int scg_search_device_noalloc(scg_index *h, const scg_search_params *
     if ((size_t)(cur - base) > SCG_NOALLOC_SCRATCH_BYTES) return fail(SCG_ERR_CAP, "allocation-free scratch overrun");
 
     TablesArgs ta;
+    memset(&ta, 0, sizeof(ta));
     ta.dim = h->dim; ta.mc = h->mc; ta.kc = h->kc; ta.mp = h->mp; ta.kp = h->kp; ta.nq = nq;
     ta.Q = dQ;
     ta.cq = h->cq.as<float>(); ta.pq = h->pq.as<float>();

@@ -18,8 +18,9 @@ namespace scg {
 
 namespace {
 
-constexpr int ERT = 64;     // rows per block (one per thread)
 constexpr int ECH = 8192;   // floats of centroid data staged per chunk
+// rows per block (one per thread): 64, or 16 when the staged rows of a wide
+// vector (D up to ~1,400) would not fit shared memory at 64
 
 __device__ __forceinline__ double l2sq(const float *x, int xstride, const float *c, int len) {
     double dis = 0.0;
@@ -32,6 +33,7 @@ __device__ __forceinline__ double l2sq(const float *x, int xstride, const float 
 
 // Stages rows [r0, r0+ERT) x dims [d0, d0+len) into xs laid out [dim][ERT]
 // (thread t reads column t: conflict-free).
+template <int ERT>
 __device__ void stage_rows(const float *X, int64_t n, int dim, int64_t r0, int d0, int len, float *xs) {
     for (int i = threadIdx.x; i < ERT * len; i += ERT) {
         int r = i / len, t = i % len;
@@ -43,7 +45,7 @@ __device__ void stage_rows(const float *X, int64_t n, int dim, int64_t r0, int d
 // Finds the nearest of `kcount` centroids of length `len` (rows of C) for
 // this thread's staged vector; first minimum in double.  nbest >= 1 keeps the
 // nbest smallest float-rounded distances instead (SC coarse step).
-template <int NB>
+template <int NB, int ERT>
 __device__ void nearest(const float *C, int kcount, int len, const float *xs, float *cs, bool float_cmp,
                         int *best_idx) {
     double bd = 1.7976931348623157e308;  // DBL_MAX, as encoder.h:143
@@ -94,7 +96,7 @@ __device__ void nearest(const float *C, int kcount, int len, const float *xs, fl
     for (int i = 0; i < NB; i++) best_idx[i] = bi[i];
 }
 
-template <int NC>
+template <int NC, int ERT>
 __global__ void __launch_bounds__(ERT) k_encode(EncodeArgs a) {
     extern __shared__ __align__(16) float esm[];
     const int mcp = NC ? 1 : a.mc;
@@ -107,12 +109,12 @@ __global__ void __launch_bounds__(ERT) k_encode(EncodeArgs a) {
     const bool live = row < a.n;
     for (int j = 0; j < mcp; j++) {
         __syncthreads();
-        stage_rows(a.X, a.n, a.dim, r0, j * bsc, bsc, xs);
+        stage_rows<ERT>(a.X, a.n, a.dim, r0, j * bsc, bsc, xs);
         __syncthreads();
         int idx[NC ? NC : 1];
         const float *C = a.cq + (size_t)j * a.kc * bsc;
-        if (NC) nearest<NC ? NC : 1>(C, a.kc, bsc, xs, cs, true, idx);
-        else nearest<1>(C, a.kc, bsc, xs, cs, false, idx);
+        if (NC) nearest<NC ? NC : 1, ERT>(C, a.kc, bsc, xs, cs, true, idx);
+        else nearest<1, ERT>(C, a.kc, bsc, xs, cs, false, idx);
         const float *c0 = C + (size_t)idx[0] * bsc;
         for (int t = 0; t < bsc; t++) rs[(j * bsc + t) * ERT + threadIdx.x] = __fsub_rn(xs[t * ERT + threadIdx.x], c0[t]);
         if (live) {
@@ -125,30 +127,43 @@ __global__ void __launch_bounds__(ERT) k_encode(EncodeArgs a) {
     }
     for (int j = 0; j < a.mp; j++) {
         int idx[1];
-        nearest<1>(a.pq + (size_t)j * a.kp * bsp, a.kp, bsp, rs + (size_t)j * bsp * ERT, cs, NC != 0, idx);
+        nearest<1, ERT>(a.pq + (size_t)j * a.kp * bsp, a.kp, bsp, rs + (size_t)j * bsp * ERT, cs, NC != 0, idx);
         if (live) a.codes[(size_t)row * a.mp + j] = (uint8_t)idx[0];
     }
 }
 
-size_t encode_smem(int dim, int mcp) { return sizeof(float) * ((size_t)ECH + (size_t)(dim / mcp) * ERT + (size_t)dim * ERT); }
+size_t encode_smem(int dim, int mcp, int ert) {
+    return sizeof(float) * ((size_t)ECH + (size_t)(dim / mcp) * ert + (size_t)dim * ert);
+}
+
+constexpr size_t SMEM_MAX = 227 * 1024;
+
+template <int NC, int ERT>
+void launch_k(const EncodeArgs &a, size_t smem, cudaStream_t s) {
+    cudaFuncSetAttribute(k_encode<NC, ERT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_encode<NC, ERT><<<(unsigned)((a.n + ERT - 1) / ERT), ERT, smem, s>>>(a);
+}
+
+template <int ERT>
+void launch_nc(const EncodeArgs &a, size_t smem, cudaStream_t s) {
+    if (a.nc == 0) launch_k<0, ERT>(a, smem, s);
+    else if (a.nc == 2) launch_k<2, ERT>(a, smem, s);
+    else launch_k<3, ERT>(a, smem, s);
+}
 
 }  // namespace
 
+size_t encode_smem_bytes(int dim, int mcp) {
+    const size_t s64 = encode_smem(dim, mcp, 64);
+    return s64 <= SMEM_MAX ? s64 : encode_smem(dim, mcp, 16);
+}
+
 void launch_encode(const EncodeArgs &a, cudaStream_t s) {
     if (a.n <= 0) return;
-    int mcp = a.nc ? 1 : a.mc;
-    size_t smem = encode_smem(a.dim, mcp);
-    unsigned grid = (unsigned)((a.n + ERT - 1) / ERT);
-    if (a.nc == 0) {
-        cudaFuncSetAttribute(k_encode<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_encode<0><<<grid, ERT, smem, s>>>(a);
-    } else if (a.nc == 2) {
-        cudaFuncSetAttribute(k_encode<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_encode<2><<<grid, ERT, smem, s>>>(a);
-    } else {
-        cudaFuncSetAttribute(k_encode<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_encode<3><<<grid, ERT, smem, s>>>(a);
-    }
+    const int mcp = a.nc ? 1 : a.mc;
+    const size_t s64 = encode_smem(a.dim, mcp, 64);
+    if (s64 <= SMEM_MAX) launch_nc<64>(a, s64, s);
+    else launch_nc<16>(a, encode_smem(a.dim, mcp, 16), s);
 }
 
 }  // namespace scg

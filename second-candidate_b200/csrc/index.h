@@ -87,6 +87,10 @@ struct scg_index {
     bool raw_u8 = false;    // raw vectors held as uint8
     int tuned_upl[2] = {2, 2};  // scan candidates per lane, per scan form (exact, fast)
     bool split = true;          // selection and scan as two kernels where possible
+    // tensor-core encoder (IVF/IMI codes): norms, per-segment maxima, chunk buffers
+    int encoder = 1;            // SCG_ENC_TENSOR or SCG_ENC_EXACT
+    bool enc_ready = false;
+    scg::DevBuf enc_nc, enc_nr, enc_cmax, enc_rmax, enc_tab, enc_res, enc_status;
     scg::Workspace ws;      // the workspace of the index's own entry points
     // scg_search (host buffers) pipelines a batch in chunks over two streams
     cudaStream_t stream2 = nullptr;

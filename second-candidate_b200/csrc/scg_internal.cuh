@@ -62,6 +62,7 @@ struct TablesArgs {
     float *qsum;           // [nq]
     int lut_only;          // 1: dqr holds -2<q,r> (the fast form keeps ||r||^2 per vector)
     int *status;           // optional status word (ST_* bits)
+    int segs;              // tensor-core tables: 0 or 3 both, 1 coarse parts only, 2 PQ subspaces only
 };
 
 void launch_precompute1(int dim, int mc, int kc, int mp, int kp, const float *cq, const float *pq,
@@ -131,6 +132,29 @@ struct EncodeArgs {
     uint8_t *codes;
 };
 void launch_encode(const EncodeArgs &a, cudaStream_t s);
+// Shared memory of the exact encoder's block for this shape (must be <= 227 KB).
+size_t encode_smem_bytes(int dim, int mcp);
+// ||c||^2 of `rows` vectors of length len (the reference's float order).
+void launch_norms(const float *C, int rows, int len, float *out, cudaStream_t s);
+
+// Nearest centroid per (row, segment) from a tensor-core distance table,
+// re-checked exactly: every centroid whose table value is within the
+// table's error margin of the row's minimum is scored with the reference's
+// double arithmetic and the first exact minimum wins.
+struct PickArgs {
+    const float *X;        // [n][dim] rows (or residuals)
+    int64_t n;
+    int dim, nseg, kseg, len;  // segments per row, centroids per segment, dims per segment
+    const float *C;        // [nseg][kseg][len]
+    const float *tab;      // [n][nseg * kseg]: ||c||^2 - 2<x_seg, c>
+    const float *segmax;   // [nseg] largest ||c||^2 of the segment
+    uint16_t *cid;         // [n][nseg] (coarse) or null
+    uint8_t *code;         // [n][nseg] (PQ) or null
+    float *resid;          // [n][dim] x - c for the chosen c (coarse), or null
+    int *status;
+};
+void launch_pick(const PickArgs &a, cudaStream_t s);
+void launch_segmax(const float *norms, int nseg, int kseg, float *out, cudaStream_t s);
 
 // Sorted coarse-list prefixes of a batch, ahead of the fused search
 // (kc <= 1024; width = coarse_sort_width(kc), 0 when kc is larger).

@@ -201,6 +201,11 @@ void launch_vterm(int mode, int kc, int mp, int kp, int mc, uint64_t ncells, int
                                                           vterm);
 }
 
+void launch_norms(const float *C, int rows, int len, float *out, cudaStream_t s) {
+    if (rows <= 0) return;
+    k_norms<<<(rows + 255) / 256, 256, 0, s>>>(C, rows, len, out);
+}
+
 void launch_precompute1(int dim, int mc, int kc, int mp, int kp, const float *cq, const float *pq,
                         float *norm_c, float *norm_r, float *dot_cr, cudaStream_t s) {
     int bsc = dim / mc, bsp = dim / mp;

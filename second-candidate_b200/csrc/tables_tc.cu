@@ -167,7 +167,7 @@ __device__ __forceinline__ void stage(const float *__restrict__ src, int nrows, 
 }
 
 template <int NSPLIT, int FMT>
-__global__ void __launch_bounds__(TC_THREADS, 1) k_tables_tc(TablesArgs a, int ctiles, int ptiles) {
+__global__ void __launch_bounds__(TC_THREADS, 1) k_tables_tc(TablesArgs a, int ctiles, int ptiles, int tile0) {
     extern __shared__ __align__(1024) unsigned char tsm[];
     constexpr bool SPLIT = NSPLIT == 3;
     unsigned char *A0 = tsm + OFF_A0, *A1 = tsm + OFF_A1, *B0 = tsm + OFF_B0, *B1 = tsm + OFF_B1;
@@ -175,7 +175,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tables_tc(TablesArgs a, int c
     uint32_t *tslot = (uint32_t *)(tsm + OFF_BAR + 8);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
-    int tile = blockIdx.x;
+    int tile = blockIdx.x + tile0;
     int e0, seglen, len, qoff, outstride, outoff;
     const float *cent, *norm;
     float *out;
@@ -299,9 +299,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tables_tc(TablesArgs a, int c
 }
 
 template <int NSPLIT, int FMT>
-void launch_tc(const TablesArgs &a, dim3 grid, int ctiles, int ptiles, cudaStream_t s) {
+void launch_tc(const TablesArgs &a, dim3 grid, int ctiles, int ptiles, int tile0, cudaStream_t s) {
     cudaFuncSetAttribute(k_tables_tc<NSPLIT, FMT>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-    k_tables_tc<NSPLIT, FMT><<<grid, TC_THREADS, TC_SMEM, s>>>(a, ctiles, ptiles);
+    k_tables_tc<NSPLIT, FMT><<<grid, TC_THREADS, TC_SMEM, s>>>(a, ctiles, ptiles, tile0);
 }
 
 }  // namespace
@@ -309,13 +309,16 @@ void launch_tc(const TablesArgs &a, dim3 grid, int ctiles, int ptiles, cudaStrea
 void launch_tables_tc(const TablesArgs &a, int nsplit, int fmt, cudaStream_t s) {
     if (a.nq <= 0) return;
     const int ctiles = (a.kc + TN - 1) / TN, ptiles = (a.kp + TN - 1) / TN;
-    dim3 grid(a.mc * ctiles + a.mp * ptiles, (a.nq + TM - 1) / TM);
+    const bool coarse = a.segs != 2, pq = a.segs != 1;
+    const int tile0 = coarse ? 0 : a.mc * ctiles;
+    const int ntiles = (coarse ? a.mc * ctiles : 0) + (pq ? a.mp * ptiles : 0);
+    dim3 grid(ntiles, (a.nq + TM - 1) / TM);
     if (nsplit == 3) {
-        if (fmt == 1) launch_tc<3, 1>(a, grid, ctiles, ptiles, s);
-        else launch_tc<3, 0>(a, grid, ctiles, ptiles, s);
+        if (fmt == 1) launch_tc<3, 1>(a, grid, ctiles, ptiles, tile0, s);
+        else launch_tc<3, 0>(a, grid, ctiles, ptiles, tile0, s);
     } else {
-        if (fmt == 1) launch_tc<1, 1>(a, grid, ctiles, ptiles, s);
-        else launch_tc<1, 0>(a, grid, ctiles, ptiles, s);
+        if (fmt == 1) launch_tc<1, 1>(a, grid, ctiles, ptiles, tile0, s);
+        else launch_tc<1, 0>(a, grid, ctiles, ptiles, tile0, s);
     }
     launch_query_norms(a, s);
 }

@@ -16,6 +16,7 @@ LIB_PATH = os.environ.get("SCG_LIBRARY") or os.path.join(HERE, "libscgpu.so")
 
 IVFADC, IMI, SC2 = 0, 1, 2
 FP32_EXACT, FAST, BF16, FP16 = 0, 1, 2, 3
+ENC_EXACT, ENC_TENSOR = 0, 1
 
 PENDING = 1
 
@@ -31,7 +32,7 @@ EXPORTS = ["scg_last_error", "scg_index_create", "scg_index_destroy", "scg_load_
            "scg_search_device_noalloc", "scg_query_tables_device", "scg_load_raw_u8",
            "scg_server_create", "scg_server_submit", "scg_server_wait", "scg_server_stats",
            "scg_server_destroy", "scg_autotune", "scg_set_scan_tuning",
-           "scg_set_kernel_split", "scg_server_wait_times"]
+           "scg_set_kernel_split", "scg_server_wait_times", "scg_set_encoder"]
 
 
 class ScgError(RuntimeError):
@@ -194,6 +195,9 @@ class Index:
         _check(_lib.scg_autotune(self._h, ctypes.byref(p), ctypes.c_void_p(dQ_ptr), nq, ctypes.c_void_p(d_ids),
                                  ctypes.c_void_p(d_d), ctypes.c_void_p(d_sums), ctypes.byref(c), _ptr(ms)))
         return c.value, ms.tolist()
+
+    def set_encoder(self, method):
+        _check(_lib.scg_set_encoder(self._h, method))
 
     def set_kernel_split(self, on):
         _check(_lib.scg_set_kernel_split(self._h, 1 if on else 0))

@@ -46,3 +46,45 @@ def test_encoder_random(oracle_mod, mc, kc, nc):
     assert np.array_equal(cid, ocid)
     assert np.array_equal(codes, ocodes)
     g.close()
+
+
+def _enc_case(kind, D, mc, kc, mp, kp, n, seed):
+    rng = np.random.default_rng(seed)
+    if kind == "u8":
+        mix = W.Mixture(D, 16, 20.0, "u8", seed=seed)
+        X = mix.sample(n, seed=seed + 1)
+        cq, pq = W.train_codebooks(X[:4000], mc, kc, mp, kp, 2, seed=seed + 2)
+    elif kind == "unit01":
+        mix = W.Mixture(D, 8, 0.08, "unit01", seed=seed)
+        X = mix.sample(n, seed=seed + 1)
+        cq, pq = W.train_codebooks(X[:3000], mc, kc, mp, kp, 2, seed=seed + 2)
+    else:
+        # integer data and centroids with duplicates: exact distance ties
+        X = rng.integers(0, 4, (n, D)).astype(np.float32)
+        cq = rng.integers(0, 4, (mc * kc * (D // mc))).astype(np.float32)
+        cq.reshape(mc, kc, -1)[:, 1::2] = cq.reshape(mc, kc, -1)[:, 0::2][:, : kc // 2]
+        pq = rng.integers(-1, 2, (mp * kp * (D // mp))).astype(np.float32)
+    return X, cq, pq
+
+
+@pytest.mark.parametrize("kind,D,mc,kc,mp,kp", [("u8", 64, 2, 256, 8, 256), ("u8", 128, 1, 300, 8, 256),
+                                               ("unit01", 960, 2, 32, 32, 256), ("ties", 32, 2, 64, 4, 16)])
+def test_tensor_encoder_is_exact(oracle_mod, kind, D, mc, kc, mp, kp):
+    """The tensor-core encoder (tcgen05 distance tables + exact re-check of
+    every centroid within the tables' error margin) gives the reference's
+    codes: identical to the double-precision kernel and to the oracle,
+    including exact ties (first minimum) and D = 960."""
+    import scgpu
+    n = 6000 if D < 960 else 1500
+    X, cq, pq = _enc_case(kind, D, mc, kc, mp, kp, n, 11 + D)
+    g = scgpu.Index(0)
+    g.load_codebooks(cq, kc, mc, pq, kp, mp, D)
+    g.set_encoder(scgpu.ENC_TENSOR)
+    cid_t, codes_t = g.encode(X)
+    g.set_encoder(scgpu.ENC_EXACT)
+    cid_e, codes_e = g.encode(X)
+    g.close()
+    assert np.array_equal(cid_t, cid_e) and np.array_equal(codes_t, codes_e)
+    m = min(n, 600)
+    ocid, ocodes = O.encode((D, mc, kc, mp, kp), cq, pq, X[:m])
+    assert np.array_equal(cid_t[:m], ocid) and np.array_equal(codes_t[:m], ocodes)
