@@ -186,6 +186,17 @@ int scg_encode(scg_index *h, const float *X, int64_t n, uint16_t *cid, uint8_t *
 int scg_sc_encode(scg_index *h, const float *X, int64_t n, int nc, uint16_t *cid,
                   uint8_t *codes);
 
+/* Codebook training on device `device` (stream may be NULL): from n training
+ * rows dX[n][dim] on the device, the coarse codebook d_cq[mc][kc][dim/mc]
+ * (kc = 1: the zero centroid of plain PQ) and the residual PQ codebook
+ * d_pq[mp][kp][dim/mp], each by k-means++ seeding (seeded, deterministic)
+ * and `iters` Lloyd steps with FP64 centroid means; assignments use
+ * tensor-core distance tables.  Replaces PQQuantizer::create_sub_quantizers
+ * / calc_residual_vector (quantizer.h:235-272, 456-510) with greg_kmeans
+ * (k-means.h:671-912), whose Lloyd loop stops after one pass. */
+int scg_train_codebooks(const float *dX, int64_t n, int dim, int mc, int kc, int mp, int kp, int iters,
+                        uint64_t seed, float *d_cq, float *d_pq, int device, void *stream);
+
 /* Encoder arithmetic for IVF/IMI codes (scg_encode, scg_encode_device with
  * nc = 0).  SCG_ENC_TENSOR (the default): distances ranked by tcgen05
  * split-BF16 GEMM tiles, every centroid within the tiles' error margin of the

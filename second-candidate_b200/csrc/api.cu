@@ -912,6 +912,53 @@ static int encode_tc(scg_index *h, const float *dX, int64_t n, uint16_t *d_cid, 
     return SCG_OK;
 }
 
+int scg_train_codebooks(const float *dX, int64_t n, int dim, int mc, int kc, int mp, int kp, int iters,
+                        uint64_t seed, float *d_cq, float *d_pq, int device, void *stream) {
+    if (!dX || !d_cq || !d_pq) return fail(SCG_ERR_ARG, "null buffer");
+    if (n < 1 || dim < 1 || mc < 1 || kc < 1 || mp < 1 || kp < 1 || iters < 0)
+        return fail(SCG_ERR_ARG, "non-positive shape");
+    if (dim % mc || dim % mp) return fail(SCG_ERR_ARG, "dim must divide by mc and mp");
+    if ((kc > 1 && n < kc) || n < kp) return fail(SCG_ERR_ARG, "fewer training rows than centroids");
+    if (kc > 65535 || kp > 256) return fail(SCG_ERR_ARG, "kc must be < 65536 and kp <= 256");
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int64_t budget = 1ll << 28;  // floats of distance table per row chunk
+    auto chunk_of = [&](int nseg, int k) { return std::max<int64_t>(128, std::min<int64_t>(n, budget / ((int64_t)nseg * k))); };
+    const int64_t ch_c = chunk_of(mc, kc), ch_p = chunk_of(mp, kp);
+    const size_t wbytes = std::max(kmeans_work_bytes(n, mc, kc, dim / mc, ch_c), kmeans_work_bytes(n, mp, kp, dim / mp, ch_p));
+    DevBuf work, resid, asg, status;
+    int rc;
+    if ((rc = work.ensure(wbytes))) return rc;
+    if ((rc = resid.ensure(4ull * n * dim))) { work.release(); return rc; }
+    if ((rc = asg.ensure(4ull * n * mc))) { work.release(); resid.release(); return rc; }
+    if ((rc = status.ensure(16))) { work.release(); resid.release(); asg.release(); return rc; }
+    auto release = [&]() { work.release(); resid.release(); asg.release(); status.release(); };
+    if ((e = cudaMemsetAsync(status.p, 0, 16, s)) != cudaSuccess) { release(); return cuda_fail(e, "memset"); }
+    // coarse codebook (kc == 1: the zero centroid of plain PQ) and residuals
+    if (kc == 1) {
+        e = cudaMemsetAsync(d_cq, 0, 4ull * dim, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(resid.p, dX, 4ull * n * dim, cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess) { release(); return cuda_fail(e, "zero coarse centroid"); }
+    } else {
+        rc = kmeans_segments(dX, n, dim, mc, kc, iters, seed, d_cq, work.as<unsigned char>(), ch_c, status.as<int>(),
+                             asg.as<int>(), s);
+        if (rc) { release(); return rc; }
+        launch_residual(dX, n, dim, mc, kc, d_cq, asg.as<int>(), resid.as<float>(), s);
+    }
+    // residual PQ codebooks
+    rc = kmeans_segments(resid.as<float>(), n, dim, mp, kp, iters, seed ^ 0x5851f42d4c957f2dull, d_pq,
+                         work.as<unsigned char>(), ch_p, status.as<int>(), nullptr, s);
+    if (rc) { release(); return rc; }
+    int st = 0;
+    e = cudaMemcpyAsync(&st, status.p, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    release();
+    if (e != cudaSuccess) return cuda_fail(e, "scg_train_codebooks");
+    if (st) return status_result(st);
+    return SCG_OK;
+}
+
 int scg_set_encoder(scg_index *h, int method) {
     if (!h) return fail(SCG_ERR_ARG, "null index");
     if (method != SCG_ENC_EXACT && method != SCG_ENC_TENSOR) return fail(SCG_ERR_ARG, "unknown encoder");

@@ -172,6 +172,13 @@ struct CoarseArgs {
 int coarse_sort_width(int kc);
 void launch_coarse_prefix(const CoarseArgs &a, cudaStream_t s);
 
+// Codebook training (train.cu).
+size_t kmeans_work_bytes(int64_t n, int nseg, int k, int len, int64_t chunk);
+int kmeans_segments(const float *X, int64_t n, int dim, int nseg, int k, int iters, uint64_t seed, float *C,
+                    unsigned char *work, int64_t chunk, int *status, int *asg_out, cudaStream_t s);
+void launch_residual(const float *X, int64_t n, int dim, int nseg, int k, const float *C, const int *asg, float *R,
+                     cudaStream_t s);
+
 size_t rerank_smem_bytes(int L, int dim);
 int launch_rerank(const float *Q, int nq, int dim, const void *raw, int raw_u8, int64_t N, const int *sl_ids, int L,
                   int R, int *out_ids, float *out_d, int *status, cudaStream_t s);

@@ -32,7 +32,16 @@ EXPORTS = ["scg_last_error", "scg_index_create", "scg_index_destroy", "scg_load_
            "scg_search_device_noalloc", "scg_query_tables_device", "scg_load_raw_u8",
            "scg_server_create", "scg_server_submit", "scg_server_wait", "scg_server_stats",
            "scg_server_destroy", "scg_autotune", "scg_set_scan_tuning",
-           "scg_set_kernel_split", "scg_server_wait_times", "scg_set_encoder"]
+           "scg_set_kernel_split", "scg_server_wait_times", "scg_set_encoder",
+           "scg_train_codebooks"]
+
+
+def train_codebooks_device(dX_ptr, n, dim, mc, kc, mp, kp, iters, seed, d_cq, d_pq, device=0, stream=None):
+    """k-means++ + Lloyd codebooks on the device (scg_train_codebooks)."""
+    lib = load()
+    _check(lib.scg_train_codebooks(ctypes.c_void_p(dX_ptr), ctypes.c_int64(n), dim, mc, kc, mp, kp, iters,
+                                   ctypes.c_uint64(seed), ctypes.c_void_p(d_cq), ctypes.c_void_p(d_pq), device,
+                                   ctypes.c_void_p(stream) if stream else None))
 
 
 class ScgError(RuntimeError):
