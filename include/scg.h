@@ -186,6 +186,19 @@ int scg_encode(scg_index *h, const float *X, int64_t n, uint16_t *cid, uint8_t *
 int scg_sc_encode(scg_index *h, const float *X, int64_t n, int nc, uint16_t *cid,
                   uint8_t *codes);
 
+/* Index build on the device: encodes dX[n][dim] (device rows, ids 0..n-1;
+ * nc = 0 IVF/IMI codes with kc^mc cells, nc = 2 second-candidate codes with
+ * kc^2 cells), orders the rows by cell and by id inside a cell, and loads the
+ * resulting CSR into the index -- the arrays Encoder::distribution /
+ * SCEncoder::distribution write and load_encoded_data reads back
+ * (encoder.cpp:170-305, sc_encoder.cpp:17-182, query.cpp:82-165). */
+int scg_build_index(scg_index *h, const float *dX, int64_t n, int nc, void *stream);
+
+/* Writes the index's CSR as an .edat_ file (int32 non-empty cells, int32 N,
+ * then per cell in id order: int32 L, int32 pid[L], uint8 codes[L][mp]), the
+ * format of Encoder::output (encoder.cpp:230-305), with 64-bit file offsets. */
+int scg_write_edat(scg_index *h, const char *path);
+
 /* Codebook training on device `device` (stream may be NULL): from n training
  * rows dX[n][dim] on the device, the coarse codebook d_cq[mc][kc][dim/mc]
  * (kc = 1: the zero centroid of plain PQ) and the residual PQ codebook

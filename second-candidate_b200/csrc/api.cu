@@ -912,6 +912,96 @@ static int encode_tc(scg_index *h, const float *dX, int64_t n, uint16_t *d_cid, 
     return SCG_OK;
 }
 
+int scg_build_index(scg_index *h, const float *dX, int64_t n, int nc, void *stream) {
+    if (!h) return fail(SCG_ERR_ARG, "null index");
+    if (!h->have_codebooks) return fail(SCG_ERR_STATE, "load codebooks first");
+    if (n < 0 || n > 0xfffffffeLL) return fail(SCG_ERR_ARG, "n out of range");
+    if (n > 0 && !dX) return fail(SCG_ERR_ARG, "null buffer");
+    if (nc != 0 && nc != 2) return fail(SCG_ERR_ARG, "nc must be 0 (IVF/IMI) or 2 (second candidate)");
+    if (nc && h->mc != 1) return fail(SCG_ERR_ARG, "the second-candidate index needs mc = 1");
+    const int parts = nc ? nc : h->mc;
+    const int64_t ncells = ipow(h->kc, parts);
+    if (ncells >= (1ll << 32)) return fail(SCG_ERR_ARG, "too many cells");
+    int rc;
+    DevBuf cid, codes, work;
+    if ((rc = cid.ensure(2ull * (n ? n : 1) * parts))) return rc;
+    if ((rc = codes.ensure((size_t)(n ? n : 1) * h->mp))) { cid.release(); return rc; }
+    auto release = [&]() { cid.release(); codes.release(); work.release(); };
+    if (n > 0 && (rc = scg_encode_device(h, dX, n, nc, cid.as<uint16_t>(), codes.as<uint8_t>(), stream))) {
+        release();
+        return rc;
+    }
+    std::lock_guard<std::mutex> g(h->mu);
+    if ((rc = set_device(h))) { release(); return rc; }
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
+    if ((rc = work.ensure(build_work_bytes(n, ncells))) ||
+        (rc = h->off.ensure(4ull * (ncells + 1))) || (rc = h->pid.ensure(4ull * (n ? n : 1))) ||
+        (rc = h->codes.ensure((size_t)(n ? n : 1) * h->mp))) {
+        release();
+        return rc;
+    }
+    if (n > 0) {
+        launch_build_csr(cid.as<uint16_t>(), codes.as<uint8_t>(), n, parts, h->kc, h->mp, ncells,
+                         work.as<unsigned char>(), h->off.as<uint32_t>(), h->pid.as<int>(), h->codes.as<uint8_t>(), s);
+    } else {
+        SCG_CUDA(cudaMemsetAsync(h->off.p, 0, 4ull * (ncells + 1), s));
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    release();
+    if (e != cudaSuccess) return cuda_fail(e, "scg_build_index");
+    h->N = n;
+    h->ncells = ncells;
+    h->have_csr = true;
+    h->have_vterm = false;
+    return SCG_OK;
+}
+
+int scg_write_edat(scg_index *h, const char *path) {
+    if (!h || !path) return fail(SCG_ERR_ARG, "null argument");
+    if (!h->have_csr) return fail(SCG_ERR_STATE, "encoded data not loaded");
+    std::lock_guard<std::mutex> g(h->mu);
+    int rc;
+    if ((rc = set_device(h))) return rc;
+    const int64_t nc = h->ncells, N = h->N;
+    std::vector<uint32_t> off((size_t)nc + 1);
+    std::vector<int> pid((size_t)(N ? N : 1));
+    std::vector<uint8_t> codes((size_t)(N ? N : 1) * h->mp);
+    SCG_CUDA(cudaMemcpy(off.data(), h->off.p, 4ull * (nc + 1), cudaMemcpyDeviceToHost));
+    if (N) {
+        SCG_CUDA(cudaMemcpy(pid.data(), h->pid.p, 4ull * N, cudaMemcpyDeviceToHost));
+        SCG_CUDA(cudaMemcpy(codes.data(), h->codes.p, (size_t)N * h->mp, cudaMemcpyDeviceToHost));
+    }
+    std::ofstream f(path, std::ios::binary | std::ios::trunc);
+    if (!f) return fail(SCG_ERR_IO, std::string("cannot write ") + path);
+    int non_empty = 0;
+    for (int64_t c = 0; c < nc; c++) non_empty += off[(size_t)c + 1] > off[(size_t)c];
+    const int hdr[2] = {non_empty, (int)N};
+    std::vector<char> buf;
+    buf.reserve(64 << 20);
+    auto put = [&](const void *p, size_t bytes) {
+        const char *q = (const char *)p;
+        buf.insert(buf.end(), q, q + bytes);
+        if (buf.size() >= (64u << 20)) {
+            f.write(buf.data(), (std::streamsize)buf.size());
+            buf.clear();
+        }
+    };
+    put(hdr, sizeof(hdr));
+    for (int64_t c = 0; c < nc; c++) {
+        const uint32_t a = off[(size_t)c], b = off[(size_t)c + 1];
+        const int l = (int)(b - a);
+        put(&l, 4);
+        if (l) {
+            put(pid.data() + a, 4ull * l);
+            put(codes.data() + (size_t)a * h->mp, (size_t)l * h->mp);
+        }
+    }
+    f.write(buf.data(), (std::streamsize)buf.size());
+    if (!f) return fail(SCG_ERR_IO, std::string("short write to ") + path);
+    return SCG_OK;
+}
+
 int scg_train_codebooks(const float *dX, int64_t n, int dim, int mc, int kc, int mp, int kp, int iters,
                         uint64_t seed, float *d_cq, float *d_pq, int device, void *stream) {
     if (!dX || !d_cq || !d_pq) return fail(SCG_ERR_ARG, "null buffer");

@@ -172,6 +172,11 @@ struct CoarseArgs {
 int coarse_sort_width(int kc);
 void launch_coarse_prefix(const CoarseArgs &a, cudaStream_t s);
 
+// Index build (build_index.cu): rows ordered by cell, CSR offsets.
+size_t build_work_bytes(int64_t n, int64_t ncells);
+void launch_build_csr(const uint16_t *cid, const uint8_t *codes, int64_t n, int parts, int kc, int mp,
+                      int64_t ncells, unsigned char *work, uint32_t *off, int *pid, uint8_t *codes_out, cudaStream_t s);
+
 // Codebook training (train.cu).
 size_t kmeans_work_bytes(int64_t n, int nseg, int k, int len, int64_t chunk);
 int kmeans_segments(const float *X, int64_t n, int dim, int nseg, int k, int iters, uint64_t seed, float *C,

@@ -33,7 +33,7 @@ EXPORTS = ["scg_last_error", "scg_index_create", "scg_index_destroy", "scg_load_
            "scg_server_create", "scg_server_submit", "scg_server_wait", "scg_server_stats",
            "scg_server_destroy", "scg_autotune", "scg_set_scan_tuning",
            "scg_set_kernel_split", "scg_server_wait_times", "scg_set_encoder",
-           "scg_train_codebooks"]
+           "scg_train_codebooks", "scg_build_index", "scg_write_edat"]
 
 
 def train_codebooks_device(dX_ptr, n, dim, mc, kc, mp, kp, iters, seed, d_cq, d_pq, device=0, stream=None):
@@ -204,6 +204,15 @@ class Index:
         _check(_lib.scg_autotune(self._h, ctypes.byref(p), ctypes.c_void_p(dQ_ptr), nq, ctypes.c_void_p(d_ids),
                                  ctypes.c_void_p(d_d), ctypes.c_void_p(d_sums), ctypes.byref(c), _ptr(ms)))
         return c.value, ms.tolist()
+
+    def build_index_device(self, dX_ptr, n, nc=0, stream=None):
+        """Encodes device rows and loads the CSR built on the device."""
+        _check(_lib.scg_build_index(self._h, ctypes.c_void_p(dX_ptr), ctypes.c_int64(n), nc,
+                                    ctypes.c_void_p(stream) if stream else None))
+        self.N = n
+
+    def write_edat(self, path):
+        _check(_lib.scg_write_edat(self._h, str(path).encode()))
 
     def set_encoder(self, method):
         _check(_lib.scg_set_encoder(self._h, method))
