@@ -340,3 +340,61 @@ def test_pool_overflow_reruns_fused(scg, oracle_mod):
     srv.close()
     assert np.array_equal(ids, ref[0]) and np.array_equal(d, ref[1]) and np.array_equal(sums, ref[2])
     g.close()
+
+
+def test_large_kc_and_m16(scg, oracle_mod):
+    """kc = 4096 per half with M = 16 (the 100M serving workload's shape,
+    scaled down): coarse lists too long for the warp pre-sort are ranked
+    inside the selection kernel; exact form against the oracle."""
+    D, mc, kc, mp, kp = 32, 2, 4096, 16, 64
+    rng = np.random.default_rng(91)
+    X = rng.normal(0, 1, (120000, D)).astype(np.float32)
+    X /= np.linalg.norm(X, axis=1, keepdims=True)
+    Q = rng.normal(0, 1, (16, D)).astype(np.float32)
+    Q /= np.linalg.norm(Q, axis=1, keepdims=True)
+    g = scg.Index(0)
+    # coarse centroids: the halves of sampled rows, [2][kc][16]
+    rows = X[rng.choice(X.shape[0], kc, replace=False)]
+    cq = np.concatenate([rows[:, :16], rows[:, 16:]]).astype(np.float32)
+    pq = rng.normal(0, 0.1, (mp * kp * (D // mp))).astype(np.float32)
+    g.load_codebooks(cq, kc, mc, pq, kp, mp, D)
+    cid, codes = g.encode(X)
+    L, pid, co, _ = O.distribution(O.IMI, kc, mc, 0, cid, codes)
+    g.load_csr(L, pid, co)
+    g.precompute()
+    ix = O.Index(D, mc, kc, mp, kp, cq, pq, L, pid, co)
+    # 120k rows in 16.7M cells: about 140 cells per candidate at first
+    g.set_cell_budget(1 << 19)
+    for T in (50, 300):
+        check_against_oracle(ix, g, O.IMI, Q, 20, 1 << 24, T)
+    g.close()
+
+
+def test_d960_m32_fp16_rerank(scg, oracle_mod):
+    """D = 960, M = 32 (the high-dimensional workload's shape): the exact form
+    against the oracle, and FP16 tables with an exact re-rank of a 200-long
+    shortlist against the oracle's re-rank of its own shortlist."""
+    D, mc, kc, mp, kp = 960, 2, 32, 32, 256
+    mix = W.Mixture(D, 8, 0.08, "unit01", seed=92)
+    X = mix.sample(20000, seed=93)
+    Q = mix.sample(12, seed=94)
+    cq, pq = W.train_codebooks(X[:3000], mc, kc, mp, kp, 2, seed=95)
+    g = gpu_index(scg, D, mc, kc, mp, kp, cq, pq, *O.distribution(O.IMI, kc, mc, 0,
+                                                                   *O.encode((D, mc, kc, mp, kp), cq, pq, X))[:3])
+    L, pid, co, _ = O.distribution(O.IMI, kc, mc, 0, *O.encode((D, mc, kc, mp, kp), cq, pq, X))
+    ix = O.Index(D, mc, kc, mp, kp, cq, pq, L, pid, co, raw=X)
+    check_against_oracle(ix, g, O.IMI, Q, 50, 1 << 20, 2000)
+    g.load_raw(X)
+    ids, d, sums = g.search(1, Q, 50, 1 << 20, 2000, precision=scg.FP16, rerank=200)
+    si, _, _ = ix.search(O.IMI, Q, 200, 1 << 20, 2000)
+    ri, rd = ix.rerank(Q, si, 50)
+    # FP16 tables may reorder the shortlist's tail; the exact re-rank of it
+    # gives the oracle's distances for the ids both keep
+    for i in range(Q.shape[0]):
+        common = set(ids[i].tolist()) & set(ri[i].tolist())
+        assert len(common) >= 45
+        dd = dict(zip(ri[i].tolist(), rd[i].tolist()))
+        for j, x in enumerate(ids[i].tolist()):
+            if x in dd:
+                assert d[i, j] == np.float32(dd[x])
+    g.close()
