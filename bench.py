@@ -163,7 +163,7 @@ def cpu_reference(w, seconds_target=12.0, threads=None, mode=None):
             "seconds": sec, "recall@100": recall_at(ids, w["gt"][:n], min(100, R))}
 
 
-def serve_leg(scgpu, ix, w, mode, wcap, T, prec, seconds, load, seed=7):
+def serve_leg(scgpu, ix, w, mode, wcap, T, prec, seconds, load, seed=7, rerank=0):
     """A request stream through the server (scg_server_*): each request a
     batch of 1..4096 queries (log-uniform) drawn from the workload's queries,
     k in {1, 10, 100}.  First the server's capacity for this mix (requests
@@ -180,8 +180,12 @@ def serve_leg(scgpu, ix, w, mode, wcap, T, prec, seconds, load, seed=7):
         starts = rng.integers(0, max(1, Q.shape[0] - 4096), n)
         return sizes, ks, starts
 
-    srv = scgpu.Server(ix, slots=4, max_batch=4096, max_R=100, arena_bytes=4 << 30)
-    for t in [srv.submit(mode, Q[:64], 10, wcap, T, precision=prec) for _ in range(8)]:
+    srv = scgpu.Server(ix, slots=4, max_batch=4096, max_R=100, arena_bytes=8 << 30)
+
+    def submit(q, k):
+        return srv.submit(mode, q, k, wcap, T, precision=prec, rerank=max(rerank, k) if rerank else 0)
+
+    for t in [submit(Q[:64], 10) for _ in range(8)]:
         srv.wait(t)
     # capacity (closed loop, 16 outstanding)
     n_cap = 600
@@ -191,7 +195,7 @@ def serve_leg(scgpu, ix, w, mode, wcap, T, prec, seconds, load, seed=7):
     for i in range(n_cap):
         if len(pending) >= 16:
             srv.wait(pending.pop(0))
-        pending.append(srv.submit(mode, Q[starts[i]:starts[i] + sizes[i]], int(ks[i]), wcap, T, precision=prec))
+        pending.append(submit(Q[starts[i]:starts[i] + sizes[i]], int(ks[i])))
     for t in pending:
         srv.wait(t)
     capacity = float(sizes.sum() / (time.perf_counter() - t0))
@@ -222,7 +226,7 @@ def serve_leg(scgpu, ix, w, mode, wcap, T, prec, seconds, load, seed=7):
         if d > 0:
             time.sleep(d)
         s0 = int(starts[i])
-        tickets.append(srv.submit(mode, Q[s0:s0 + int(sizes[i])], int(ks[i]), wcap, T, precision=prec))
+        tickets.append(submit(Q[s0:s0 + int(sizes[i])], int(ks[i])))
     th.join()
     span = time.perf_counter() - t0
     st = srv.stats()
@@ -249,11 +253,8 @@ def encode_leg(scgpu, ix, cfg, rows, dev):
     buffers): the tensor-core encoder (tcgen05 distance tables + exact
     re-check) against the all-double kernel; both must give the same codes."""
     import torch
-    g = torch.Generator(device=dev).manual_seed(99)
-    D = cfg["D"]
-    means = torch.rand(cfg["comps"], D, generator=g, device=dev) * 128.0
-    comp = torch.randint(0, cfg["comps"], (rows,), generator=g, device=dev)
-    X = (means[comp] + cfg["sigma"] * torch.randn(rows, D, generator=g, device=dev)).round_().clamp_(0, 255)
+    import workloads as W
+    X = W.mixture_sampler(cfg, 99, dev)(rows)
     mcp = 1 if cfg["mode"] == "sc" else cfg["mc"]
     out = {}
     codes = {}
@@ -299,7 +300,8 @@ def main():
     ap.add_argument("--workload", default="C2")
     ap.add_argument("--cache", default="/tmp/scg_bench_cache")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--precision", default="fast", choices=list(PRECISIONS))
+    ap.add_argument("--precision", default=None, choices=list(PRECISIONS),
+                    help="arithmetic of the tables (default: the workload's; fast for the IMI 10M one)")
     ap.add_argument("--queries", type=int, default=0, help="use only the first N queries")
     ap.add_argument("--no-plain", action="store_true", help="skip the FP32 plain comparison")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
@@ -369,11 +371,23 @@ def main():
         w["Q"] = w["Q"][: args.queries]
         w["gt"] = w["gt"][: args.queries]
     nq = w["Q"].shape[0]
+    if args.precision is None:
+        args.precision = cfg.get("precision", "fast")
+    rerank = int(cfg.get("shortlist", 0))
+    # per-query candidate targets (log-uniform over the config's range, seeded)
+    Ts = None
+    if not isinstance(cfg["T"], int):
+        lo, hi = cfg["T"]
+        Ts = np.exp(np.random.default_rng(17).uniform(np.log(lo), np.log(hi), nq)).astype(np.int32)
+        T = int(Ts.max())
 
     ix = scgpu.Index(local)
     ix.load_codebooks(w["cq"], cfg["kc"], mcp, w["pq"], cfg["kp"], cfg["mp"], cfg["D"])
     ix.load_csr(w["L"], w["pid"], w["codes"])
     ix.precompute()
+    if rerank:
+        ix.load_raw(w["raw"])
+        ix.set_cell_budget(1 << 19)  # long per-query lists of the large targets
 
     dQ = torch.from_numpy(w["Q"]).to(dev)
     d_ids = torch.empty(nq * R, dtype=torch.int32, device=dev)
@@ -389,12 +403,18 @@ def main():
     tuning = {}
     for name, pv in ((("fast", prec), ("fp32", 0)) if not args.no_autotune else ()):
         choice, ms = ix.autotune(mode, dQ.data_ptr(), nq, R, wcap, T, d_ids.data_ptr(), d_d.data_ptr(),
-                                 d_s.data_ptr(), precision=pv)
+                                 d_s.data_ptr(), precision=pv, rerank=rerank)
         tuning[name] = {"candidates_per_lane": choice, "ms_by_choice": dict(zip((2, 4, 8), ms))}
+
+    d_T = None
+    if Ts is not None:
+        d_T = torch.from_numpy(Ts).to(dev)
+        ix.set_query_targets(d_T.data_ptr())
 
     def step(p=None):
         ix.search_device(mode, dQ.data_ptr(), nq, R, wcap, T, d_ids.data_ptr(), d_d.data_ptr(),
-                         d_s.data_ptr(), stream=stream.cuda_stream, precision=prec if p is None else p)
+                         d_s.data_ptr(), stream=stream.cuda_stream, precision=prec if p is None else p,
+                         rerank=rerank)
 
     # every other arithmetic form on the same queries, for the comparison
     # (QPS at recall@100): a few timed steps each
@@ -499,11 +519,27 @@ def main():
                 torch.empty((nq, R), dtype=torch.float32).pin_memory().numpy(),
                 torch.empty(nq, dtype=torch.int32).pin_memory().numpy())
         e2e_times = []
+        if Ts is not None:
+            # per-query targets ride on the device entry point: pinned
+            # queries in, search, pinned results out, on one stream
+            hq = torch.from_numpy(w["Q"]).pin_memory()
+            hi = torch.empty(nq * R, dtype=torch.int32).pin_memory()
+            hdd = torch.empty(nq * R, dtype=torch.float32).pin_memory()
+            hs = torch.empty(nq, dtype=torch.int32).pin_memory()
         for i in range(args.warmup + args.steps):
             flush.zero_()  # same cold-L2 start as the device-timed steps
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            hid, hd, hs = ix.search(mode, Qh, R, wcap, T, precision=prec, out=outs)
+            if Ts is None:
+                hid, hd, hs_ = ix.search(mode, Qh, R, wcap, T, precision=prec, out=outs, rerank=rerank)
+            else:
+                dQ.copy_(hq, non_blocking=True)
+                step()
+                hi.copy_(d_ids, non_blocking=True)
+                hdd.copy_(d_d, non_blocking=True)
+                hs.copy_(d_s, non_blocking=True)
+                torch.cuda.current_stream().synchronize()
+                hid = hi.numpy().reshape(nq, R)
             dt = time.perf_counter() - t0
             if i >= args.warmup:
                 e2e_times.append(dt)
@@ -521,6 +557,9 @@ def main():
                    "l2": "flushed between steps (256 MB write)", "parallelism": "replicas" if world > 1 else "1 GPU",
                    "timing": "CUDA events per step on the launching stream"},
         "recall@100": recall,
+        "rerank_shortlist": rerank or None,
+        "per_query_T": None if Ts is None else {"min": int(Ts.min()), "median": int(np.median(Ts)),
+                                                "max": int(Ts.max())},
         "fp32_plain": forms.get("fp32"),
         "other_forms": {k: v for k, v in forms.items() if k != "fp32"},
         "phases": phases,
@@ -546,11 +585,16 @@ def main():
     if args.encode_rows > 0:
         line["encode"] = encode_leg(scgpu, ix, cfg, args.encode_rows, dev)
     if args.serve_seconds > 0:
-        line["serving"] = serve_leg(scgpu, ix, w, mode, wcap, T, prec, args.serve_seconds, args.serve_load)
+        line["serving"] = serve_leg(scgpu, ix, w, mode, wcap, T if Ts is None else int(np.median(Ts)), prec,
+                                    args.serve_seconds, args.serve_load, rerank=rerank)
         line["latency_ms"] = {"p50": line["serving"]["p50_ms"], "p99": line["serving"]["p99_ms"],
                               "what": "per request of the serving leg"}
+    if d_T is not None:
+        ix.set_query_targets(None)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
+            if Ts is not None:
+                raise RuntimeError("per-query candidate targets are not in the reference's CPU harness")
             line["cpu_baseline"] = cpu_reference(w)
         except Exception as ex:  # reported, never silently dropped
             line["cpu_baseline"] = {"unavailable": repr(ex)}

@@ -29,13 +29,13 @@ CONFIGS = {
                train=100_000, iters=25),
     "C3": dict(name="sc-10m-d128", N=10_000_000, D=128, mode="sc", mc=1, kc=1024,
                mp=8, kp=256, nq=10_000, T=(5_000, 200_000), w=1 << 20, R=100, comps=64,
-               sigma=20.0, train=100_000, iters=25, shortlist=1000),
+               sigma=20.0, train=100_000, iters=25, shortlist=1000, precision="bf16"),
     "C4": dict(name="imi-1m-d960", N=1_000_000, D=960, mode="imi", mc=2, kc=256,
                mp=32, kp=256, nq=1000, T=30_000, w=1 << 16, R=100, comps=32, sigma=0.08,
-               train=50_000, iters=25),
+               train=50_000, iters=25, shortlist=1000, precision="fp16"),
     "C5": dict(name="imi-100m-d96", N=100_000_000, D=96, mode="imi", mc=2, kc=4096,
                mp=16, kp=256, nq=4096, T=30_000, w=1 << 24, R=100, comps=256, sigma=0.05,
-               train=200_000, iters=15),
+               train=200_000, iters=15, precision="bf16"),
 }
 
 
@@ -197,38 +197,16 @@ def _torch_nearest(X, C):
     return out
 
 
-def build_gpu_workload(name, seed=1234, cache_dir=None, log=print):
-    """Generates config `name` on cuda:0 and returns a dict of host arrays:
-    cq, pq (codebooks), L, pid, codes (CSR index in cell order), Q (queries),
-    gt (exact nearest neighbour of each query) and the shape facts.  The
-    index is encoded by the library's exact encoder (bit-identical to the
-    reference's Encoder/SCEncoder) and bucketed by cell id in row order (as
-    Encoder::distribution does).  With cache_dir the result is kept as .npz
-    and reused."""
-    import hashlib
-    import os
-    import time
-
+def mixture_sampler(cfg, seed, dev):
+    """The workload's generator on the device: `sample(n)` draws n rows
+    (torch tensor) from the config's mixture -- "u8" rounded and clipped to
+    [0,255] (means ~ U[0,128]), "unit01" clipped to [0,1] (means ~
+    U[0.2,0.8]), or unit-normalised; successive calls continue one seeded
+    stream."""
     import torch
-
-    cfg = dict(CONFIGS[name])
-    key = hashlib.sha1(repr((name, seed, sorted(cfg.items()), 3)).encode()).hexdigest()[:16]
-    path = os.path.join(cache_dir, "%s_%s.npz" % (cfg["name"], key)) if cache_dir else None
-    if path and os.path.exists(path):
-        z = np.load(path)
-        out = {k: z[k] for k in z.files}
-        out.update(cfg=cfg)
-        log("workload %s loaded from cache" % cfg["name"])
-        return out
-
-    import scgpu
-    t0 = time.time()
-    dev = torch.device("cuda:0")
-    torch.backends.cuda.matmul.allow_tf32 = False
-    N, D, mc, kc, mp, kp = cfg["N"], cfg["D"], cfg["mc"], cfg["kc"], cfg["mp"], cfg["kp"]
-    sc = cfg["mode"] == "sc"
+    D = cfg["D"]
     g = torch.Generator(device=dev).manual_seed(seed)
-    kind = "u8" if cfg["sigma"] >= 1 else ("unit01" if name == "C4" else "sphere")
+    kind = "u8" if cfg["sigma"] >= 1 else ("unit01" if cfg["name"].startswith("imi-1m") else "sphere")
     if kind == "u8":
         means = torch.rand(cfg["comps"], D, generator=g, device=dev) * 128.0
     elif kind == "unit01":
@@ -248,6 +226,41 @@ def build_gpu_workload(name, seed=1234, cache_dir=None, log=print):
             x /= x.norm(dim=1, keepdim=True).clamp_min(1e-12)
         return x.contiguous()
 
+    sample.kind = kind
+    return sample
+
+
+def build_gpu_workload(name, seed=1234, cache_dir=None, log=print):
+    """Generates config `name` on cuda:0 and returns a dict of host arrays:
+    cq, pq (codebooks), L, pid, codes (CSR index in cell order), Q (queries),
+    gt (exact nearest neighbour of each query), raw (the base rows, for
+    configs with a re-rank shortlist) and the shape facts.  The index is
+    encoded by the library's encoder (the reference's Encoder/SCEncoder codes)
+    and bucketed by cell id in row order (as Encoder::distribution does).
+    With cache_dir the result is kept as .npz and reused."""
+    import hashlib
+    import os
+    import time
+
+    import torch
+
+    cfg = dict(CONFIGS[name])
+    key = hashlib.sha1(repr((name, seed, sorted(cfg.items()), 4)).encode()).hexdigest()[:16]
+    path = os.path.join(cache_dir, "%s_%s.npz" % (cfg["name"], key)) if cache_dir else None
+    if path and os.path.exists(path):
+        z = np.load(path)
+        out = {k: z[k] for k in z.files}
+        out.update(cfg=cfg)
+        log("workload %s loaded from cache" % cfg["name"])
+        return out
+
+    import scgpu
+    t0 = time.time()
+    dev = torch.device("cuda:0")
+    torch.backends.cuda.matmul.allow_tf32 = False
+    N, D, mc, kc, mp, kp = cfg["N"], cfg["D"], cfg["mc"], cfg["kc"], cfg["mp"], cfg["kp"]
+    sc = cfg["mode"] == "sc"
+    sample = mixture_sampler(cfg, seed, dev)
     X = sample(N)
     Q = sample(cfg["nq"])
     log("generated %d x %d in %.1fs" % (N, D, time.time() - t0))
@@ -296,6 +309,9 @@ def build_gpu_workload(name, seed=1234, cache_dir=None, log=print):
     log("index + ground truth in %.1fs" % (time.time() - t0))
     out = dict(cq=cq_h, pq=pq_h, L=L.cpu().numpy(), pid=perm.to(torch.int32).cpu().numpy(),
                codes=codes_sorted.cpu().numpy(), Q=Q.cpu().numpy(), gt=gt.cpu().numpy())
+    if cfg.get("shortlist"):
+        # raw vectors for the exact re-rank (uint8 when the data are bytes)
+        out["raw"] = (X.to(torch.uint8) if sample.kind == "u8" else X).cpu().numpy()
     del X, codes, cid, cell, perm, codes_sorted
     torch.cuda.empty_cache()
     if path:
