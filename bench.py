@@ -500,6 +500,27 @@ def main():
         except Exception:
             traffic = None
 
+    # the same step replayed from a CUDA graph (captured once by the library)
+    graph = None
+    if Ts is None:
+        gstream = torch.cuda.Stream(dev)
+        gt_ = []
+        for i in range(args.warmup + args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            g0 = torch.cuda.Event(enable_timing=True)
+            g1 = torch.cuda.Event(enable_timing=True)
+            g0.record(gstream)
+            ix.search_graph(mode, dQ.data_ptr(), nq, R, wcap, T, d_ids.data_ptr(), d_d.data_ptr(), d_s.data_ptr(),
+                            gstream.cuda_stream, precision=prec, rerank=rerank)
+            g1.record(gstream)
+            g1.synchronize()
+            if i >= args.warmup:
+                gt_.append(g0.elapsed_time(g1))
+        graph = {"value": nq / (statistics.mean(gt_) / 1e3) * world, "unit": "queries/s",
+                 "ms_per_step": statistics.mean(gt_),
+                 "what": "scg_search_graph: the step's launch sequence captured once, replayed as one graph launch"}
+
     phases = None
     if args.phases:
         ix.set_phase_counters(True)
@@ -579,6 +600,7 @@ def main():
         # selection, scan (the fused kernel replaces the last two)
         "gpu_launches": (5 if split else 4) * args.steps,
         "autotune": tuning,
+        "graph": graph,
         "clocks": ck,
         "candidates_per_query": float(sums.mean()), "cells_per_query": float(nvis.mean() + empty.mean()),
     }

@@ -122,6 +122,18 @@ int scg_search(scg_index *h, const scg_search_params *p, const float *Q, int nq,
 int scg_search_device(scg_index *h, const scg_search_params *p, const float *dQ, int nq,
                       int *d_ids, float *d_dists, int *d_sums, void *stream);
 
+/* scg_search_device replayed from a CUDA graph: the first call with a given
+ * set of arguments (parameters, buffers, batch size, stream, per-query
+ * targets) runs the search once, captures its launch sequence (tables,
+ * coarse prefixes, selection, scan, re-rank, status copy) on `stream` (which
+ * must be the caller's, not NULL) and instantiates it; later calls with the
+ * same arguments launch the graph (one launch instead of about eight).  The
+ * buffers' contents may change between calls, their addresses may not.
+ * Synchronises to read the status word, like scg_search_device.  No
+ * counterpart in the reference. */
+int scg_search_graph(scg_index *h, const scg_search_params *p, const float *dQ, int nq,
+                     int *d_ids, float *d_dists, int *d_sums, void *stream);
+
 /* scg_search_device without any device allocation, for callers that cannot
  * allocate at search time (a memory pool that forbids cudaMalloc, or an
  * allocator owned by someone else).  No counterpart in the reference.  All

@@ -502,6 +502,7 @@ int scg_index_destroy(scg_index *h) {
                      &h->enc_status};
     for (DevBuf *b : all) b->release();
     if (h->stream2) cudaStreamSynchronize(h->stream2);
+    if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
     h->ws.release();
     h->ws2.release();
     if (h->h_chunk_status) cudaFreeHost(h->h_chunk_status);
@@ -753,6 +754,57 @@ int scg_search(scg_index *h, const scg_search_params *p, const float *Q, int nq,
         }
     }
     return SCG_OK;
+}
+
+int scg_search_graph(scg_index *h, const scg_search_params *p, const float *dQ, int nq, int *d_ids, float *d_dists,
+                     int *d_sums, void *stream) {
+    int rc;
+    if ((rc = check_ready(h))) return rc;
+    if ((rc = check_params(h, p, nq))) return rc;
+    if (nq < 1 || !dQ || !d_ids || !d_dists || !d_sums) return fail(SCG_ERR_ARG, "null buffer or empty batch");
+    if (!stream) return fail(SCG_ERR_ARG, "scg_search_graph needs a stream of the caller's");
+    std::lock_guard<std::mutex> g(h->mu);
+    if ((rc = set_device(h))) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    // everything the captured sequence reads or writes, as one key
+    char key[512];
+    snprintf(key, sizeof(key), "%d %d %d %d %d %d|%p %d %p %p %p|%p %d %d %d %d %lld %d", p->mode, p->R, p->w, p->T,
+             p->precision, p->rerank, (const void *)dQ, nq, (void *)d_ids, (void *)d_dists, (void *)d_sums,
+             (const void *)h->d_Tq, (int)h->split, h->tuned_upl[0], h->tuned_upl[1], h->cap_rec, (long long)h->N,
+             h->device);
+    if (!h->graph_exec || h->graph_key != key || h->graph_stream != s) {
+        if (h->graph_exec) {
+            cudaGraphExecDestroy(h->graph_exec);
+            h->graph_exec = nullptr;
+        }
+        // one ordinary run sizes every buffer and builds the per-vector term,
+        // so that nothing allocates or synchronises inside the capture
+        if ((rc = run_search(h, &h->ws, nullptr, p, dQ, nq, d_ids, d_dists, d_sums, s, true))) return rc;
+        cudaGraph_t graph = nullptr;
+        SCG_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+        rc = run_search(h, &h->ws, nullptr, p, dQ, nq, d_ids, d_dists, d_sums, s, false, nullptr, true);
+        cudaError_t e = cudaStreamEndCapture(s, &graph);
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&h->graph_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            h->graph_exec = nullptr;
+            return cuda_fail(e, "cudaGraphInstantiate");
+        }
+        h->graph_key = key;
+        h->graph_stream = s;
+    }
+    SCG_CUDA(cudaGraphLaunch(h->graph_exec, s));
+    SCG_CUDA(cudaStreamSynchronize(s));
+    h->ws.last_nq = nq;
+    int st = *h->ws.h_status;
+    if (st & ST_POOL)  // the visited lists outgrew the pool: search again fused
+        return run_search(h, &h->ws, nullptr, p, dQ, nq, d_ids, d_dists, d_sums, s, true, nullptr, false);
+    return status_result(st);
 }
 
 int scg_query_tables_device(scg_index *h, int precision, const float *dQ, int nq, float *d_diff_qc, float *d_diff_qr,

@@ -3,7 +3,8 @@
 // The reference sorts each coarse list of a query completely
 // (nth_element_id + sort_id with M = kc, multi_query.h:114-128,
 // sc_query.h:98-106, query.h:230-234), but the multi-sequence walk only
-// reaches a prefix.  For kc <= 1024 one warp handles one list: the keys
+// reaches a prefix.  For kc <= 1024 one warp handles one list (longer lists,
+// up to 8192, one block: k_coarse_prefix_block): the keys
 // (ordered float of q_part + diff_qc, << 32 | centroid id, so equal keys go
 // by id) sit 32 per lane at most; a binary search over the high words finds
 // vm, the M-th smallest (M from the query's candidate target, the same rule
@@ -147,6 +148,138 @@ __global__ void __launch_bounds__(CS_THREADS) k_coarse_prefix(CoarseArgs a) {
     }
 }
 
+// Lists longer than 1024 (kc up to 8192): one block of 256 threads per list,
+// P keys per thread, striped (element i = r * 256 + tid); the same
+// prefix rule by a block-wide radix select (4 x 8 bits); keys at or below vm are
+// gathered in shared memory (unordered, then sorted by warp 0).  A prefix
+// longer than 1024 keys (many ties) is left to the selection kernel
+// (length 0 in the metadata).
+template <int P>
+__global__ void __launch_bounds__(256) k_coarse_prefix_block(CoarseArgs a) {
+    constexpr int NTB = 256;
+    __shared__ uint64_t buf[CS_CAP];
+    __shared__ uint32_t hist[NTB];
+    __shared__ int s_cnt[NTB / 32];
+    __shared__ uint32_t s_min[NTB / 32];
+    __shared__ int s_c, s_acc;
+    __shared__ uint32_t s_bin;
+    const unsigned FULL = 0xffffffffu;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int list = blockIdx.x;
+    const int nlists = a.imi ? 2 : 1;
+    const int q = list / nlists, part = list - q * nlists;
+    const float base = a.imi ? a.qn[2 * q + part] : a.qsum[q];
+    const float *row = a.dqc + (size_t)q * a.mc * a.kc + (size_t)part * a.kc;
+    uint64_t v[P];
+#pragma unroll
+    for (int r = 0; r < P; r++) {
+        const int i = r * NTB + tid;
+        v[r] = i < a.kc ? (((uint64_t)f2o(__fadd_rn(base, row[i])) << 32) | (uint32_t)i) : ~0ull;
+    }
+    const int T = a.Tq ? a.Tq[q] : a.T;
+    const double c0 = (T > 0 ? (double)T : 1.0) / (a.avg_density > 1e-9 ? a.avg_density : 1e-9);
+    int M = 1;
+    while (M < 4 * (int)sqrt(c0) + 1) M <<= 1;
+    if (M < 128) M = 128;
+    if (M > a.max_prefix) M = a.max_prefix;
+    auto block_count = [&](uint32_t lim) {
+        int cnt = 0;
+#pragma unroll
+        for (int r = 0; r < P; r++) cnt += (uint32_t)(v[r] >> 32) <= lim;
+        cnt = __reduce_add_sync(FULL, cnt);
+        __syncthreads();
+        if (lane == 0) s_cnt[wid] = cnt;
+        __syncthreads();
+        int t = 0;
+        for (int w = 0; w < NTB / 32; w++) t += s_cnt[w];
+        return t;
+    };
+    uint32_t vm = 0xffffffffu;
+    if (M < a.kc) {
+        // vm = the M-th smallest high word: radix select, 4 passes of 8 bits
+        // (one histogram bin per thread)
+        uint32_t prefix = 0;
+        int need = M;
+        for (int shift = 24; shift >= 0; shift -= 8) {
+            hist[tid] = 0;
+            __syncthreads();
+#pragma unroll
+            for (int r = 0; r < P; r++) {
+                const uint32_t hw = (uint32_t)(v[r] >> 32);
+                if (v[r] != ~0ull && (shift == 24 || (hw >> (shift + 8)) == (prefix >> (shift + 8))))
+                    atomicAdd(&hist[(hw >> shift) & 255u], 1u);
+            }
+            __syncthreads();
+            // exclusive scan of the 256 bins (thread = bin)
+            const uint32_t cnt = hist[tid];
+            uint32_t x = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(FULL, x, o);
+                if (lane >= o) x += y;
+            }
+            if (lane == 31) s_cnt[wid] = (int)x;
+            __syncthreads();
+            uint32_t wpre = 0;
+            for (int w = 0; w < wid; w++) wpre += (uint32_t)s_cnt[w];
+            const uint32_t ex = wpre + x - cnt;
+            if (ex < (uint32_t)need && ex + cnt >= (uint32_t)need) {
+                s_bin = (uint32_t)tid;
+                s_acc = (int)ex;
+            }
+            __syncthreads();
+            prefix |= s_bin << shift;
+            need -= s_acc;
+            __syncthreads();
+        }
+        vm = prefix;
+    }
+    // prefix length and the smallest high word above vm
+    uint32_t nxt = 0xffffffffu;
+#pragma unroll
+    for (int r = 0; r < P; r++) {
+        const uint32_t hw = (uint32_t)(v[r] >> 32);
+        if (v[r] != ~0ull && hw > vm && hw < nxt) nxt = hw;
+    }
+    nxt = __reduce_min_sync(FULL, nxt);
+    if (lane == 0) s_min[wid] = nxt;
+    if (tid == 0) s_c = 0;
+    __syncthreads();
+    for (int w = 0; w < NTB / 32; w++) nxt = min(nxt, s_min[w]);
+    const int c = block_count(vm);
+    uint64_t *dst = a.out + (size_t)list * a.width;
+    if (c > CS_CAP) {
+        if (tid == 0) {
+            a.meta[2 * list] = 0u;  // the selection kernel ranks this list itself
+            a.meta[2 * list + 1] = 0xffffffffu;
+        }
+        return;
+    }
+#pragma unroll
+    for (int r = 0; r < P; r++) {
+        if (v[r] != ~0ull && (uint32_t)(v[r] >> 32) <= vm) buf[atomicAdd(&s_c, 1)] = v[r];
+    }
+    __syncthreads();
+    int c2 = 32;
+    while (c2 < c) c2 <<= 1;
+    for (int i = c + tid; i < c2; i += NTB) buf[i] = ~0ull;
+    __syncthreads();
+    if (wid == 0) {
+        switch (c2) {
+            case 32: sort_out<1>(buf, dst, lane); break;
+            case 64: sort_out<2>(buf, dst, lane); break;
+            case 128: sort_out<4>(buf, dst, lane); break;
+            case 256: sort_out<8>(buf, dst, lane); break;
+            case 512: sort_out<16>(buf, dst, lane); break;
+            default: sort_out<32>(buf, dst, lane); break;
+        }
+        if (lane == 0) {
+            a.meta[2 * list] = (uint32_t)c;
+            a.meta[2 * list + 1] = nxt;
+        }
+    }
+}
+
 template <int P>
 void launch_p(const CoarseArgs &a, cudaStream_t s) {
     const int lists = a.nq * (a.imi ? 2 : 1);
@@ -159,7 +292,8 @@ void launch_p(const CoarseArgs &a, cudaStream_t s) {
 int coarse_sort_width(int kc) {
     int p = 32;
     while (p < kc) p <<= 1;
-    return p <= CS_CAP ? p : 0;
+    if (p <= CS_CAP) return p;
+    return kc <= 8192 ? CS_CAP : 0;  // long lists keep a prefix of at most CS_CAP keys
 }
 
 void launch_coarse_prefix(const CoarseArgs &a, cudaStream_t s) {
@@ -170,7 +304,16 @@ void launch_coarse_prefix(const CoarseArgs &a, cudaStream_t s) {
         case 128: launch_p<4>(a, s); break;
         case 256: launch_p<8>(a, s); break;
         case 512: launch_p<16>(a, s); break;
-        case 1024: launch_p<32>(a, s); break;
+        case 1024:
+            if (a.kc <= 1024) {
+                launch_p<32>(a, s);
+            } else {
+                const int lists = a.nq * (a.imi ? 2 : 1);
+                if (a.kc <= 2048) k_coarse_prefix_block<8><<<lists, 256, 0, s>>>(a);
+                else if (a.kc <= 4096) k_coarse_prefix_block<16><<<lists, 256, 0, s>>>(a);
+                else k_coarse_prefix_block<32><<<lists, 256, 0, s>>>(a);
+            }
+            break;
         default: break;
     }
 }

@@ -97,6 +97,10 @@ struct scg_index {
     scg::Workspace ws2;
     int *h_chunk_status = nullptr;  // pinned [8]
     scg::DevBuf q, ids, dists, sums, reqbuf;  // device staging of scg_search
+    // scg_search_graph: the captured launch sequence and the arguments it holds
+    cudaGraphExec_t graph_exec = nullptr;
+    cudaStream_t graph_stream = nullptr;
+    std::string graph_key;
     std::mutex mu;
 };
 

@@ -47,7 +47,10 @@ constexpr int HBITS = 11;
 constexpr int HBINS = 1 << HBITS;
 constexpr int TIECAP = 64;
 constexpr int RMAX = 1024;      // largest R
-constexpr int WARMN = 4096;     // candidates scored before the threshold is set
+#ifndef SCG_WARMN
+#define SCG_WARMN 4096
+#endif
+constexpr int WARMN = SCG_WARMN;  // candidates scored before the threshold is set
 constexpr int WWIN = 32;        // per-warp window of visited cells
 // Candidates per lane per claimed chunk (U, a template parameter of the
 // scan: 2, 4 or 8); a warp claims 32 * U candidates at a time.
@@ -921,11 +924,12 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
         for (int attempt = 0; attempt < 2; attempt++) {
             const bool full = attempt == 1 || M >= kc;
             bool done_a = false, done_b = !imi;
-            if (a.slist && attempt == 0) {
-                // prefixes sorted ahead by k_coarse_prefix (same prefix rule)
+            const uint32_t *meta = a.slist ? a.smeta + (size_t)q * (imi ? 2 : 1) * 2 : nullptr;
+            if (a.slist && attempt == 0 && meta[0] > 0 && (!imi || meta[2] > 0)) {
+                // prefixes sorted ahead by k_coarse_prefix (same prefix rule;
+                // length 0 = left to this kernel)
                 const int nl = imi ? 2 : 1;
                 const uint64_t *src = a.slist + (size_t)q * nl * a.slist_w;
-                const uint32_t *meta = a.smeta + (size_t)q * nl * 2;
                 const int ca = (int)meta[0], cb = imi ? (int)meta[2] : 0;
                 for (int h = tid; h < ca; h += NT) S.LA[h] = src[h];
                 for (int h = tid; h < cb; h += NT) S.LB[h] = src[a.slist_w + h];

@@ -33,7 +33,7 @@ EXPORTS = ["scg_last_error", "scg_index_create", "scg_index_destroy", "scg_load_
            "scg_server_create", "scg_server_submit", "scg_server_wait", "scg_server_stats",
            "scg_server_destroy", "scg_autotune", "scg_set_scan_tuning",
            "scg_set_kernel_split", "scg_server_wait_times", "scg_set_encoder",
-           "scg_train_codebooks", "scg_build_index", "scg_write_edat"]
+           "scg_train_codebooks", "scg_build_index", "scg_write_edat", "scg_search_graph"]
 
 
 def train_codebooks_device(dX_ptr, n, dim, mc, kc, mp, kp, iters, seed, d_cq, d_pq, device=0, stream=None):
@@ -179,6 +179,12 @@ class Index:
                                       ctypes.c_void_p(d_ids), ctypes.c_void_p(d_d),
                                       ctypes.c_void_p(d_sums),
                                       ctypes.c_void_p(stream) if stream else None))
+
+    def search_graph(self, mode, dQ_ptr, nq, R, w, T, d_ids, d_d, d_sums, stream, precision=FP32_EXACT, rerank=0):
+        """Device-buffer search replayed from a captured CUDA graph."""
+        p = SearchParams(mode, R, w, T, precision, rerank)
+        _check(_lib.scg_search_graph(self._h, ctypes.byref(p), ctypes.c_void_p(dQ_ptr), nq, ctypes.c_void_p(d_ids),
+                                     ctypes.c_void_p(d_d), ctypes.c_void_p(d_sums), ctypes.c_void_p(stream)))
 
     def search_device_noalloc(self, mode, dQ_ptr, nq, R, w, T, d_ids, d_d, d_sums, stream=None,
                               precision=FP32_EXACT, rerank=0):
