@@ -222,6 +222,15 @@ int scg_write_edat(scg_index *h, const char *path);
 int scg_train_codebooks(const float *dX, int64_t n, int dim, int mc, int kc, int mp, int kp, int iters,
                         uint64_t seed, float *d_cq, float *d_pq, int device, void *stream);
 
+/* k-means of nseg segments at once, HOST buffers: X[n][dim] (segment j =
+ * dims [j dim/nseg, (j+1) dim/nseg)), centers[nseg][k][dim/nseg] and labels
+ * [nseg][n] (may be NULL) out; k-means++ seeding (deterministic per seed) and
+ * `iters` Lloyd steps with FP64 means, on device `device`.  The clustering of
+ * PQQuantizer::create_sub_quantizers (quantizer.h:235-272) with greg_kmeans
+ * (k-means.h:671-912) replaced by the published algorithm. */
+int scg_kmeans(const float *X, int64_t n, int dim, int nseg, int k, int iters, uint64_t seed,
+               float *centers, int *labels, int device);
+
 /* Encoder arithmetic for IVF/IMI codes (scg_encode, scg_encode_device with
  * nc = 0).  SCG_ENC_TENSOR (the default): distances ranked by tcgen05
  * split-BF16 GEMM tiles, every centroid within the tiles' error margin of the

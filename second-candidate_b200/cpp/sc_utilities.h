@@ -78,6 +78,55 @@ inline int load_and_convert_data(const char *filename, DataType2 *&data, int hea
     return (int)rows;
 }
 
+/* distance_l2_square (lib/simple-cluster/include/utilities.h:217-230):
+ * float differences, squared and summed in double. */
+template <typename DataType1, typename DataType2>
+inline double distance_l2_square(const DataType1 *x, const DataType2 *y, int d) {
+    double dis = 0.0, tmp;
+    for (int i = 0; i < d; i++) {
+        tmp = static_cast<float>(x[i]) - static_cast<float>(y[i]);
+        dis += tmp * tmp;
+    }
+    return dis;
+}
+
+/* load_codebook (sc_utilities.h:897-980) for the coarse (type 0) and product
+ * (type 1) codebooks: the .ctr_ header {k, m, dim} fills config (kc/mc or
+ * kp/mp, dim) and `codebook` receives k * dim values (::operator new). */
+template <typename DataType>
+inline void load_codebook(const char *filename, PQConfig &config, DataType *&codebook, int type, bool verbose) {
+    FILE *f = fopen(filename, "rb");
+    if (!f) {
+        if (verbose) std::cerr << "Cannot open the file" << std::endl;
+        exit(1);
+    }
+    DataType hdr[3];
+    if (fread(hdr, sizeof(DataType), 3, f) != 3) {
+        std::cerr << "Wrong data" << std::endl;
+        exit(EXIT_FAILURE);
+    }
+    config.dim = static_cast<int>(hdr[2]);
+    const int k = static_cast<int>(hdr[0]), m = static_cast<int>(hdr[1]);
+    if (type == 1) {
+        config.kp = k;
+        config.mp = m;
+    } else {
+        config.kc = k;
+        config.mc = m;
+    }
+    if (m == 0) {
+        std::cerr << "Wrong data" << std::endl;
+        exit(EXIT_FAILURE);
+    }
+    codebook = (DataType *)::operator new(sizeof(DataType) * (size_t)k * config.dim);
+    if (fread(codebook, sizeof(DataType), (size_t)k * config.dim, f) != (size_t)k * config.dim) {
+        std::cerr << "Wrong data" << std::endl;
+        exit(EXIT_FAILURE);
+    }
+    fclose(f);
+    if (verbose) std::cout << "Loaded a codebook at " << filename << " with " << m << " sub codes" << std::endl;
+}
+
 /* load_data (sc_utilities.h:817-886): no conversion. */
 template <typename DataType>
 inline int load_data(const char *filename, DataType *&data, int header, int d, bool verbose) {

@@ -1101,6 +1101,40 @@ int scg_train_codebooks(const float *dX, int64_t n, int dim, int mc, int kc, int
     return SCG_OK;
 }
 
+int scg_kmeans(const float *X, int64_t n, int dim, int nseg, int k, int iters, uint64_t seed, float *centers,
+               int *labels, int device) {
+    if (!X || !centers) return fail(SCG_ERR_ARG, "null buffer");
+    if (n < 1 || dim < 1 || nseg < 1 || k < 1 || iters < 0 || dim % nseg) return fail(SCG_ERR_ARG, "bad shape");
+    if (n < k) return fail(SCG_ERR_ARG, "fewer rows than centroids");
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    const int64_t chunk = std::max<int64_t>(128, std::min<int64_t>(n, (1ll << 28) / ((int64_t)nseg * k)));
+    DevBuf dx, dc, work, asg, status;
+    int rc;
+    auto release = [&]() { dx.release(); dc.release(); work.release(); asg.release(); status.release(); };
+    if ((rc = dx.ensure(4ull * n * dim)) || (rc = dc.ensure(4ull * nseg * k * (dim / nseg))) ||
+        (rc = work.ensure(kmeans_work_bytes(n, nseg, k, dim / nseg, chunk))) || (rc = asg.ensure(4ull * nseg * n)) ||
+        (rc = status.ensure(16))) {
+        release();
+        return rc;
+    }
+    e = cudaMemcpy(dx.p, X, 4ull * n * dim, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(status.p, 0, 16);
+    if (e != cudaSuccess) { release(); return cuda_fail(e, "scg_kmeans copies"); }
+    rc = kmeans_segments(dx.as<float>(), n, dim, nseg, k, iters, seed, dc.as<float>(), work.as<unsigned char>(), chunk,
+                         status.as<int>(), asg.as<int>(), nullptr);
+    int st = 0;
+    if (rc == SCG_OK) {
+        e = cudaMemcpy(centers, dc.p, 4ull * nseg * k * (dim / nseg), cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && labels) e = cudaMemcpy(labels, asg.p, 4ull * nseg * n, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(&st, status.p, sizeof(int), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = cuda_fail(e, "scg_kmeans results");
+    }
+    release();
+    if (rc) return rc;
+    return st ? status_result(st) : SCG_OK;
+}
+
 int scg_set_encoder(scg_index *h, int method) {
     if (!h) return fail(SCG_ERR_ARG, "null index");
     if (method != SCG_ENC_EXACT && method != SCG_ENC_TENSOR) return fail(SCG_ERR_ARG, "unknown encoder");

@@ -33,7 +33,8 @@ EXPORTS = ["scg_last_error", "scg_index_create", "scg_index_destroy", "scg_load_
            "scg_server_create", "scg_server_submit", "scg_server_wait", "scg_server_stats",
            "scg_server_destroy", "scg_autotune", "scg_set_scan_tuning",
            "scg_set_kernel_split", "scg_server_wait_times", "scg_set_encoder",
-           "scg_train_codebooks", "scg_build_index", "scg_write_edat", "scg_search_graph"]
+           "scg_train_codebooks", "scg_build_index", "scg_write_edat", "scg_search_graph",
+           "scg_kmeans"]
 
 
 def train_codebooks_device(dX_ptr, n, dim, mc, kc, mp, kp, iters, seed, d_cq, d_pq, device=0, stream=None):

@@ -5,6 +5,8 @@
 //
 //   dropin_driver search <ivf|imi|sc> <cq.ctr_> <pq.ctr_> <x.edat_> <q.fvecs> <dim> <R> <w> <T> <out.txt>
 //   dropin_driver encode <0|2> <cq.ctr_> <pq.ctr_> <x.fvecs> <outdir> <prefix>
+//   dropin_driver quantize <x.fvecs> <dim> <m> <nsc> <out_prefix>      (PQQuantizer, test_quantizer.cpp-style)
+//   dropin_driver residual <pq|sc> <x.fvecs> <dim> <m> <cq.ctr_> <out.fvecs>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
@@ -14,6 +16,7 @@
 #include "evaluation.h"
 #include "multi_query.h"
 #include "sc_encoder.h"
+#include "sc_quantizer.h"
 #include "sc_query.h"
 
 using namespace SC;
@@ -120,9 +123,44 @@ static int encode(int argc, char **argv) {
     return 0;
 }
 
+// Trains `m` sub-codebooks of `nsc` centres on the rows of x.fvecs, writes
+// out_prefix.ctr_ and prints the distortion.
+static int quantize(int, char **argv) {
+    const int dim = atoi(argv[3]), m = atoi(argv[4]), nsc = atoi(argv[5]);
+    PQQuantizer<float> q(dim, m, nsc, 4, false);
+    q.load_data(argv[2], false);
+    q.create_sub_quantizers(false);
+    q.output(argv[6], false);
+    std::cout << std::setprecision(17) << q.distortion(false) << std::endl;
+    return 0;
+}
+
+// Subtracts the nearest (pq) or second-nearest (sc) centroid of the coarse
+// codebook cq.ctr_ from every part of every row; writes the rows as fvecs.
+static int residual(int, char **argv) {
+    const bool sc = !strcmp(argv[2], "sc");
+    const int dim = atoi(argv[4]), m = atoi(argv[5]);
+    char *files[1] = {argv[6]};
+    PQQuantizer<float> *q = sc ? new SCQuantizer<float>(dim, m, 1, 4, 1, false) : new PQQuantizer<float>(dim, m, 1, 4, 1, false);
+    q->load_data(argv[3], false);
+    q->load_codebooks(files, false);
+    if (sc) static_cast<SCQuantizer<float> *>(q)->calc_residual_vector(false);
+    else q->calc_residual_vector(false);
+    FILE *f = fopen(argv[7], "wb");
+    for (int i = 0; i < q->size(); i++) {
+        fwrite(&dim, sizeof(int), 1, f);
+        fwrite(q->data + (size_t)i * dim, sizeof(float), (size_t)dim, f);
+    }
+    fclose(f);
+    delete q;
+    return 0;
+}
+
 int main(int argc, char **argv) {
     if (argc >= 12 && !strcmp(argv[1], "search")) return search(argc, argv);
     if (argc >= 8 && !strcmp(argv[1], "encode")) return encode(argc, argv);
+    if (argc >= 7 && !strcmp(argv[1], "quantize")) return quantize(argc, argv);
+    if (argc >= 8 && !strcmp(argv[1], "residual")) return residual(argc, argv);
     std::cerr << "usage: see the header of dropin_driver.cpp" << std::endl;
     return 1;
 }

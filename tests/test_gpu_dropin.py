@@ -74,3 +74,45 @@ def test_encoder_through_dropin(driver, oracle_mod, tmp_path, name, nc):
     got = open(tmp_path / ("d_mr2_ivf.edat_" if nc else "d_ivf.edat_"), "rb").read()
     formats.write_edat(tmp_path / "ref.edat_", c["L"], c["pid"], c["icodes"])
     assert got == open(tmp_path / "ref.edat_", "rb").read()
+
+
+def test_quantizer_through_dropin(driver, oracle_mod, tmp_path):
+    """PQQuantizer (drop-in): trains the strips on the GPU, writes a .ctr_
+    with the reference's header, deterministic, and prints the reference's
+    distortion formula for the final assignment; calc_residual_vector of
+    PQQuantizer / SCQuantizer subtracts the nearest / second-nearest
+    centroid per part."""
+    import workloads as W
+    D, m, nsc = 32, 4, 64
+    mix = W.Mixture(D, 8, 20.0, "u8", seed=121)
+    X = mix.sample(5000, seed=122)
+    formats.write_vecs(tmp_path / "x.fvecs", X)
+    outs = []
+    for run in range(2):
+        r = subprocess.run([driver, "quantize", str(tmp_path / "x.fvecs"), str(D), str(m), str(nsc),
+                            str(tmp_path / ("cb%d" % run))], check=True, capture_output=True, text=True)
+        outs.append((float(r.stdout.split()[-1]), open(tmp_path / ("cb%d.ctr_" % run), "rb").read()))
+    assert outs[0][1] == outs[1][1]  # deterministic
+    raw = np.frombuffer(outs[0][1], np.float32)
+    assert raw[:3].tolist() == [nsc, m, D] and raw.size == 3 + nsc * D
+    C = raw[3:].reshape(m, nsc, D // m).astype(np.float64)
+    e = 0.0
+    for i in range(m):
+        part = X[:, i * (D // m):(i + 1) * (D // m)].astype(np.float64)
+        d = ((part[:, None, :] - C[i][None]) ** 2).sum(2).min(1)
+        e += d.sum()
+    assert abs(outs[0][0] - np.sqrt(e)) <= 1e-3 * np.sqrt(e)
+    # residuals against a 2-part coarse codebook
+    cq = np.asarray(W.train_codebooks(X[:2000], 2, 16, 4, 8, 2, seed=123)[0], np.float32)
+    formats.write_ctr(tmp_path / "cq.ctr_", cq, 16, 2, D)
+    for kind in ("pq", "sc"):
+        subprocess.run([driver, "residual", kind, str(tmp_path / "x.fvecs"), str(D), "2", str(tmp_path / "cq.ctr_"),
+                        str(tmp_path / "r.fvecs")], check=True)
+        Rr = formats.read_vecs(tmp_path / "r.fvecs", np.float32)
+        for i in range(2):
+            part = X[:, i * 16:(i + 1) * 16]
+            diff = (part[:, None, :] - cq[i][None]).astype(np.float64)  # float differences, double squares
+            d = (diff ** 2).sum(2).astype(np.float32)
+            order = np.argsort(d, axis=1, kind="stable")
+            pick = order[:, 0] if kind == "pq" else order[:, 1]
+            assert np.array_equal(Rr[:, i * 16:(i + 1) * 16], part - cq[i][pick]), kind
