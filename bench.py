@@ -352,13 +352,11 @@ def main():
         return
 
     import scgpu
+    import replicas
+    torch.cuda.set_device(local)
     if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    else:
-        torch.cuda.set_device(local)
+        # replicas: every rank searches its own copy; only the timing is reduced
+        replicas.init("nccl")
     dev = torch.device("cuda", local)
 
     w = W.build_gpu_workload(args.workload, cache_dir=args.cache, log=log)
@@ -449,8 +447,7 @@ def main():
 
     clocks = Clocks(local)
     clocks.start()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     torch.cuda.synchronize()
     clocks.mark(True)
     times, kern = [], []
@@ -466,13 +463,8 @@ def main():
         kern.append(ix.last_timings())
     torch.cuda.synchronize()
     clocks.mark(False)
-    if world > 1:
-        dist.barrier()
-    total_ms = sum(times)
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    replicas.barrier()
+    job_qps, total_ms = replicas.job_throughput(sum(times), nq * args.steps, device=dev)
     ck = clocks.stop()
 
     ids = d_ids.view(nq, R).cpu().numpy()
@@ -568,7 +560,7 @@ def main():
         same = bool(np.array_equal(hid, ids))
 
     line = {
-        "metric": METRIC, "value": nq * args.steps * world / (total_ms / 1e3), "unit": "queries/s",
+        "metric": METRIC, "value": job_qps, "unit": "queries/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": {"fp32": "f32", "fast": "bf16", "bf16": "bf16", "fp16": "f16"}[args.precision],
@@ -623,8 +615,7 @@ def main():
     if rank == 0:
         print(json.dumps(line), flush=True)
     ix.close()
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.finish()
 
 
 if __name__ == "__main__":
