@@ -231,6 +231,19 @@ int scg_train_codebooks(const float *dX, int64_t n, int dim, int mc, int kc, int
 int scg_kmeans(const float *X, int64_t n, int dim, int nseg, int k, int iters, uint64_t seed,
                float *centers, int *labels, int device);
 
+/* Exact nearest neighbour of each query among base rows, all buffers on the
+ * device: dX[n][dim] and dQ[nq][dim] float32 in, d_ids[nq] (row index) and
+ * d_dists[nq] (may be NULL; the squared distance of distance_l2_square --
+ * float differences squared and summed in double, stored as float) out.
+ * Equal distances keep the lowest row index.  The ground truth that
+ * Evaluation::load_groundtruth / calc_recall (evaluation.h:34-92) read from
+ * a file made outside the reference; candidates are ranked by tcgen05
+ * split-BF16 distance tiles over chunks of rows and every row within their
+ * error margin of the chunk minimum is re-scored exactly, so the result is
+ * the brute-force argmin.  Synchronises `stream` before it returns. */
+int scg_exact_nn(const float *dX, int64_t n, const float *dQ, int nq, int dim, int *d_ids, float *d_dists,
+                 int device, void *stream);
+
 /* Encoder arithmetic for IVF/IMI codes (scg_encode, scg_encode_device with
  * nc = 0).  SCG_ENC_TENSOR (the default): distances ranked by tcgen05
  * split-BF16 GEMM tiles, every centroid within the tiles' error margin of the

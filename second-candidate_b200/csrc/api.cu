@@ -1135,6 +1135,32 @@ int scg_kmeans(const float *X, int64_t n, int dim, int nseg, int k, int iters, u
     return st ? status_result(st) : SCG_OK;
 }
 
+int scg_exact_nn(const float *dX, int64_t n, const float *dQ, int nq, int dim, int *d_ids, float *d_dists,
+                 int device, void *stream) {
+    if (!dX || !dQ || !d_ids) return fail(SCG_ERR_ARG, "null buffer");
+    if (n < 1 || nq < 1 || dim < 1) return fail(SCG_ERR_ARG, "non-positive shape");
+    if (n > 0x7fffffffll) return fail(SCG_ERR_ARG, "row indices must fit int32");
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+    cudaStream_t s = (cudaStream_t)stream;
+    // distance tables of at most 2^28 floats per chunk of rows
+    const int64_t chunk = std::max<int64_t>(256, std::min<int64_t>(n, (1ll << 28) / nq));
+    DevBuf work, status;
+    int rc;
+    if ((rc = work.ensure(exact_nn_work_bytes(nq, chunk)))) return rc;
+    if ((rc = status.ensure(16))) { work.release(); return rc; }
+    auto release = [&]() { work.release(); status.release(); };
+    if ((e = cudaMemsetAsync(status.p, 0, 16, s)) != cudaSuccess) { release(); return cuda_fail(e, "memset"); }
+    rc = exact_nn(dX, n, dQ, nq, dim, d_ids, d_dists, work.as<unsigned char>(), chunk, status.as<int>(), s);
+    int st = 0;
+    e = cudaMemcpyAsync(&st, status.p, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    release();
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_fail(e, "scg_exact_nn");
+    return st ? status_result(st) : SCG_OK;
+}
+
 int scg_set_encoder(scg_index *h, int method) {
     if (!h) return fail(SCG_ERR_ARG, "null index");
     if (method != SCG_ENC_EXACT && method != SCG_ENC_TENSOR) return fail(SCG_ERR_ARG, "unknown encoder");

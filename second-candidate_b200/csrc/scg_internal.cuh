@@ -184,6 +184,11 @@ int kmeans_segments(const float *X, int64_t n, int dim, int nseg, int k, int ite
 void launch_residual(const float *X, int64_t n, int dim, int nseg, int k, const float *C, const int *asg, float *R,
                      cudaStream_t s);
 
+// Exact nearest neighbour (gt.cu).
+size_t exact_nn_work_bytes(int nq, int64_t chunk);
+int exact_nn(const float *X, int64_t n, const float *Q, int nq, int dim, int *ids, float *dists, unsigned char *work,
+             int64_t chunk, int *status, cudaStream_t s);
+
 size_t rerank_smem_bytes(int L, int dim);
 int launch_rerank(const float *Q, int nq, int dim, const void *raw, int raw_u8, int64_t N, const int *sl_ids, int L,
                   int R, int *out_ids, float *out_d, int *status, cudaStream_t s);

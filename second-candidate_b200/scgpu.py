@@ -34,7 +34,7 @@ EXPORTS = ["scg_last_error", "scg_index_create", "scg_index_destroy", "scg_load_
            "scg_server_destroy", "scg_autotune", "scg_set_scan_tuning",
            "scg_set_kernel_split", "scg_server_wait_times", "scg_set_encoder",
            "scg_train_codebooks", "scg_build_index", "scg_write_edat", "scg_search_graph",
-           "scg_kmeans"]
+           "scg_kmeans", "scg_exact_nn"]
 
 
 def train_codebooks_device(dX_ptr, n, dim, mc, kc, mp, kp, iters, seed, d_cq, d_pq, device=0, stream=None):
@@ -43,6 +43,15 @@ def train_codebooks_device(dX_ptr, n, dim, mc, kc, mp, kp, iters, seed, d_cq, d_
     _check(lib.scg_train_codebooks(ctypes.c_void_p(dX_ptr), ctypes.c_int64(n), dim, mc, kc, mp, kp, iters,
                                    ctypes.c_uint64(seed), ctypes.c_void_p(d_cq), ctypes.c_void_p(d_pq), device,
                                    ctypes.c_void_p(stream) if stream else None))
+
+
+
+def exact_nn_device(dX_ptr, n, dQ_ptr, nq, dim, d_ids, d_dists=None, device=0, stream=None):
+    """Exact nearest base row of each query, device buffers (scg_exact_nn)."""
+    lib = load()
+    _check(lib.scg_exact_nn(ctypes.c_void_p(dX_ptr), ctypes.c_int64(n), ctypes.c_void_p(dQ_ptr), nq, dim,
+                            ctypes.c_void_p(d_ids), ctypes.c_void_p(d_dists) if d_dists else None, device,
+                            ctypes.c_void_p(stream) if stream else None))
 
 
 class ScgError(RuntimeError):
