@@ -270,7 +270,7 @@ struct QState {
     // scan
     int ncur, npend;
     uint64_t thr;
-    uint32_t next_flat;  // next unclaimed candidate of the scan
+    uint32_t next_flat;  // next unclaimed candidate of the scan (shared claims)
     uint32_t pool_off, pool_cap;  // the query's visited-list region (selection kernel)
 };
 
@@ -618,50 +618,86 @@ struct ScanCtx {
     const float *dqc;
 };
 
-// Warp-centric ADC scan of the candidates [st.next_flat, limit): warps claim
-// chunks of 32 * U candidates from a shared counter, keep their own window of
-// visited cells, load U candidates per lane at once and add the table
-// entries in the reference's order.  WARM == true stores every candidate's
-// (distance, position) at warm[flat]; otherwise candidates with a distance
-// word <= tau are appended to out[] (global, capacity cap) through
-// warp-aggregated atomics on st.npend.
-template <int MPC, bool WARM, int U>
+// One float of shared memory at a 32-bit shared-window address.
+__device__ __forceinline__ float lds_f32(uint32_t addr) {
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+    return v;
+}
+
+// Warp-centric ADC scan of the candidates [first, limit), cut into chunks of
+// 32 * U candidates.  FK (the fast form with kp == 256): every warp takes an
+// equal, contiguous run of chunks, so it walks its visited cells in order,
+// and the LUT entries are read with 32-bit shared addresses and constant row
+// offsets.  Otherwise warps claim chunks from a shared counter
+// (st.next_flat, set to `first` by the caller), which keeps the warps of a
+// CTA on neighbouring cells: the exact forms gather dot_cr rows per cell,
+// and neighbouring cells share rows in L1.  A warp keeps a window of WWIN
+// visited cells; when the scan leaves it at its end the next WWIN cells are
+// loaded, otherwise a binary search over the visited-cell prefix finds the
+// cell that holds the chunk.  U candidates per lane are loaded at once and
+// the table entries are added in the reference's order.  WARM == true stores
+// every candidate's (distance, position) at warm[flat]; otherwise candidates
+// with a distance word <= tau are appended to out[] (global, capacity cap)
+// through warp-aggregated atomics on st.npend.
+template <int MPC, bool WARM, int U, bool FK>
 __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, QState &st, const ScanCtx &c,
-                                            uint32_t limit, uint32_t tau, uint64_t *warm, uint64_t *out,
-                                            uint32_t cap) {
+                                            uint32_t first, uint32_t limit, uint32_t tau, uint64_t *warm,
+                                            uint64_t *out, uint32_t cap) {
     const unsigned FULL = 0xffffffffu;
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     CellWin *W = S.wwin + wid * WWIN;
-    uint32_t wlo = 1, whi = 0;
-    int wcn = 0;
+    const uint32_t lut_s = (uint32_t)__cvta_generic_to_shared(S.lut);
+    constexpr bool KP256 = FK && MPC > 0;
+    const bool fast = FK || c.fast;
+    uint32_t whi = 0;
+    int wcn = 0, wci = -1;
     // this lane's window index: candidates only move forward within a window,
     // so the cell lookup resumes where the last one stopped; the current cell
     // is cached in registers ([r_pre, r_next) of the flat candidate index)
     int ci_l = 0;
     uint32_t r_pre = 0, r_next = 0, r_start = 0, r_h34 = 0;
     float r_d0 = 0.0f;
+    constexpr uint32_t WCH = 32u * U;
+    // FK: this warp's run of chunks
+    const uint64_t nch = limit > first ? ((uint64_t)(limit - first) + WCH - 1) / WCH : 0;
+    const uint64_t per = (nch + NWARP - 1) / NWARP;
+    const uint64_t lo64 = (uint64_t)first + (uint64_t)wid * per * WCH;
+    const uint32_t hi = FK ? (uint32_t)min(lo64 + per * WCH, (uint64_t)limit) : limit;
+    uint32_t next = (uint32_t)min(lo64, (uint64_t)limit);
     for (;;) {
-        uint32_t base = 0;
-        constexpr uint32_t WCH = 32u * U;
-        if (lane == 0) base = atomicAdd(&st.next_flat, WCH);
-        base = __shfl_sync(FULL, base, 0);
-        if (base >= limit) break;
-        const uint32_t end = min(base + WCH, limit);
+        uint32_t base;
+        if constexpr (FK) {
+            base = next;
+            next += WCH;
+        } else {
+            base = 0;
+            if (lane == 0) base = atomicAdd(&st.next_flat, WCH);
+            base = __shfl_sync(FULL, base, 0);
+        }
+        if (base >= hi) break;
+        const uint32_t end = min(base + WCH, hi);
         uint32_t f = base;
         while (f < end) {
-            if (f < wlo || f >= whi) {
-                // window of visited cells from the one holding f
+            if (f >= whi) {
+                // window of visited cells from the one holding f (f only
+                // grows): the next WWIN cells when f is the old window's end
                 int ci = 0;
-                if (lane == 0) {
-                    int lo = 0, hi = c.nvis - 1;
-                    while (lo < hi) {
-                        int mid = (lo + hi + 1) >> 1;
-                        if (c.vis_pre[mid] <= f) lo = mid;
-                        else hi = mid - 1;
+                if (wci >= 0 && f == whi) {
+                    ci = wci + wcn;
+                } else {
+                    if (lane == 0) {
+                        int lo2 = 0, hi2 = c.nvis - 1;
+                        while (lo2 < hi2) {
+                            int mid = (lo2 + hi2 + 1) >> 1;
+                            if (c.vis_pre[mid] <= f) lo2 = mid;
+                            else hi2 = mid - 1;
+                        }
+                        ci = lo2;
                     }
-                    ci = lo;
+                    ci = __shfl_sync(FULL, ci, 0);
                 }
-                ci = __shfl_sync(FULL, ci, 0);
+                __syncwarp();  // the previous window's readers are done
                 const int cc = ci + lane;
                 if (cc < c.nvis) {
                     uint32_t cell = c.vis_cell[cc];
@@ -685,9 +721,9 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
                     cw.h34 = h3 | (h4 << 16);
                     W[lane] = cw;
                 }
+                wci = ci;
                 wcn = min(WWIN, c.nvis - ci);
                 __syncwarp();
-                wlo = W[0].pre;
                 whi = (ci + wcn < c.nvis) ? c.vis_pre[ci + wcn] : c.Svis;
                 ci_l = 0;
                 r_next = 0;  // the cached cell belongs to the old window
@@ -716,7 +752,7 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
                     dd[u] = r_d0;
                     h34[u] = r_h34;
                     cwd[u].load(a.codes, pos[u], c.mp);
-                    if (c.fast) vt[u] = __ldg(a.vterm + pos[u]);
+                    if (fast) vt[u] = __ldg(a.vterm + pos[u]);
                 }
             }
             ci_l = ci;
@@ -727,14 +763,20 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
                 if (pos[u] != 0xffffffffu) {
                     float d = dd[u];
                     const uint32_t h3 = h34[u] & 0xffffu, h4 = h34[u] >> 16;
-                    if (c.fast) {
+                    if (fast) {
                         // d0 + per-vector term + sum_k LUT[k][c_k], the LUT
                         // entries summed as a tree (independent adds)
                         d = __fadd_rn(d, vt[u]);
                         if constexpr (MPC > 0) {
                             float v[MPC];
+                            if constexpr (KP256) {
 #pragma unroll
-                            for (int k = 0; k < MPC; k++) v[k] = S.lut[k * c.kp + cwd[u].code(k)];
+                                for (int k = 0; k < MPC; k++)
+                                    v[k] = lds_f32(lut_s + (cwd[u].code(k) << 2) + (uint32_t)k * 1024u);
+                            } else {
+#pragma unroll
+                                for (int k = 0; k < MPC; k++) v[k] = S.lut[k * c.kp + cwd[u].code(k)];
+                            }
 #pragma unroll
                             for (int s2 = 1; s2 < MPC; s2 <<= 1)
 #pragma unroll
@@ -836,8 +878,9 @@ __device__ uint32_t block_kth_hi(const uint64_t *keys, int n, int k, uint32_t *h
 #endif
 
 // PART 0: selection and scan fused; 1: selection only, publishing each
-// query's visited cells (a.qmeta, a.pool_*); 2: scan only, from them.
-template <int MPC, int U, int PART>
+// query's visited cells (a.qmeta, a.pool_*); 2: scan only, from them.  FK:
+// the scan-only kernel of the fast form with kp == 256 (scan_chunks).
+template <int MPC, int U, int PART, bool FK = false>
 __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
                                       : PART == 1 ? SCG_SELECT_MIN_BLOCKS
                                                   : SCG_SEARCH_MIN_BLOCKS) k_search(SearchArgs a) {
@@ -1360,7 +1403,7 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
             c.qs = qs;
             c.dqc = dqc;
             const uint32_t K = Svis < (uint32_t)WARMN ? Svis : (uint32_t)WARMN;
-            scan_chunks<MPC, true, U>(a, S, st, c, K, 0u, S.warm, nullptr, 0u);
+            scan_chunks<MPC, true, U, FK>(a, S, st, c, 0u, K, 0u, S.warm, nullptr, 0u);
             __syncthreads();
             uint32_t tau = 0xffffffffu;
             if (K > (uint32_t)R) tau = block_kth_hi(S.warm, (int)K, R, S.hist2, red, st);
@@ -1380,7 +1423,7 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
                 }
                 __syncthreads();
             }
-            scan_chunks<MPC, false, U>(a, S, st, c, Svis, tau, nullptr, pend_g, a.pcap);
+            scan_chunks<MPC, false, U, FK>(a, S, st, c, K, Svis, tau, nullptr, pend_g, a.pcap);
             __syncthreads();
             PHASE_MARK(4);  // scan
             if ((uint32_t)st.npend > a.pcap) {
@@ -1435,14 +1478,14 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
 
 // Dynamic shared memory already granted to a kernel variant, per device
 // (the attribute is set once, not on every launch).
-template <int MPC, int U, int PART>
+template <int MPC, int U, int PART, bool FK>
 int grant_smem(size_t smem) {
     static int granted[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64 || granted[dev] < (int)smem) {
         cudaError_t e =
-            cudaFuncSetAttribute(k_search<MPC, U, PART>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cudaFuncSetAttribute(k_search<MPC, U, PART, FK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_search)");
         if (dev >= 0 && dev < 64) granted[dev] = (int)smem;
     }
@@ -1451,9 +1494,9 @@ int grant_smem(size_t smem) {
 
 template <int MPC, int U, int PART>
 int occupancy(size_t smem) {
-    if (grant_smem<MPC, U, PART>(smem)) return 0;
+    if (grant_smem<MPC, U, PART, false>(smem)) return 0;
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<MPC, U, PART>, NT, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<MPC, U, PART, false>, NT, smem);
     return nb;
 }
 
@@ -1468,24 +1511,33 @@ int occupancy_mp(int mp, size_t smem) {
     }
 }
 
-template <int MPC, int U, int PART>
+template <int MPC, int U, int PART, bool FK = false>
 int launch(const SearchArgs &a, int grid, size_t smem, cudaStream_t s) {
-    int rc = grant_smem<MPC, U, PART>(smem);
+    int rc = grant_smem<MPC, U, PART, FK>(smem);
     if (rc) return rc;
-    k_search<MPC, U, PART><<<grid, NT, smem, s>>>(a);
+    k_search<MPC, U, PART, FK><<<grid, NT, smem, s>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "k_search launch");
     return SCG_OK;
 }
 
+// The scan-only kernel of the fast form with kp == 256 has its own variant.
+template <int MPC, int U, int PART>
+int launch_fk(const SearchArgs &a, int grid, size_t smem, cudaStream_t s) {
+    if constexpr (PART == 2 && MPC > 0) {
+        if (a.precision == SCG_FAST && a.kp == 256) return launch<MPC, U, PART, true>(a, grid, smem, s);
+    }
+    return launch<MPC, U, PART, false>(a, grid, smem, s);
+}
+
 template <int U, int PART>
 int launch_mp(const SearchArgs &a, int grid, size_t smem, cudaStream_t s) {
     switch (a.mp) {
-        case 4: return launch<4, U, PART>(a, grid, smem, s);
-        case 8: return launch<8, U, PART>(a, grid, smem, s);
-        case 16: return launch<16, U, PART>(a, grid, smem, s);
-        case 32: return launch<32, U, PART>(a, grid, smem, s);
-        default: return launch<0, U, PART>(a, grid, smem, s);
+        case 4: return launch_fk<4, U, PART>(a, grid, smem, s);
+        case 8: return launch_fk<8, U, PART>(a, grid, smem, s);
+        case 16: return launch_fk<16, U, PART>(a, grid, smem, s);
+        case 32: return launch_fk<32, U, PART>(a, grid, smem, s);
+        default: return launch_fk<0, U, PART>(a, grid, smem, s);
     }
 }
 
