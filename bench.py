@@ -307,6 +307,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--phases", action="store_true", help="report per-phase cycle counters")
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default scan chunking")
+    ap.add_argument("--upl", type=int, default=0, choices=[0, 2, 4, 8],
+                    help="fix the scan's candidates per lane for every form (skips the autotuner)")
     ap.add_argument("--encode-rows", type=int, default=2_000_000,
                     help="rows of the encoder leg (tensor-core vs exact encoder); 0 skips it")
     ap.add_argument("--serve-seconds", type=float, default=3.0,
@@ -399,7 +401,11 @@ def main():
     # the scan's chunking picked by the library's autotuner on this batch, for
     # both scan forms (exact and fast)
     tuning = {}
-    for name, pv in ((("fast", prec), ("fp32", 0)) if not args.no_autotune else ()):
+    if args.upl:
+        for pv in (prec, 0):
+            ix.set_scan_tuning(pv, args.upl)
+        tuning = {"fixed_candidates_per_lane": args.upl}
+    for name, pv in ((("fast", prec), ("fp32", 0)) if not (args.no_autotune or args.upl) else ()):
         choice, ms = ix.autotune(mode, dQ.data_ptr(), nq, R, wcap, T, d_ids.data_ptr(), d_d.data_ptr(),
                                  d_s.data_ptr(), precision=pv, rerank=rerank)
         tuning[name] = {"candidates_per_lane": choice, "ms_by_choice": dict(zip((2, 4, 8), ms))}

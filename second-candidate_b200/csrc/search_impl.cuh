@@ -271,6 +271,7 @@ struct QState {
     int ncur, npend;
     uint64_t thr;
     uint32_t next_flat;  // next unclaimed candidate of the scan (shared claims)
+    int top_sorted;      // top[0..ncur) is already in (distance, id) order
     uint32_t pool_off, pool_cap;  // the query's visited-list region (selection kernel)
 };
 
@@ -495,13 +496,40 @@ struct CodeWords<0> {
             atomicAdd((unsigned long long *)&a.phase_cycles[(i)], (unsigned long long)(v));        \
     } while (0)
 
+// The R smallest (distance, id) keys of nb pending entries by one bitonic
+// sort in top[] (room for WARMN keys, nb <= WARMN), in order; pid != null
+// turns the entries' CSR positions into ids first.
+__device__ void sort_merge(uint64_t *top, const uint64_t *pend, int nb, int R, const int *pid, QState &st) {
+    const int tid = threadIdx.x;
+    const int n2 = next_pow2(nb > 1 ? nb : 1);
+    for (int i = tid; i < n2; i += NT) {
+        uint64_t e = ~0ull;
+        if (i < nb) {
+            e = pend[i];
+            if (pid) e = (e & 0xffffffff00000000ull) | (uint32_t)__ldg(pid + (uint32_t)e);
+        }
+        top[i] = e;
+    }
+    __syncthreads();
+    if (n2 > 1) bitonic_sort64(top, n2);
+    if (tid == 0) {
+        st.ncur = nb < R ? nb : R;
+        st.npend = 0;
+        st.thr = nb < R ? ~0ull : top[R - 1];
+        st.top_sorted = 1;
+    }
+    __syncthreads();
+}
+
 // Keeps the R smallest of top[0..ncur) and the pending entries.  Pending
 // entries hold (distance, CSR position); they become (distance, id) here,
 // where the id loads of a whole buffer are issued together.  A radix select
 // over the distance words finds the R-th smallest distance v; every entry
 // below v is kept and the entries equal to v are taken in id order.  The top
 // list stays unsorted (the output step sorts it); st.thr becomes the R-th
-// smallest (distance, id) once R entries exist.
+// smallest (distance, id) once R entries exist.  More than TIECAP entries
+// equal to v: the pending buffer is merged again by one sort (sort_merge)
+// when it fits, else ST_TIE_OVERFLOW is raised.
 __device__ void merge_topk(uint64_t *top, uint64_t *pend, uint64_t *tmp, uint32_t *hist, uint64_t *ties, int R,
                            const int *pid, uint64_t *red, QState &st, int *status) {
     const int tid = threadIdx.x;
@@ -579,6 +607,13 @@ __device__ void merge_topk(uint64_t *top, uint64_t *pend, uint64_t *tmp, uint32_
         }
     }
     __syncthreads();
+    const bool resort = st.nties > TIECAP && na == 0 && nb <= WARMN;
+    if (resort) {
+        // the tie buffer kept only some of the entries equal to v
+        __syncthreads();
+        sort_merge(top, pend, nb, R, nullptr, st);
+        return;
+    }
     if (tid == 0) {
         // `need` entries equal to v complete the R: the smallest ids
         int nt = st.nties < TIECAP ? st.nties : TIECAP;
@@ -592,10 +627,10 @@ __device__ void merge_topk(uint64_t *top, uint64_t *pend, uint64_t *tmp, uint32_
             ties[j + 1] = x;
         }
         int take = (int)need;
-        if (take > nt) {
+        if (st.nties > TIECAP) {
             // more equal distances at the R-th place than the tie buffer holds
             atomicOr(status, ST_TIE_OVERFLOW);
-            take = nt;
+            if (take > nt) take = nt;
         }
         for (int i = 0; i < take; i++) tmp[total + i] = ties[i];
         st.ncur = (int)total + take;
@@ -1377,14 +1412,15 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
         // (5) ADC scan with the fused top-R.  The first WARMN candidates are
         // scored into shared memory; their R-th smallest distance bounds the
         // final R-th distance from above, so the rest of the scan keeps only
-        // candidates at or below it, appended to a per-CTA buffer; one
-        // radix-select merge over that buffer gives the R best.
+        // candidates at or below it, appended to a per-CTA buffer; one merge
+        // over that buffer (merge_topk) gives the R best.
         uint64_t *top = S.top, *tmpk = S.tmp;
         uint64_t *pend_g = a.pend + (size_t)blockIdx.x * a.pcap;
         if (tid == 0) {
             st.ncur = 0;
             st.npend = 0;
             st.next_flat = 0;
+            st.top_sorted = 0;
         }
         __syncthreads();
         if (!qerr2 && nvis > 0) {
@@ -1433,6 +1469,7 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
                 }
                 __syncthreads();
             } else if (st.npend > 0) {
+                COUNT(6, st.npend);
                 merge_topk(top, pend_g, tmpk, S.hist2, S.ties2, R, a.pid, red, st, a.status);
             }
         }
@@ -1442,7 +1479,7 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
         {
             const bool qerr3 = st.err != 0;
             int keep = (qerr3 || nvis == 0) ? 0 : st.ncur;
-            if (keep > 1) {
+            if (keep > 1 && !st.top_sorted) {
                 const int k2 = next_pow2(keep);
                 for (int i = keep + tid; i < k2; i += NT) top[i] = ~0ull;
                 __syncthreads();

@@ -299,6 +299,44 @@ def test_split_kernels_and_per_query_targets(scg, oracle_mod, mode, mc, kc):
     g.close()
 
 
+def test_many_ties_at_the_rth_distance(scg, oracle_mod):
+    """Base rows repeated 150 times (identical cells and codes, so identical
+    ADC distances in every arithmetic form): the R-th distance falls inside a
+    group of more equal distances than the merge's tie buffer holds.  The R
+    best are still the (distance, id) order -- the oracle's in the exact form,
+    the smallest ids of each tied group in the fast form -- in the fused and
+    the split kernels."""
+    D, mc, kc, mp, kp = 32, 2, 16, 8, 256
+    rng = np.random.default_rng(91)
+    base = rng.integers(0, 256, (40, D)).astype(np.float32)
+    X = base[rng.permutation(np.repeat(np.arange(40), 150))]
+    Q = np.clip(base[:20] + rng.normal(0, 2, (20, D)), 0, 255).astype(np.float32)
+    cq, pq = W.train_codebooks(rng.integers(0, 256, (5000, D)).astype(np.float32), mc, kc, mp, kp, 3, seed=92)
+    cid, codes = O.encode((D, mc, kc, mp, kp), cq, pq, X)
+    L, pid, co, _ = O.distribution(O.IMI, kc, mc, 0, cid, codes)
+    # rows with the same cell and codes have the same distance in every form
+    key = np.concatenate([np.asarray(cid).reshape(X.shape[0], -1).astype(np.int64),
+                          np.asarray(codes).reshape(X.shape[0], -1).astype(np.int64)], 1)
+    ix = O.Index(D, mc, kc, mp, kp, cq, pq, L, pid, co)
+    g = gpu_index(scg, D, mc, kc, mp, kp, cq, pq, L, pid, co)
+    for split in (True, False):
+        g.set_kernel_split(split)
+        for R, T in ((100, 3000), (230, 5000)):
+            check_against_oracle(ix, g, O.IMI, Q, R, 1 << 20, T)
+            ids, d, _ = g.search(MODES[O.IMI], Q, R, 1 << 20, T, precision=scg.FAST)
+            for i in range(Q.shape[0]):
+                # within each run of equal distances the ids ascend, and a
+                # run cut at the R-th place holds its group's smallest ids
+                for v in np.unique(d[i]):
+                    sel = ids[i][d[i] == v]
+                    assert (np.diff(sel) > 0).all()
+                    grp = np.nonzero(np.isin(key.view([("", key.dtype)] * key.shape[1]).ravel(),
+                                             key[sel].view([("", key.dtype)] * key.shape[1]).ravel()))[0]
+                    assert np.array_equal(sel, grp[: sel.size]), (i, v)
+    g.set_kernel_split(True)
+    g.close()
+
+
 def test_pool_overflow_reruns_fused(scg, oracle_mod):
     """Long visited lists (hundreds of cells per query) overflow the split
     kernels' shared pool area; the batch is then searched by the fused
