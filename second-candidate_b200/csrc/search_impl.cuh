@@ -272,6 +272,7 @@ struct QState {
     uint64_t thr;
     uint32_t next_flat;  // next unclaimed candidate of the scan (shared claims)
     int top_sorted;      // top[0..ncur) is already in (distance, id) order
+    double dens_est;     // candidates per cell seen by this CTA's last query
     uint32_t pool_off, pool_cap;  // the query's visited-list region (selection kernel)
 };
 
@@ -943,6 +944,7 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
     const int bsI = kp * mp / a.mc;  // dot_cr block of one coarse centroid
     const double avg_density = (double)a.N / (double)(a.ncells ? a.ncells : 1);
 
+    if (tid == 0) st.dens_est = 0.0;
     for (;;) {
         if (tid == 0) s_q = atomicAdd(a.qcounter, 1);
         __syncthreads();
@@ -1106,7 +1108,11 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
             uint32_t tau_prev = 0;
             const uint32_t lo_key = f2o(__fadd_rn(L.a(0), L.b(0)));
             const uint32_t hi_key = f2o(__fadd_rn(L.a(L.kA - 1), L.b(L.kB - 1)));
-            uint64_t target = (uint64_t)(c0 / 8.0);
+            // first round: an eighth of the cells the density of this CTA's
+            // previous query (else the index average) predicts; the visited
+            // set does not depend on the round sizes
+            const double dloc = st.dens_est > 1e-9 ? st.dens_est : (avg_density > 1e-9 ? avg_density : 1e-9);
+            uint64_t target = (uint64_t)((T > 0 ? (double)T : 1.0) / dloc / 8.0);
             if (target < 64) target = 64;
             if (target > 1024) target = 1024;
             if (sc) target += 1;
@@ -1226,6 +1232,7 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
                     atomicOr(a.status, ST_ITER_CAP);
                 }
             }
+            if (tid == 0 && Ncell > 0 && Ssum > 0) st.dens_est = (double)Ssum / (double)Ncell;
             __syncthreads();
             const bool qerr = st.err != 0;
             PHASE_MARK(1);  // staircase rounds
