@@ -907,7 +907,7 @@ __device__ uint32_t block_kth_hi(const uint64_t *keys, int n, int k, uint32_t *h
 #endif
 // ... of the selection-only kernel (part 1) and of the scan-only kernel (part 2).
 #ifndef SCG_SELECT_MIN_BLOCKS
-#define SCG_SELECT_MIN_BLOCKS 3
+#define SCG_SELECT_MIN_BLOCKS 5
 #endif
 #ifndef SCG_SCAN_MIN_BLOCKS
 #define SCG_SCAN_MIN_BLOCKS 4
