@@ -250,24 +250,26 @@ int reserve_search(scg_index *h, Workspace *ws, int mode, int grid) {
 // entries (or fewer when T, w or N bound its list below that: each visited
 // non-empty cell holds a candidate, so a list has at most min(T, w, N) cells
 // plus its closing prefix); longer lists take a range of a shared overflow
-// area.  Should that run out, the batch is searched again by the fused
-// kernel.
+// area (128 entries per query with per-query targets, whose long lists the
+// host cannot bound).  Should that run out, the batch is searched again by
+// the fused kernel.
 constexpr int64_t POOL_SLOT = 128;
 
-static void pool_dims(const scg_index *h, const scg_search_params *p, int nq, int64_t *stride, int64_t *over) {
+static void pool_dims(const scg_index *h, const scg_search_params *p, int nq, bool per_query_T, int64_t *stride,
+                      int64_t *over) {
     int64_t b = POOL_SLOT - 1;
     if (p) {
-        b = std::min<int64_t>(b, p->T > 0 ? (int64_t)p->T : 1);
+        if (!per_query_T) b = std::min<int64_t>(b, p->T > 0 ? (int64_t)p->T : 1);
         b = std::min<int64_t>(b, p->w > 0 ? (int64_t)p->w : 1);
     }
     b = std::min<int64_t>(b, h->N > 0 ? h->N : 1);
     *stride = b + 1;
-    *over = std::max<int64_t>(65536, 16 * (int64_t)nq);
+    *over = std::max<int64_t>(65536, (per_query_T ? 128 : 16) * (int64_t)nq);
 }
 
 int reserve_pool(scg_index *h, Workspace *ws, int nq) {
     int64_t stride, over;
-    pool_dims(h, nullptr, nq, &stride, &over);
+    pool_dims(h, nullptr, nq, false, &stride, &over);
     int rc;
     if ((rc = ws->qmeta.ensure(sizeof(QMeta) * (size_t)nq))) return rc;
     if ((rc = ws->pool_cell.ensure(4 * (size_t)(stride * nq + over)))) return rc;
@@ -321,10 +323,9 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     const int upl = h->tuned_upl[scan_form(p->precision) == SCG_FAST ? 1 : 0];
     const int *Tq = rb ? nullptr : h->d_Tq;
     // split kernels (selection, then a lighter scan at higher occupancy)
-    // unless per-query targets make the visited-list bound unknown here
     int64_t stride = 0, over = 0;
-    pool_dims(h, p, nq, &stride, &over);
-    const bool split = allow_split && h->split && !Tq && stride * (int64_t)nq + over < (1ll << 32);
+    pool_dims(h, p, nq, Tq != nullptr, &stride, &over);
+    const bool split = allow_split && h->split && stride * (int64_t)nq + over < (1ll << 32);
     auto grid_of = [&](int part) {
         int g = h->num_sms * search_max_blocks_per_sm(p->mode, h->kc, h->mp, h->kp, upl, part);
         return std::max(1, std::min(g, nq));

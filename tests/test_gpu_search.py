@@ -250,8 +250,8 @@ def test_host_path_chunks_equal_device_path(scg, oracle_mod):
 @pytest.mark.parametrize("mode,mc,kc", [(O.IVFADC, 1, 64), (O.IMI, 2, 48), (O.SC, 1, 48)])
 def test_split_kernels_and_per_query_targets(scg, oracle_mod, mode, mc, kc):
     """Selection and scan as two kernels (the default) give exactly the fused
-    kernel's results; per-query candidate targets (device array, fused
-    kernel) give, for each query, the result of a call with that T."""
+    kernel's results; per-query candidate targets (device array; split and
+    fused kernels) give, for each query, the result of a call with that T."""
     import torch
     D, mp, kp = 64, 8, 256
     mix = W.Mixture(D, 16, 20.0, "u8", seed=61 + mode)
@@ -288,10 +288,17 @@ def test_split_kernels_and_per_query_targets(scg, oracle_mod, mode, mc, kc):
     ds = torch.empty(nq, dtype=torch.int32, device="cuda")
     torch.cuda.synchronize()
     g.set_query_targets(dT.data_ptr())
+    g.set_kernel_split(False)
+    g.search_device(m, dQ.data_ptr(), nq, R, w, 999, di.data_ptr(), dd.data_ptr(), ds.data_ptr(), precision=scg.FAST)
+    torch.cuda.synchronize()
+    fused = (di.cpu().numpy().reshape(nq, R), dd.cpu().numpy().reshape(nq, R), ds.cpu().numpy())
+    g.set_kernel_split(True)
     g.search_device(m, dQ.data_ptr(), nq, R, w, 999, di.data_ptr(), dd.data_ptr(), ds.data_ptr(), precision=scg.FAST)
     g.set_query_targets(None)
     torch.cuda.synchronize()
     ids, d, sums = di.cpu().numpy().reshape(nq, R), dd.cpu().numpy().reshape(nq, R), ds.cpu().numpy()
+    for x, y in zip((ids, d, sums), fused):
+        assert np.array_equal(x, y)
     for T in np.unique(Ts):
         rows = np.nonzero(Ts == T)[0]
         ai, ad, asum = g.search(m, Q[rows], R, w, int(T), precision=scg.FAST)
