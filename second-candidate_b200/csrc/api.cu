@@ -667,6 +667,11 @@ int scg_search_device(scg_index *h, const scg_search_params *p, const float *dQ,
     return run_search(h, &h->ws, nullptr, p, dQ, nq, d_ids, d_dists, d_sums, s, true);
 }
 
+// Smallest chunk of the host-buffer search (at most 4 chunks per batch).
+#ifndef SCG_HOST_CHUNK_MIN
+#define SCG_HOST_CHUNK_MIN 1024
+#endif
+
 int scg_search(scg_index *h, const scg_search_params *p, const float *Q, int nq, int *ids, float *dists, int *sums) {
     int rc;
     if ((rc = check_ready(h))) return rc;
@@ -683,10 +688,21 @@ int scg_search(scg_index *h, const scg_search_params *p, const float *Q, int nq,
     if ((rc = h->ws.nvis.ensure(sizeof(int) * (size_t)nq))) return rc;
     if ((rc = h->ws.empty.ensure(sizeof(int) * (size_t)nq))) return rc;
     // The batch runs in chunks alternating over two streams, so that the
-    // copies of one chunk overlap the search of another.  All chunks are
-    // enqueued before the first copy-out (a copy into pageable memory waits
-    // for its stream).
-    const int nch = nq >= 4096 ? 4 : (nq >= 1024 ? 2 : 1);
+    // copies of one chunk overlap the search of another.  Results go to
+    // page-locked caller buffers right after each chunk; a copy into pageable
+    // memory waits for its stream, so there every chunk is enqueued before
+    // the first copy-out.
+    auto pinned = [](const void *ptr) {
+        if (!ptr) return true;
+        cudaPointerAttributes at;
+        if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return at.type == cudaMemoryTypeHost;
+    };
+    const bool eager_out = pinned(ids) && pinned(dists) && pinned(sums);
+    const int nch = std::max(1, std::min(4, nq / SCG_HOST_CHUNK_MIN));
     const int per = (nq + nch - 1) / nch;
     size_t off_b[8];
     size_t total = 0;
@@ -719,8 +735,17 @@ int scg_search(scg_index *h, const scg_search_params *p, const float *Q, int nq,
                                  cudaMemcpyDeviceToDevice, s));
         SCG_CUDA(cudaMemcpyAsync(h->ws.empty.as<int>() + q0, rb.empty, sizeof(int) * (size_t)n,
                                  cudaMemcpyDeviceToDevice, s));
+        if (eager_out) {
+            SCG_CUDA(cudaMemcpyAsync(ids + (size_t)q0 * R, h->ids.as<int>() + (size_t)q0 * R,
+                                     sizeof(int) * (size_t)n * R, cudaMemcpyDeviceToHost, s));
+            SCG_CUDA(cudaMemcpyAsync(dists + (size_t)q0 * R, h->dists.as<float>() + (size_t)q0 * R,
+                                     sizeof(float) * (size_t)n * R, cudaMemcpyDeviceToHost, s));
+            if (sums)
+                SCG_CUDA(cudaMemcpyAsync(sums + q0, h->sums.as<int>() + q0, sizeof(int) * (size_t)n,
+                                         cudaMemcpyDeviceToHost, s));
+        }
     }
-    for (int c = 0; c < nch; c++) {
+    for (int c = 0; c < nch && !eager_out; c++) {
         const int q0 = c * per, n = std::min(per, nq - q0);
         cudaStream_t s = ss[c & 1];
         SCG_CUDA(cudaMemcpyAsync(ids + (size_t)q0 * R, h->ids.as<int>() + (size_t)q0 * R, sizeof(int) * (size_t)n * R,

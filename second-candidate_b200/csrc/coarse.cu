@@ -102,8 +102,19 @@ __global__ void __launch_bounds__(CS_THREADS) k_coarse_prefix(CoarseArgs a) {
     if (M > a.max_prefix) M = a.max_prefix;
     uint32_t vm = 0xffffffffu;
     if (M < a.kc) {
-        // vm = the M-th smallest high word (binary search on the value)
-        uint32_t lo = 0, hi = 0xffffffffu;
+        // vm = the M-th smallest high word (binary search on the value,
+        // between the list's smallest and largest high words)
+        uint32_t lo = 0xffffffffu, hi = 0;
+#pragma unroll
+        for (int r = 0; r < P; r++) {
+            if (v[r] != ~0ull) {
+                const uint32_t hw = (uint32_t)(v[r] >> 32);
+                lo = hw < lo ? hw : lo;
+                hi = hw > hi ? hw : hi;
+            }
+        }
+        lo = __reduce_min_sync(FULL, lo);
+        hi = __reduce_max_sync(FULL, hi);
         while (lo < hi) {
             const uint32_t mid = lo + ((hi - lo) >> 1);
             int cnt = 0;

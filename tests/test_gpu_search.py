@@ -244,6 +244,13 @@ def test_host_path_chunks_equal_device_path(scg, oracle_mod):
             assert np.array_equal(sums, ds.cpu().numpy())
             nv2, em2 = g.last_query_stats(nq)
             assert np.array_equal(nvis, nv2) and np.array_equal(empty, em2)
+            # page-locked result buffers: each chunk's results are copied out
+            # right after its search
+            pi = torch.empty((nq, 20), dtype=torch.int32).pin_memory().numpy()
+            pd = torch.empty((nq, 20), dtype=torch.float32).pin_memory().numpy()
+            ps = torch.empty(nq, dtype=torch.int32).pin_memory().numpy()
+            g.search(1, Q, 20, 1 << 20, 1500, precision=prec, out=(pi, pd, ps))
+            assert np.array_equal(pi, ids) and np.array_equal(pd, d) and np.array_equal(ps, sums)
     g.close()
 
 
