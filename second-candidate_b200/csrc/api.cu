@@ -373,6 +373,7 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
         ca.Tq = rb ? nullptr : h->d_Tq;
         ca.T = p->T;
         ca.avg_density = (double)h->N / (double)(h->ncells ? h->ncells : 1);
+        ca.dens_acc = h->dens.as<unsigned long long>();
         ca.max_prefix = 1024;
         ca.width = coarse_sort_width(h->kc);
         ca.out = b.slist;
@@ -414,6 +415,7 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     sa.out_nvis = b.nvis; sa.out_empty = b.empty;
     sa.status = ws->status.as<int>();
     sa.phase_cycles = nullptr;
+    sa.dens_acc = h->dens.as<unsigned long long>();
     if (ws->phase_on) {
         if ((rc = ws->phase.ensure(sizeof(long long) * 16))) return rc;
         SCG_CUDA(cudaMemsetAsync(ws->phase.p, 0, sizeof(long long) * 16, s));
@@ -577,6 +579,7 @@ int scg_load_csr(scg_index *h, const int *L, const int *pid, const uint8_t *code
     h->N = N;
     h->ncells = ncells;
     h->have_csr = true;
+    if (h->dens.p) SCG_CUDA(cudaMemset(h->dens.p, 0, 16));
     h->have_vterm = false;
     return SCG_OK;
 }
@@ -650,6 +653,8 @@ int scg_precompute(scg_index *h) {
                        h->norm_c.as<float>(), h->norm_r.as<float>(), h->dot_cr.as<float>(), h->stream);
     SCG_CUDA(cudaGetLastError());
     SCG_CUDA(cudaStreamSynchronize(h->stream));
+    if ((rc = h->dens.ensure(16))) return rc;
+    SCG_CUDA(cudaMemset(h->dens.p, 0, 16));
     h->precomputed = true;
     h->have_vterm = false;
     return SCG_OK;
@@ -1031,6 +1036,7 @@ int scg_build_index(scg_index *h, const float *dX, int64_t n, int nc, void *stre
     h->N = n;
     h->ncells = ncells;
     h->have_csr = true;
+    if (h->dens.p) SCG_CUDA(cudaMemset(h->dens.p, 0, 16));
     h->have_vterm = false;
     return SCG_OK;
 }

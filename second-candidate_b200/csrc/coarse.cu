@@ -7,9 +7,10 @@
 // up to 8192, one block: k_coarse_prefix_block): the keys
 // (ordered float of q_part + diff_qc, << 32 | centroid id, so equal keys go
 // by id) sit 32 per lane at most; a binary search over the high words finds
-// vm, the M-th smallest (M from the query's candidate target, the same rule
-// the fused kernel uses), every key with high word <= vm is compacted through
-// shared memory and sorted by a register bitonic network (register swaps for
+// vm, the M-th smallest (M from the query's candidate target and the cell
+// density seen so far, prefix_density), every key with high word <= vm is
+// compacted through shared memory and sorted by a register bitonic network
+// (register swaps for
 // partner distances >= 32, warp shuffles below).  Per list the kernel writes
 // the sorted prefix, its length and the smallest high word after it; the
 // fused kernel then treats the prefix exactly as its own radix-selected
@@ -21,6 +22,18 @@ namespace scg {
 namespace {
 
 constexpr int CS_THREADS = 128;  // 4 warps, one list each
+
+// Candidates per cell for the prefix length rule: what the selection kernel
+// has seen on this index so far (cells near queries are denser than the
+// average), else N / cells.  A prefix too short for a query only costs that
+// query a complete sort inside the selection kernel.
+__device__ __forceinline__ double prefix_density(const CoarseArgs &a) {
+    if (a.dens_acc) {
+        const unsigned long long cells = __ldcg(a.dens_acc + 1);
+        if (cells > 0) return (double)__ldcg(a.dens_acc) / (double)cells;
+    }
+    return a.avg_density;
+}
 constexpr int CS_CAP = 1024;     // keys per list
 
 __device__ __forceinline__ uint64_t shfl_xor64(uint64_t v, int m) {
@@ -95,7 +108,8 @@ __global__ void __launch_bounds__(CS_THREADS) k_coarse_prefix(CoarseArgs a) {
     }
     // prefix length rule of the fused kernel
     const int T = a.Tq ? a.Tq[q] : a.T;
-    const double c0 = (T > 0 ? (double)T : 1.0) / (a.avg_density > 1e-9 ? a.avg_density : 1e-9);
+    const double dens = prefix_density(a);
+    const double c0 = (T > 0 ? (double)T : 1.0) / (dens > 1e-9 ? dens : 1e-9);
     int M = 1;
     while (M < 4 * (int)sqrt(c0) + 1) M <<= 1;
     if (M < 128) M = 128;
@@ -188,7 +202,8 @@ __global__ void __launch_bounds__(256) k_coarse_prefix_block(CoarseArgs a) {
         v[r] = i < a.kc ? (((uint64_t)f2o(__fadd_rn(base, row[i])) << 32) | (uint32_t)i) : ~0ull;
     }
     const int T = a.Tq ? a.Tq[q] : a.T;
-    const double c0 = (T > 0 ? (double)T : 1.0) / (a.avg_density > 1e-9 ? a.avg_density : 1e-9);
+    const double dens = prefix_density(a);
+    const double c0 = (T > 0 ? (double)T : 1.0) / (dens > 1e-9 ? dens : 1e-9);
     int M = 1;
     while (M < 4 * (int)sqrt(c0) + 1) M <<= 1;
     if (M < 128) M = 128;

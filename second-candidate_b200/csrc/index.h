@@ -82,6 +82,9 @@ struct scg_index {
     int cap_rec = 131072;
     const int *d_Tq = nullptr;
     scg::DevBuf cq, pq, norm_c, norm_r, dot_cr, off, pid, codes, raw, vterm;
+    // candidates and cells seen by the selection so far (u64 x 2): the
+    // coarse prefix length rule uses their ratio instead of N / cells
+    scg::DevBuf dens;
     bool have_vterm = false;
     int64_t raw_rows = 0;   // rows of raw vectors loaded (0: none)
     bool raw_u8 = false;    // raw vectors held as uint8

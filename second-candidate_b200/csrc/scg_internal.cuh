@@ -117,6 +117,7 @@ struct SearchArgs {
     int *out_sum, *out_nvis, *out_empty;
     int *status;
     long long *phase_cycles;  // optional [16] counters
+    unsigned long long *dens_acc;  // optional: adds each query's (candidates, cells)
 };
 
 // part 0: fused selection + scan; 1: selection only; 2: scan only.
@@ -164,6 +165,7 @@ struct CoarseArgs {
     const int *Tq;       // optional per-query T
     int T;
     double avg_density;  // N / cells, for the prefix length rule
+    const unsigned long long *dens_acc;  // optional: candidates, cells seen so far
     int max_prefix;
     int width;           // stride of a list in out
     uint64_t *out;       // [nq][lists][width] sorted prefix keys

@@ -1232,7 +1232,13 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
                     atomicOr(a.status, ST_ITER_CAP);
                 }
             }
-            if (tid == 0 && Ncell > 0 && Ssum > 0) st.dens_est = (double)Ssum / (double)Ncell;
+            if (tid == 0 && Ncell > 0 && Ssum > 0) {
+                st.dens_est = (double)Ssum / (double)Ncell;
+                if (a.dens_acc) {
+                    atomicAdd(&a.dens_acc[0], (unsigned long long)Ssum);
+                    atomicAdd(&a.dens_acc[1], (unsigned long long)Ncell);
+                }
+            }
             __syncthreads();
             const bool qerr = st.err != 0;
             PHASE_MARK(1);  // staircase rounds
