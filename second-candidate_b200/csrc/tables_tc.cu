@@ -151,13 +151,22 @@ __device__ __forceinline__ void pack8(const float (&x)[8], uint4 &hi, uint4 &lo)
 template <int FMT, bool SPLIT>
 __device__ __forceinline__ void stage(const float *__restrict__ src, int nrows, size_t ld, int len, int k0, int rows,
                                       int ngroups, unsigned char *hi, unsigned char *lo) {
+    // whole groups of 8 load as two float4 when every row starts 16-byte aligned
+    const bool vec = ((reinterpret_cast<uintptr_t>(src) & 15) == 0) && (ld % 4 == 0);
     for (int u = threadIdx.x; u < rows * ngroups; u += TC_THREADS) {
         const int r = u % rows, g = u / rows;
         float x[8];
         const int kb = k0 + g * 8;
         const float *p = src + (size_t)r * ld + kb;
+        if (vec && r < nrows && kb + 8 <= len) {
+            const float4 v0 = __ldg(reinterpret_cast<const float4 *>(p));
+            const float4 v1 = __ldg(reinterpret_cast<const float4 *>(p) + 1);
+            x[0] = v0.x; x[1] = v0.y; x[2] = v0.z; x[3] = v0.w;
+            x[4] = v1.x; x[5] = v1.y; x[6] = v1.z; x[7] = v1.w;
+        } else {
 #pragma unroll
-        for (int j = 0; j < 8; j++) x[j] = (r < nrows && kb + j < len) ? __ldg(p + j) : 0.0f;
+            for (int j = 0; j < 8; j++) x[j] = (r < nrows && kb + j < len) ? __ldg(p + j) : 0.0f;
+        }
         uint4 h, l;
         pack8<FMT, SPLIT>(x, h, l);
         const size_t off = ((size_t)g * rows + r) * 16;
