@@ -273,6 +273,7 @@ struct QState {
     uint32_t next_flat;  // next unclaimed candidate of the scan (shared claims)
     int top_sorted;      // top[0..ncur) is already in (distance, id) order
     double dens_est;     // candidates per cell seen by this CTA's last query
+    uint32_t tau_gap;    // first-round tau - lowest key of that query (0: none)
     uint32_t pool_off, pool_cap;  // the query's visited-list region (selection kernel)
 };
 
@@ -944,7 +945,10 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
     const int bsI = kp * mp / a.mc;  // dot_cr block of one coarse centroid
     const double avg_density = (double)a.N / (double)(a.ncells ? a.ncells : 1);
 
-    if (tid == 0) st.dens_est = 0.0;
+    if (tid == 0) {
+        st.dens_est = 0.0;
+        st.tau_gap = 0u;
+    }
     for (;;) {
         if (tid == 0) s_q = atomicAdd(a.qcounter, 1);
         __syncthreads();
@@ -1133,6 +1137,17 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
                     COUNT(8, 1);
                     if (lo > hi) lo = hi;
                     int it = 0;
+                    const uint32_t gap0 = st.tau_gap;
+                    if (round == 0 && gap0 != 0u && lo < hi) {
+                        // first probe where this CTA's previous query ended
+                        const uint32_t mid = (hi - lo > gap0) ? lo + gap0 : hi - 1;
+                        uint64_t c = staircase_count(L, mid, red);
+                        COUNT(9, 1);
+                        if (c >= target) hi = mid;
+                        else lo = mid + 1;
+                        if (c >= target && c <= thi) lo = hi;
+                        it++;
+                    }
                     while (lo < hi && it < 40) {
                         uint32_t mid = lo + ((hi - lo) >> 1);
                         uint64_t c = staircase_count(L, mid, red);
@@ -1147,6 +1162,7 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
                     }
                     const uint32_t tau = hi;
                     tau_prev = tau;
+                    if (round == 0 && tid == 0) st.tau_gap = tau - lo_key;
                     // row counts at tau and the new cells per row
                     uint32_t mycnt = 0;
                     const int per = (L.kA + NT - 1) / NT;
