@@ -22,6 +22,7 @@ ranks exit at once) on the same workload and prints the same line with
 "impl": "reference".
 """
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -459,6 +460,8 @@ def main():
     times, kern = [], []
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    gc.collect()
+    gc.disable()
     for _ in range(args.steps):
         flush.zero_()
         e0.record(stream)
@@ -468,6 +471,7 @@ def main():
         times.append(e0.elapsed_time(e1))
         kern.append(ix.last_timings())
     torch.cuda.synchronize()
+    gc.enable()
     clocks.mark(False)
     replicas.barrier()
     job_qps, total_ms = replicas.job_throughput(sum(times), nq * args.steps, device=dev)
@@ -529,7 +533,7 @@ def main():
         ix.set_phase_counters(False)
 
     # end to end through the public host-buffer entry point
-    e2e_qps, same = None, None
+    e2e_qps, same, e2e_ms = None, None, None
     if not args.no_e2e:
         # queries in and results out through pinned host buffers (the
         # caller's), reused every step
@@ -545,6 +549,8 @@ def main():
             hi = torch.empty(nq * R, dtype=torch.int32).pin_memory()
             hdd = torch.empty(nq * R, dtype=torch.float32).pin_memory()
             hs = torch.empty(nq, dtype=torch.int32).pin_memory()
+        gc.collect()
+        gc.disable()  # no collector pauses inside the timed calls
         for i in range(args.warmup + args.steps):
             flush.zero_()  # same cold-L2 start as the device-timed steps
             torch.cuda.synchronize()
@@ -562,7 +568,10 @@ def main():
             dt = time.perf_counter() - t0
             if i >= args.warmup:
                 e2e_times.append(dt)
+        gc.enable()
         e2e_qps = nq * len(e2e_times) / sum(e2e_times) * world
+        e2e_ms = {"mean": 1e3 * statistics.mean(e2e_times), "p50": 1e3 * statistics.median(e2e_times),
+                  "max": 1e3 * max(e2e_times)}
         same = bool(np.array_equal(hid, ids))
 
     line = {
@@ -593,7 +602,8 @@ def main():
                                 else "k_search (fused selection + ADC scan + top-R)"),
                      "alg_bytes_per_launch": alg_bytes},
         "e2e": {"value": e2e_qps, "unit": "queries/s", "h2d_bytes_per_step": int(nq * cfg["D"] * 4),
-                "d2h_bytes_per_step": int(nq * R * 8 + nq * 4), "same_ids_as_device_path": same},
+                "d2h_bytes_per_step": int(nq * R * 8 + nq * 4), "same_ids_as_device_path": same,
+                "step_ms": e2e_ms},
         # per step: tensor-core tables, query norms, coarse prefixes,
         # selection, scan (the fused kernel replaces the last two)
         "gpu_launches": (5 if split else 4) * args.steps,
