@@ -672,7 +672,8 @@ int scg_search_device(scg_index *h, const scg_search_params *p, const float *dQ,
     return run_search(h, &h->ws, nullptr, p, dQ, nq, d_ids, d_dists, d_sums, s, true);
 }
 
-// Smallest chunk of the host-buffer search (at most 4 chunks per batch).
+// Smallest chunk of the host-buffer search with pageable buffers (at most 4
+// chunks per batch).
 #ifndef SCG_HOST_CHUNK_MIN
 #define SCG_HOST_CHUNK_MIN 1024
 #endif
@@ -692,11 +693,12 @@ int scg_search(scg_index *h, const scg_search_params *p, const float *Q, int nq,
     if ((rc = h->sums.ensure(sizeof(int) * (size_t)nq))) return rc;
     if ((rc = h->ws.nvis.ensure(sizeof(int) * (size_t)nq))) return rc;
     if ((rc = h->ws.empty.ensure(sizeof(int) * (size_t)nq))) return rc;
-    // The batch runs in chunks alternating over two streams, so that the
-    // copies of one chunk overlap the search of another.  Results go to
-    // page-locked caller buffers right after each chunk; a copy into pageable
-    // memory waits for its stream, so there every chunk is enqueued before
-    // the first copy-out.
+    // With page-locked caller buffers the batch is one launch sequence on one
+    // stream between its two copies: the copies take about a tenth of the
+    // search, and smaller launches would each leave a tail of idle SMs.  With
+    // pageable buffers (staged copies that block the host) the batch runs in
+    // chunks alternating over two streams, every chunk enqueued before the
+    // first copy-out, so that staging overlaps the search of other chunks.
     auto pinned = [](const void *ptr) {
         if (!ptr) return true;
         cudaPointerAttributes at;
@@ -707,7 +709,8 @@ int scg_search(scg_index *h, const scg_search_params *p, const float *Q, int nq,
         return at.type == cudaMemoryTypeHost;
     };
     const bool eager_out = pinned(ids) && pinned(dists) && pinned(sums);
-    const int nch = std::max(1, std::min(4, nq / SCG_HOST_CHUNK_MIN));
+    const bool q_pinned = pinned(Q);
+    const int nch = (eager_out && q_pinned) ? 1 : std::max(1, std::min(4, nq / SCG_HOST_CHUNK_MIN));
     const int per = (nq + nch - 1) / nch;
     size_t off_b[8];
     size_t total = 0;

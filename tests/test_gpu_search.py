@@ -245,12 +245,14 @@ def test_host_path_chunks_equal_device_path(scg, oracle_mod):
             nv2, em2 = g.last_query_stats(nq)
             assert np.array_equal(nvis, nv2) and np.array_equal(empty, em2)
             # page-locked result buffers: each chunk's results are copied out
-            # right after its search
+            # right after its search; page-locked queries too: one chunk
             pi = torch.empty((nq, 20), dtype=torch.int32).pin_memory().numpy()
             pd = torch.empty((nq, 20), dtype=torch.float32).pin_memory().numpy()
             ps = torch.empty(nq, dtype=torch.int32).pin_memory().numpy()
-            g.search(1, Q, 20, 1 << 20, 1500, precision=prec, out=(pi, pd, ps))
-            assert np.array_equal(pi, ids) and np.array_equal(pd, d) and np.array_equal(ps, sums)
+            for qsrc in (Q, torch.from_numpy(Q).pin_memory().numpy()):
+                pi[:] = -7
+                g.search(1, qsrc, 20, 1 << 20, 1500, precision=prec, out=(pi, pd, ps))
+                assert np.array_equal(pi, ids) and np.array_equal(pd, d) and np.array_equal(ps, sums)
     g.close()
 
 
