@@ -23,14 +23,18 @@ namespace {
 
 constexpr int CS_THREADS = 128;  // 4 warps, one list each
 
-// Candidates per cell for the prefix length rule: what the selection kernel
-// has seen on this index so far (cells near queries are denser than the
-// average), else N / cells.  A prefix too short for a query only costs that
-// query a complete sort inside the selection kernel.
+// Candidates per cell for the prefix length rule: a quarter of what the
+// selection kernel has seen on this index so far (cells near queries are
+// denser than the average, but a query in a sparser region reaches further:
+// the quarter doubles the prefix), else N / cells.  A prefix too short for a
+// query only costs that query a complete sort inside the selection kernel.
 __device__ __forceinline__ double prefix_density(const CoarseArgs &a) {
     if (a.dens_acc) {
         const unsigned long long cells = __ldcg(a.dens_acc + 1);
-        if (cells > 0) return (double)__ldcg(a.dens_acc) / (double)cells;
+        if (cells > 0) {
+            const double d = 0.25 * (double)__ldcg(a.dens_acc) / (double)cells;
+            return d < a.avg_density ? a.avg_density : d;
+        }
     }
     return a.avg_density;
 }

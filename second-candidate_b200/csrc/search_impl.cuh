@@ -274,6 +274,7 @@ struct QState {
     int top_sorted;      // top[0..ncur) is already in (distance, id) order
     double dens_est;     // candidates per cell seen by this CTA's last query
     uint32_t tau_gap;    // first-round tau - lowest key of that query (0: none)
+    int tau_T;           // and its candidate target
     uint32_t pool_off, pool_cap;  // the query's visited-list region (selection kernel)
 };
 
@@ -948,6 +949,7 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
     if (tid == 0) {
         st.dens_est = 0.0;
         st.tau_gap = 0u;
+        st.tau_T = 0;
     }
     for (;;) {
         if (tid == 0) s_q = atomicAdd(a.qcounter, 1);
@@ -1137,7 +1139,9 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
                     COUNT(8, 1);
                     if (lo > hi) lo = hi;
                     int it = 0;
-                    const uint32_t gap0 = st.tau_gap;
+                    // a previous query with a target within 25% of this one
+                    const int tp = st.tau_T;
+                    const uint32_t gap0 = (4ll * (tp > T ? tp - T : T - tp) <= (long long)tp) ? st.tau_gap : 0u;
                     if (round == 0 && gap0 != 0u && lo < hi) {
                         // first probe where this CTA's previous query ended
                         const uint32_t mid = (hi - lo > gap0) ? lo + gap0 : hi - 1;
@@ -1162,7 +1166,10 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
                     }
                     const uint32_t tau = hi;
                     tau_prev = tau;
-                    if (round == 0 && tid == 0) st.tau_gap = tau - lo_key;
+                    if (round == 0 && tid == 0) {
+                        st.tau_gap = tau - lo_key;
+                        st.tau_T = T;
+                    }
                     // row counts at tau and the new cells per row
                     uint32_t mycnt = 0;
                     const int per = (L.kA + NT - 1) / NT;
