@@ -525,8 +525,8 @@ __device__ void sort_merge(uint64_t *top, const uint64_t *pend, int nb, int R, c
 }
 
 // Keeps the R smallest of top[0..ncur) and the pending entries.  Pending
-// entries hold (distance, CSR position); they become (distance, id) here,
-// where the id loads of a whole buffer are issued together.  A radix select
+// entries hold (distance, CSR position); the kept ones and those tied at the
+// R-th distance become (distance, id) here.  A radix select
 // over the distance words finds the R-th smallest distance v; every entry
 // below v is kept and the entries equal to v are taken in id order.  The top
 // list stays unsorted (the output step sorts it); st.thr becomes the R-th
@@ -537,16 +537,15 @@ __device__ void merge_topk(uint64_t *top, uint64_t *pend, uint64_t *tmp, uint32_
                            const int *pid, uint64_t *red, QState &st, int *status) {
     const int tid = threadIdx.x;
     const int na = st.ncur, nb = st.npend;
-    if (pid) {
-        for (int i = tid; i < nb; i += NT) {
-            uint64_t e = pend[i];
-            pend[i] = (e & 0xffffffff00000000ull) | (uint32_t)__ldg(pid + (uint32_t)e);
-        }
-    }
-    __syncthreads();
+    // (distance, id) of entry i: top entries carry ids already, pending ones
+    // carry CSR positions until they are kept (the id loads of the entries
+    // the merge drops are never issued)
+    auto as_id = [&](uint64_t e) -> uint64_t {
+        return pid ? (e & 0xffffffff00000000ull) | (uint32_t)__ldg(pid + (uint32_t)e) : e;
+    };
     const int n = na + nb;
     if (n <= R) {
-        for (int i = tid; i < nb; i += NT) top[na + i] = pend[i];
+        for (int i = tid; i < nb; i += NT) top[na + i] = as_id(pend[i]);
         __syncthreads();
         if (tid == 0) {
             st.ncur = n;
@@ -603,10 +602,10 @@ __device__ void merge_topk(uint64_t *top, uint64_t *pend, uint64_t *tmp, uint32_
     for (int i = tid; i < n; i += NT) {
         uint64_t e = i < na ? top[i] : pend[i - na];
         uint32_t hv = (uint32_t)(e >> 32);
-        if (hv < v) tmp[pos++] = e;
+        if (hv < v) tmp[pos++] = i < na ? e : as_id(e);
         else if (hv == v) {
             int slot = atomicAdd(&st.nties, 1);
-            if (slot < TIECAP) ties[slot] = e;
+            if (slot < TIECAP) ties[slot] = i < na ? e : as_id(e);
         }
     }
     __syncthreads();
@@ -614,7 +613,7 @@ __device__ void merge_topk(uint64_t *top, uint64_t *pend, uint64_t *tmp, uint32_
     if (resort) {
         // the tie buffer kept only some of the entries equal to v
         __syncthreads();
-        sort_merge(top, pend, nb, R, nullptr, st);
+        sort_merge(top, pend, nb, R, pid, st);
         return;
     }
     if (tid == 0) {
