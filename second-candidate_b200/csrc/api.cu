@@ -412,6 +412,7 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     sa.pcap = (uint32_t)pcap;
     sa.qcounter = ws->counter.as<int>();
     sa.out_ids = s_ids; sa.out_d = s_d; sa.out_sum = d_sums;
+    sa.shortlist = rr ? 1 : 0;
     sa.out_nvis = b.nvis; sa.out_empty = b.empty;
     sa.status = ws->status.as<int>();
     sa.phase_cycles = nullptr;

@@ -86,6 +86,7 @@ struct SearchArgs {
     int mode, dim, mc, kc, mp, kp, nq, R, w, T;
     int precision;
     int upl;                // candidates per lane per scan chunk: 2, 4 or 8
+    int shortlist;          // 1: the R best feed the exact re-rank, which orders them itself
     const int *Tq;          // optional per-query T
     const uint64_t *slist;  // optional coarse-list prefixes sorted ahead: [nq][lists][slist_w]
     const uint32_t *smeta;  // their lengths and next high words: [nq][lists][2]

@@ -1510,11 +1510,12 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
         }
         __syncthreads();
         PHASE_MARK(5);  // final merge
-        // (6) outputs: the R best sorted by (distance, id)
+        // (6) outputs: the R best sorted by (distance, id) (a shortlist for
+        // the exact re-rank in any order: the re-rank sorts it itself)
         {
             const bool qerr3 = st.err != 0;
             int keep = (qerr3 || nvis == 0) ? 0 : st.ncur;
-            if (keep > 1 && !st.top_sorted) {
+            if (keep > 1 && !st.top_sorted && !a.shortlist) {
                 const int k2 = next_pow2(keep);
                 for (int i = keep + tid; i < k2; i += NT) top[i] = ~0ull;
                 __syncthreads();
