@@ -490,6 +490,7 @@ def main():
     tables_ms = statistics.mean(k[0] for k in kern)
     select_ms = statistics.mean(k[3] for k in kern)
     scan_ms = statistics.mean(k[4] for k in kern)
+    rerank_ms = statistics.mean(k[2] for k in kern)
     split = scan_ms > 0
     alg_bytes = float(sums.astype(np.int64).sum() * cfg["mp"] + 8 * nvis.astype(np.int64).sum() + 4 * nq * R)
     hbm, _, peak_kind = peaks()
@@ -595,7 +596,7 @@ def main():
                        "what": "whole batch of %d queries" % nq},
         "batch_ms": {"p50": float(np.percentile(times, 50)), "p99": float(np.percentile(times, 99))},
         "kernels_ms": {"tables_and_prefix": tables_ms, "select_scan": search_ms, "select": select_ms,
-                       "scan": scan_ms},
+                       "scan": scan_ms, "rerank": rerank_ms},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
                      "kernel": ("k_search<.., 2> (ADC scan + top-R; selection runs as its own kernel)" if split

@@ -32,6 +32,39 @@ __device__ __forceinline__ float exact_dist(const float *__restrict__ q, const T
     return (float)dis;
 }
 
+__device__ __forceinline__ void acc(double &dis, float qv, float xv) {
+    const double tmp = (double)__fsub_rn(qv, xv);
+    dis = __dadd_rn(dis, __dmul_rn(tmp, tmp));
+}
+
+// The same sum with the row read 16 bytes at a time (rows 16-byte aligned,
+// dim a multiple of 16 bytes): the dimension order, hence the value, is
+// unchanged; one load brings 16 uint8 or 4 float elements.
+__device__ __forceinline__ float exact_dist_vec(const float *__restrict__ q, const uint8_t *__restrict__ x, int dim) {
+    double dis = 0.0;
+    const uint4 *xv = reinterpret_cast<const uint4 *>(x);
+    for (int c = 0; c < dim / 16; c++) {
+        const uint4 v = __ldg(xv + c);
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int j = 0; j < 16; j++) acc(dis, q[c * 16 + j], (float)((w[j >> 2] >> ((j & 3) * 8)) & 0xffu));
+    }
+    return (float)dis;
+}
+
+__device__ __forceinline__ float exact_dist_vec(const float *__restrict__ q, const float *__restrict__ x, int dim) {
+    double dis = 0.0;
+    const float4 *xv = reinterpret_cast<const float4 *>(x);
+    for (int c = 0; c < dim / 4; c++) {
+        const float4 v = __ldg(xv + c);
+        acc(dis, q[c * 4], v.x);
+        acc(dis, q[c * 4 + 1], v.y);
+        acc(dis, q[c * 4 + 2], v.z);
+        acc(dis, q[c * 4 + 3], v.w);
+    }
+    return (float)dis;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(RR_THREADS) k_rerank(const float *__restrict__ Q, int dim,
                                                        const T *__restrict__ raw, int64_t N,
@@ -43,13 +76,16 @@ __global__ void __launch_bounds__(RR_THREADS) k_rerank(const float *__restrict__
     float *qs = (float *)(rsm + (size_t)Lp * 8);      // [dim]
     const int q = blockIdx.x;
     for (int t = threadIdx.x; t < dim; t += RR_THREADS) qs[t] = Q[(size_t)q * dim + t];
+    // whole rows as 16-byte loads when every row starts 16-byte aligned
+    const bool vec = ((reinterpret_cast<uintptr_t>(raw) & 15) == 0) && ((dim * sizeof(T)) % 16 == 0);
     __syncthreads();
     for (int i = threadIdx.x; i < Lp; i += RR_THREADS) {
         uint64_t key = ~0ull;
         if (i < L) {
             const int id = sl_ids[(size_t)q * L + i];
             if (id >= 0 && id < N) {
-                const float d = exact_dist(qs, raw + (size_t)id * dim, dim);
+                const float d = vec ? exact_dist_vec(qs, raw + (size_t)id * dim, dim)
+                                    : exact_dist(qs, raw + (size_t)id * dim, dim);
                 key = ((uint64_t)f2o(d) << 32) | (uint32_t)id;
             } else if (id >= N) {
                 atomicOr(status, ST_BAD_ARG);
