@@ -38,16 +38,32 @@ __device__ __forceinline__ void acc(double &dis, float qv, float xv) {
 }
 
 // The same sum with the row read 16 bytes at a time (rows 16-byte aligned,
-// dim a multiple of 16 bytes): the dimension order, hence the value, is
-// unchanged; one load brings 16 uint8 or 4 float elements.
+// dim a multiple of 16 bytes), eight loads in flight per thread and the
+// query read as float4 from shared memory: the dimension order, hence the
+// value, is unchanged.
 __device__ __forceinline__ float exact_dist_vec(const float *__restrict__ q, const uint8_t *__restrict__ x, int dim) {
     double dis = 0.0;
     const uint4 *xv = reinterpret_cast<const uint4 *>(x);
-    for (int c = 0; c < dim / 16; c++) {
-        const uint4 v = __ldg(xv + c);
-        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+    const float4 *q4 = reinterpret_cast<const float4 *>(q);
+    const int n = dim / 16;
+    int c = 0;
+    for (; c < n; c += 8) {
+        uint4 v[8];
 #pragma unroll
-        for (int j = 0; j < 16; j++) acc(dis, q[c * 16 + j], (float)((w[j >> 2] >> ((j & 3) * 8)) & 0xffu));
+        for (int j = 0; j < 8; j++) v[j] = c + j < n ? __ldg(xv + c + j) : make_uint4(0, 0, 0, 0);
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            if (c + j >= n) break;
+            const uint32_t w[4] = {v[j].x, v[j].y, v[j].z, v[j].w};
+#pragma unroll
+            for (int g = 0; g < 4; g++) {
+                const float4 qq = q4[(c + j) * 4 + g];
+                acc(dis, qq.x, (float)(w[g] & 0xffu));
+                acc(dis, qq.y, (float)((w[g] >> 8) & 0xffu));
+                acc(dis, qq.z, (float)((w[g] >> 16) & 0xffu));
+                acc(dis, qq.w, (float)(w[g] >> 24));
+            }
+        }
     }
     return (float)dis;
 }
@@ -55,12 +71,21 @@ __device__ __forceinline__ float exact_dist_vec(const float *__restrict__ q, con
 __device__ __forceinline__ float exact_dist_vec(const float *__restrict__ q, const float *__restrict__ x, int dim) {
     double dis = 0.0;
     const float4 *xv = reinterpret_cast<const float4 *>(x);
-    for (int c = 0; c < dim / 4; c++) {
-        const float4 v = __ldg(xv + c);
-        acc(dis, q[c * 4], v.x);
-        acc(dis, q[c * 4 + 1], v.y);
-        acc(dis, q[c * 4 + 2], v.z);
-        acc(dis, q[c * 4 + 3], v.w);
+    const float4 *q4 = reinterpret_cast<const float4 *>(q);
+    const int n = dim / 4;
+    for (int c = 0; c < n; c += 8) {
+        float4 v[8];
+#pragma unroll
+        for (int j = 0; j < 8; j++) v[j] = c + j < n ? __ldg(xv + c + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            if (c + j >= n) break;
+            const float4 qq = q4[c + j];
+            acc(dis, qq.x, v[j].x);
+            acc(dis, qq.y, v[j].y);
+            acc(dis, qq.z, v[j].z);
+            acc(dis, qq.w, v[j].w);
+        }
     }
     return (float)dis;
 }
@@ -73,7 +98,7 @@ __global__ void __launch_bounds__(RR_THREADS) k_rerank(const float *__restrict__
                                                        int *__restrict__ status) {
     extern __shared__ __align__(16) unsigned char rsm[];
     uint64_t *keys = (uint64_t *)rsm;                 // [Lp]
-    float *qs = (float *)(rsm + (size_t)Lp * 8);      // [dim]
+    float *qs = (float *)(rsm + (((size_t)Lp * 8 + 15) & ~(size_t)15));  // [dim], 16-byte aligned
     const int q = blockIdx.x;
     for (int t = threadIdx.x; t < dim; t += RR_THREADS) qs[t] = Q[(size_t)q * dim + t];
     // whole rows as 16-byte loads when every row starts 16-byte aligned
@@ -124,7 +149,7 @@ __global__ void __launch_bounds__(RR_THREADS) k_rerank(const float *__restrict__
 size_t rerank_smem_bytes(int L, int dim) {
     int Lp = 1;
     while (Lp < L) Lp <<= 1;
-    return (size_t)Lp * 8 + (size_t)dim * 4;
+    return (((size_t)Lp * 8 + 15) & ~(size_t)15) + (size_t)dim * 4;
 }
 
 int launch_rerank(const float *Q, int nq, int dim, const void *raw, int raw_u8, int64_t N, const int *sl_ids, int L,
