@@ -143,12 +143,13 @@ int scg_search_graph(scg_index *h, const scg_search_params *p, const float *dQ, 
  * search slots (SCG_ERR_CAP names the largest nq for the index), and each
  * query may enumerate at most 8192 cells and keep 8192 scan survivors
  * (SCG_ERR_CAP otherwise).  The first call on a device looks up the array's
- * device address; make that first call before any stream capture.  Every
- * call shares the one array: calls that overlap on the GPU (other streams,
- * other threads, the same device) race and must be serialised by the caller.
- * The tensor-core forms (SCG_FAST, SCG_BF16, SCG_FP16) need the per-vector
- * term, built by an earlier call of scg_search or scg_search_device in one of
- * them. */
+ * device address; make that first call before any stream capture.  Like
+ * scg_search_device, every call synchronises `stream` to read the kernels'
+ * status word before it returns.  Every call shares the one array: calls that
+ * overlap on the GPU (other streams, other threads, the same device) race and
+ * must be serialised by the caller.  The tensor-core forms (SCG_FAST,
+ * SCG_BF16, SCG_FP16) need the per-vector term, built by an earlier call of
+ * scg_search or scg_search_device in one of them (SCG_ERR_STATE otherwise). */
 int scg_search_device_noalloc(scg_index *h, const scg_search_params *p, const float *dQ, int nq,
                               int *d_ids, float *d_dists, int *d_sums, void *stream);
 

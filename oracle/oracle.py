@@ -17,7 +17,6 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libscref.so")
-REF_TREE = "/root/reference"
 
 IVFADC, IMI, SC = 0, 1, 2
 ORDER_HEAP, ORDER_EXACT = 0, 1
@@ -30,10 +29,11 @@ _u16p = ctypes.POINTER(ctypes.c_ushort)
 
 def build(ref=True):
     """Builds liboracle.so, and the reference harness when the reference tree
-    is present (it is only present where the sources can be read)."""
+    is readable (oracle/Makefile decides: SCG_REFERENCE_TREE or its default;
+    without the tree an existing _ref/libscref.so is kept as it is)."""
     targets = ["oracle"]
-    if ref and os.path.isdir(REF_TREE):
-        targets.append("ref")
+    if ref:
+        targets.append("ref-if-present")
     subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
 
 
@@ -235,6 +235,7 @@ def ref():
             raise FileNotFoundError(REF_SO)
         _ref = ctypes.CDLL(REF_SO)
         _ref.ref_search_batch.restype = ctypes.c_int
+        _ref.ref_search_batch_ex.restype = ctypes.c_int
         _ref.ref_search_one.restype = ctypes.c_int
         _ref.ref_encode.restype = ctypes.c_int
     return _ref
@@ -274,18 +275,22 @@ def ref_search_one(ix, mode, q, R, w, T, real_dist=False):
     return dict(ids=ids[:s].copy(), dist=dist[:s].copy(), sum=s, empty=e.value)
 
 
-def ref_search_batch(ix, mode, Q, R, w, T, nthreads=0, real_dist=False):
-    """Reference search over a query batch with OpenMP threads.
-    Returns (ids[nq,R], dist[nq,R], sums[nq], seconds)."""
+def ref_search_batch(ix, mode, Q, R, w, T, nthreads=0, real_dist=False, Tq=None, M=None):
+    """Reference search over a query batch with OpenMP threads; Tq: optional
+    per-query candidate targets; M: the coarse-list argument of search_multi2
+    / search_mr_ivf (default kc).  Returns (ids[nq,R], dist[nq,R], sums[nq],
+    seconds)."""
     Q = np.ascontiguousarray(Q, np.float32).reshape(-1, ix.dim)
     nq = Q.shape[0]
     ids = np.zeros((nq, R), np.int32)
     dist = np.zeros((nq, R), np.float32)
     sums = np.zeros(nq, np.int32)
     sec = ctypes.c_double(0.0)
-    rc = ref().ref_search_batch(mode, *_ref_index_args(ix), _p(Q, _f32p), nq, R, w, T,
-                                1 if real_dist else 0, nthreads, _p(ids, _i32p),
-                                _p(dist, _f32p), _p(sums, _i32p), ctypes.byref(sec))
+    tq = None if Tq is None else np.ascontiguousarray(Tq, np.int32)
+    rc = ref().ref_search_batch_ex(mode, *_ref_index_args(ix), _p(Q, _f32p), nq, R, w, T,
+                                   _p(tq, _i32p) if tq is not None else None, ix.kc if M is None else M,
+                                   1 if real_dist else 0, nthreads, _p(ids, _i32p),
+                                   _p(dist, _f32p), _p(sums, _i32p), ctypes.byref(sec))
     if rc != 0:
         raise RuntimeError("ref_search_batch failed")
     return ids, dist, sums, sec.value

@@ -97,7 +97,7 @@ static SCQuery *as_sc(OSC &o) { return &o; }
  * (0 IVFADC query.h:202, 1 IMI multi_query.h:62, 2 SC sc_query.h:60).
  * Returns sum; result/dist are allocated by the reference. */
 static int run_one(PQQuery &obj, MultiQuery *mq, SCQuery *sq, int mode, Scratch &s, float *q,
-                   int R, int w, int T, int kc, bool real_dist, int *&result, float *&dist,
+                   int R, int w, int T, int M, bool real_dist, int *&result, float *&dist,
                    int *empty) {
     int sum = 0;
     float *v_tmp = s.v_tmp.data(), *q2 = s.q2.data();
@@ -112,12 +112,12 @@ static int run_one(PQQuery &obj, MultiQuery *mq, SCQuery *sq, int mode, Scratch 
         int e = 0; double t1 = 0, t2 = 0;
         mq->search_multi2(q, v_tmp, dist, q2, s.tmp.data(), result,
                           hid1, hid2, hid3, hid4, s1, s2, prebuck, cache, trav,
-                          sum, R, w, T, kc, e, t1, t2, real_dist, false);
+                          sum, R, w, T, M, e, t1, t2, real_dist, false);
         if (empty) *empty = e;
     } else if (mode == 2 && sq) {
         sq->search_mr_ivf(q, v_tmp, dist, s.tmp.data(), result,
                           hid1, hid2, hid3, hid4, s1, s2, prebuck, cache, trav,
-                          sum, R, w, T, kc, real_dist, false);
+                          sum, R, w, T, M, real_dist, false);
     }
     return sum;
 }
@@ -125,8 +125,8 @@ static int run_one(PQQuery &obj, MultiQuery *mq, SCQuery *sq, int mode, Scratch 
 template <class Q>
 int search_batch(int mode, int dim, int mc, int kc, int mp, int kp, int N,
                  float *cq, float *pq, int *L, int *pid, unsigned char *codes, float *raw,
-                 const float *Qs, int nq, int R, int w, int T, int real_dist, int nthreads,
-                 int *ids_out, float *dist_out, int *sum_out, double *seconds_out) {
+                 const float *Qs, int nq, int R, int w, int T, const int *Tq, int M, int real_dist,
+                 int nthreads, int *ids_out, float *dist_out, int *sum_out, double *seconds_out) {
     Q master;
     master.set_index(dim, mc, kc, mp, kp, N, cq, pq, L, pid, codes, raw);
     master.pre_compute1();
@@ -159,7 +159,7 @@ int search_batch(int mode, int dim, int mc, int kc, int mp, int kp, int N,
         std::vector<float> qv(Qs + (size_t)i * dim, Qs + (size_t)(i + 1) * dim);
         int *result; float *dist;
         int sum = run_one(*clones[tid], as_multi(*clones[tid]), as_sc(*clones[tid]), mode,
-                          scratch[tid], qv.data(), R, w, T, kc, real_dist != 0, result, dist,
+                          scratch[tid], qv.data(), R, w, Tq ? Tq[i] : T, M, real_dist != 0, result, dist,
                           nullptr);
         int m = sum < R ? sum : R;
         for (int j = 0; j < R; j++) {
@@ -192,9 +192,28 @@ int ref_search_batch(int mode, int dim, int mc, int kc, int mp, int kp, int N,
                      int *ids_out, float *dist_out, int *sum_out, double *seconds_out) {
     if (mode == 2)
         return search_batch<OSC>(mode, dim, mc, kc, mp, kp, N, cq, pq, L, pid, codes, raw,
-                                 Qs, nq, R, w, T, real_dist, nthreads, ids_out, dist_out, sum_out, seconds_out);
+                                 Qs, nq, R, w, T, nullptr, kc, real_dist, nthreads, ids_out, dist_out, sum_out,
+                                 seconds_out);
     return search_batch<OMulti>(mode, dim, mc, kc, mp, kp, N, cq, pq, L, pid, codes, raw,
-                                Qs, nq, R, w, T, real_dist, nthreads, ids_out, dist_out, sum_out, seconds_out);
+                                Qs, nq, R, w, T, nullptr, kc, real_dist, nthreads, ids_out, dist_out, sum_out,
+                                seconds_out);
+}
+
+/* ref_search_batch with a per-query candidate target Tq[nq] (NULL: T for
+ * every query; search_mr_ivf and search_multi2 take T per call,
+ * sc_query.h:60-67, multi_query.h:62-70) and the coarse-list argument M of
+ * search_multi2 / search_mr_ivf (kc in the reference's own tests). */
+int ref_search_batch_ex(int mode, int dim, int mc, int kc, int mp, int kp, int N,
+                        float *cq, float *pq, int *L, int *pid, unsigned char *codes, float *raw,
+                        const float *Qs, int nq, int R, int w, int T, const int *Tq, int M, int real_dist,
+                        int nthreads, int *ids_out, float *dist_out, int *sum_out, double *seconds_out) {
+    if (mode == 2)
+        return search_batch<OSC>(mode, dim, mc, kc, mp, kp, N, cq, pq, L, pid, codes, raw,
+                                 Qs, nq, R, w, T, Tq, M, real_dist, nthreads, ids_out, dist_out, sum_out,
+                                 seconds_out);
+    return search_batch<OMulti>(mode, dim, mc, kc, mp, kp, N, cq, pq, L, pid, codes, raw,
+                                Qs, nq, R, w, T, Tq, M, real_dist, nthreads, ids_out, dist_out, sum_out,
+                                seconds_out);
 }
 
 /* One query; copies all `sum` candidate (id, distance) pairs the reference

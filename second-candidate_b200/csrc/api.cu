@@ -1387,11 +1387,14 @@ extern "C" int scg_search_device_noalloc(scg_index *h, const scg_search_params *
     if ((rc = check_params(h, p, nq))) return rc;
     if (nq > 0 && (!dQ || !d_ids || !d_dists || !d_sums)) return fail(SCG_ERR_ARG, "null buffer");
     if (p->rerank != 0) return fail(SCG_ERR_ARG, "the allocation-free search does not re-rank (rerank must be 0)");
+    std::lock_guard<std::mutex> g(h->mu);
+    // read under the lock: every builder of the per-vector term holds it and
+    // synchronises its stream before setting the flag, so a set flag means
+    // the term is complete in device memory before this call enqueues work
     if (scan_form(p->precision) == SCG_FAST && !h->have_vterm)
         return fail(SCG_ERR_STATE,
                     "the per-vector term of the tensor-core forms is built by their first call of scg_search or "
                     "scg_search_device; make one before searching without allocation");
-    std::lock_guard<std::mutex> g(h->mu);
     if ((rc = set_device(h))) return rc;
     if (nq == 0) return SCG_OK;
     unsigned char *base = nullptr;
@@ -1400,21 +1403,28 @@ extern "C" int scg_search_device_noalloc(scg_index *h, const scg_search_params *
 
     // carve the scratch: per-query tables first, then per-CTA slots
     const size_t per_query = up256(sizeof(float) * (size_t)h->mc * h->kc) + up256(sizeof(float) * (size_t)h->mp * h->kp);
-    const size_t fixed = 4 * up256(sizeof(float) * (size_t)nq * 2) + 2 * 256;  // qn, qsum, nvis, empty; status, counter
     const size_t slot_bytes = up256(4ull * NOALLOC_CELLS) * 3 + up256(4ull * (NOALLOC_CELLS + 1)) * 2 +
                               up256(8ull * NOALLOC_SURVIVORS);
+    // bytes n queries need besides the per-CTA slots: qn, qsum, nvis, empty,
+    // the status word and the counter, and the per-query tables
+    auto fixed_of = [&](size_t n) { return 4 * up256(sizeof(float) * n * 2) + 2 * 256 + per_query * n; };
     const int upl = h->tuned_upl[scan_form(p->precision) == SCG_FAST ? 1 : 0];
     int per_sm = search_max_blocks_per_sm(p->mode, h->kc, h->mp, h->kp, upl, 0);
     if (per_sm < 1) return fail(SCG_ERR_ARG, "search kernel does not fit on an SM for this shape");
     int grid = h->num_sms * per_sm;
     if (grid > nq) grid = nq;
-    const size_t tables = per_query * (size_t)nq;
-    if (fixed + tables + slot_bytes > SCG_NOALLOC_SCRATCH_BYTES) {
-        size_t maxq = (SCG_NOALLOC_SCRATCH_BYTES - slot_bytes - 4096) / (per_query + 4 * 2 * sizeof(float));
+    if (fixed_of((size_t)nq) + slot_bytes > SCG_NOALLOC_SCRATCH_BYTES) {
+        // the largest batch the same rule admits (one search slot at least)
+        size_t lo = 0, hi = SCG_NOALLOC_SCRATCH_BYTES / per_query + 1;
+        while (lo < hi) {
+            const size_t mid = (lo + hi + 1) / 2;
+            if (fixed_of(mid) + slot_bytes <= SCG_NOALLOC_SCRATCH_BYTES) lo = mid;
+            else hi = mid - 1;
+        }
         return fail(SCG_ERR_CAP, "nq = " + std::to_string(nq) + " exceeds the 48 MiB scratch of the allocation-free "
-                    "search for this index (at most " + std::to_string(maxq) + " queries per call)");
+                    "search for this index (at most " + std::to_string(lo) + " queries per call)");
     }
-    const size_t left = SCG_NOALLOC_SCRATCH_BYTES - fixed - tables;
+    const size_t left = SCG_NOALLOC_SCRATCH_BYTES - fixed_of((size_t)nq);
     if ((size_t)grid * slot_bytes > left) grid = (int)(left / slot_bytes);
     if (grid < 1) return fail(SCG_ERR_CAP, "the allocation-free scratch has no room for a search slot");
 
@@ -1484,6 +1494,7 @@ extern "C" int scg_search_device_noalloc(scg_index *h, const scg_search_params *
     if (st & ST_TIE_OVERFLOW) return fail(SCG_ERR_CAP, "too many cells tie exactly at the cut key");
     if (st & ST_ITER_CAP) return fail(SCG_ERR_CAP, "cell selection did not converge within its round cap");
     if (st & ST_TC_TIMEOUT) return fail(SCG_ERR_CUDA, "a tensor-core table tile did not complete in time");
+    if (st & ST_BAD_ARG) return fail(SCG_ERR_ARG, "the search kernel rejected its arguments");
     if (st) return fail(SCG_ERR_CUDA, "search kernel reported status " + std::to_string(st));
     return SCG_OK;
 }

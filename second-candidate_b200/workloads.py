@@ -230,14 +230,58 @@ def mixture_sampler(cfg, seed, dev):
     return sample
 
 
-def build_gpu_workload(name, seed=1234, cache_dir=None, log=print):
+def _nearest64(X, C, k=1, chunk=1 << 17):
+    """Indices [n, k] of the k nearest rows of C (ascending distance) for each
+    row of X, from float64 distances ||x||^2 + ||c||^2 - 2<x, c> on the device
+    (torch); k = 1 takes the lowest index among equal distances."""
+    import torch
+    Cd = C.double()
+    Cn = (Cd * Cd).sum(1)[None]
+    out = torch.empty(X.shape[0], k, dtype=torch.long, device=X.device)
+    for s in range(0, X.shape[0], chunk):
+        x = X[s:s + chunk].double()
+        d = (x * x).sum(1, keepdim=True) + Cn - 2.0 * (x @ Cd.T)
+        if k == 1:
+            out[s:s + x.shape[0], 0] = d.argmin(1)
+        else:
+            out[s:s + x.shape[0]] = torch.topk(d, k, dim=1, largest=False, sorted=True).indices
+    return out
+
+
+def _exact_nn64(X, Q, chunk=1 << 17):
+    """Exact nearest row of X for each query (float64 distances, the lowest
+    row among equal distances), torch on the device."""
+    import torch
+    Qd = Q.double()
+    Qn = (Qd * Qd).sum(1)[:, None]
+    best = torch.full((Q.shape[0],), float("inf"), dtype=torch.float64, device=Q.device)
+    arg = torch.zeros(Q.shape[0], dtype=torch.long, device=Q.device)
+    for s in range(0, X.shape[0], chunk):
+        x = X[s:s + chunk].double()
+        d = Qn + (x * x).sum(1)[None, :] - 2.0 * (Qd @ x.T)
+        v, j = d.min(1)
+        better = v < best
+        best = torch.where(better, v, best)
+        arg = torch.where(better, j + s, arg)
+    return arg
+
+
+def build_gpu_workload(name, seed=1234, cache_dir=None, log=print, device=None, overrides=None):
     """Generates config `name` on cuda:0 and returns a dict of host arrays:
     cq, pq (codebooks), L, pid, codes (CSR index in cell order), Q (queries),
     gt (exact nearest neighbour of each query), raw (the base rows, for
-    configs with a re-rank shortlist) and the shape facts.  The index is
-    encoded by the library's encoder (the reference's Encoder/SCEncoder codes)
-    and bucketed by cell id in row order (as Encoder::distribution does).
-    With cache_dir the result is kept as .npz and reused."""
+    configs with a re-rank shortlist) and the shape facts.
+
+    Data preparation only, in torch on the device -- it loads none of this
+    project's kernels, so that the reference's CPU arm and the GPU arm can
+    share one cached workload.  The codes are those of Encoder::encode /
+    SCEncoder::encode (nearest coarse centroid(s) per part, the float residual
+    to the nearest, nearest PQ centroid per subspace), found with float64
+    distances; rows are bucketed by cell id in row order (as
+    Encoder::distribution does).  Ground truth: the exact nearest base row in
+    float64 (exact for the integer-valued configs).  With cache_dir the result
+    is kept as .npz and reused.  `device` (default cuda:0) and `overrides`
+    (config keys replaced, e.g. a smaller N) serve the tests."""
     import hashlib
     import os
     import time
@@ -245,7 +289,8 @@ def build_gpu_workload(name, seed=1234, cache_dir=None, log=print):
     import torch
 
     cfg = dict(CONFIGS[name])
-    key = hashlib.sha1(repr((name, seed, sorted(cfg.items()), 5)).encode()).hexdigest()[:16]
+    cfg.update(overrides or {})
+    key = hashlib.sha1(repr((name, seed, sorted(cfg.items()), 6)).encode()).hexdigest()[:16]
     path = os.path.join(cache_dir, "%s_%s.npz" % (cfg["name"], key)) if cache_dir else None
     if path and os.path.exists(path):
         z = np.load(path)
@@ -254,9 +299,8 @@ def build_gpu_workload(name, seed=1234, cache_dir=None, log=print):
         log("workload %s loaded from cache" % cfg["name"])
         return out
 
-    import scgpu
     t0 = time.time()
-    dev = torch.device("cuda:0")
+    dev = torch.device(device or "cuda:0")
     torch.backends.cuda.matmul.allow_tf32 = False
     N, D, mc, kc, mp, kp = cfg["N"], cfg["D"], cfg["mc"], cfg["kc"], cfg["mp"], cfg["kp"]
     sc = cfg["mode"] == "sc"
@@ -279,42 +323,47 @@ def build_gpu_workload(name, seed=1234, cache_dir=None, log=print):
         resid[:, i * bsc:(i + 1) * bsc] -= cq[i][_torch_nearest(part, cq[i])]
     pq = torch.stack([_torch_kmeans(resid[:, j * bsp:(j + 1) * bsp].contiguous(), kp, cfg["iters"], seed + 101 + 7 * j)
                       for j in range(mp)])
+    del resid
     cq_h = cq.cpu().numpy().astype(np.float32).ravel()
     pq_h = pq.cpu().numpy().astype(np.float32).ravel()
     log("trained codebooks in %.1fs" % (time.time() - t0))
-    # exact encoding with the library's encoder
-    ix = scgpu.Index(0)
-    ix.load_codebooks(cq_h, kc, mcp, pq_h, kp, mp, D)
-    nc = 2 if sc else 0
-    ncid = 2 if sc else mcp
-    cid = torch.empty(N, ncid, dtype=torch.int16, device=dev)
-    codes = torch.empty(N, mp, dtype=torch.uint8, device=dev)
+    # codes: nearest coarse centroid per part (second candidate: the two
+    # nearest of the one codebook), float residual to the nearest, nearest PQ
+    # centroid per subspace
     step = 1 << 22
+    ncid = 2 if sc else mcp
+    cid = torch.empty(N, ncid, dtype=torch.long, device=dev)
+    codes = torch.empty(N, mp, dtype=torch.uint8, device=dev)
     for s in range(0, N, step):
-        n = min(step, N - s)
-        ix.encode_device(X[s:s + n].data_ptr(), n, nc, cid[s:s + n].data_ptr(), codes[s:s + n].data_ptr())
-    torch.cuda.synchronize()
-    ix.close()
+        x = X[s:s + step]
+        r = x.clone()
+        for i in range(mcp):
+            part = x[:, i * bsc:(i + 1) * bsc]
+            nn = _nearest64(part, cq[i], 2 if sc else 1)
+            cid[s:s + x.shape[0], i:i + nn.shape[1]] = nn
+            r[:, i * bsc:(i + 1) * bsc] -= cq[i][nn[:, 0]]
+        for j in range(mp):
+            codes[s:s + x.shape[0], j] = _nearest64(r[:, j * bsp:(j + 1) * bsp], pq[j])[:, 0].to(torch.uint8)
+        del r
+    if dev.type == "cuda":
+        torch.cuda.synchronize()
     log("encoded in %.1fs" % (time.time() - t0))
-    c = cid.to(torch.int64) & 0xFFFF
-    cell = c[:, 0] * kc + c[:, 1] if ncid == 2 else c[:, 0]
+    cell = cid[:, 0] * kc + cid[:, 1] if ncid == 2 else cid[:, 0]
     ncells = kc * kc if (sc or mc == 2) else kc
     cell_sorted, perm = torch.sort(cell, stable=True)
     counts = torch.bincount(cell, minlength=ncells)
     L = counts.cumsum(0).to(torch.int32)
     codes_sorted = codes[perm]
-    # exact nearest neighbour of each query (scg_exact_nn: the brute-force
-    # argmin of distance_l2_square, ties to the lowest id)
-    gt = torch.empty(Q.shape[0], dtype=torch.int32, device=dev)
-    scgpu.exact_nn_device(X.data_ptr(), N, Q.data_ptr(), Q.shape[0], D, gt.data_ptr())
+    gt = _exact_nn64(X, Q)
     log("index + ground truth in %.1fs" % (time.time() - t0))
     out = dict(cq=cq_h, pq=pq_h, L=L.cpu().numpy(), pid=perm.to(torch.int32).cpu().numpy(),
-               codes=codes_sorted.cpu().numpy(), Q=Q.cpu().numpy(), gt=gt.cpu().numpy())
+               codes=codes_sorted.cpu().numpy(), Q=Q.cpu().numpy(), gt=gt.to(torch.int32).cpu().numpy())
     if cfg.get("shortlist"):
         # raw vectors for the exact re-rank (uint8 when the data are bytes)
         out["raw"] = (X.to(torch.uint8) if sample.kind == "u8" else X).cpu().numpy()
     del X, codes, cid, cell, perm, codes_sorted
-    torch.cuda.empty_cache()
+    if dev.type == "cuda":
+        torch.cuda.empty_cache()
     if path:
         os.makedirs(cache_dir, exist_ok=True)
         tmp = path + ".%d.tmp.npz" % os.getpid()

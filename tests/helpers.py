@@ -6,6 +6,27 @@ import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
+# Golden queries (over all (T, w) rules of a case) whose exact-order result --
+# candidate count, top-R ids and distances -- equals the compiled reference's.
+# IVFADC / IMI / plain PQ: all of them.  Second candidate: the reference heap
+# orders the exactly tied cells (a,b) / (b,a) arbitrarily, so 3 of 20 differ
+# by one tied boundary cell.
+GOLDEN_SAME_AS_REF = {"imi_d32": 40, "ivf_d32": 40, "plainpq_d32": 10, "sc_d32": 17}
+
+
+def same_as_reference(c, ri, ids, d, sums):
+    """Queries of rule ri whose result equals the reference's golden one."""
+    R = int(c["R"])
+    n = 0
+    for i in range(c["Q"].shape[0]):
+        if sums[i] == c["r%d_sum" % ri][i]:
+            m = min(R, int(sums[i]))
+            rid, rd = c["r%d_top_ids" % ri][i][:m], c["r%d_top_d" % ri][i][:m]
+            o = np.lexsort((rid, rd))
+            if same_topk(ids[i], d[i], rid[o], rd[o], m):
+                n += 1
+    return n
+
 
 def golden_cases():
     return sorted(glob.glob(os.path.join(GOLDEN, "*.npz")))

@@ -18,8 +18,8 @@ pytestmark = pytest.mark.gpu
 MODES = {O.IVFADC: 0, O.IMI: 1, O.SC: 2}
 
 
-def _build(mode, mc, kc, D, kind, seed):
-    mp, kp = 8, 256
+def _build(mode, mc, kc, D, kind, seed, mp=8):
+    kp = 256
     if kind == "u8":
         mix = W.Mixture(D, 16, 20.0, "u8", seed=seed)
         X = mix.sample(30000, seed=seed + 1)
@@ -65,6 +65,29 @@ def test_rerank_matches_oracle(oracle_mod, mode, mc, kc, kind):
         g.load_raw(X.astype(np.uint8))
         ids8, d8, _ = g.search(MODES[mode], Q, 50, w, 3000, rerank=300)
         assert np.array_equal(ids32, ids8) and np.array_equal(d32, d8)
+    g.close()
+
+
+@pytest.mark.parametrize("mode,mc,kc,kind,D,mp", [(O.IMI, 2, 16, "u8", 40, 8), (O.IVFADC, 1, 32, "f32", 30, 6)])
+def test_rerank_unaligned_rows(oracle_mod, mode, mc, kc, kind, D, mp):
+    """Rows whose length is not a multiple of 16 bytes (uint8 D = 40, float
+    D = 30) take the element-by-element path of the re-rank kernel; it must
+    give the same ids and bit-identical distances as the oracle's re-rank."""
+    import scgpu
+    X, Q, cq, pq, L, pid, co, ix, (D, mc, kc, mp, kp) = _build(mode, mc, kc, D, kind, 80 + mode, mp=mp)
+    g = scgpu.Index(0)
+    g.load_codebooks(cq, kc, mc, pq, kp, mp, D)
+    g.load_csr(L, pid, co)
+    g.precompute()
+    g.load_raw(X.astype(np.uint8) if kind == "u8" else X.astype(np.float32))
+    w = kc if mode == O.IVFADC else 1 << 20
+    for Lsl, R, T in ((200, 20, 3000), (1000, 100, 8000)):
+        ids, d, sums = g.search(MODES[mode], Q, R, w, T, rerank=Lsl)
+        si, sd, ssum = ix.search(mode, Q, Lsl, w, T, order=O.ORDER_EXACT)
+        assert np.array_equal(sums, ssum)
+        ri, rd = ix.rerank(Q, si, R)
+        for i in range(Q.shape[0]):
+            assert helpers.same_topk(ids[i], d[i], ri[i], rd[i], R), (Lsl, R, T, i)
     g.close()
 
 

@@ -51,16 +51,14 @@ def test_golden_cases(scg, oracle_mod, path):
         ids, d, sums = check_against_oracle(ix, g, mode, c["Q"], R, int(w), int(T))
         # against the reference itself: identical wherever its heap visited
         # the same cells as the exact order
-        for i in range(c["Q"].shape[0]):
-            total += 1
-            if sums[i] == c["r%d_sum" % ri][i]:
-                m = min(R, int(sums[i]))
-                rid, rd = c["r%d_top_ids" % ri][i][:m], c["r%d_top_d" % ri][i][:m]
-                o = np.lexsort((rid, rd))
-                if helpers.same_topk(ids[i], d[i], rid[o], rd[o], m):
-                    same_as_ref += 1
+        total += c["Q"].shape[0]
+        same_as_ref += helpers.same_as_reference(c, ri, ids, d, sums)
     g.close()
-    assert same_as_ref >= 0.6 * total
+    # IVFADC, IMI and plain PQ: every golden query has the reference's own
+    # top-R.  Second candidate: cells (a,b) and (b,a) have identical keys and
+    # the reference heap takes such ties in arbitrary order, so 3 of its 20
+    # golden queries cut one tied boundary cell differently.
+    assert same_as_ref >= helpers.GOLDEN_SAME_AS_REF[os.path.basename(path)[:-4]], (same_as_ref, total)
 
 
 @pytest.mark.parametrize("mode,mc,kc", [(O.IVFADC, 1, 64), (O.IMI, 2, 48), (O.SC, 1, 48)])

@@ -79,3 +79,17 @@ def test_exact_order_differs_only_at_the_boundary(case):
             b = ix.search_one(mode, case["Q"][i], int(w), int(T), order=O.ORDER_EXACT)
             ca, cb = set(a["cells"].tolist()), set(b["cells"].tolist())
             assert len(ca ^ cb) <= 4
+
+
+def test_exact_order_same_as_reference(case, request):
+    """The exact order (which the CUDA search reproduces bit for bit) gives
+    the reference's own result on every IVFADC / IMI / plain-PQ golden query
+    and on all but the recorded tied-boundary SC queries."""
+    ix = helpers.oracle_index(O, case)
+    mode, R = int(case["mode"]), int(case["R"])
+    same = 0
+    for ri, (T, w) in enumerate(case["rules"]):
+        ids, d, sums = ix.search(mode, case["Q"], R, int(w), int(T), order=O.ORDER_EXACT)
+        same += helpers.same_as_reference(case, ri, ids, d, sums)
+    key = [k for k in helpers.GOLDEN_SAME_AS_REF if k in request.node.nodeid][0]
+    assert same >= helpers.GOLDEN_SAME_AS_REF[key], (key, same)

@@ -70,3 +70,57 @@ def test_noalloc_matches_allocating_search(oracle_mod):
                 assert torch.equal(ai, ri), (name, precision, call)
                 assert torch.equal(ad, rd), (name, precision, call)
         g.close()
+
+
+def test_noalloc_limits(oracle_mod):
+    """The scratch's batch limit is the one the error message names: one
+    query more is refused with SCG_ERR_CAP, exactly that many run.  The
+    tensor-core forms are refused (SCG_ERR_STATE) until an allocating call
+    has built their per-vector term."""
+    import re
+
+    import torch
+
+    import scgpu
+    c = helpers.load_case(os.path.join(helpers.GOLDEN, "imi_d32.npz"))
+    D, mc, kc, mp, kp = (int(c[k]) for k in ("D", "mc", "kc", "mp", "kp"))
+    g = _index(scgpu, D, mc, kc, mp, kp, c["cq"], c["pq"], c["L"], c["pid"], c["icodes"])
+    R, w, T = 10, 1 << 20, 300
+    nq0 = c["Q"].shape[0]
+    dQ0 = torch.from_numpy(np.ascontiguousarray(c["Q"], np.float32)).cuda()
+    o = [torch.empty(nq0 * R, dtype=torch.int32, device="cuda"),
+         torch.empty(nq0 * R, dtype=torch.float32, device="cuda"),
+         torch.empty(nq0, dtype=torch.int32, device="cuda")]
+    with pytest.raises(scgpu.ScgError) as e:
+        g.search_device_noalloc(1, dQ0.data_ptr(), nq0, R, w, T, *(t.data_ptr() for t in o), precision=scgpu.FAST)
+    assert e.value.code == -6
+    # find the limit: a batch far beyond it names it (buffers of its full
+    # size, so that even a wrong admission stays within them)
+    big = 1 << 18
+    bq = torch.zeros(big, D, dtype=torch.float32, device="cuda")
+    bo = [torch.empty(big * R, dtype=torch.int32, device="cuda"),
+          torch.empty(big * R, dtype=torch.float32, device="cuda"),
+          torch.empty(big, dtype=torch.int32, device="cuda")]
+    with pytest.raises(scgpu.ScgError) as e:
+        g.search_device_noalloc(1, bq.data_ptr(), big, R, w, T, *(t.data_ptr() for t in bo))
+    assert e.value.code == -5
+    del bq, bo
+    maxq = int(re.search(r"at most (\d+) queries", str(e.value)).group(1))
+    assert 0 < maxq < big
+    reps = (maxq + 1 + nq0 - 1) // nq0
+    dQ = dQ0.repeat(reps, 1)[: maxq + 1].contiguous()
+    ids = torch.empty((maxq + 1) * R, dtype=torch.int32, device="cuda")
+    ds = torch.empty((maxq + 1) * R, dtype=torch.float32, device="cuda")
+    sums = torch.empty(maxq + 1, dtype=torch.int32, device="cuda")
+    with pytest.raises(scgpu.ScgError) as e:
+        g.search_device_noalloc(1, dQ.data_ptr(), maxq + 1, R, w, T, ids.data_ptr(), ds.data_ptr(), sums.data_ptr())
+    assert e.value.code == -5
+    g.search_device_noalloc(1, dQ.data_ptr(), maxq, R, w, T, ids.data_ptr(), ds.data_ptr(), sums.data_ptr())
+    torch.cuda.synchronize()
+    # every repeated query gives its original's result
+    ri, rd, rs = g.search(1, c["Q"], R, w, T)
+    got_i = ids[: maxq * R].view(maxq, R).cpu().numpy()
+    got_s = sums[:maxq].cpu().numpy()
+    for i in range(maxq):
+        assert got_s[i] == rs[i % nq0] and np.array_equal(got_i[i], ri[i % nq0])
+    g.close()
