@@ -10,8 +10,6 @@ import formats
 import oracle as O
 import workloads as W
 
-pytestmark = pytest.mark.skipif(not os.path.isdir(O.REF_TREE) and not O.ref_available(),
-                                reason="reference not built here")
 
 
 @pytest.fixture(scope="module")
