@@ -86,13 +86,11 @@ int check_params(scg_index *h, const scg_search_params *p, int nq) {
     if (nq < 0) return fail(SCG_ERR_ARG, "nq < 0");
     if (p->R < 1 || p->R > 1024) return fail(SCG_ERR_ARG, "R must be in [1, 1024]");
     if (p->precision < SCG_FP32_EXACT || p->precision > SCG_FP16) return fail(SCG_ERR_ARG, "unknown precision");
-    if (p->rerank < 0)
-        return fail(SCG_ERR_ARG, "rerank = -1 (exact distance for every candidate) is not served; "
-                                 "use a shortlist rerank = L (R <= L <= 1024)");
-    if (p->rerank > 0) {
-        if (p->rerank < p->R || p->rerank > 1024) return fail(SCG_ERR_ARG, "rerank shortlist L must be in [R, 1024]");
-        if (h->raw_rows < h->N) return fail(SCG_ERR_STATE, "re-rank needs the raw vectors (scg_load_raw)");
-    }
+    if (p->rerank < -1) return fail(SCG_ERR_ARG, "rerank must be -1, 0 or a shortlist length L");
+    if (p->rerank > 0 && (p->rerank < p->R || p->rerank > 1024))
+        return fail(SCG_ERR_ARG, "rerank shortlist L must be in [R, 1024]");
+    if (p->rerank != 0 && h->raw_rows < h->N)
+        return fail(SCG_ERR_STATE, "exact distances need the raw vectors (scg_load_raw)");
     switch (p->mode) {
         case SCG_IVFADC:
             if (h->mc != 1 || h->ncells != h->kc) return fail(SCG_ERR_ARG, "This search method is for IVFADC only");
@@ -221,13 +219,16 @@ int reserve_search(scg_index *h, Workspace *ws, int mode, int grid) {
     // the largest grid of each slot kind over the kernel variants
     int g_rec = 0, g_vis = 0, g_pend = 0;
     for (int u : {2, 4, 8}) {
-        const int f = h->num_sms * search_max_blocks_per_sm(mode, h->kc, h->mp, h->kp, u, 0);
-        const int c = h->num_sms * search_max_blocks_per_sm(mode, h->kc, h->mp, h->kp, u, 2);
-        g_rec = std::max(g_rec, f);
-        g_vis = std::max(g_vis, f);
-        g_pend = std::max(g_pend, std::max(f, c));
+        for (int rot : {0, 1}) {
+            if (rot && !search_rot_form(SCG_FAST, h->mp, h->kp)) continue;
+            const int f = h->num_sms * search_max_blocks_per_sm(mode, h->kc, h->mp, h->kp, u, 0, rot);
+            const int c = h->num_sms * search_max_blocks_per_sm(mode, h->kc, h->mp, h->kp, u, 2, rot);
+            g_rec = std::max(g_rec, f);
+            g_vis = std::max(g_vis, f);
+            g_pend = std::max(g_pend, std::max(f, c));
+        }
     }
-    g_rec = std::max(g_rec, h->num_sms * search_max_blocks_per_sm(mode, h->kc, h->mp, h->kp, 4, 1));
+    g_rec = std::max(g_rec, h->num_sms * search_max_blocks_per_sm(mode, h->kc, h->mp, h->kp, 4, 1, 0));
     if (g_rec < 1) return fail(SCG_ERR_ARG, "search kernel does not fit on an SM for this shape");
     if (grid > 0) {
         g_rec = std::min(g_rec, grid);
@@ -321,13 +322,16 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     if ((rc = ws->status.ensure(sizeof(int) * 4))) return rc;
     if ((rc = ws->counter.ensure(sizeof(int) * 4))) return rc;
     const int upl = h->tuned_upl[scan_form(p->precision) == SCG_FAST ? 1 : 0];
+    // rerank = -1: the scan scores every candidate by its exact distance
+    const int qdim = p->rerank < 0 ? h->dim : 0;
+    const int rot = (!qdim && search_rot_form(scan_form(p->precision), h->mp, h->kp)) ? 1 : 0;
     const int *Tq = rb ? nullptr : h->d_Tq;
     // split kernels (selection, then a lighter scan at higher occupancy)
     int64_t stride = 0, over = 0;
     pool_dims(h, p, nq, Tq != nullptr, &stride, &over);
     const bool split = allow_split && h->split && stride * (int64_t)nq + over < (1ll << 32);
     auto grid_of = [&](int part) {
-        int g = h->num_sms * search_max_blocks_per_sm(p->mode, h->kc, h->mp, h->kp, upl, part);
+        int g = h->num_sms * search_max_blocks_per_sm(p->mode, h->kc, h->mp, h->kp, upl, part, rot, qdim);
         return std::max(1, std::min(g, nq));
     };
     const int g_fused = split ? 0 : grid_of(0);
@@ -386,6 +390,11 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     memset(&sa, 0, sizeof(sa));
     sa.mode = p->mode; sa.dim = h->dim; sa.mc = h->mc; sa.kc = h->kc; sa.mp = h->mp; sa.kp = h->kp;
     sa.nq = nq; sa.R = R; sa.w = p->w; sa.T = p->T; sa.precision = scan_form(p->precision);
+    sa.rot = rot;
+    sa.raw_dim = qdim;
+    sa.Q = dQ;
+    sa.raw = qdim ? h->raw.p : nullptr;
+    sa.raw_u8 = h->raw_u8 ? 1 : 0;
     sa.upl = upl;
     sa.slist = b.slist;
     sa.smeta = b.smeta;
@@ -1409,7 +1418,8 @@ extern "C" int scg_search_device_noalloc(scg_index *h, const scg_search_params *
     // the status word and the counter, and the per-query tables
     auto fixed_of = [&](size_t n) { return 4 * up256(sizeof(float) * n * 2) + 2 * 256 + per_query * n; };
     const int upl = h->tuned_upl[scan_form(p->precision) == SCG_FAST ? 1 : 0];
-    int per_sm = search_max_blocks_per_sm(p->mode, h->kc, h->mp, h->kp, upl, 0);
+    const int rot = search_rot_form(scan_form(p->precision), h->mp, h->kp) ? 1 : 0;
+    int per_sm = search_max_blocks_per_sm(p->mode, h->kc, h->mp, h->kp, upl, 0, rot);
     if (per_sm < 1) return fail(SCG_ERR_ARG, "search kernel does not fit on an SM for this shape");
     int grid = h->num_sms * per_sm;
     if (grid > nq) grid = nq;
@@ -1467,6 +1477,7 @@ extern "C" int scg_search_device_noalloc(scg_index *h, const scg_search_params *
     memset(&sa, 0, sizeof(sa));
     sa.mode = p->mode; sa.dim = h->dim; sa.mc = h->mc; sa.kc = h->kc; sa.mp = h->mp; sa.kp = h->kp;
     sa.nq = nq; sa.R = p->R; sa.w = p->w; sa.T = p->T; sa.precision = scan_form(p->precision);
+    sa.rot = rot;
     sa.upl = upl;
     sa.Tq = h->d_Tq;
     sa.dqc = dqc; sa.dqr = dqr; sa.qn = qn; sa.qsum = qsum;

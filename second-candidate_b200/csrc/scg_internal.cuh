@@ -85,6 +85,7 @@ struct QMeta {
 struct SearchArgs {
     int mode, dim, mc, kc, mp, kp, nq, R, w, T;
     int precision;
+    int rot;                // the fast form's rotated, bank-private LUT (kp == 256, mp in {8, 16, 32})
     int upl;                // candidates per lane per scan chunk: 2, 4 or 8
     int shortlist;          // 1: the R best feed the exact re-rank, which orders them itself
     const int *Tq;          // optional per-query T
@@ -97,6 +98,11 @@ struct SearchArgs {
     const uint8_t *codes;
     const float *dot_cr;
     const float *vterm;     // per-vector term of the fast form (may be null)
+    // exact-distance scan (the real_dist branch for every candidate):
+    // raw_dim > 0 scores each candidate against its raw row instead of ADC
+    const float *Q;         // [nq][raw_dim] queries
+    const void *raw;        // [N][raw_dim] raw rows by id, float or uint8
+    int raw_u8, raw_dim;
     uint64_t ncells;
     int64_t N;
     // per-CTA scratch slots
@@ -121,10 +127,14 @@ struct SearchArgs {
     unsigned long long *dens_acc;  // optional: adds each query's (candidates, cells)
 };
 
-// part 0: fused selection + scan; 1: selection only; 2: scan only.
-size_t search_smem_bytes(int mode, int kc, int mp, int kp, int part);
+// part 0: fused selection + scan; 1: selection only; 2: scan only.  rot:
+// the scan uses the fast form's rotated LUT (search_rot_form).
+// qdim > 0: the exact-distance scan over raw rows of qdim floats.
+size_t search_smem_bytes(int mode, int kc, int mp, int kp, int part, int rot, int qdim);
 int search_launch(const SearchArgs &a, int part, int grid, cudaStream_t s);
-int search_max_blocks_per_sm(int mode, int kc, int mp, int kp, int upl, int part);
+int search_max_blocks_per_sm(int mode, int kc, int mp, int kp, int upl, int part, int rot, int qdim = 0);
+// Whether searches in `precision` on this shape use the rotated LUT.
+bool search_rot_form(int precision, int mp, int kp);
 
 struct EncodeArgs {
     int dim, mc, kc, mp, kp, nc;  // nc = 0: IVF/IMI encoder; nc >= 2: SC encoder

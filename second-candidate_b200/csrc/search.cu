@@ -15,45 +15,51 @@ int search_launch_u2(const SearchArgs &a, int part, int grid, size_t smem, cudaS
 int search_launch_u4(const SearchArgs &a, int part, int grid, size_t smem, cudaStream_t s);
 int search_launch_u8(const SearchArgs &a, int part, int grid, size_t smem, cudaStream_t s);
 int search_launch_select(const SearchArgs &a, int grid, size_t smem, cudaStream_t s);
-int search_occupancy_u2(int mp, int part, size_t smem);
-int search_occupancy_u4(int mp, int part, size_t smem);
-int search_occupancy_u8(int mp, int part, size_t smem);
+int search_occupancy_u2(int mp, int part, size_t smem, bool fk);
+int search_occupancy_u4(int mp, int part, size_t smem, bool fk);
+int search_occupancy_u8(int mp, int part, size_t smem, bool fk);
 int search_occupancy_select(size_t smem);
 
-size_t search_smem_bytes(int mode, int kc, int mp, int kp, int part) {
-    return carve(mode, kc, mp, kp, part, nullptr, nullptr);
+size_t search_smem_bytes(int mode, int kc, int mp, int kp, int part, int rot, int qdim) {
+    return carve(mode, kc, mp, kp, part, rot, qdim, nullptr, nullptr);
 }
 
-static int occupancy_query(int mode, int kc, int mp, int kp, int upl, int part) {
-    const size_t smem = search_smem_bytes(mode, kc, mp, kp, part);
+bool search_rot_form(int precision, int mp, int kp) { return rot_form(precision, mp, kp); }
+
+static int occupancy_query(int mode, int kc, int mp, int kp, int upl, int part, int rot, int qdim) {
+    const size_t smem = search_smem_bytes(mode, kc, mp, kp, part, rot, qdim);
     if (part == 1) return search_occupancy_select(smem);
+    const bool fk = part == 2 && rot;  // the rotated LUT's scan runs the fast-form variant
     switch (upl) {
-        case 2: return search_occupancy_u2(mp, part, smem);
-        case 8: return search_occupancy_u8(mp, part, smem);
-        default: return search_occupancy_u4(mp, part, smem);
+        case 2: return search_occupancy_u2(mp, part, smem, fk);
+        case 8: return search_occupancy_u8(mp, part, smem, fk);
+        default: return search_occupancy_u4(mp, part, smem, fk);
     }
 }
 
 // Resident CTAs per SM, asked of the runtime once per device and shape.
-int search_max_blocks_per_sm(int mode, int kc, int mp, int kp, int upl, int part) {
+int search_max_blocks_per_sm(int mode, int kc, int mp, int kp, int upl, int part, int rot, int qdim) {
     static std::mutex mu;
-    static std::map<std::tuple<int, int, int, int, int, int, int>, int> cache;
+    static std::map<std::tuple<int, int, int, int, int, int, int, int, int>, int> cache;
     int dev = 0;
     cudaGetDevice(&dev);
-    const auto key = std::make_tuple(dev, mode, kc, mp, kp, upl, part);
+    if (part == 1) rot = qdim = 0;  // the selection kernel has no LUT
+    if (qdim > 0) rot = 0;          // the exact-distance scan has none either
+    const auto key = std::make_tuple(dev, mode, kc, mp, kp, upl, part, rot, qdim);
     {
         std::lock_guard<std::mutex> g(mu);
         auto it = cache.find(key);
         if (it != cache.end()) return it->second;
     }
-    const int nb = occupancy_query(mode, kc, mp, kp, upl, part);
+    const int nb = occupancy_query(mode, kc, mp, kp, upl, part, rot, qdim);
     std::lock_guard<std::mutex> g(mu);
     if (nb > 0) cache[key] = nb;
     return nb;
 }
 
 int search_launch(const SearchArgs &a, int part, int grid, cudaStream_t s) {
-    const size_t smem = search_smem_bytes(a.mode, a.kc, a.mp, a.kp, part);
+    const size_t smem = search_smem_bytes(a.mode, a.kc, a.mp, a.kp, part, part == 1 ? 0 : a.rot,
+                                          part == 1 ? 0 : a.raw_dim);
     if (part == 1) return search_launch_select(a, grid, smem, s);
     switch (a.upl) {
         case 2: return search_launch_u2(a, part, grid, smem, s);

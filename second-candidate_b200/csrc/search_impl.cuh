@@ -35,7 +35,7 @@
 // bound, and one radix-select merge over them gives the R best.
 #pragma once
 
-#include "scg_internal.cuh"
+#include "exact_dist.cuh"
 
 namespace scg {
 
@@ -95,11 +95,24 @@ struct Smem {
     uint64_t *ties2;
 };
 
-__host__ __device__ inline size_t carve(int mode, int kc, int mp, int kp, int part, Smem *s, unsigned char *base) {
+// Bytes of the rotated LUT of the fast form (kp == 256, mp in {8, 16, 32}):
+// 256 code rows x 32 banks of words, 32/mp copies of the [mp][256] table.
+constexpr int ROT_LUT_BYTES = 256 * 32 * 4;
+
+// The scan form that uses the rotated, bank-private LUT.
+__host__ __device__ inline bool rot_form(int precision, int mp, int kp) {
+    return precision == SCG_FAST && kp == 256 && (mp == 8 || mp == 16 || mp == 32);
+}
+
+// qdim > 0: the exact-distance scan (every candidate scored against its raw
+// row), whose query of qdim floats takes the LUT's place.
+__host__ __device__ inline size_t carve(int mode, int kc, int mp, int kp, int part, int rot, int qdim, Smem *s,
+                                        unsigned char *base) {
     const int kcP = next_pow2(kc);
     size_t off = 0;
     if (s) s->lut = (float *)(base + off);
-    if (part != 1) off += align16((size_t)mp * kp * 4);
+    if (part != 1)
+        off += qdim > 0 ? align16((size_t)qdim * 4) : (rot ? (size_t)ROT_LUT_BYTES : align16((size_t)mp * kp * 4));
     const size_t phase0 = off;
     size_t end1 = phase0, end2 = phase0;
     if (part != 2) {
@@ -145,6 +158,7 @@ __host__ __device__ inline size_t carve(int mode, int kc, int mp, int kp, int pa
 }
 
 static_assert(2 * RMAX <= WARMN, "top-R buffers live inside the warm-up scores");
+static_assert(WARMN % 32 == 0, "scan chunks start at multiples of 32 (the rotated LUT relies on it)");
 
 // ---------------------------------------------------------------------------
 // Block-wide helpers (NT threads, all threads must call)
@@ -650,10 +664,39 @@ struct ScanCtx {
     int nvis;
     uint32_t Svis;
     int kc, mp, kp, bsI;
-    bool imi, sc, fast;
+    bool imi, sc, fast, rot;
     float qs;
     const float *dqc;
+    // exact-distance scan (raw_dim > 0): the query in shared memory, raw rows
+    // by id (uint8 or float; raw_vec: rows read 16 bytes at a time)
+    int raw_dim;
+    bool raw_u8, raw_vec;
+    const float *qv;
 };
+
+// The MPC code bytes of one candidate rotated by rb bytes (byte s of r is
+// byte (s + rb) mod MPC of w): words first (log steps of selects), then the
+// bytes inside a word (funnel shifts).
+template <int MPC>
+__device__ __forceinline__ void rotate_code(const uint32_t *w, uint32_t *r, uint32_t rb) {
+    constexpr int n = MPC / 4;
+    uint32_t t[n];
+#pragma unroll
+    for (int i = 0; i < n; i++) t[i] = w[i];
+    const uint32_t qw = rb >> 2;
+#pragma unroll
+    for (int b = 1; b < n; b <<= 1) {
+        uint32_t x[n];
+#pragma unroll
+        for (int i = 0; i < n; i++) x[i] = t[(i + b) % n];
+        const bool on = (qw & (uint32_t)b) != 0;
+#pragma unroll
+        for (int i = 0; i < n; i++) t[i] = on ? x[i] : t[i];
+    }
+    const uint32_t sh = (rb & 3u) * 8u;
+#pragma unroll
+    for (int i = 0; i < n; i++) r[i] = __funnelshift_r(t[i], t[(i + 1) % n], sh);
+}
 
 // One float of shared memory at a 32-bit shared-window address.
 __device__ __forceinline__ float lds_f32(uint32_t addr) {
@@ -663,20 +706,32 @@ __device__ __forceinline__ float lds_f32(uint32_t addr) {
 }
 
 // Warp-centric ADC scan of the candidates [first, limit), cut into chunks of
-// 32 * U candidates.  FK (the fast form with kp == 256): every warp takes an
-// equal, contiguous run of chunks, so it walks its visited cells in order,
-// and the LUT entries are read with 32-bit shared addresses and constant row
-// offsets.  Otherwise warps claim chunks from a shared counter
-// (st.next_flat, set to `first` by the caller), which keeps the warps of a
-// CTA on neighbouring cells: the exact forms gather dot_cr rows per cell,
-// and neighbouring cells share rows in L1.  A warp keeps a window of WWIN
-// visited cells; when the scan leaves it at its end the next WWIN cells are
-// loaded, otherwise a binary search over the visited-cell prefix finds the
-// cell that holds the chunk.  U candidates per lane are loaded at once and
-// the table entries are added in the reference's order.  WARM == true stores
-// every candidate's (distance, position) at warm[flat]; otherwise candidates
-// with a distance word <= tau are appended to out[] (global, capacity cap)
-// through warp-aggregated atomics on st.npend.
+// 32 * U candidates; `first` and every chunk start are multiples of 32, and
+// lane l of a warp scores the chunk's candidates with flat index = l (mod
+// 32).  FK (the fast form with kp == 256): every warp takes an equal,
+// contiguous run of chunks, so it walks its visited cells in order.
+// Otherwise warps claim chunks from a shared counter (st.next_flat, set to
+// `first` by the caller), which keeps the warps of a CTA on neighbouring
+// cells: the exact forms gather dot_cr rows per cell, and neighbouring cells
+// share rows in L1.  A warp keeps a window of WWIN visited cells; when the
+// scan leaves it at its end the next WWIN cells are loaded, otherwise a
+// binary search over the visited-cell prefix finds the cell that holds the
+// chunk (a chunk that crosses a window end is scored in two passes).  U
+// candidates per lane are loaded at once and the table entries are added in
+// the reference's order (exact forms) or as a tree (fast form).
+//
+// The fast form with kp == 256 and mp in {8, 16, 32} (ScanCtx::rot) reads
+// the rotated LUT: bank b holds table b mod mp, and at step s lane l reads
+// table k = (l + s) mod mp from bank (l - l mod mp) + k, so the 32 lookups of
+// a warp hit 32 different banks (no conflicts).  The lane rotates its
+// candidate's code by l mod mp bytes first, so that step s uses code byte k;
+// the entries are summed as a tree over s.  l mod mp = flat index mod mp, so
+// the sum order depends on the candidate only, and the fused and split
+// kernels give identical results.
+//
+// WARM == true stores every candidate's (distance, position) at warm[flat];
+// otherwise candidates with a distance word <= tau are appended to out[]
+// (global, capacity cap) through warp-aggregated atomics on st.npend.
 template <int MPC, bool WARM, int U, bool FK>
 __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, QState &st, const ScanCtx &c,
                                             uint32_t first, uint32_t limit, uint32_t tau, uint64_t *warm,
@@ -686,7 +741,19 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
     CellWin *W = S.wwin + wid * WWIN;
     const uint32_t lut_s = (uint32_t)__cvta_generic_to_shared(S.lut);
     constexpr bool KP256 = FK && MPC > 0;
+    constexpr bool ROTC = MPC == 8 || MPC == 16 || MPC == 32;
+    const bool rawm = !FK && c.raw_dim > 0;
     const bool fast = FK || c.fast;
+    const bool rot = ROTC && (FK || c.rot);
+    // rotated LUT: this lane's shared address of step s (mp <= 16: kept in
+    // registers; mp == 32: computed per lookup)
+    constexpr int NROFF = (ROTC && MPC <= 16) ? MPC : 1;
+    uint32_t roff[NROFF];
+    if constexpr (ROTC && MPC <= 16) {
+#pragma unroll
+        for (int s2 = 0; s2 < MPC; s2++)
+            roff[s2] = lut_s + ((uint32_t)((lane & ~(MPC - 1)) + ((lane + s2) & (MPC - 1))) << 2);
+    }
     uint32_t whi = 0;
     int wcn = 0, wci = -1;
     // this lane's window index: candidates only move forward within a window,
@@ -766,16 +833,17 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
                 r_next = 0;  // the cached cell belongs to the old window
             }
             const uint32_t e2 = min(end, whi);
-            // loads of U candidates per lane, issued together
+            // loads of U candidates per lane, issued together (the lanes whose
+            // candidate lies in [f, e2) of this pass)
             uint32_t pos[U], h34[U];
             float dd[U], vt[U];
             CodeWords<MPC> cwd[U];
             int ci = ci_l;
 #pragma unroll
             for (int u = 0; u < U; u++) {
-                const uint32_t ff = f + lane + 32u * u;
+                const uint32_t ff = base + lane + 32u * u;
                 pos[u] = 0xffffffffu;
-                if (ff < e2) {
+                if (ff >= f && ff < e2) {
                     if (ff >= r_next || ff < r_pre) {
                         while (ci + 1 < wcn && W[ci + 1].pre <= ff) ci++;
                         const CellWin cw = W[ci];
@@ -788,8 +856,10 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
                     pos[u] = r_start + (ff - r_pre);
                     dd[u] = r_d0;
                     h34[u] = r_h34;
-                    cwd[u].load(a.codes, pos[u], c.mp);
-                    if (fast) vt[u] = __ldg(a.vterm + pos[u]);
+                    if (!rawm) {
+                        cwd[u].load(a.codes, pos[u], c.mp);
+                        if (fast) vt[u] = __ldg(a.vterm + pos[u]);
+                    }
                 }
             }
             ci_l = ci;
@@ -800,27 +870,61 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
                 if (pos[u] != 0xffffffffu) {
                     float d = dd[u];
                     const uint32_t h3 = h34[u] & 0xffffu, h4 = h34[u] >> 16;
-                    if (fast) {
+                    if (rawm) {
+                        // the real_dist branch (query.h:307-312,
+                        // multi_query.h:255-259, sc_query.h:232-236): the
+                        // exact distance of the candidate's raw row
+                        const int id = __ldg(a.pid + pos[u]);
+                        d = c.raw_u8 ? exact_dist_row(c.qv, (const uint8_t *)a.raw + (size_t)id * c.raw_dim, c.raw_dim,
+                                                      c.raw_vec)
+                                     : exact_dist_row(c.qv, (const float *)a.raw + (size_t)id * c.raw_dim, c.raw_dim,
+                                                      c.raw_vec);
+                    } else if (fast) {
                         // d0 + per-vector term + sum_k LUT[k][c_k], the LUT
                         // entries summed as a tree (independent adds)
                         d = __fadd_rn(d, vt[u]);
-                        if constexpr (MPC > 0) {
-                            float v[MPC];
-                            if constexpr (KP256) {
+                        bool done = false;
+                        if constexpr (ROTC) {
+                            if (rot) {
+                                uint32_t rw[MPC / 4];
+                                rotate_code<MPC>(cwd[u].w, rw, (uint32_t)lane & (MPC - 1));
+                                float v[MPC];
 #pragma unroll
-                                for (int k = 0; k < MPC; k++)
-                                    v[k] = lds_f32(lut_s + (cwd[u].code(k) << 2) + (uint32_t)k * 1024u);
-                            } else {
+                                for (int s2 = 0; s2 < MPC; s2++) {
+                                    const uint32_t cb = __byte_perm(rw[s2 >> 2], 0u, 0x4440u | (uint32_t)(s2 & 3));
+                                    uint32_t ro;
+                                    if constexpr (MPC <= 16) ro = roff[s2];
+                                    else ro = lut_s + ((uint32_t)((lane + s2) & (MPC - 1)) << 2);
+                                    v[s2] = lds_f32(ro + (cb << 7));
+                                }
 #pragma unroll
-                                for (int k = 0; k < MPC; k++) v[k] = S.lut[k * c.kp + cwd[u].code(k)];
+                                for (int s2 = 1; s2 < MPC; s2 <<= 1)
+#pragma unroll
+                                    for (int k = 0; k + s2 < MPC; k += 2 * s2) v[k] = __fadd_rn(v[k], v[k + s2]);
+                                d = __fadd_rn(d, v[0]);
+                                done = true;
                             }
+                        }
+                        if (!done) {
+                            if constexpr (MPC > 0) {
+                                float v[MPC];
+                                if constexpr (KP256) {
 #pragma unroll
-                            for (int s2 = 1; s2 < MPC; s2 <<= 1)
+                                    for (int k = 0; k < MPC; k++)
+                                        v[k] = lds_f32(lut_s + (cwd[u].code(k) << 2) + (uint32_t)k * 1024u);
+                                } else {
 #pragma unroll
-                                for (int k = 0; k + s2 < MPC; k += 2 * s2) v[k] = __fadd_rn(v[k], v[k + s2]);
-                            d = __fadd_rn(d, v[0]);
-                        } else {
-                            for (int k = 0; k < cwd[u].n(c.mp); k++) d = __fadd_rn(d, S.lut[k * c.kp + cwd[u].code(k)]);
+                                    for (int k = 0; k < MPC; k++) v[k] = S.lut[k * c.kp + cwd[u].code(k)];
+                                }
+#pragma unroll
+                                for (int s2 = 1; s2 < MPC; s2 <<= 1)
+#pragma unroll
+                                    for (int k = 0; k + s2 < MPC; k += 2 * s2) v[k] = __fadd_rn(v[k], v[k + s2]);
+                                d = __fadd_rn(d, v[0]);
+                            } else {
+                                for (int k = 0; k < cwd[u].n(c.mp); k++)
+                                    d = __fadd_rn(d, S.lut[k * c.kp + cwd[u].code(k)]);
+                            }
                         }
                     } else if (c.imi) {
                         // multi_query.h:237-254: two adds per subspace
@@ -841,7 +945,7 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
                         }
                     }
                     du = f2o(d);
-                    if (WARM) warm[f + lane + 32u * u] = ((uint64_t)du << 32) | pos[u];
+                    if (WARM) warm[base + lane + 32u * u] = ((uint64_t)du << 32) | pos[u];
                     else pass = du <= tau;
                 }
                 if (!WARM) {
@@ -913,12 +1017,17 @@ __device__ uint32_t block_kth_hi(const uint64_t *keys, int n, int k, uint32_t *h
 #ifndef SCG_SCAN_MIN_BLOCKS
 #define SCG_SCAN_MIN_BLOCKS 4
 #endif
+// ... of the fast form's scan-only kernel (its 32 KB rotated LUT leaves room
+// for fewer CTAs, each with more registers)
+#ifndef SCG_SCAN_FK_MIN_BLOCKS
+#define SCG_SCAN_FK_MIN_BLOCKS 3
+#endif
 
 // PART 0: selection and scan fused; 1: selection only, publishing each
 // query's visited cells (a.qmeta, a.pool_*); 2: scan only, from them.  FK:
 // the scan-only kernel of the fast form with kp == 256 (scan_chunks).
 template <int MPC, int U, int PART, bool FK = false>
-__global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
+__global__ void __launch_bounds__(NT, PART == 2   ? (FK ? SCG_SCAN_FK_MIN_BLOCKS : SCG_SCAN_MIN_BLOCKS)
                                       : PART == 1 ? SCG_SELECT_MIN_BLOCKS
                                                   : SCG_SEARCH_MIN_BLOCKS) k_search(SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -926,7 +1035,7 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
     __shared__ QState st;
     __shared__ int s_q;
     Smem S;
-    carve(a.mode, a.kc, a.mp, a.kp, PART, &S, smem);
+    carve(a.mode, a.kc, a.mp, a.kp, PART, a.rot, a.raw_dim, &S, smem);
     const int tid = threadIdx.x;
     const int kc = a.kc, mp = a.mp, kp = a.kp;
     const int kcP = next_pow2(kc);
@@ -961,8 +1070,20 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
         const int R = a.R;
         const float *dqc = a.dqc + (size_t)q * a.mc * kc;
         const float qn0 = a.qn[2 * q], qn1 = a.qn[2 * q + 1], qs = a.qsum[q];
-        if constexpr (PART != 1)
-            for (int i = tid; i < mp * kp; i += NT) S.lut[i] = a.dqr[(size_t)q * mp * kp + i];
+        if constexpr (PART != 1) {
+            const float *src = a.dqr + (size_t)q * mp * kp;
+            if (a.raw_dim > 0) {
+                // the exact-distance scan keeps the query instead of a LUT
+                for (int i = tid; i < a.raw_dim; i += NT) S.lut[i] = a.Q[(size_t)q * a.raw_dim + i];
+            } else if (a.rot) {
+                // rotated LUT: word c * 32 + b holds table (b mod mp) at code
+                // c, so bank b serves table b mod mp (32 / mp copies)
+                for (int wd = tid; wd < ROT_LUT_BYTES / 4; wd += NT)
+                    S.lut[wd] = __ldg(src + (size_t)(wd & (mp - 1)) * 256 + (wd >> 5));
+            } else {
+                for (int i = tid; i < mp * kp; i += NT) S.lut[i] = src[i];
+            }
+        }
 
         bool nothing_q = false;  // the query visits nothing (T <= 0 or w <= 0)
         int nvis = 0;
@@ -1471,6 +1592,12 @@ __global__ void __launch_bounds__(NT, PART == 2   ? SCG_SCAN_MIN_BLOCKS
             c.imi = imi;
             c.sc = sc;
             c.fast = fast;
+            c.rot = a.rot != 0;
+            c.raw_dim = a.raw_dim;
+            c.raw_u8 = a.raw_u8 != 0;
+            c.raw_vec = a.raw_dim > 0 && ((reinterpret_cast<uintptr_t>(a.raw) & 15) == 0) &&
+                        (((size_t)a.raw_dim * (a.raw_u8 ? 1 : 4)) % 16 == 0);
+            c.qv = S.lut;
             c.qs = qs;
             c.dqc = dqc;
             const uint32_t K = Svis < (uint32_t)WARMN ? Svis : (uint32_t)WARMN;
@@ -1565,22 +1692,31 @@ int grant_smem(size_t smem) {
     return SCG_OK;
 }
 
-template <int MPC, int U, int PART>
+template <int MPC, int U, int PART, bool FK = false>
 int occupancy(size_t smem) {
-    if (grant_smem<MPC, U, PART, false>(smem)) return 0;
+    if (grant_smem<MPC, U, PART, FK>(smem)) return 0;
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<MPC, U, PART, false>, NT, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<MPC, U, PART, FK>, NT, smem);
     return nb;
 }
 
+// fk: the scan-only kernel of the fast form with kp == 256 (its own variant).
+template <int MPC, int U, int PART>
+int occupancy_fk(size_t smem, bool fk) {
+    if constexpr (PART == 2 && MPC > 0) {
+        if (fk) return occupancy<MPC, U, PART, true>(smem);
+    }
+    return occupancy<MPC, U, PART, false>(smem);
+}
+
 template <int U, int PART>
-int occupancy_mp(int mp, size_t smem) {
+int occupancy_mp(int mp, size_t smem, bool fk = false) {
     switch (mp) {
-        case 4: return occupancy<4, U, PART>(smem);
-        case 8: return occupancy<8, U, PART>(smem);
-        case 16: return occupancy<16, U, PART>(smem);
-        case 32: return occupancy<32, U, PART>(smem);
-        default: return occupancy<0, U, PART>(smem);
+        case 4: return occupancy_fk<4, U, PART>(smem, fk);
+        case 8: return occupancy_fk<8, U, PART>(smem, fk);
+        case 16: return occupancy_fk<16, U, PART>(smem, fk);
+        case 32: return occupancy_fk<32, U, PART>(smem, fk);
+        default: return occupancy_fk<0, U, PART>(smem, fk);
     }
 }
 
@@ -1598,7 +1734,8 @@ int launch(const SearchArgs &a, int grid, size_t smem, cudaStream_t s) {
 template <int MPC, int U, int PART>
 int launch_fk(const SearchArgs &a, int grid, size_t smem, cudaStream_t s) {
     if constexpr (PART == 2 && MPC > 0) {
-        if (a.precision == SCG_FAST && a.kp == 256) return launch<MPC, U, PART, true>(a, grid, smem, s);
+        if (a.precision == SCG_FAST && a.kp == 256 && a.raw_dim == 0)
+            return launch<MPC, U, PART, true>(a, grid, smem, s);
     }
     return launch<MPC, U, PART, false>(a, grid, smem, s);
 }

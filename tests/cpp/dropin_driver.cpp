@@ -4,6 +4,7 @@
 // caller-owned scratch, results freed with ::delete.
 //
 //   dropin_driver search <ivf|imi|sc> <cq.ctr_> <pq.ctr_> <x.edat_> <q.fvecs> <dim> <R> <w> <T> <out.txt>
+//                        [<base.fvecs>|- [M]]   (base: load_data + real_dist = true; M: the coarse-list argument)
 //   dropin_driver encode <0|2> <cq.ctr_> <pq.ctr_> <x.fvecs> <outdir> <prefix>
 //   dropin_driver quantize <x.fvecs> <dim> <m> <nsc> <out_prefix>      (PQQuantizer, test_quantizer.cpp-style)
 //   dropin_driver residual <pq|sc> <x.fvecs> <dim> <m> <cq.ctr_> <out.fvecs>
@@ -24,6 +25,9 @@ using namespace SC;
 static int search(int argc, char **argv) {
     const char *mode = argv[2];
     int d = atoi(argv[7]), R = atoi(argv[8]), w = atoi(argv[9]), T = atoi(argv[10]);
+    const char *base = argc > 12 && strcmp(argv[12], "-") ? argv[12] : nullptr;
+    const bool real_dist = base != nullptr;
+    const int M_arg = argc > 13 ? atoi(argv[13]) : 0;
     float *data = nullptr;
     int N = load_and_convert_data<float, float>(argv[6], data, 4, d, false);
     std::ofstream out(argv[11]);
@@ -35,8 +39,10 @@ static int search(int argc, char **argv) {
         MultiQuery q;
         q.load_codebooks(argv[3], argv[4], false);
         q.load_encoded_data(argv[5], false);
+        if (base) q.load_data<float>(base, 4, false);
         q.pre_compute1();
         int kc = q.get_full_size() > 0 ? (int)(0.5 + std::sqrt((double)q.get_full_size())) : 0;
+        const int M = M_arg > 0 ? M_arg : kc;
         float *v_tmp = new float[2 * kc + w], *q2 = new float[2];
         int *it = new int[2 * kc], *h1 = new int[w], *h2 = new int[w], *h3 = new int[w], *h4 = new int[w];
         int *s1 = new int[w], *s2 = new int[w], *pb = new int[w], *cache = new int[w];
@@ -45,7 +51,7 @@ static int search(int argc, char **argv) {
         for (int i = 0; i < N; i++) {
             int e = 0;
             q.search_multi2(data + (size_t)i * d, v_tmp, dist, q2, it, result, h1, h2, h3, h4, s1, s2, pb, cache,
-                            trav, sum, R, w, T, kc, e, t1, t2, false, false);
+                            trav, sum, R, w, T, M, e, t1, t2, real_dist, false);
             if (trav[0]) bad++;  // test_multi_query.cpp:191
             out << sum << " " << e;
             for (int j = 0; j < (R > sum ? sum : R); j++) out << " " << result[j] << ":" << dist[j];
@@ -59,8 +65,10 @@ static int search(int argc, char **argv) {
         SCQuery q;
         q.load_codebooks(argv[3], argv[4], false);
         q.load_encoded_data(argv[5], false);
+        if (base) q.load_data<float>(base, 4, false);
         q.pre_compute1();
         int kc = q.get_full_size();
+        const int M = M_arg > 0 ? M_arg : kc;
         float *v_tmp = new float[kc + w];
         int *it = new int[kc], *h1 = new int[w], *h2 = new int[w], *h3 = new int[w], *h4 = new int[w];
         int *s1 = new int[w], *s2 = new int[w], *pb = new int[w], *cache = new int[w];
@@ -68,7 +76,7 @@ static int search(int argc, char **argv) {
         trav[0] = true;  // test_sc_query.cpp:160-161
         for (int i = 0; i < N; i++) {
             q.search_mr_ivf(data + (size_t)i * d, v_tmp, dist, it, result, h1, h2, h3, h4, s1, s2, pb, cache, trav,
-                            sum, R, w, T, kc, false, false);
+                            sum, R, w, T, M, real_dist, false);
             if (!trav[0] || trav[1]) bad++;  // test_sc_query.cpp:182-183
             out << sum << " 0";
             for (int j = 0; j < (R > sum ? sum : R); j++) out << " " << result[j] << ":" << dist[j];
@@ -82,12 +90,13 @@ static int search(int argc, char **argv) {
         PQQuery q;
         q.load_codebooks(argv[3], argv[4], false);
         q.load_encoded_data(argv[5], false);
+        if (base) q.load_data<float>(base, 4, false);
         q.pre_compute1();
         int kc = q.get_full_size();
         float *v_tmp = new float[kc];
         int *buckets = new int[kc], *bk = new int[kc];
         for (int i = 0; i < N; i++) {
-            q.search_ivfadc(data + (size_t)i * d, v_tmp, dist, result, buckets, bk, sum, R, w, T, false, false);
+            q.search_ivfadc(data + (size_t)i * d, v_tmp, dist, result, buckets, bk, sum, R, w, T, real_dist, false);
             out << sum << " 0";
             for (int j = 0; j < (R > sum ? sum : R); j++) out << " " << result[j] << ":" << dist[j];
             out << "\n";

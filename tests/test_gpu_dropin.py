@@ -62,6 +62,33 @@ def test_search_through_dropin(driver, oracle_mod, tmp_path, name, mode, tag):
             assert e == ix.search_one(mode, c["Q"][i], w, T)["empty"]
 
 
+@pytest.mark.parametrize("name,mode,tag", [("imi_d32", O.IMI, "imi"), ("sc_d32", O.SC, "sc"),
+                                           ("ivf_d32", O.IVFADC, "ivf")])
+def test_real_dist_through_dropin(driver, oracle_mod, tmp_path, name, mode, tag):
+    """real_dist = true after load_data: every candidate of the visited cells
+    scored by its exact distance (query.h:307-312, multi_query.h:255-259,
+    sc_query.h:232-236), the R best returned -- the oracle's real_dist
+    branch in the exact order, bit for bit."""
+    c = helpers.load_case(os.path.join(helpers.GOLDEN, name + ".npz"))
+    D, mc, kc, mp, kp = (int(c[k]) for k in ("D", "mc", "kc", "mp", "kp"))
+    formats.write_ctr(tmp_path / "cq.ctr_", c["cq"], kc, mc, D)
+    formats.write_ctr(tmp_path / "pq.ctr_", c["pq"], kp, mp, D)
+    formats.write_edat(tmp_path / "x.edat_", c["L"], c["pid"], c["icodes"])
+    formats.write_vecs(tmp_path / "q.fvecs", c["Q"])
+    formats.write_vecs(tmp_path / "x.fvecs", c["X"].astype(np.float32))
+    T, w, R = 300, (16 if mode == O.IVFADC else 1 << 16), 20
+    subprocess.run([driver, "search", tag, str(tmp_path / "cq.ctr_"), str(tmp_path / "pq.ctr_"),
+                    str(tmp_path / "x.edat_"), str(tmp_path / "q.fvecs"), str(D), str(R), str(w), str(T),
+                    str(tmp_path / "out.txt"), str(tmp_path / "x.fvecs")], check=True)
+    rows = parse(tmp_path / "out.txt")
+    ix = helpers.oracle_index(O, c)
+    oi, od, osum = ix.search(mode, c["Q"], R, w, T, order=O.ORDER_EXACT, real_dist=True)
+    for i, (s, e, ids, d) in enumerate(rows):
+        assert s == osum[i]
+        m = min(R, s)
+        assert helpers.same_topk(np.array(ids), np.array(d, np.float32), oi[i], od[i], m)
+
+
 @pytest.mark.parametrize("name,nc", [("imi_d32", 0), ("sc_d32", 2)])
 def test_encoder_through_dropin(driver, oracle_mod, tmp_path, name, nc):
     c = helpers.load_case(os.path.join(helpers.GOLDEN, name + ".npz"))

@@ -91,6 +91,39 @@ def test_rerank_unaligned_rows(oracle_mod, mode, mc, kc, kind, D, mp):
     g.close()
 
 
+@pytest.mark.parametrize("mode,mc,kc,kind,D,mp", [(O.IMI, 2, 32, "u8", 48, 8), (O.SC, 1, 32, "f32", 48, 8),
+                                                  (O.IVFADC, 1, 64, "f32", 30, 6), (O.IMI, 2, 16, "u8", 40, 8)])
+def test_exact_distance_every_candidate(oracle_mod, mode, mc, kc, kind, D, mp):
+    """rerank = -1, the reference's real_dist branch (query.h:307-312,
+    multi_query.h:255-259, sc_query.h:232-236): every candidate of the visited
+    cells gets its exact distance and the R smallest are returned -- the same
+    candidate counts, ids and bit-identical distances as the oracle's
+    real_dist search in the exact order (the fast form's coarse tables may
+    move a boundary cell of a few queries), split and fused kernels alike."""
+    import scgpu
+    X, Q, cq, pq, L, pid, co, ix, (D, mc, kc, mp, kp) = _build(mode, mc, kc, D, kind, 90 + mode, mp=mp)
+    g = scgpu.Index(0)
+    g.load_codebooks(cq, kc, mc, pq, kp, mp, D)
+    g.load_csr(L, pid, co)
+    g.precompute()
+    g.load_raw(X.astype(np.uint8) if kind == "u8" else X.astype(np.float32))
+    w = kc if mode == O.IVFADC else 1 << 20
+    for R, T in ((20, 3000), (100, 12000), (1, 50)):
+        oi, od, osum = ix.search(mode, Q, R, w, T, order=O.ORDER_EXACT, real_dist=True)
+        for prec in (scgpu.FP32_EXACT, scgpu.FAST):
+            for split in (True, False):
+                g.set_kernel_split(split)
+                ids, d, sums = g.search(MODES[mode], Q, R, w, T, precision=prec, rerank=-1)
+                same = [sums[i] == osum[i] and helpers.same_topk(ids[i], d[i], oi[i], od[i], R)
+                        for i in range(Q.shape[0])]
+                if prec == scgpu.FP32_EXACT:
+                    assert all(same), (R, T, split, np.nonzero(~np.array(same)))
+                else:
+                    # the fast form's coarse tables may move a boundary cell
+                    assert np.mean(same) >= 0.9, (R, T, split, np.mean(same))
+    g.close()
+
+
 def test_rerank_errors(oracle_mod):
     import scgpu
     X, Q, cq, pq, L, pid, co, ix, (D, mc, kc, mp, kp) = _build(O.IMI, 2, 16, 32, "u8", 70)
@@ -101,8 +134,11 @@ def test_rerank_errors(oracle_mod):
     with pytest.raises(scgpu.ScgError) as e:      # no raw vectors yet
         g.search(1, Q, 10, 1 << 20, 500, rerank=100)
     assert e.value.code == -6
+    with pytest.raises(scgpu.ScgError) as e:      # every-candidate branch without raw vectors
+        g.search(1, Q, 10, 1 << 20, 500, rerank=-1)
+    assert e.value.code == -6
     g.load_raw(X)
-    for bad in (5, 2000, -1):                    # L < R, L > 1024, every-candidate branch
+    for bad in (5, 2000, -2):                    # L < R, L > 1024, no such mode
         with pytest.raises(scgpu.ScgError) as e:
             g.search(1, Q, 10, 1 << 20, 500, rerank=bad)
         assert e.value.code == -1
