@@ -238,6 +238,8 @@ def ref():
         _ref.ref_search_batch_ex.restype = ctypes.c_int
         _ref.ref_search_one.restype = ctypes.c_int
         _ref.ref_encode.restype = ctypes.c_int
+        _ref.ref_calc_recall.restype = ctypes.c_int
+        _ref.ref_calc_comb_recall.restype = ctypes.c_int
     return _ref
 
 
@@ -294,6 +296,22 @@ def ref_search_batch(ix, mode, Q, R, w, T, nthreads=0, real_dist=False, Tq=None,
     if rc != 0:
         raise RuntimeError("ref_search_batch failed")
     return ids, dist, sums, sec.value
+
+
+def ref_calc_recall(result, gt, R):
+    """Evaluation::calc_recall of the reference: the count of queries whose
+    ground truth is among the first R of result[N][R]."""
+    result = np.ascontiguousarray(result, np.int32)
+    gt = np.ascontiguousarray(gt, np.int32)
+    return ref().ref_calc_recall(_p(result, _i32p), _p(gt, _i32p), R, result.shape[0])
+
+
+def ref_calc_comb_recall(results, gt, R):
+    """Evaluation::calc_comb_recall of the reference over S arrays [N][R]."""
+    arrs = [np.ascontiguousarray(r, np.int32) for r in results]
+    gt = np.ascontiguousarray(gt, np.int32)
+    ptrs = (_i32p * len(arrs))(*[_p(a, _i32p) for a in arrs])
+    return ref().ref_calc_comb_recall(ptrs, _p(gt, _i32p), R, arrs[0].shape[0], len(arrs))
 
 
 def ref_encode(cq_path, pq_path, fvecs_path, nc, n, mc, mp, nthreads=0):

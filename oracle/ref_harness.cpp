@@ -29,6 +29,7 @@
 #include "sc_query.h"
 #include "encoder.h"
 #include "sc_encoder.h"
+#include "evaluation.h"
 
 using namespace SC;
 
@@ -332,6 +333,22 @@ int ref_build_edat(const char *cq_path, const char *pq_path, const char *fvecs_p
     e.distribution(false);
     e.output(db_path, prefix, false);
     return 0;
+}
+
+/* Evaluation::calc_recall (evaluation.h:58-92) and calc_comb_recall
+ * (evaluation.h:103-140) of the reference, on caller arrays. */
+int ref_calc_recall(int *result, int *gt, int R, int N) {
+    Evaluation e;
+    int recall = 0;
+    e.calc_recall(result, gt, R, N, recall, false);
+    return recall;
+}
+
+int ref_calc_comb_recall(int **results, int *gt, int R, int N, int S) {
+    Evaluation e;
+    int recall = 0;
+    e.calc_comb_recall(results, gt, R, N, S, recall, false);
+    return recall;
 }
 
 } // extern "C"

@@ -1,8 +1,9 @@
 /*
  * evaluation.h -- drop-in for the reference's Evaluation
  * (include/evaluation.h:20-25): ground truth (first column of an .ivecs
- * file) and recall@R = the number of queries whose true nearest neighbour is
- * among their first R results (evaluation.h:58-92).
+ * file), recall@R = the number of queries whose true nearest neighbour is
+ * among their first R results (evaluation.h:58-92), and the same over the
+ * union of several result sets (evaluation.h:103-140).
  */
 #ifndef SCG_DROPIN_EVALUATION_H_
 #define SCG_DROPIN_EVALUATION_H_
@@ -27,6 +28,23 @@ public:
                     recall++;
                     break;
                 }
+        }
+        if (verbose) std::cout << "Recall@" << R << " = " << recall << std::endl;
+    }
+    /* Evaluation::calc_comb_recall (evaluation.h:103-140): the number of
+     * queries whose true nearest neighbour is among the first R results of
+     * any of the S result arrays results[0..S) (each [N][R]). */
+    void calc_comb_recall(int **results, int *groundtruth, int R, int N, int S, int &recall, bool verbose) {
+        recall = 0;
+        for (int i = 0; i < N; i++) {
+            bool found = false;
+            for (int j = 0; j < S && !found; j++)
+                for (int k = 0; k < R; k++)
+                    if (results[j][(size_t)i * R + k] == groundtruth[i]) {
+                        found = true;
+                        break;
+                    }
+            if (found) recall++;
         }
         if (verbose) std::cout << "Recall@" << R << " = " << recall << std::endl;
     }

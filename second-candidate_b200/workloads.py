@@ -153,6 +153,17 @@ def recall_at(ids, gt, R):
     return float((ids == np.asarray(gt)[:, None]).any(axis=1).mean())
 
 
+def comb_recall_at(id_sets, gt, R):
+    """Evaluation::calc_comb_recall (evaluation.h:103-140): the fraction of
+    queries whose true nearest neighbour is among the first R ids of any of
+    the result sets (each [N][>= R])."""
+    g = np.asarray(gt)[:, None]
+    hit = np.zeros(g.shape[0], bool)
+    for ids in id_sets:
+        hit |= (np.asarray(ids)[:, :R] == g).any(axis=1)
+    return float(hit.mean())
+
+
 # ---------------------------------------------------------------------------
 # Full-size workloads, built on the GPU (data preparation for bench.py; the
 # timed search never runs through this code).
