@@ -15,9 +15,9 @@ int search_launch_u2(const SearchArgs &a, int part, int grid, size_t smem, cudaS
 int search_launch_u4(const SearchArgs &a, int part, int grid, size_t smem, cudaStream_t s);
 int search_launch_u8(const SearchArgs &a, int part, int grid, size_t smem, cudaStream_t s);
 int search_launch_select(const SearchArgs &a, int grid, size_t smem, cudaStream_t s);
-int search_occupancy_u2(int mp, int part, size_t smem, bool fk);
-int search_occupancy_u4(int mp, int part, size_t smem, bool fk);
-int search_occupancy_u8(int mp, int part, size_t smem, bool fk);
+int search_occupancy_u2(int mp, int part, size_t smem, int var);
+int search_occupancy_u4(int mp, int part, size_t smem, int var);
+int search_occupancy_u8(int mp, int part, size_t smem, int var);
 int search_occupancy_select(size_t smem);
 
 size_t search_smem_bytes(int mode, int kc, int mp, int kp, int part, int rot, int qdim) {
@@ -29,11 +29,13 @@ bool search_rot_form(int precision, int mp, int kp) { return rot_form(precision,
 static int occupancy_query(int mode, int kc, int mp, int kp, int upl, int part, int rot, int qdim) {
     const size_t smem = search_smem_bytes(mode, kc, mp, kp, part, rot, qdim);
     if (part == 1) return search_occupancy_select(smem);
-    const bool fk = part == 2 && rot;  // the rotated LUT's scan runs the fast-form variant
+    // the variant the launch picks: exact-distance scan, the fast form's
+    // scan-only kernel (rotated LUT), or the general ADC kernel
+    const int var = qdim > 0 ? V_EXACT : ((part == 2 && rot) ? V_FAST256 : V_ADC);
     switch (upl) {
-        case 2: return search_occupancy_u2(mp, part, smem, fk);
-        case 8: return search_occupancy_u8(mp, part, smem, fk);
-        default: return search_occupancy_u4(mp, part, smem, fk);
+        case 2: return search_occupancy_u2(mp, part, smem, var);
+        case 8: return search_occupancy_u8(mp, part, smem, var);
+        default: return search_occupancy_u4(mp, part, smem, var);
     }
 }
 

@@ -46,6 +46,7 @@ constexpr int NWARP = NT / 32;
 constexpr int HBITS = 11;
 constexpr int HBINS = 1 << HBITS;
 constexpr int TIECAP = 64;
+constexpr int RBINS = 256;      // bins of the 8-bit radix selects of the scan phase (one per thread)
 constexpr int RMAX = 1024;      // largest R
 #ifndef SCG_WARMN
 #define SCG_WARMN 4096
@@ -55,6 +56,10 @@ constexpr int WWIN = 32;        // per-warp window of visited cells
 // Candidates per lane per claimed chunk (U, a template parameter of the
 // scan: 2, 4 or 8); a warp claims 32 * U candidates at a time.
 constexpr int SBCAP = 2048;     // sorted coarse prefix capacity
+// Kernel variants (template parameter VAR): the ADC scan in any form, the
+// scan-only kernel of the fast form with kp == 256 (its own chunking and
+// LUT), and the exact-distance scan over raw rows (rerank = -1).
+constexpr int V_ADC = 0, V_FAST256 = 1, V_EXACT = 2;
 constexpr int MAX_ROUNDS = 64;
 
 struct CellWin {
@@ -140,7 +145,14 @@ __host__ __device__ inline size_t carve(int mode, int kc, int mp, int kp, int pa
     if (part != 1) {
         // scan phase (aliases the selection phase)
         off = phase0;
-        if (s) s->wwin = (CellWin *)(base + off);
+        // the radix-select bins and the tie buffer of the threshold and the
+        // final merge alias the per-warp cell windows: both run between
+        // scans, when no window is live
+        if (s) {
+            s->wwin = (CellWin *)(base + off);
+            s->hist2 = (uint32_t *)(base + off);
+            s->ties2 = (uint64_t *)(base + off + (size_t)RBINS * 4);
+        }
         off += (size_t)NWARP * WWIN * sizeof(CellWin);
         if (s) {
             s->warm = (uint64_t *)(base + off);
@@ -148,16 +160,13 @@ __host__ __device__ inline size_t carve(int mode, int kc, int mp, int kp, int pa
             s->tmp = s->warm + RMAX;
         }
         off += (size_t)WARMN * 8;
-        if (s) s->hist2 = (uint32_t *)(base + off);
-        off += (size_t)HBINS * 4;
-        if (s) s->ties2 = (uint64_t *)(base + off);
-        off += (size_t)TIECAP * 8;
         end2 = off;
     }
     return end1 > end2 ? end1 : end2;
 }
 
 static_assert(2 * RMAX <= WARMN, "top-R buffers live inside the warm-up scores");
+static_assert(RBINS * 4 + TIECAP * 8 <= NWARP * WWIN * sizeof(CellWin), "select bins alias the cell windows");
 static_assert(WARMN % 32 == 0, "scan chunks start at multiples of 32 (the rotated LUT relies on it)");
 
 // ---------------------------------------------------------------------------
@@ -447,8 +456,8 @@ __device__ __forceinline__ uint32_t cell_of(const Lists &L, uint32_t rank) {
 template <int MPC>
 struct CodeWords {
     uint32_t w[(MPC + 3) / 4];
-    __device__ __forceinline__ void load(const uint8_t *codes, uint32_t pos, int) {
-        const uint8_t *p = codes + (size_t)pos * MPC;
+    __device__ __forceinline__ void load(const uint8_t *codes, uint32_t pos, int) { load_at(codes + (size_t)pos * MPC); }
+    __device__ __forceinline__ void load_at(const uint8_t *p) {
         if constexpr (MPC % 16 == 0) {
 #pragma unroll
             for (int i = 0; i < MPC / 16; i++) {
@@ -513,6 +522,40 @@ struct CodeWords<0> {
             atomicAdd((unsigned long long *)&a.phase_cycles[(i)], (unsigned long long)(v));        \
     } while (0)
 
+// The k-th smallest (1-based) of n 32-bit words word(i): a radix select of
+// 4 x 8 bits over RBINS = NT bins (one per thread).  Returns the word;
+// `need` becomes how many entries equal to it complete the k smallest.
+template <class Word>
+__device__ uint32_t radix_kth_word(Word word, int n, uint64_t k, uint32_t *hist, uint64_t *red, QState &st,
+                                   uint64_t &need) {
+    static_assert(RBINS == NT, "one bin per thread");
+    const int tid = threadIdx.x;
+    uint32_t prefix = 0;
+    need = k;
+#pragma unroll 1
+    for (int sh = 24; sh >= 0; sh -= 8) {
+        hist[tid] = 0;
+        __syncthreads();
+        for (int i = tid; i < n; i += NT) {
+            const uint32_t v = word(i);
+            if (sh == 24 || (v >> (sh + 8)) == (prefix >> (sh + 8))) atomicAdd(&hist[(v >> sh) & 255u], 1u);
+        }
+        __syncthreads();
+        const uint64_t cnt = hist[tid];
+        uint64_t tot;
+        const uint64_t ex = block_exscan(cnt, red, tot);
+        if (ex < need && ex + cnt >= need) {
+            st.s_bin = (uint32_t)tid;
+            st.s_acc = ex;
+        }
+        __syncthreads();
+        prefix |= st.s_bin << sh;
+        need -= st.s_acc;
+        __syncthreads();
+    }
+    return prefix;
+}
+
 // The R smallest (distance, id) keys of nb pending entries by one bitonic
 // sort in top[] (room for WARMN keys, nb <= WARMN), in order; pid != null
 // turns the entries' CSR positions into ids first.
@@ -569,42 +612,11 @@ __device__ void merge_topk(uint64_t *top, uint64_t *pend, uint64_t *tmp, uint32_
         __syncthreads();
         return;
     }
-    // radix select (11 + 11 + 10 bits) of the R-th smallest distance word
-    uint32_t prefix = 0;
-    uint64_t need = (uint64_t)R;
-#pragma unroll
-    for (int p = 0; p < 3; p++) {
-        const int sh = p == 0 ? 21 : (p == 1 ? 10 : 0), bits = p == 2 ? 10 : 11, nbins = 1 << bits, hs = sh + bits;
-        for (int i = tid; i < nbins; i += NT) hist[i] = 0;
-        __syncthreads();
-        for (int i = tid; i < n; i += NT) {
-            uint32_t v = (uint32_t)((i < na ? top[i] : pend[i - na]) >> 32);
-            if (hs < 32 && (v >> hs) != (prefix >> hs)) continue;
-            atomicAdd(&hist[(v >> sh) & (nbins - 1)], 1u);
-        }
-        __syncthreads();
-        const int per = (nbins + NT - 1) / NT;
-        const int b0 = tid * per;
-        uint64_t mine = 0;
-        for (int i = 0; i < per; i++)
-            if (b0 + i < nbins) mine += hist[b0 + i];
-        uint64_t tot;
-        uint64_t run = block_exscan(mine, red, tot);
-        for (int i = 0; i < per; i++) {
-            int bb = b0 + i;
-            if (bb >= nbins) break;
-            uint64_t nxt = run + hist[bb];
-            if (run < need && nxt >= need) {
-                st.s_bin = (uint32_t)bb;
-                st.s_acc = run;
-            }
-            run = nxt;
-        }
-        __syncthreads();
-        prefix |= st.s_bin << sh;
-        need -= st.s_acc;
-        __syncthreads();
-    }
+    // radix select of the R-th smallest distance word
+    uint64_t need;
+    const uint32_t prefix = radix_kth_word(
+        [&](int i) { return (uint32_t)((i < na ? top[i] : pend[i - na]) >> 32); }, n, (uint64_t)R, hist, red, st,
+        need);
     const uint32_t v = prefix;
     // keep everything below v; gather the entries equal to v
     uint64_t mine = 0;
@@ -674,28 +686,23 @@ struct ScanCtx {
     const float *qv;
 };
 
-// The MPC code bytes of one candidate rotated by rb bytes (byte s of r is
-// byte (s + rb) mod MPC of w): words first (log steps of selects), then the
-// bytes inside a word (funnel shifts).
+// The MPC / 4 code words of one candidate with word i moved to i ^ xw (log
+// steps of selects on a lane-constant xw): word (s ^ x) / 4 of the code is
+// then word s / 4 of the result.
 template <int MPC>
-__device__ __forceinline__ void rotate_code(const uint32_t *w, uint32_t *r, uint32_t rb) {
+__device__ __forceinline__ void permute_words(const uint32_t *w, uint32_t *r, uint32_t xw) {
     constexpr int n = MPC / 4;
-    uint32_t t[n];
 #pragma unroll
-    for (int i = 0; i < n; i++) t[i] = w[i];
-    const uint32_t qw = rb >> 2;
+    for (int i = 0; i < n; i++) r[i] = w[i];
 #pragma unroll
     for (int b = 1; b < n; b <<= 1) {
+        const bool on = (xw & (uint32_t)b) != 0;
         uint32_t x[n];
 #pragma unroll
-        for (int i = 0; i < n; i++) x[i] = t[(i + b) % n];
-        const bool on = (qw & (uint32_t)b) != 0;
+        for (int i = 0; i < n; i++) x[i] = r[i ^ b];
 #pragma unroll
-        for (int i = 0; i < n; i++) t[i] = on ? x[i] : t[i];
+        for (int i = 0; i < n; i++) r[i] = on ? x[i] : r[i];
     }
-    const uint32_t sh = (rb & 3u) * 8u;
-#pragma unroll
-    for (int i = 0; i < n; i++) r[i] = __funnelshift_r(t[i], t[(i + 1) % n], sh);
 }
 
 // One float of shared memory at a 32-bit shared-window address.
@@ -705,34 +712,62 @@ __device__ __forceinline__ float lds_f32(uint32_t addr) {
     return v;
 }
 
+// Sum of the LUT entries of one candidate's code words `w` on the
+// bank-private LUT (see scan_chunks): word permutation by xl / 4, then per
+// step s the byte select, the lane's bank of table s ^ xl and one LDS; the
+// entries summed as a tree over s (the same float as the tree over k).
+template <int MPC>
+__device__ __forceinline__ float rot_lut_sum(const uint32_t *w, const uint32_t *roff, const uint32_t *bsel, uint32_t xl,
+                                             uint32_t lut_s, int lane) {
+    uint32_t pw[MPC / 4];
+    permute_words<MPC>(w, pw, xl >> 2);
+    float v[MPC];
+#pragma unroll
+    for (int s2 = 0; s2 < MPC; s2++) {
+        // code byte s2 ^ x: word (s2 ^ x) / 4 = pw[s2 / 4]
+        const uint32_t cb = __byte_perm(pw[s2 >> 2], 0u, bsel[s2 & 3]);
+        uint32_t ro;
+        if constexpr (MPC <= 16) ro = roff[s2];
+        else ro = lut_s + (((uint32_t)lane - xl + ((uint32_t)s2 ^ xl)) << 2);
+        v[s2] = lds_f32(ro + (cb << 7));
+    }
+#pragma unroll
+    for (int s2 = 1; s2 < MPC; s2 <<= 1)
+#pragma unroll
+        for (int k = 0; k + s2 < MPC; k += 2 * s2) v[k] = __fadd_rn(v[k], v[k + s2]);
+    return v[0];
+}
+
 // Warp-centric ADC scan of the candidates [first, limit), cut into chunks of
-// 32 * U candidates; `first` and every chunk start are multiples of 32, and
-// lane l of a warp scores the chunk's candidates with flat index = l (mod
-// 32).  FK (the fast form with kp == 256): every warp takes an equal,
-// contiguous run of chunks, so it walks its visited cells in order.
+// 32 * U candidates.  FK (the fast form with kp == 256): every warp takes an
+// equal, contiguous run of chunks, so it walks its visited cells in order.
 // Otherwise warps claim chunks from a shared counter (st.next_flat, set to
 // `first` by the caller), which keeps the warps of a CTA on neighbouring
 // cells: the exact forms gather dot_cr rows per cell, and neighbouring cells
 // share rows in L1.  A warp keeps a window of WWIN visited cells; when the
 // scan leaves it at its end the next WWIN cells are loaded, otherwise a
 // binary search over the visited-cell prefix finds the cell that holds the
-// chunk (a chunk that crosses a window end is scored in two passes).  U
-// candidates per lane are loaded at once and the table entries are added in
-// the reference's order (exact forms) or as a tree (fast form).
+// chunk.  U candidates per lane are loaded at once and the table entries are
+// added in the reference's order (exact forms) or as a tree (fast form).
 //
-// The fast form with kp == 256 and mp in {8, 16, 32} (ScanCtx::rot) reads
-// the rotated LUT: bank b holds table b mod mp, and at step s lane l reads
-// table k = (l + s) mod mp from bank (l - l mod mp) + k, so the 32 lookups of
-// a warp hit 32 different banks (no conflicts).  The lane rotates its
-// candidate's code by l mod mp bytes first, so that step s uses code byte k;
-// the entries are summed as a tree over s.  l mod mp = flat index mod mp, so
-// the sum order depends on the candidate only, and the fused and split
-// kernels give identical results.
+// The fast form with kp == 256 and mp in {8, 16, 32} (ScanCtx::rot) reads a
+// bank-private LUT: bank b holds table b mod mp (32 / mp copies), and at
+// step s lane l reads table k = s ^ x, x = l mod mp, from bank
+// (l - x) + k, so the 32 lookups of a warp hit 32 different banks (no
+// conflicts).  The lane permutes its code's words by x / 4 first, so that a
+// byte select with a lane-constant selector gives code byte k.  Summed as a
+// tree over s, step pairs (s, s ^ 1), (s, s ^ 2), ... hold exactly the table
+// pairs of the tree over k, so with commutative adds the sum is the same
+// float for every lane -- identical codes in one cell give identical
+// distances, and all kernels agree.
+//
+// The exact-distance variant (VAR == V_EXACT, rerank = -1) scores each
+// candidate by the distance_l2_square of its raw row instead.
 //
 // WARM == true stores every candidate's (distance, position) at warm[flat];
 // otherwise candidates with a distance word <= tau are appended to out[]
 // (global, capacity cap) through warp-aggregated atomics on st.npend.
-template <int MPC, bool WARM, int U, bool FK>
+template <int MPC, bool WARM, int U, int VAR, bool ROTOK>
 __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, QState &st, const ScanCtx &c,
                                             uint32_t first, uint32_t limit, uint32_t tau, uint64_t *warm,
                                             uint64_t *out, uint32_t cap) {
@@ -740,20 +775,27 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     CellWin *W = S.wwin + wid * WWIN;
     const uint32_t lut_s = (uint32_t)__cvta_generic_to_shared(S.lut);
+    constexpr bool FK = VAR == V_FAST256;
     constexpr bool KP256 = FK && MPC > 0;
-    constexpr bool ROTC = MPC == 8 || MPC == 16 || MPC == 32;
-    const bool rawm = !FK && c.raw_dim > 0;
+    // ROTOK: the kernel can meet the bank-private LUT (the fused kernel and
+    // the fast form's scan-only kernel; the general scan-only kernel never)
+    constexpr bool ROTC = ROTOK && (MPC == 8 || MPC == 16 || MPC == 32);
+    constexpr bool rawm = VAR == V_EXACT;
     const bool fast = FK || c.fast;
     const bool rot = ROTC && (FK || c.rot);
-    // rotated LUT: this lane's shared address of step s (mp <= 16: kept in
-    // registers; mp == 32: computed per lookup)
+    // bank-private LUT: this lane's shared address of step s (mp <= 16: kept
+    // in registers; mp == 32: computed per lookup) and the byte selectors of
+    // code byte (4 j) ^ x within a permuted word
+    const uint32_t xl = (uint32_t)lane & (ROTC ? MPC - 1 : 0);
     constexpr int NROFF = (ROTC && MPC <= 16) ? MPC : 1;
-    uint32_t roff[NROFF];
+    uint32_t roff[NROFF], bsel[4];
     if constexpr (ROTC && MPC <= 16) {
 #pragma unroll
         for (int s2 = 0; s2 < MPC; s2++)
-            roff[s2] = lut_s + ((uint32_t)((lane & ~(MPC - 1)) + ((lane + s2) & (MPC - 1))) << 2);
+            roff[s2] = lut_s + (((uint32_t)lane - xl + ((uint32_t)s2 ^ xl)) << 2);
     }
+#pragma unroll
+    for (int j = 0; j < 4; j++) bsel[j] = 0x4440u | ((uint32_t)j ^ (xl & 3u));
     uint32_t whi = 0;
     int wcn = 0, wci = -1;
     // this lane's window index: candidates only move forward within a window,
@@ -833,17 +875,16 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
                 r_next = 0;  // the cached cell belongs to the old window
             }
             const uint32_t e2 = min(end, whi);
-            // loads of U candidates per lane, issued together (the lanes whose
-            // candidate lies in [f, e2) of this pass)
+            // loads of U candidates per lane, issued together
             uint32_t pos[U], h34[U];
             float dd[U], vt[U];
             CodeWords<MPC> cwd[U];
             int ci = ci_l;
 #pragma unroll
             for (int u = 0; u < U; u++) {
-                const uint32_t ff = base + lane + 32u * u;
+                const uint32_t ff = f + lane + 32u * u;
                 pos[u] = 0xffffffffu;
-                if (ff >= f && ff < e2) {
+                if (ff < e2) {
                     if (ff >= r_next || ff < r_pre) {
                         while (ci + 1 < wcn && W[ci + 1].pre <= ff) ci++;
                         const CellWin cw = W[ci];
@@ -886,22 +927,7 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
                         bool done = false;
                         if constexpr (ROTC) {
                             if (rot) {
-                                uint32_t rw[MPC / 4];
-                                rotate_code<MPC>(cwd[u].w, rw, (uint32_t)lane & (MPC - 1));
-                                float v[MPC];
-#pragma unroll
-                                for (int s2 = 0; s2 < MPC; s2++) {
-                                    const uint32_t cb = __byte_perm(rw[s2 >> 2], 0u, 0x4440u | (uint32_t)(s2 & 3));
-                                    uint32_t ro;
-                                    if constexpr (MPC <= 16) ro = roff[s2];
-                                    else ro = lut_s + ((uint32_t)((lane + s2) & (MPC - 1)) << 2);
-                                    v[s2] = lds_f32(ro + (cb << 7));
-                                }
-#pragma unroll
-                                for (int s2 = 1; s2 < MPC; s2 <<= 1)
-#pragma unroll
-                                    for (int k = 0; k + s2 < MPC; k += 2 * s2) v[k] = __fadd_rn(v[k], v[k + s2]);
-                                d = __fadd_rn(d, v[0]);
+                                d = __fadd_rn(d, rot_lut_sum<MPC>(cwd[u].w, roff, bsel, xl, lut_s, lane));
                                 done = true;
                             }
                         }
@@ -945,7 +971,7 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
                         }
                     }
                     du = f2o(d);
-                    if (WARM) warm[base + lane + 32u * u] = ((uint64_t)du << 32) | pos[u];
+                    if (WARM) warm[f + lane + 32u * u] = ((uint64_t)du << 32) | pos[u];
                     else pass = du <= tau;
                 }
                 if (!WARM) {
@@ -964,46 +990,150 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
     }
 }
 
-// The k-th smallest (1-based) high word of keys[0..n) in shared memory
-// (radix select, 11 + 11 + 10 bits).
-__device__ uint32_t block_kth_hi(const uint64_t *keys, int n, int k, uint32_t *hist, uint64_t *red, QState &st) {
-    const int tid = threadIdx.x;
-    uint32_t prefix = 0;
-    uint64_t need = (uint64_t)k;
+// The fast form's scan-only kernel with kp == 256 and mp in {8, 16, 32}: each
+// warp takes an equal, contiguous run of the candidates [first, limit) and
+// walks it cell by cell, so the cell is the same for the whole warp.  Each
+// cell's candidates go in chunks of 32 * U (lane l takes the chunk's
+// candidates l, l + 32, ...): a full chunk loads from one base at immediate
+// offsets; the cell's last, partial chunk clamps positions to the cell and
+// masks its distances.  Distances are d0 + per-vector term + the
+// bank-private LUT sum (rot_lut_sum), the same floats as in scan_chunks.
+// Cells come from the warp's window of WWIN visited cells in shared memory.
+// WARM == true stores every candidate's (distance, position) at
+// warm[flat]; otherwise candidates with a distance at or below tau are
+// appended to out[] through warp-aggregated atomics on st.npend.
+template <int MPC, bool WARM, int U>
+__device__ __forceinline__ void scan_cells(const SearchArgs &a, const Smem &S, QState &st, const ScanCtx &c,
+                                           uint32_t first, uint32_t limit, uint32_t tau, uint64_t *warm,
+                                           uint64_t *out, uint32_t cap) {
+    static_assert(MPC == 8 || MPC == 16 || MPC == 32, "bank-private LUT widths");
+    const unsigned FULL = 0xffffffffu;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    CellWin *W = S.wwin + wid * WWIN;
+    const uint32_t lut_s = (uint32_t)__cvta_generic_to_shared(S.lut);
+    const uint32_t xl = (uint32_t)lane & (MPC - 1);
+    constexpr int NROFF = MPC <= 16 ? MPC : 1;
+    uint32_t roff[NROFF], bsel[4];
+    if constexpr (MPC <= 16) {
 #pragma unroll
-    for (int p = 0; p < 3; p++) {
-        const int sh = p == 0 ? 21 : (p == 1 ? 10 : 0), bits = p == 2 ? 10 : 11, nbins = 1 << bits, hs = sh + bits;
-        for (int i = tid; i < nbins; i += NT) hist[i] = 0;
-        __syncthreads();
-        for (int i = tid; i < n; i += NT) {
-            uint32_t v = (uint32_t)(keys[i] >> 32);
-            if (hs < 32 && (v >> hs) != (prefix >> hs)) continue;
-            atomicAdd(&hist[(v >> sh) & (nbins - 1)], 1u);
-        }
-        __syncthreads();
-        const int per = (nbins + NT - 1) / NT;
-        const int b0 = tid * per;
-        uint64_t mine = 0;
-        for (int i = 0; i < per; i++)
-            if (b0 + i < nbins) mine += hist[b0 + i];
-        uint64_t tot;
-        uint64_t run = block_exscan(mine, red, tot);
-        for (int i = 0; i < per; i++) {
-            int bb = b0 + i;
-            if (bb >= nbins) break;
-            uint64_t nxt = run + hist[bb];
-            if (run < need && nxt >= need) {
-                st.s_bin = (uint32_t)bb;
-                st.s_acc = run;
-            }
-            run = nxt;
-        }
-        __syncthreads();
-        prefix |= st.s_bin << sh;
-        need -= st.s_acc;
-        __syncthreads();
+        for (int s2 = 0; s2 < MPC; s2++) roff[s2] = lut_s + (((uint32_t)lane - xl + ((uint32_t)s2 ^ xl)) << 2);
     }
-    return prefix;
+#pragma unroll
+    for (int j = 0; j < 4; j++) bsel[j] = 0x4440u | ((uint32_t)j ^ (xl & 3u));
+    const float tauf = tau == 0xffffffffu ? __int_as_float(0x7f800000) : o2f(tau);
+    constexpr uint32_t WCH = 32u * U;
+    // this warp's run
+    const uint64_t nch = limit > first ? ((uint64_t)(limit - first) + WCH - 1) / WCH : 0;
+    const uint64_t per = (nch + NWARP - 1) / NWARP;
+    const uint64_t lo64 = (uint64_t)first + (uint64_t)wid * per * WCH;
+    const uint32_t hi = (uint32_t)min(lo64 + per * WCH, (uint64_t)limit);
+    uint32_t f = (uint32_t)min(lo64, (uint64_t)limit);
+    if (f >= hi) return;
+    // the visited cell holding f
+    int ci = 0;
+    if (lane == 0) {
+        int lo2 = 0, hi2 = c.nvis - 1;
+        while (lo2 < hi2) {
+            const int mid = (lo2 + hi2 + 1) >> 1;
+            if (c.vis_pre[mid] <= f) lo2 = mid;
+            else hi2 = mid - 1;
+        }
+        ci = lo2;
+    }
+    ci = __shfl_sync(FULL, ci, 0);
+    int wci = 0, wcn = 0;
+    uint32_t whi = 0;
+    while (f < hi) {
+        if (ci >= wci + wcn) {
+            // the next window of visited cells, from ci
+            __syncwarp();  // the previous window's readers are done
+            const int cc = ci + lane;
+            if (cc < c.nvis) {
+                const uint32_t cell = c.vis_cell[cc];
+                CellWin cw;
+                cw.pre = c.vis_pre[cc];
+                cw.start = a.off[cell];
+                if (c.imi) {
+                    const uint32_t h3 = cell / (uint32_t)c.kc, h4 = cell - h3 * (uint32_t)c.kc;
+                    cw.d0 = __fadd_rn(__fadd_rn(c.qs, c.dqc[h3]), c.dqc[c.kc + h4]);
+                } else {
+                    cw.d0 = __fadd_rn(c.qs, c.dqc[c.sc ? cell / (uint32_t)c.kc : cell]);
+                }
+                cw.h34 = 0;
+                W[lane] = cw;
+            }
+            wci = ci;
+            wcn = min(WWIN, c.nvis - ci);
+            __syncwarp();
+            whi = (ci + wcn < c.nvis) ? c.vis_pre[ci + wcn] : c.Svis;
+        }
+        const CellWin cw = W[ci - wci];
+        const uint32_t cnext = (ci + 1 < wci + wcn) ? W[ci - wci + 1].pre : whi;
+        const uint32_t cend = min(cnext, hi);
+        const float d0 = cw.d0;
+        for (uint32_t g = f; g < cend; g += WCH) {
+            const uint32_t ff0 = g + lane;
+            const uint32_t p0 = cw.start + (ff0 - cw.pre);
+            CodeWords<MPC> cwd[U];
+            float dist[U];
+            const bool full = g + WCH <= cend;
+            if (full) {
+                const uint8_t *cp = a.codes + (size_t)p0 * MPC;
+                const float *vp = a.vterm + p0;
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    cwd[u].load_at(cp + (size_t)u * 32u * MPC);
+                    dist[u] = __ldg(vp + 32u * u);
+                }
+            } else {
+                // the cell's last chunk: positions clamped to the cell
+                const uint32_t plast = cw.start + (cend - 1u - cw.pre);
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const uint32_t pu = min(p0 + 32u * u, plast);
+                    cwd[u].load(a.codes, pu, MPC);
+                    dist[u] = __ldg(a.vterm + pu);
+                }
+            }
+            bool act[U];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                act[u] = full || ff0 + 32u * u < cend;
+                dist[u] = __fadd_rn(__fadd_rn(d0, dist[u]), rot_lut_sum<MPC>(cwd[u].w, roff, bsel, xl, lut_s, lane));
+            }
+            if constexpr (WARM) {
+#pragma unroll
+                for (int u = 0; u < U; u++)
+                    if (act[u]) warm[ff0 + 32u * u] = ((uint64_t)f2o(dist[u]) << 32) | (p0 + 32u * u);
+            } else {
+                bool anyp = false;
+#pragma unroll
+                for (int u = 0; u < U; u++) anyp |= act[u] && dist[u] <= tauf;
+                if (__any_sync(FULL, anyp)) {
+#pragma unroll
+                    for (int u = 0; u < U; u++) {
+                        const bool pass = act[u] && dist[u] <= tauf;
+                        const unsigned m = __ballot_sync(FULL, pass);
+                        if (m) {
+                            uint32_t slot0 = 0;
+                            if (lane == __ffs(m) - 1) slot0 = atomicAdd((unsigned *)&st.npend, (unsigned)__popc(m));
+                            slot0 = __shfl_sync(FULL, slot0, __ffs(m) - 1);
+                            const uint32_t slot = slot0 + __popc(m & ((1u << lane) - 1));
+                            if (pass && slot < cap) out[slot] = ((uint64_t)f2o(dist[u]) << 32) | (p0 + 32u * u);
+                        }
+                    }
+                }
+            }
+        }
+        f = cend;
+        ci++;
+    }
+}
+
+// The k-th smallest (1-based) high word of keys[0..n) in shared memory.
+__device__ uint32_t block_kth_hi(const uint64_t *keys, int n, int k, uint32_t *hist, uint64_t *red, QState &st) {
+    uint64_t need;
+    return radix_kth_word([&](int i) { return (uint32_t)(keys[i] >> 32); }, n, (uint64_t)k, hist, red, st, need);
 }
 
 // Resident CTAs per SM the register allocation is sized for.
@@ -1026,8 +1156,8 @@ __device__ uint32_t block_kth_hi(const uint64_t *keys, int n, int k, uint32_t *h
 // PART 0: selection and scan fused; 1: selection only, publishing each
 // query's visited cells (a.qmeta, a.pool_*); 2: scan only, from them.  FK:
 // the scan-only kernel of the fast form with kp == 256 (scan_chunks).
-template <int MPC, int U, int PART, bool FK = false>
-__global__ void __launch_bounds__(NT, PART == 2   ? (FK ? SCG_SCAN_FK_MIN_BLOCKS : SCG_SCAN_MIN_BLOCKS)
+template <int MPC, int U, int PART, int VAR = V_ADC>
+__global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN_FK_MIN_BLOCKS : SCG_SCAN_MIN_BLOCKS)
                                       : PART == 1 ? SCG_SELECT_MIN_BLOCKS
                                                   : SCG_SEARCH_MIN_BLOCKS) k_search(SearchArgs a) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -1072,12 +1202,13 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (FK ? SCG_SCAN_FK_MIN_BLOCKS
         const float qn0 = a.qn[2 * q], qn1 = a.qn[2 * q + 1], qs = a.qsum[q];
         if constexpr (PART != 1) {
             const float *src = a.dqr + (size_t)q * mp * kp;
-            if (a.raw_dim > 0) {
+            if (VAR == V_EXACT) {
                 // the exact-distance scan keeps the query instead of a LUT
                 for (int i = tid; i < a.raw_dim; i += NT) S.lut[i] = a.Q[(size_t)q * a.raw_dim + i];
             } else if (a.rot) {
                 // rotated LUT: word c * 32 + b holds table (b mod mp) at code
                 // c, so bank b serves table b mod mp (32 / mp copies)
+#pragma unroll 8
                 for (int wd = tid; wd < ROT_LUT_BYTES / 4; wd += NT)
                     S.lut[wd] = __ldg(src + (size_t)(wd & (mp - 1)) * 256 + (wd >> 5));
             } else {
@@ -1601,7 +1732,10 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (FK ? SCG_SCAN_FK_MIN_BLOCKS
             c.qs = qs;
             c.dqc = dqc;
             const uint32_t K = Svis < (uint32_t)WARMN ? Svis : (uint32_t)WARMN;
-            scan_chunks<MPC, true, U, FK>(a, S, st, c, 0u, K, 0u, S.warm, nullptr, 0u);
+            constexpr bool ROTOK = PART == 0 || VAR == V_FAST256;
+            constexpr bool CELLS = VAR == V_FAST256 && (MPC == 8 || MPC == 16 || MPC == 32);
+            if constexpr (CELLS) scan_cells<(CELLS ? MPC : 8), true, U>(a, S, st, c, 0u, K, 0u, S.warm, nullptr, 0u);
+            else scan_chunks<MPC, true, U, VAR, ROTOK>(a, S, st, c, 0u, K, 0u, S.warm, nullptr, 0u);
             __syncthreads();
             uint32_t tau = 0xffffffffu;
             if (K > (uint32_t)R) tau = block_kth_hi(S.warm, (int)K, R, S.hist2, red, st);
@@ -1621,7 +1755,8 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (FK ? SCG_SCAN_FK_MIN_BLOCKS
                 }
                 __syncthreads();
             }
-            scan_chunks<MPC, false, U, FK>(a, S, st, c, K, Svis, tau, nullptr, pend_g, a.pcap);
+            if constexpr (CELLS) scan_cells<(CELLS ? MPC : 8), false, U>(a, S, st, c, K, Svis, tau, nullptr, pend_g, a.pcap);
+            else scan_chunks<MPC, false, U, VAR, ROTOK>(a, S, st, c, K, Svis, tau, nullptr, pend_g, a.pcap);
             __syncthreads();
             PHASE_MARK(4);  // scan
             if ((uint32_t)st.npend > a.pcap) {
@@ -1678,76 +1813,81 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (FK ? SCG_SCAN_FK_MIN_BLOCKS
 
 // Dynamic shared memory already granted to a kernel variant, per device
 // (the attribute is set once, not on every launch).
-template <int MPC, int U, int PART, bool FK>
+template <int MPC, int U, int PART, int VAR>
 int grant_smem(size_t smem) {
     static int granted[64] = {0};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64 || granted[dev] < (int)smem) {
         cudaError_t e =
-            cudaFuncSetAttribute(k_search<MPC, U, PART, FK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            cudaFuncSetAttribute(k_search<MPC, U, PART, VAR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return cuda_fail(e, "cudaFuncSetAttribute(k_search)");
         if (dev >= 0 && dev < 64) granted[dev] = (int)smem;
     }
     return SCG_OK;
 }
 
-template <int MPC, int U, int PART, bool FK = false>
+template <int MPC, int U, int PART, int VAR = V_ADC>
 int occupancy(size_t smem) {
-    if (grant_smem<MPC, U, PART, FK>(smem)) return 0;
+    if (grant_smem<MPC, U, PART, VAR>(smem)) return 0;
     int nb = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<MPC, U, PART, FK>, NT, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_search<MPC, U, PART, VAR>, NT, smem);
     return nb;
 }
 
-// fk: the scan-only kernel of the fast form with kp == 256 (its own variant).
+// var: the kernel variant the launch will pick (V_FAST256 only for the
+// scan-only kernel with a fixed code width; V_EXACT is one variant for every
+// code width).
 template <int MPC, int U, int PART>
-int occupancy_fk(size_t smem, bool fk) {
+int occupancy_var(size_t smem, int var) {
+    if (var == V_EXACT) return occupancy<0, U, PART, V_EXACT>(smem);
     if constexpr (PART == 2 && MPC > 0) {
-        if (fk) return occupancy<MPC, U, PART, true>(smem);
+        if (var == V_FAST256) return occupancy<MPC, U, PART, V_FAST256>(smem);
     }
-    return occupancy<MPC, U, PART, false>(smem);
+    return occupancy<MPC, U, PART, V_ADC>(smem);
 }
 
 template <int U, int PART>
-int occupancy_mp(int mp, size_t smem, bool fk = false) {
+int occupancy_mp(int mp, size_t smem, int var = V_ADC) {
     switch (mp) {
-        case 4: return occupancy_fk<4, U, PART>(smem, fk);
-        case 8: return occupancy_fk<8, U, PART>(smem, fk);
-        case 16: return occupancy_fk<16, U, PART>(smem, fk);
-        case 32: return occupancy_fk<32, U, PART>(smem, fk);
-        default: return occupancy_fk<0, U, PART>(smem, fk);
+        case 4: return occupancy_var<4, U, PART>(smem, var);
+        case 8: return occupancy_var<8, U, PART>(smem, var);
+        case 16: return occupancy_var<16, U, PART>(smem, var);
+        case 32: return occupancy_var<32, U, PART>(smem, var);
+        default: return occupancy_var<0, U, PART>(smem, var);
     }
 }
 
-template <int MPC, int U, int PART, bool FK = false>
+template <int MPC, int U, int PART, int VAR = V_ADC>
 int launch(const SearchArgs &a, int grid, size_t smem, cudaStream_t s) {
-    int rc = grant_smem<MPC, U, PART, FK>(smem);
+    int rc = grant_smem<MPC, U, PART, VAR>(smem);
     if (rc) return rc;
-    k_search<MPC, U, PART, FK><<<grid, NT, smem, s>>>(a);
+    k_search<MPC, U, PART, VAR><<<grid, NT, smem, s>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "k_search launch");
     return SCG_OK;
 }
 
-// The scan-only kernel of the fast form with kp == 256 has its own variant.
+// The variant of a launch: the exact-distance scan (one variant for every
+// code width), the fast form's scan-only kernel with kp == 256, or the
+// general ADC kernel.
 template <int MPC, int U, int PART>
-int launch_fk(const SearchArgs &a, int grid, size_t smem, cudaStream_t s) {
+int launch_var(const SearchArgs &a, int grid, size_t smem, cudaStream_t s) {
+    if (a.raw_dim > 0) return launch<0, U, PART, V_EXACT>(a, grid, smem, s);
     if constexpr (PART == 2 && MPC > 0) {
-        if (a.precision == SCG_FAST && a.kp == 256 && a.raw_dim == 0)
-            return launch<MPC, U, PART, true>(a, grid, smem, s);
+        if (a.precision == SCG_FAST && a.kp == 256) return launch<MPC, U, PART, V_FAST256>(a, grid, smem, s);
     }
-    return launch<MPC, U, PART, false>(a, grid, smem, s);
+    return launch<MPC, U, PART, V_ADC>(a, grid, smem, s);
 }
 
 template <int U, int PART>
 int launch_mp(const SearchArgs &a, int grid, size_t smem, cudaStream_t s) {
     switch (a.mp) {
-        case 4: return launch_fk<4, U, PART>(a, grid, smem, s);
-        case 8: return launch_fk<8, U, PART>(a, grid, smem, s);
-        case 16: return launch_fk<16, U, PART>(a, grid, smem, s);
-        case 32: return launch_fk<32, U, PART>(a, grid, smem, s);
-        default: return launch_fk<0, U, PART>(a, grid, smem, s);
+        case 4: return launch_var<4, U, PART>(a, grid, smem, s);
+        case 8: return launch_var<8, U, PART>(a, grid, smem, s);
+        case 16: return launch_var<16, U, PART>(a, grid, smem, s);
+        case 32: return launch_var<32, U, PART>(a, grid, smem, s);
+        default: return launch_var<0, U, PART>(a, grid, smem, s);
     }
 }
 
