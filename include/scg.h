@@ -278,10 +278,12 @@ int scg_last_timings(scg_index *h, float *ms, int n);
 int scg_cell_counts(scg_index *h, int *L, int64_t ncells);
 
 /* Diagnostics: with counters on, each search accumulates per-phase cycle
- * counts of the fused kernel (thread 0 of every CTA, summed over queries):
+ * counts of the search kernels (thread 0 of every CTA, summed over queries):
  * [0] coarse-list sort, [1] staircase rounds, [2] cut, [3] compaction,
  * [4] scan rounds, [5] final merge, [7] merges, [8] rounds, [9] bisection
- * steps, [10] enumerated cells.  n is the capacity of out (<= 16). */
+ * steps, [10] enumerated cells, and in the scan-only kernel [12] the LUT (or
+ * query) staging and [13] the warm-up scores and threshold.  n is the
+ * capacity of out (<= 16). */
 int scg_set_phase_counters(scg_index *h, int on);
 int scg_last_phase_counters(scg_index *h, long long *out, int n);
 

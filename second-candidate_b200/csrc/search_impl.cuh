@@ -259,7 +259,71 @@ __device__ uint64_t block_exscan(uint64_t v, uint64_t *red, uint64_t &total) {
 }
 
 // Ascending bitonic sort of n (a power of two) u64 keys in shared memory.
+// n <= NT (one key per thread) and n == 2 NT (two): keys in registers;
+// partners closer than 32 are exchanged by warp shuffles, partners NT apart
+// inside the thread, the rest through shared memory (two barriers per such
+// stage instead of one per stage).
 __device__ void bitonic_sort64(uint64_t *key, int n) {
+    if (n <= NT) {
+        const int t = threadIdx.x;
+        uint64_t v = t < n ? key[t] : ~0ull;
+        for (int k = 2; k <= n; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                uint64_t p;
+                if (j >= 32) {
+                    if (t < n) key[t] = v;
+                    __syncthreads();
+                    p = t < n ? key[t ^ j] : ~0ull;
+                    __syncthreads();
+                } else {
+                    p = __shfl_xor_sync(0xffffffffu, v, j);
+                }
+                // the lower index of a pair keeps the minimum in ascending runs
+                const bool keep_min = ((t & j) == 0) == ((t & k) == 0);
+                v = keep_min ? (v < p ? v : p) : (v > p ? v : p);
+            }
+        }
+        if (t < n) key[t] = v;
+        __syncthreads();
+        return;
+    }
+    if (n == 2 * NT) {
+        // two keys per thread (indices t and t + NT): partners NT apart are
+        // in the same thread, closer than 32 in the same warp
+        const int t = threadIdx.x;
+        uint64_t v0 = key[t], v1 = key[t + NT];
+        for (int k = 2; k <= n; k <<= 1) {
+            for (int j = k >> 1; j > 0; j >>= 1) {
+                if (j == NT) {
+                    // index t < t + NT: ascending iff (t & k) == 0 (k = 2 NT: always)
+                    const uint64_t lo = v0 < v1 ? v0 : v1, hi = v0 < v1 ? v1 : v0;
+                    v0 = lo;
+                    v1 = hi;
+                    continue;
+                }
+                uint64_t p0, p1;
+                if (j >= 32) {
+                    key[t] = v0;
+                    key[t + NT] = v1;
+                    __syncthreads();
+                    p0 = key[t ^ j];
+                    p1 = key[(t + NT) ^ j];
+                    __syncthreads();
+                } else {
+                    p0 = __shfl_xor_sync(0xffffffffu, v0, j);
+                    p1 = __shfl_xor_sync(0xffffffffu, v1, j);
+                }
+                const bool lower = (t & j) == 0;
+                const bool min0 = lower == ((t & k) == 0), min1 = lower == (((t + NT) & k) == 0);
+                v0 = min0 ? (v0 < p0 ? v0 : p0) : (v0 > p0 ? v0 : p0);
+                v1 = min1 ? (v1 < p1 ? v1 : p1) : (v1 > p1 ? v1 : p1);
+            }
+        }
+        key[t] = v0;
+        key[t + NT] = v1;
+        __syncthreads();
+        return;
+    }
     for (int k = 2; k <= n; k <<= 1) {
         for (int j = k >> 1; j > 0; j >>= 1) {
             for (int i = threadIdx.x; i < n; i += NT) {
@@ -524,16 +588,17 @@ struct CodeWords<0> {
 
 // The k-th smallest (1-based) of n 32-bit words word(i): a radix select of
 // 4 x 8 bits over RBINS = NT bins (one per thread).  Returns the word;
-// `need` becomes how many entries equal to it complete the k smallest.
+// `need` becomes how many entries equal to it complete the k smallest.  With
+// npass < 4 only the top 8 npass bits are selected (the low bits are 0).
 template <class Word>
 __device__ uint32_t radix_kth_word(Word word, int n, uint64_t k, uint32_t *hist, uint64_t *red, QState &st,
-                                   uint64_t &need) {
+                                   uint64_t &need, int npass = 4) {
     static_assert(RBINS == NT, "one bin per thread");
     const int tid = threadIdx.x;
     uint32_t prefix = 0;
     need = k;
 #pragma unroll 1
-    for (int sh = 24; sh >= 0; sh -= 8) {
+    for (int sh = 24; sh >= 32 - 8 * npass; sh -= 8) {
         hist[tid] = 0;
         __syncthreads();
         for (int i = tid; i < n; i += NT) {
@@ -610,6 +675,12 @@ __device__ void merge_topk(uint64_t *top, uint64_t *pend, uint64_t *tmp, uint32_
             st.thr = ~0ull;
         }
         __syncthreads();
+        return;
+    }
+    if (na == 0 && nb <= 2 * NT) {
+        // few survivors: one register sort of (distance, id) keys gives the R
+        // best in order
+        sort_merge(top, pend, nb, R, pid, st);
         return;
     }
     // radix select of the R-th smallest distance word
@@ -1130,10 +1201,15 @@ __device__ __forceinline__ void scan_cells(const SearchArgs &a, const Smem &S, Q
     }
 }
 
-// The k-th smallest (1-based) high word of keys[0..n) in shared memory.
-__device__ uint32_t block_kth_hi(const uint64_t *keys, int n, int k, uint32_t *hist, uint64_t *red, QState &st) {
+// An upper bound of the k-th smallest (1-based) high word of keys[0..n) in
+// shared memory: the word's top 24 bits by three radix passes, all low bits
+// set (at most 2^-15 relative above the k-th distance).  The scan's
+// threshold only has to bound the final R-th distance from above.
+__device__ uint32_t block_kth_hi_bound(const uint64_t *keys, int n, int k, uint32_t *hist, uint64_t *red,
+                                       QState &st) {
     uint64_t need;
-    return radix_kth_word([&](int i) { return (uint32_t)(keys[i] >> 32); }, n, (uint64_t)k, hist, red, st, need);
+    return radix_kth_word([&](int i) { return (uint32_t)(keys[i] >> 32); }, n, (uint64_t)k, hist, red, st, need, 3) |
+           0xffu;
 }
 
 // Resident CTAs per SM the register allocation is sized for.
@@ -1231,6 +1307,7 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
             vpre = a.pool_pre + m.off;
             if (tid == 0) st.err = qerr2 ? 1 : 0;
             __syncthreads();
+            PHASE_MARK(12);  // LUT (or query) staging
         } else {
             // PART 1 compacts straight into the query's pool region (set
             // after the cut, when the list's length is known)
@@ -1738,7 +1815,7 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
             else scan_chunks<MPC, true, U, VAR, ROTOK>(a, S, st, c, 0u, K, 0u, S.warm, nullptr, 0u);
             __syncthreads();
             uint32_t tau = 0xffffffffu;
-            if (K > (uint32_t)R) tau = block_kth_hi(S.warm, (int)K, R, S.hist2, red, st);
+            if (K > (uint32_t)R) tau = block_kth_hi_bound(S.warm, (int)K, R, S.hist2, red, st);
             // the warm entries at or below tau open the pending buffer
             {
                 uint64_t mine = 0;
@@ -1755,6 +1832,7 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
                 }
                 __syncthreads();
             }
+            PHASE_MARK(13);  // warm-up scores and the threshold
             if constexpr (CELLS) scan_cells<(CELLS ? MPC : 8), false, U>(a, S, st, c, K, Svis, tau, nullptr, pend_g, a.pcap);
             else scan_chunks<MPC, false, U, VAR, ROTOK>(a, S, st, c, K, Svis, tau, nullptr, pend_g, a.pcap);
             __syncthreads();

@@ -255,7 +255,7 @@ class Index:
         out = np.zeros(16, np.int64)
         _check(_lib.scg_last_phase_counters(self._h, _ptr(out), 16))
         names = ["sort", "rounds", "cut", "compact", "scan", "final_merge", "pending", "merges", "round_count",
-                 "bisection_steps", "enumerated_cells", "full_sorts"]
+                 "bisection_steps", "enumerated_cells", "full_sorts", "lut_fill", "warm_threshold"]
         return {n: int(v) for n, v in zip(names, out) if n != "-"}
 
     def last_timings(self):
