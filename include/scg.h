@@ -36,6 +36,7 @@ extern "C" {
 #define SCG_IVFADC 0  /* PQQuery::search_ivfadc      query.h:202-325        */
 #define SCG_IMI 1     /* MultiQuery::search_multi2   multi_query.h:62-273   */
 #define SCG_SC2 2     /* SCQuery::search_mr_ivf      sc_query.h:60-256      */
+#define SCG_SC3 3     /* SCQuery::search_mr_ivf3     sc_query.h:265-475     */
 
 /* Arithmetic of the per-query tables and of the ADC sum.  The three
  * tensor-core forms build the tables as tcgen05 GEMMs with FP32 accumulation
@@ -48,7 +49,7 @@ extern "C" {
 typedef struct scg_index scg_index;
 
 typedef struct {
-    int mode;       /* SCG_IVFADC / SCG_IMI / SCG_SC2                              */
+    int mode;       /* SCG_IVFADC / SCG_IMI / SCG_SC2 / SCG_SC3                    */
     int R;          /* results per query (1..1024)                                 */
     int w;          /* cell cap: popped cells (IVFADC, IMI) or non-empty cells (SC) */
     int T;          /* candidate target: stop after the cell that reaches T         */
@@ -82,12 +83,13 @@ int scg_load_codebooks_file(scg_index *h, const char *cq_path, const char *pq_pa
 
 /* The CSR index: L[ncells] inclusive prefix counts, pid[N], codes[N][mp] in
  * cell order (the arrays PQQuery::load_encoded_data builds, query.cpp:82-165).
- * ncells must be kc^mc (IVFADC/IMI) or kc^2 (SC, mc = 1). */
+ * ncells must be kc^mc (IVFADC/IMI), kc^2 (second candidate, mc = 1) or kc^3
+ * (second candidate with three nearest centroids, mc = 1, kc <= 1024). */
 int scg_load_csr(scg_index *h, const int *L, const int *pid, const uint8_t *codes,
                  int64_t N, int64_t ncells);
 
-/* Reads an .edat_ file with kc^nc cells (nc = mc for IVFADC/IMI indexes, 2 for
- * second-candidate indexes).  Replaces PQQuery::load_encoded_data
+/* Reads an .edat_ file with kc^nc cells (nc = mc for IVFADC/IMI indexes, 2 or
+ * 3 for second-candidate indexes).  Replaces PQQuery::load_encoded_data
  * (query.cpp:82-165) and SCQuery::load_encoded_data (sc_query.cpp:36-123). */
 int scg_load_encoded_file(scg_index *h, const char *path, int nc);
 
@@ -200,11 +202,14 @@ int scg_sc_encode(scg_index *h, const float *X, int64_t n, int nc, uint16_t *cid
                   uint8_t *codes);
 
 /* Index build on the device: encodes dX[n][dim] (device rows, ids 0..n-1;
- * nc = 0 IVF/IMI codes with kc^mc cells, nc = 2 second-candidate codes with
- * kc^2 cells), orders the rows by cell and by id inside a cell, and loads the
- * resulting CSR into the index -- the arrays Encoder::distribution /
+ * nc = 0 IVF/IMI codes with kc^mc cells, nc = 2 or 3 second-candidate codes
+ * with kc^nc cells), orders the rows by cell and by id inside a cell, and
+ * loads the resulting CSR into the index -- the arrays Encoder::distribution /
  * SCEncoder::distribution write and load_encoded_data reads back
- * (encoder.cpp:170-305, sc_encoder.cpp:17-182, query.cpp:82-165). */
+ * (encoder.cpp:170-305, sc_encoder.cpp:17-182, query.cpp:82-165).  With
+ * nc = 3 a row's cell is its own (nn1, nn2, nn3); the reference's
+ * distribution reads a misaligned window of the centroid ids there
+ * (sc_encoder.cpp:41-59 advances by 2 per row). */
 int scg_build_index(scg_index *h, const float *dX, int64_t n, int nc, void *stream);
 
 /* Writes the index's CSR as an .edat_ file (int32 non-empty cells, int32 N,

@@ -18,7 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libscref.so")
 
-IVFADC, IMI, SC = 0, 1, 2
+IVFADC, IMI, SC, SC3 = 0, 1, 2, 3
 ORDER_HEAP, ORDER_EXACT = 0, 1
 
 _f32p = ctypes.POINTER(ctypes.c_float)
@@ -135,7 +135,7 @@ class Index:
             raise RuntimeError("orc_search failed: %d" % rc)
         n = s.value
         return dict(dist=dist[:n].copy(), ids=ids[:n].copy(), cells=cells[:ncells.value].copy(),
-                    sum=n, empty=e.value)
+                    sum=n, empty=e.value, max_rank=int(lib().orc_last_max_rank()))
 
     def search(self, mode, Q, R, w, T, order=ORDER_EXACT, real_dist=False):
         """Top-R per query (ascending distance; equal distances by id), the

@@ -73,26 +73,40 @@ struct Opened : public Base {
 
 typedef Opened<MultiQuery> OMulti;
 typedef Opened<SCQuery> OSC;
+/* SCQuery with three nearest centroids per cell (sc_query.cpp:21-25). */
+struct OSC3 : public Opened<SCQuery> {
+    OSC3() : Opened<SCQuery>(3) {}
+};
 
 struct Scratch {
     std::vector<float> v_tmp, q2;
-    std::vector<int> tmp, hid1, hid2, hid3, hid4, s1, s2, prebuck, cache;
+    std::vector<int> tmp, hid1, hid2, hid3, hid4, hid5, hid6, s1, s2, prebuck, cache;
     std::vector<unsigned char> trav;
-    void init(int kc, int w, bool sc) {
+    /* mode 2: traversed[0] preset (test_sc_query.cpp:160-161); mode 3: the
+     * kc^3 rank grid, nothing preset (the walk starts at (0, 0, 0)). */
+    void init(int kc, int w, int mode) {
         v_tmp.assign((size_t)2 * kc + w, 0.0f);
         q2.assign(2, 0.0f);
         tmp.assign((size_t)2 * kc, 0);
         hid1.assign(w, 0); hid2.assign(w, 0); hid3.assign(w, 0); hid4.assign(w, 0);
-        s1.assign(w, 0); s2.assign(w, 0); prebuck.assign(w, 0); cache.assign(w, 0);
-        trav.assign((size_t)kc * kc, 0);
-        if (sc) trav[0] = 1; /* test_sc_query.cpp:160-161 */
+        hid5.assign(w, 0); hid6.assign(w, 0);
+        s1.assign(w, 0); s2.assign(w, 0); prebuck.assign(w, 0);
+        /* the SC walks write cache[count2++] for every popped cell, empty ones
+         * included, while w counts non-empty cells (sc_query.h:130,148,
+         * 327,345): size it for the whole grid */
+        const size_t grid = (size_t)kc * kc * (mode == 3 ? kc : 1);
+        cache.assign(mode >= 2 ? grid + (size_t)w : (size_t)w, 0);
+        trav.assign(grid, 0);
+        if (mode == 2) trav[0] = 1;
     }
 };
 
 static MultiQuery *as_multi(OMulti &o) { return &o; }
 static MultiQuery *as_multi(OSC &) { return nullptr; }
+static MultiQuery *as_multi(OSC3 &) { return nullptr; }
 static SCQuery *as_sc(OMulti &) { return nullptr; }
 static SCQuery *as_sc(OSC &o) { return &o; }
+static SCQuery *as_sc(OSC3 &o) { return &o; }
 
 /* One query through the reference entry point for `mode`
  * (0 IVFADC query.h:202, 1 IMI multi_query.h:62, 2 SC sc_query.h:60).
@@ -119,6 +133,11 @@ static int run_one(PQQuery &obj, MultiQuery *mq, SCQuery *sq, int mode, Scratch 
         sq->search_mr_ivf(q, v_tmp, dist, s.tmp.data(), result,
                           hid1, hid2, hid3, hid4, s1, s2, prebuck, cache, trav,
                           sum, R, w, T, M, real_dist, false);
+    } else if (mode == 3 && sq) {
+        int *hid5 = s.hid5.data(), *hid6 = s.hid6.data();
+        sq->search_mr_ivf3(q, v_tmp, dist, s.tmp.data(), result,
+                           hid1, hid2, hid3, hid4, hid5, hid6, s1, prebuck, cache, trav,
+                           sum, R, w, T, M, real_dist, false);
     }
     return sum;
 }
@@ -146,7 +165,7 @@ int search_batch(int mode, int dim, int mc, int kc, int mp, int kp, int N,
         clones[t] = new Q();
         clones[t]->set_index(dim, mc, kc, mp, kp, N, cq, pq, L, pid, codes, raw);
         clones[t]->share_tables(master);
-        scratch[t].init(kc, wcap, mode == 2);
+        scratch[t].init(kc, wcap, mode);
     }
     auto t0 = std::chrono::steady_clock::now();
 #ifdef _OPENMP
@@ -187,17 +206,17 @@ extern "C" {
  * returns per query (padding with -1) and each query's sum.  The wall time of
  * the query loop (pre_compute2 through top-R, steady_clock) goes to
  * *seconds_out. */
+int ref_search_batch_ex(int mode, int dim, int mc, int kc, int mp, int kp, int N,
+                        float *cq, float *pq, int *L, int *pid, unsigned char *codes, float *raw,
+                        const float *Qs, int nq, int R, int w, int T, const int *Tq, int M, int real_dist,
+                        int nthreads, int *ids_out, float *dist_out, int *sum_out, double *seconds_out);
+
 int ref_search_batch(int mode, int dim, int mc, int kc, int mp, int kp, int N,
                      float *cq, float *pq, int *L, int *pid, unsigned char *codes, float *raw,
                      const float *Qs, int nq, int R, int w, int T, int real_dist, int nthreads,
                      int *ids_out, float *dist_out, int *sum_out, double *seconds_out) {
-    if (mode == 2)
-        return search_batch<OSC>(mode, dim, mc, kc, mp, kp, N, cq, pq, L, pid, codes, raw,
-                                 Qs, nq, R, w, T, nullptr, kc, real_dist, nthreads, ids_out, dist_out, sum_out,
-                                 seconds_out);
-    return search_batch<OMulti>(mode, dim, mc, kc, mp, kp, N, cq, pq, L, pid, codes, raw,
-                                Qs, nq, R, w, T, nullptr, kc, real_dist, nthreads, ids_out, dist_out, sum_out,
-                                seconds_out);
+    return ref_search_batch_ex(mode, dim, mc, kc, mp, kp, N, cq, pq, L, pid, codes, raw, Qs, nq, R, w, T, nullptr, kc,
+                               real_dist, nthreads, ids_out, dist_out, sum_out, seconds_out);
 }
 
 /* ref_search_batch with a per-query candidate target Tq[nq] (NULL: T for
@@ -212,6 +231,10 @@ int ref_search_batch_ex(int mode, int dim, int mc, int kc, int mp, int kp, int N
         return search_batch<OSC>(mode, dim, mc, kc, mp, kp, N, cq, pq, L, pid, codes, raw,
                                  Qs, nq, R, w, T, Tq, M, real_dist, nthreads, ids_out, dist_out, sum_out,
                                  seconds_out);
+    if (mode == 3)
+        return search_batch<OSC3>(mode, dim, mc, kc, mp, kp, N, cq, pq, L, pid, codes, raw,
+                                  Qs, nq, R, w, T, Tq, M, real_dist, nthreads, ids_out, dist_out, sum_out,
+                                  seconds_out);
     return search_batch<OMulti>(mode, dim, mc, kc, mp, kp, N, cq, pq, L, pid, codes, raw,
                                 Qs, nq, R, w, T, Tq, M, real_dist, nthreads, ids_out, dist_out, sum_out,
                                 seconds_out);
@@ -224,18 +247,19 @@ int ref_search_one(int mode, int dim, int mc, int kc, int mp, int kp, int N,
                    float *cq, float *pq, int *L, int *pid, unsigned char *codes, float *raw,
                    const float *q, int R, int w, int T, int real_dist,
                    int *ids_all, float *dist_all, int cap, int *empty_out) {
-    OMulti m1; OSC m2;
+    OMulti m1; OSC m2; OSC3 m3;
     Scratch s;
     int wcap = (mode == 0) ? (kc > w ? kc : w) : w;
-    s.init(kc, wcap, mode == 2);
+    s.init(kc, wcap, mode);
     std::vector<float> qv(q, q + dim);
     int *result; float *dist; int sum, e = 0;
-    if (mode == 2) {
-        m2.set_index(dim, mc, kc, mp, kp, N, cq, pq, L, pid, codes, raw);
-        m2.pre_compute1();
-        sum = run_one(m2, nullptr, &m2, mode, s, qv.data(), R, w, T, kc, real_dist != 0, result,
+    if (mode == 2 || mode == 3) {
+        OSC &m = mode == 2 ? m2 : static_cast<OSC &>(m3);
+        m.set_index(dim, mc, kc, mp, kp, N, cq, pq, L, pid, codes, raw);
+        m.pre_compute1();
+        sum = run_one(m, nullptr, &m, mode, s, qv.data(), R, w, T, kc, real_dist != 0, result,
                       dist, &e);
-        m2.release(true);
+        m.release(true);
     } else {
         m1.set_index(dim, mc, kc, mp, kp, N, cq, pq, L, pid, codes, raw);
         m1.pre_compute1();

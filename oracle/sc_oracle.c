@@ -200,6 +200,85 @@ static void heap_free(heap4 *hp) {
     for (int t = 0; t < 4; t++) free(hp->h[t]);
 }
 
+/* The six-payload heap of the three-list walk: pq_insert6 / pq_pop6
+ * (sc_utilities.h:505-544, :629-675), and an exact binary heap on (key,
+ * rank1, rank2, rank3) for ORC_ORDER_EXACT. */
+typedef struct { float *key; int *h[6]; int pos, cap; } heap6;
+
+static int heap6_alloc(heap6 *hp, int cap) {
+    hp->pos = 0; hp->cap = cap;
+    hp->key = (float *)malloc(sizeof(float) * (size_t)(cap > 0 ? cap : 1));
+    for (int t = 0; t < 6; t++) hp->h[t] = (int *)malloc(sizeof(int) * (size_t)(cap > 0 ? cap : 1));
+    return hp->key != NULL;
+}
+static void heap6_free(heap6 *hp) {
+    free(hp->key);
+    for (int t = 0; t < 6; t++) free(hp->h[t]);
+}
+static void h6_swap(heap6 *hp, int x, int y) {
+    swap_flt(&hp->key[x], &hp->key[y]);
+    for (int t = 0; t < 6; t++) swap_int(&hp->h[t][x], &hp->h[t][y]);
+}
+/* pq_insert6: inserts past capacity are dropped; parent of i is i >> 1. */
+static void ref_insert6(heap6 *hp, float data, const int *v) {
+    if (hp->pos >= hp->cap || hp->pos < 0) return;
+    int p = hp->pos;
+    hp->key[p] = data;
+    for (int t = 0; t < 6; t++) hp->h[t][p] = v[t];
+    hp->pos++;
+    int i = hp->pos - 1, j = i >> 1;
+    while (i > 0) {
+        if (hp->key[i] < hp->key[j]) h6_swap(hp, i, j);
+        else break;
+        i = j; j = i >> 1;
+    }
+}
+/* pq_pop6: the sift-down compares children 2i and 2i+1 only while both exist. */
+static void ref_pop6(heap6 *hp, int *v) {
+    for (int t = 0; t < 6; t++) v[t] = hp->h[t][0];
+    int last = hp->pos - 1;
+    hp->key[0] = hp->key[last];
+    for (int t = 0; t < 6; t++) hp->h[t][0] = hp->h[t][last];
+    hp->pos--;
+    int cur = hp->pos, i = 0, j = 0, m;
+    while (j + 1 < cur) {
+        m = (hp->key[j] < hp->key[j + 1]) ? j : j + 1;
+        if (hp->key[m] < hp->key[i]) { h6_swap(hp, i, m); i = m; }
+        else break;
+        j = i << 1;
+    }
+}
+static int ex6_less(const heap6 *hp, int x, int y) {
+    if (hp->key[x] < hp->key[y]) return 1;
+    if (hp->key[x] > hp->key[y]) return 0;
+    for (int t = 0; t < 3; t++)
+        if (hp->h[t][x] != hp->h[t][y]) return hp->h[t][x] < hp->h[t][y];
+    return 0;
+}
+static void ex_insert6(heap6 *hp, float data, const int *v) {
+    int p = hp->pos++;
+    hp->key[p] = data;
+    for (int t = 0; t < 6; t++) hp->h[t][p] = v[t];
+    while (p > 0) {
+        int par = (p - 1) >> 1;
+        if (ex6_less(hp, p, par)) { h6_swap(hp, p, par); p = par; } else break;
+    }
+}
+static void ex_pop6(heap6 *hp, int *v) {
+    for (int t = 0; t < 6; t++) v[t] = hp->h[t][0];
+    hp->pos--;
+    if (hp->pos == 0) return;
+    h6_swap(hp, 0, hp->pos);
+    int i = 0;
+    for (;;) {
+        int l = 2 * i + 1, r = l + 1, m = i;
+        if (l < hp->pos && ex6_less(hp, l, m)) m = l;
+        if (r < hp->pos && ex6_less(hp, r, m)) m = r;
+        if (m == i) break;
+        h6_swap(hp, i, m); i = m;
+    }
+}
+
 /* ------------------------------------------------------------------------ */
 
 typedef struct { float v; int id; } vid;
@@ -221,6 +300,11 @@ static void sort_keys(const float *v, int n, float *vs, int *ids) {
 }
 
 static int cell_len(const int *L, long bid) { return bid > 0 ? L[bid] - L[bid - 1] : L[0]; }
+
+/* The largest rank of any coarse list among the cells the last orc_search
+ * popped, empty cells included (IMI and second candidate; -1 otherwise). */
+static int g_max_rank = -1;
+int orc_last_max_rank(void) { return g_max_rank; }
 static long cell_start(const int *L, long bid) { return bid > 0 ? L[bid - 1] : 0; }
 
 /* One query of PQQuery::search_ivfadc (query.h:202-325),
@@ -235,7 +319,9 @@ int orc_search(const orc_index *ix, int mode, int order, const float *q,
                int *cells, int cap_cells, int *ncells_out,
                int *sum_out, int *empty_out) {
     const int dim = ix->dim, kc = ix->kc, kp = ix->kp, mp = ix->mp, mc = ix->mc;
+    g_max_rank = -1;
     if ((mode == ORC_IMI && mc != 2) || (mode != ORC_IMI && mc != 1)) return -1;
+    if (mode == ORC_SC3 && (long)kc * kc * kc > 0x7fffffffL) return -1;
     if (real_dist && !ix->raw) return -1;
     const int *L = ix->L;
 
@@ -282,6 +368,69 @@ int orc_search(const orc_index *ix, int mode, int order, const float *q,
             if (sum >= T) break;
         }
         free(keys); free(order_ids);
+    } else if (mode == ORC_SC3) {
+        /* SCQuery::search_mr_ivf3, sc_query.h:265-405: one sorted coarse list,
+         * a multi-sequence over rank triples (h1, h2, h3) with key
+         * (v[h1] + v[h2]) + v[h3]; cell (t[h1], t[h2], t[h3]) = t[h1] kc^2 +
+         * t[h2] kc + t[h3]; the residual is relative to t[h1]. */
+        for (int i2 = 0; i2 < dim; i2++) { float t = q[i2]; q_sum += t * t; }
+        float *keys = (float *)malloc(sizeof(float) * (size_t)kc);
+        float *v = (float *)malloc(sizeof(float) * (size_t)kc);
+        int *t = (int *)malloc(sizeof(int) * (size_t)kc);
+        for (int j = 0; j < kc; j++) keys[j] = q_sum + diff_qc[j];
+        sort_keys(keys, kc, v, t);
+        free(keys);
+        const long kc2 = (long)kc * kc, size3 = kc2 * kc;
+        unsigned char *trav = (unsigned char *)calloc((size_t)size3, 1);
+        heap6 hp;
+        heap6_alloc(&hp, order == ORC_ORDER_HEAP ? w : (int)(3 * kc2 + 8));
+        void (*ins)(heap6 *, float, const int *) = (order == ORC_ORDER_HEAP) ? ref_insert6 : ex_insert6;
+        void (*pop)(heap6 *, int *) = (order == ORC_ORDER_HEAP) ? ref_pop6 : ex_pop6;
+        int hv[6] = {0, 0, 0, t[0], t[0], t[0]};
+        ins(&hp, 3.0f * v[0], hv);                     /* sc_query.h:316-324 */
+        long i = 0, count2 = 0;
+        int h1 = 0, h2 = 0, h3 = 0;
+        /* while(count < w && sum < T && count2 < size2), sc_query.h:327 */
+        while (nvis < w && sum < T && count2 < size3) {
+            /* An empty heap: the whole grid is exhausted (exact order) or the
+             * capped heap dropped cells; the reference then re-pushes the
+             * last cell's neighbours, the restatement stops. */
+            if (hp.pos <= 0) break;
+            pop(&hp, hv);
+            h1 = hv[0]; h2 = hv[1]; h3 = hv[2];
+            for (int t2 = 0; t2 < 3; t2++)
+                if (hv[t2] > g_max_rank) g_max_rank = hv[t2];
+            long bid = (long)hv[3] * kc2 + (long)hv[4] * kc + hv[5];
+            int l = bid > 0 ? L[bid] - L[bid - 1] : 0;  /* sc_query.h:336-339 */
+            if (l > 0) {
+                if (nvis >= cap_cells) { rc = -2; break; }
+                cells[nvis] = (int)bid; vis_h3[nvis] = hv[3]; vis_h4[nvis] = 0; nvis++;
+                sum += l;
+            } else empty++;
+            i = kc2 * h1 + (long)kc * h2 + h3;
+            trav[i] = 1;
+            count2++;
+            if (sum < T) {
+                /* sc_query.h:350-400: push each neighbour once all its other
+                 * predecessors are traversed */
+                const long m1 = i + kc2 - kc, m2 = i + kc2 - 1, m3 = i + kc - 1;
+                const long m4 = i + kc - kc2, m5 = i - kc + 1, m6 = i - kc2 + 1;
+                if (h1 < kc - 1 && (h2 == 0 || (m1 < size3 && trav[m1])) && (h3 == 0 || (m2 < size3 && trav[m2]))) {
+                    int nv[6] = {h1 + 1, h2, h3, t[h1 + 1], t[h2], t[h3]};
+                    ins(&hp, v[h1 + 1] + v[h2] + v[h3], nv);
+                }
+                if (h2 < kc - 1 && (h3 == 0 || (m3 < size3 && trav[m3])) && (h1 == 0 || (m4 >= 0 && trav[m4]))) {
+                    int nv[6] = {h1, h2 + 1, h3, t[h1], t[h2 + 1], t[h3]};
+                    ins(&hp, v[h1] + v[h2 + 1] + v[h3], nv);
+                }
+                if (h3 < kc - 1 && (h2 == 0 || (m5 >= 0 && trav[m5])) && (h1 == 0 || (m6 >= 0 && trav[m6]))) {
+                    int nv[6] = {h1, h2, h3 + 1, t[h1], t[h2], t[h3 + 1]};
+                    ins(&hp, v[h1] + v[h2] + v[h3 + 1], nv);
+                }
+            }
+        }
+        heap6_free(&hp);
+        free(trav); free(v); free(t);
     } else {
         const int two = (mode == ORC_IMI);
         float *v1 = (float *)malloc(sizeof(float) * (size_t)kc);
@@ -345,6 +494,8 @@ int orc_search(const orc_index *ix, int mode, int order, const float *q,
              * keeps looping there, the restatement stops. */
             if (hp.pos <= 0) break;
             pop(&hp, &h1, &h2, &h3, &h4);
+            if (h1 > g_max_rank) g_max_rank = h1;
+            if (h2 > g_max_rank) g_max_rank = h2;
             long bid = (long)h3 * kc + h4;
             int l;
             if (two) l = cell_len(L, bid);                /* multi_query.h:160-164 */

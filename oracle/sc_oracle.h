@@ -38,7 +38,7 @@ typedef struct {
     const float *raw;           /* [N][dim] raw vectors, or NULL             */
 } orc_index;
 
-enum { ORC_IVFADC = 0, ORC_IMI = 1, ORC_SC = 2 };
+enum { ORC_IVFADC = 0, ORC_IMI = 1, ORC_SC = 2, ORC_SC3 = 3 };
 enum { ORC_ORDER_HEAP = 0, ORC_ORDER_EXACT = 1 };
 
 void orc_pre_compute1(int dim, int mc, int kc, int mp, int kp,
@@ -55,6 +55,10 @@ int orc_search(const orc_index *ix, int mode, int order, const float *q,
                float *dist, int *ids, int cap,
                int *cells, int cap_cells, int *ncells_out,
                int *sum_out, int *empty_out);
+
+/* The largest coarse-list rank the last orc_search popped (empty cells
+ * included; -1 for IVFADC). */
+int orc_last_max_rank(void);
 
 void orc_topk(const float *dist, const int *ids, int n, int R,
               float *out_d, int *out_i);

@@ -1,9 +1,8 @@
 /*
  * sc_query.h -- drop-in for the reference's SCQuery (include/sc_query.h:21-51):
  * the second-candidate search over ordered pairs of nearest coarse centroids.
- * search_mr_ivf returns its R best in ascending distance (the reference
- * leaves them unsorted, sc_query.h:250-252).  search_mr_ivf3 (nc = 3) is not
- * served by the device library and reports so.
+ * search_mr_ivf and search_mr_ivf3 return their R best in ascending distance
+ * (the reference leaves them unsorted, sc_query.h:250-252, :469-473).
  */
 #ifndef SCG_DROPIN_SC_QUERY_H_
 #define SCG_DROPIN_SC_QUERY_H_
@@ -37,15 +36,18 @@ public:
         run_one(SCG_SC2, query, R, w, T, real_dist, dist, result, sum);
     }
 
-    /* SCQuery::search_mr_ivf3 (sc_query.h:265-475). */
-    void search_mr_ivf3(float *, float *&, float *&, int *, int *&, int *&, int *&, int *&, int *&, int *&, int *&,
-                        int *&, int *&, int *&, bool *, int &sum, int, int, int, int, bool, bool) {
+    /* SCQuery::search_mr_ivf3 (sc_query.h:265-475): the three-nearest-centroid
+     * cells of an SCQuery(3) index, walked over rank triples. */
+    void search_mr_ivf3(float *query, float *&v_tmp, float *&dist, int *tmp, int *&result, int *&hid1, int *&hid2,
+                        int *&hid3, int *&hid4, int *&hid5, int *&hid6, int *&s1, int *&prebuck, int *&cache,
+                        bool *traversed, int &sum, int R, int w, int T, int M, bool real_dist, bool verbose) {
+        (void)v_tmp; (void)tmp; (void)hid1; (void)hid2; (void)hid3; (void)hid4; (void)hid5; (void)hid6; (void)s1;
+        (void)prebuck; (void)cache; (void)traversed; (void)M; (void)verbose;
         if (config.mc != 1 || nc != 3) {
             std::cerr << "This search method is for MultiRank IVFADC-3 only" << std::endl;
             return;
         }
-        std::cerr << "search_mr_ivf3 is not provided by the GPU library" << std::endl;
-        sum = 0;
+        run_one(SCG_SC3, query, R, w, T, real_dist, dist, result, sum);
     }
 };
 

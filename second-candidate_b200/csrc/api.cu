@@ -103,6 +103,10 @@ int check_params(scg_index *h, const scg_search_params *p, int nq) {
             if (h->mc != 1 || h->ncells != (int64_t)h->kc * h->kc)
                 return fail(SCG_ERR_ARG, "This search method is for MultiRank IVFADC only");
             break;
+        case SCG_SC3:
+            if (h->mc != 1 || h->kc > 1024 || h->ncells != (int64_t)h->kc * h->kc * h->kc)
+                return fail(SCG_ERR_ARG, "This search method is for MultiRank IVFADC-3 only");
+            break;
         default:
             return fail(SCG_ERR_ARG, "unknown search mode");
     }
@@ -279,7 +283,9 @@ int reserve_pool(scg_index *h, Workspace *ws, int nq) {
 }
 
 int index_mode(const scg_index *h) {
-    return h->mc == 2 ? SCG_IMI : (h->ncells == h->kc ? SCG_IVFADC : SCG_SC2);
+    if (h->mc == 2) return SCG_IMI;
+    if (h->ncells == h->kc) return SCG_IVFADC;
+    return h->ncells == (int64_t)h->kc * h->kc ? SCG_SC2 : SCG_SC3;
 }
 
 int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_params *p, const float *dQ, int nq,
@@ -329,7 +335,8 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     // split kernels (selection, then a lighter scan at higher occupancy)
     int64_t stride = 0, over = 0;
     pool_dims(h, p, nq, Tq != nullptr, &stride, &over);
-    const bool split = allow_split && h->split && stride * (int64_t)nq + over < (1ll << 32);
+    // the three-list walk of SCG_SC3 runs in the fused kernel only
+    const bool split = allow_split && h->split && p->mode != SCG_SC3 && stride * (int64_t)nq + over < (1ll << 32);
     auto grid_of = [&](int part) {
         int g = h->num_sms * search_max_blocks_per_sm(p->mode, h->kc, h->mp, h->kp, upl, part, rot, qdim);
         return std::max(1, std::min(g, nq));
@@ -559,9 +566,9 @@ int scg_load_csr(scg_index *h, const int *L, const int *pid, const uint8_t *code
     if (!h || !L || (N > 0 && (!pid || !codes))) return fail(SCG_ERR_ARG, "null argument");
     if (!h->have_codebooks) return fail(SCG_ERR_STATE, "load codebooks before encoded data");
     if (N < 0 || N > 0xfffffffeLL) return fail(SCG_ERR_ARG, "N out of range");
-    int64_t imi_cells = ipow(h->kc, h->mc), sc_cells = (int64_t)h->kc * h->kc;
-    if (ncells != imi_cells && !(h->mc == 1 && ncells == sc_cells))
-        return fail(SCG_ERR_ARG, "ncells must be kc^mc or kc^2 (second-candidate)");
+    int64_t imi_cells = ipow(h->kc, h->mc), sc_cells = (int64_t)h->kc * h->kc, sc3_cells = sc_cells * h->kc;
+    if (ncells != imi_cells && !(h->mc == 1 && (ncells == sc_cells || (ncells == sc3_cells && h->kc <= 1024))))
+        return fail(SCG_ERR_ARG, "ncells must be kc^mc, kc^2 or kc^3 (second candidate, kc <= 1024)");
     std::vector<uint32_t> off((size_t)ncells + 1);
     off[0] = 0;
     int prev = 0;
@@ -1013,7 +1020,7 @@ int scg_build_index(scg_index *h, const float *dX, int64_t n, int nc, void *stre
     if (!h->have_codebooks) return fail(SCG_ERR_STATE, "load codebooks first");
     if (n < 0 || n > 0xfffffffeLL) return fail(SCG_ERR_ARG, "n out of range");
     if (n > 0 && !dX) return fail(SCG_ERR_ARG, "null buffer");
-    if (nc != 0 && nc != 2) return fail(SCG_ERR_ARG, "nc must be 0 (IVF/IMI) or 2 (second candidate)");
+    if (nc != 0 && nc != 2 && nc != 3) return fail(SCG_ERR_ARG, "nc must be 0 (IVF/IMI), 2 or 3 (second candidate)");
     if (nc && h->mc != 1) return fail(SCG_ERR_ARG, "the second-candidate index needs mc = 1");
     const int parts = nc ? nc : h->mc;
     const int64_t ncells = ipow(h->kc, parts);

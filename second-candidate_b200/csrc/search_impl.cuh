@@ -455,6 +455,37 @@ __device__ uint64_t staircase_count(const Lists &L, uint32_t tau, uint64_t *red)
     return block_sum(c, red);
 }
 
+// Three-list staircase of the second candidate with three nearest
+// centroids (sc_query.h:265-405): rank triples (h1, h2, h3) of one sorted
+// coarse list with key (A[h1] + A[h2]) + A[h3] (float adds in the reference's
+// order, sc_query.h:355-390).  With L.LB == L.LA, L.row_count(base, tau) is
+// the number of h3 with base + A[h3] <= tau.  The number of triples with key
+// <= tau (rows (h1, h2) in parallel over h1):
+__device__ uint64_t staircase3_count(const Lists &L, uint32_t tau, uint64_t *red) {
+    uint64_t c = 0;
+    const float a0 = L.a(0);
+    for (int h1 = threadIdx.x; h1 < L.kA; h1 += NT) {
+        const float a1 = L.a(h1);
+        for (int h2 = 0; h2 < L.kA; h2++) {
+            const float base = __fadd_rn(a1, L.a(h2));
+            if (f2o(__fadd_rn(base, a0)) > tau) break;
+            c += (uint64_t)L.row_count(base, tau);
+        }
+    }
+    return block_sum(c, red);
+}
+
+// Rank triple packing of the three-list walk (kc <= 1024): lexicographic
+// order of (h1, h2, h3) is the order of the packed word.
+__device__ __forceinline__ uint32_t rank3(int h1, int h2, int h3) {
+    return ((uint32_t)h1 << 20) | ((uint32_t)h2 << 10) | (uint32_t)h3;
+}
+// Cell of a rank triple: t[h1] kc^2 + t[h2] kc + t[h3] (sc_query.h:335).
+__device__ __forceinline__ uint32_t cell_of3(const Lists &L, uint32_t rank) {
+    const uint32_t kc = (uint32_t)L.kc;
+    return (L.ta((int)(rank >> 20)) * kc + L.ta((int)((rank >> 10) & 1023u))) * kc + L.ta((int)(rank & 1023u));
+}
+
 // Radix select over the last round's records [r0, r1): the smallest key x
 // with base + sum_{key <= x} weight >= need.  weight: 0 = length, 1 = one per
 // cell, 2 = one per non-empty cell.
@@ -747,6 +778,7 @@ struct ScanCtx {
     int nvis;
     uint32_t Svis;
     int kc, mp, kp, bsI;
+    uint32_t cdiv;  // second candidate: cell / cdiv is the residual's centroid (kc, or kc^2 with three)
     bool imi, sc, fast, rot;
     float qs;
     const float *dqc;
@@ -927,7 +959,7 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
                         h4 = cell - h3 * (uint32_t)c.kc;
                         cw.d0 = __fadd_rn(__fadd_rn(c.qs, c.dqc[h3]), c.dqc[c.kc + h4]);
                     } else if (c.sc) {
-                        h3 = cell / (uint32_t)c.kc;
+                        h3 = cell / c.cdiv;
                         h4 = 0;
                         cw.d0 = __fadd_rn(c.qs, c.dqc[h3]);
                     } else {
@@ -1128,7 +1160,7 @@ __device__ __forceinline__ void scan_cells(const SearchArgs &a, const Smem &S, Q
                     const uint32_t h3 = cell / (uint32_t)c.kc, h4 = cell - h3 * (uint32_t)c.kc;
                     cw.d0 = __fadd_rn(__fadd_rn(c.qs, c.dqc[h3]), c.dqc[c.kc + h4]);
                 } else {
-                    cw.d0 = __fadd_rn(c.qs, c.dqc[c.sc ? cell / (uint32_t)c.kc : cell]);
+                    cw.d0 = __fadd_rn(c.qs, c.dqc[c.sc ? cell / c.cdiv : cell]);
                 }
                 cw.h34 = 0;
                 W[lane] = cw;
@@ -1246,6 +1278,9 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
     const int kc = a.kc, mp = a.mp, kp = a.kp;
     const int kcP = next_pow2(kc);
     const bool imi = a.mode == SCG_IMI, sc = a.mode == SCG_SC2, ivf = a.mode == SCG_IVFADC;
+    // the three-list walk (fused kernel only): like sc for the w rule, the
+    // cell-0 rule and the residual's centroid
+    const bool sc3 = a.mode == SCG_SC3, scx = sc || sc3;
     const bool fast = a.precision == SCG_FAST;
     const int kBfull = ivf ? 1 : kc;
     const int cap = a.cap_rec;
@@ -1419,14 +1454,21 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
             L.LA = S.LA;
             L.LB = S.LB;
             L.kA = st.kA;
-            L.kB = sc ? st.kA : st.kB;
+            L.kB = scx ? st.kA : st.kB;
             L.kc = kc;
             L.ivf = ivf;
             const uint32_t nextB = sc ? st.nextA : st.nextB;
             // every cell outside the prefix grid has a key >= bound
             uint32_t bound = 0xffffffffu;
-            if (st.nextA != 0xffffffffu) bound = min(bound, f2o(__fadd_rn(o2f(st.nextA), L.b(0))));
-            if (!ivf && nextB != 0xffffffffu) bound = min(bound, f2o(__fadd_rn(L.a(0), o2f(nextB))));
+            if (sc3) {
+                if (st.nextA != 0xffffffffu) {
+                    const float nx = o2f(st.nextA), a0 = L.a(0);
+                    bound = min(f2o(__fadd_rn(__fadd_rn(nx, a0), a0)), f2o(__fadd_rn(__fadd_rn(a0, a0), nx)));
+                }
+            } else {
+                if (st.nextA != 0xffffffffu) bound = min(bound, f2o(__fadd_rn(o2f(st.nextA), L.b(0))));
+                if (!ivf && nextB != 0xffffffffu) bound = min(bound, f2o(__fadd_rn(L.a(0), o2f(nextB))));
+            }
             const bool whole = L.kA == kc && (ivf || L.kB == kc);
             PHASE_MARK(0);  // lists
 
@@ -1437,11 +1479,14 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
             nrec = 0;
             r0 = 0;
             trig = false;
-            const uint64_t grid_cells = (uint64_t)L.kA * L.kB;
+            const uint64_t grid_cells = (uint64_t)L.kA * L.kB * (sc3 ? (uint64_t)L.kA : 1ull);
             const uint64_t total_cells = grid_cells - (sc ? 1 : 0);
-            uint32_t tau_prev = 0;
-            const uint32_t lo_key = f2o(__fadd_rn(L.a(0), L.b(0)));
-            const uint32_t hi_key = f2o(__fadd_rn(L.a(L.kA - 1), L.b(L.kB - 1)));
+            uint32_t tau_prev = 0, tau_old = 0;  // tau_old: the last enumerated round's tau
+            const uint32_t lo_key = sc3 ? f2o(__fadd_rn(__fadd_rn(L.a(0), L.a(0)), L.a(0)))
+                                        : f2o(__fadd_rn(L.a(0), L.b(0)));
+            const uint32_t hi_key =
+                sc3 ? f2o(__fadd_rn(__fadd_rn(L.a(L.kA - 1), L.a(L.kA - 1)), L.a(L.kA - 1)))
+                    : f2o(__fadd_rn(L.a(L.kA - 1), L.b(L.kB - 1)));
             // first round: an eighth of the cells the density of this CTA's
             // previous query (else the index average) predicts; the visited
             // set does not depend on the round sizes
@@ -1455,7 +1500,7 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
             if (!nothing) {
                 for (; round < MAX_ROUNDS; round++) {
                     if (target > grid_cells) target = grid_cells;
-                    if (!sc && needW < target) {
+                    if (!scx && needW < target) {
                         // the w rule caps popped cells: never enumerate past w
                         uint64_t tw = needW;
                         if (tw < Ncell + 1) tw = Ncell + 1;
@@ -1473,7 +1518,7 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
                     if (round == 0 && gap0 != 0u && lo < hi) {
                         // first probe where this CTA's previous query ended
                         const uint32_t mid = (hi - lo > gap0) ? lo + gap0 : hi - 1;
-                        uint64_t c = staircase_count(L, mid, red);
+                        uint64_t c = sc3 ? staircase3_count(L, mid, red) : staircase_count(L, mid, red);
                         COUNT(9, 1);
                         if (c >= target) hi = mid;
                         else lo = mid + 1;
@@ -1482,7 +1527,7 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
                     }
                     while (lo < hi && it < 40) {
                         uint32_t mid = lo + ((hi - lo) >> 1);
-                        uint64_t c = staircase_count(L, mid, red);
+                        uint64_t c = sc3 ? staircase3_count(L, mid, red) : staircase_count(L, mid, red);
                         COUNT(9, 1);
                         if (c >= target) {
                             hi = mid;
@@ -1493,11 +1538,59 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
                         it++;
                     }
                     const uint32_t tau = hi;
-                    tau_prev = tau;
+                    tau_prev = tau;  // the next round's bisection starts above tau
                     if (round == 0 && tid == 0) {
                         st.tau_gap = tau - lo_key;
                         st.tau_T = T;
                     }
+                    uint64_t ls = 0, lne = 0, dummy = 0;
+                    int nnew = 0;
+                    if (sc3) {
+                        // the triples with tau_prev < key <= tau (round 0: key <=
+                        // tau): per row (h1, h2) the h3 between the two counts;
+                        // a counting pass, then the records
+                        const float a0 = L.a(0);
+                        auto rows = [&](auto &&emit) {
+                            for (int h1 = tid; h1 < L.kA; h1 += NT) {
+                                const float a1 = L.a(h1);
+                                for (int h2 = 0; h2 < L.kA; h2++) {
+                                    const float base = __fadd_rn(a1, L.a(h2));
+                                    if (f2o(__fadd_rn(base, a0)) > tau) break;
+                                    const int c1 = L.row_count(base, tau);
+                                    const int c0 = round == 0 ? 0 : min(c1, L.row_count(base, tau_old));
+                                    if (c1 > c0) emit(h1, h2, base, c0, c1);
+                                }
+                            }
+                        };
+                        uint64_t mine = 0;
+                        rows([&](int, int, float, int c0, int c1) { mine += (uint64_t)(c1 - c0); });
+                        uint64_t tot_new;
+                        uint64_t pos = block_exscan(mine, red, tot_new);
+                        if ((uint64_t)nrec + tot_new > (uint64_t)cap) {
+                            if (tid == 0) {
+                                st.err = 1;
+                                atomicOr(a.status, ST_CELL_BUDGET);
+                            }
+                            __syncthreads();
+                            break;
+                        }
+                        rows([&](int h1, int h2, float base, int c0, int c1) {
+                            for (int h3 = c0; h3 < c1; h3++) {
+                                const uint32_t rank = rank3(h1, h2, h3);
+                                const uint32_t cell = cell_of3(L, rank);
+                                uint32_t c = a.off[cell + 1] - a.off[cell];
+                                if (cell == 0) c = 0;  // sc_query.h:336-339
+                                const size_t r = (size_t)nrec + pos++;
+                                rec_key[r] = f2o(__fadd_rn(base, L.a(h3)));
+                                rec_rank[r] = rank;
+                                rec_cnt[r] = c;
+                                ls += c;
+                                lne += (c > 0);
+                            }
+                        });
+                        nnew = (int)tot_new;
+                        COUNT(10, nnew);
+                    } else {
                     // row counts at tau and the new cells per row
                     uint32_t mycnt = 0;
                     const int per = (L.kA + NT - 1) / NT;
@@ -1531,9 +1624,8 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
                         break;
                     }
                     __syncthreads();
-                    const int nnew = (int)tot_new;
+                    nnew = (int)tot_new;
                     COUNT(10, nnew);
-                    uint64_t ls = 0, lne = 0, dummy = 0;
                     int h1 = 0;
                     for (int idx = tid; idx < nnew; idx += NT) {
                         // row of idx: last h with rowpre[h] <= idx (rows only grow)
@@ -1556,7 +1648,10 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
                         ls += c;
                         lne += (c > 0);
                     }
-                    block_sum3(ls, lne, dummy, red);
+                    }
+                    block_sum3(ls, lne, dummy, red);  // also orders the record loop's rowp reads before the update
+                    if (!sc3)
+                        for (int h = tid; h < L.kA; h += NT) S.rowp[h] = S.rowc[h];
                     S0 = Ssum;
                     N0 = Ncell;
                     NE0 = NEc;
@@ -1565,9 +1660,9 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
                     Ssum += ls;
                     Ncell += (uint64_t)nnew;
                     NEc += lne;
-                    for (int h = tid; h < L.kA; h += NT) S.rowp[h] = S.rowc[h];
+                    tau_old = tau;
                     __syncthreads();
-                    uint64_t wcnt = sc ? NEc : Ncell;
+                    uint64_t wcnt = scx ? NEc : Ncell;
                     trig = (Ssum >= needT) || (wcnt >= needW);
                     if (trig || Ncell >= total_cells || tau >= hi_key) break;
                     // next target from the density seen so far
@@ -1607,9 +1702,9 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
                 uint32_t kap = 0xffffffffu;
                 if (Ssum >= needT)
                     kap = radix_cut(rec_key, rec_cnt, r0, nrec, klo, khi, S0, needT, 0, hist, red, st);
-                uint64_t wcnt = sc ? NEc : Ncell;
+                uint64_t wcnt = scx ? NEc : Ncell;
                 if (wcnt >= needW) {
-                    uint32_t kw = radix_cut(rec_key, rec_cnt, r0, nrec, klo, khi, sc ? NE0 : N0, needW, sc ? 2 : 1,
+                    uint32_t kw = radix_cut(rec_key, rec_cnt, r0, nrec, klo, khi, scx ? NE0 : N0, needW, scx ? 2 : 1,
                                             hist, red, st);
                     if (kw < kap) kap = kw;
                 }
@@ -1655,7 +1750,7 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
                         n += 1;
                         ne += (c > 0);
                         rc_ = (uint32_t)(ties[i] >> 32);
-                        if (s >= needT || (sc ? ne : n) >= needW) break;
+                        if (s >= needT || (scx ? ne : n) >= needW) break;
                     }
                     st.kappa = kap;
                     st.rank_cut = rc_;
@@ -1730,7 +1825,7 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
                 if (f) {
                     uint64_t p = pos + (ex >> 40);
                     if (p < vcap) {
-                        vis_cell_w[p] = cell_of(L, rank);
+                        vis_cell_w[p] = sc3 ? cell_of3(L, rank) : cell_of(L, rank);
                         vis_pre_w[p] = (uint32_t)(runc + (ex & 0xffffffffffull));
                     }
                 }
@@ -1798,7 +1893,8 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
             c.kp = kp;
             c.bsI = bsI;
             c.imi = imi;
-            c.sc = sc;
+            c.sc = scx;
+            c.cdiv = sc3 ? (uint32_t)kc * (uint32_t)kc : (uint32_t)kc;
             c.fast = fast;
             c.rot = a.rot != 0;
             c.raw_dim = a.raw_dim;

@@ -178,7 +178,8 @@ __global__ void k_vterm(int mode, int kc, int mp, int kp, int mc, uint64_t ncell
         r1 = dot_cr + (size_t)h3 * bs;
         r2 = dot_cr + (size_t)(h4 + kc - 1) * bs;
     } else {
-        uint32_t h3 = (mode == SCG_SC2) ? cell / (uint32_t)kc : cell;
+        // the residual's centroid: the cell's first nearest one (second candidate)
+        uint32_t h3 = (mode == SCG_SC2) ? cell / (uint32_t)kc : (mode == SCG_SC3 ? cell / ((uint32_t)kc * kc) : cell);
         r1 = dot_cr + (size_t)h3 * bs;
         r2 = r1;
     }

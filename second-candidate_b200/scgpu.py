@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 # different tuning defines); the default is the in-tree build.
 LIB_PATH = os.environ.get("SCG_LIBRARY") or os.path.join(HERE, "libscgpu.so")
 
-IVFADC, IMI, SC2 = 0, 1, 2
+IVFADC, IMI, SC2, SC3 = 0, 1, 2, 3
 FP32_EXACT, FAST, BF16, FP16 = 0, 1, 2, 3
 ENC_EXACT, ENC_TENSOR = 0, 1
 

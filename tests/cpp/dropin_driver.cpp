@@ -3,7 +3,7 @@
 // test_sc_query.cpp:111-203, test_encoder.cpp:58-88): one query per call with
 // caller-owned scratch, results freed with ::delete.
 //
-//   dropin_driver search <ivf|imi|sc> <cq.ctr_> <pq.ctr_> <x.edat_> <q.fvecs> <dim> <R> <w> <T> <out.txt>
+//   dropin_driver search <ivf|imi|sc|sc3> <cq.ctr_> <pq.ctr_> <x.edat_> <q.fvecs> <dim> <R> <w> <T> <out.txt>
 //                        [<base.fvecs>|- [M]]   (base: load_data + real_dist = true; M: the coarse-list argument)
 //   dropin_driver encode <0|2> <cq.ctr_> <pq.ctr_> <x.fvecs> <outdir> <prefix>
 //   dropin_driver quantize <x.fvecs> <dim> <m> <nsc> <out_prefix>      (PQQuantizer, test_quantizer.cpp-style)
@@ -54,6 +54,30 @@ static int search(int argc, char **argv) {
                             trav, sum, R, w, T, M, e, t1, t2, real_dist, false);
             if (trav[0]) bad++;  // test_multi_query.cpp:191
             out << sum << " " << e;
+            for (int j = 0; j < (R > sum ? sum : R); j++) out << " " << result[j] << ":" << dist[j];
+            out << "\n";
+            ::operator delete(result);
+            ::operator delete(dist);
+            result = nullptr;
+            dist = nullptr;
+        }
+    } else if (!strcmp(mode, "sc3")) {
+        SCQuery q(3);
+        q.load_codebooks(argv[3], argv[4], false);
+        q.load_encoded_data(argv[5], false);
+        if (base) q.load_data<float>(base, 4, false);
+        q.pre_compute1();
+        int kc = q.get_full_size();
+        const int M = M_arg > 0 ? M_arg : kc;
+        float *v_tmp = new float[kc + w];
+        int *it = new int[kc], *h1 = new int[w], *h2 = new int[w], *h3 = new int[w], *h4 = new int[w];
+        int *h5 = new int[w], *h6 = new int[w], *s1 = new int[w], *pb = new int[w];
+        int *cache = new int[(size_t)kc * kc * kc + w];
+        bool *trav = new bool[(size_t)kc * kc * kc]();
+        for (int i = 0; i < N; i++) {
+            q.search_mr_ivf3(data + (size_t)i * d, v_tmp, dist, it, result, h1, h2, h3, h4, h5, h6, s1, pb, cache,
+                             trav, sum, R, w, T, M, real_dist, false);
+            out << sum << " 0";
             for (int j = 0; j < (R > sum ? sum : R); j++) out << " " << result[j] << ":" << dist[j];
             out << "\n";
             ::operator delete(result);

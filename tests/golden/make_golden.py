@@ -2,7 +2,7 @@
 itself (its own headers and sources compiled by oracle/Makefile into
 oracle/_ref/libscref.so) on small seeded synthetic inputs.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]   (default: every case)
 
 Needs the reference tree (only readable where the sources live).  Each
 fixture ``<name>.npz`` holds the inputs (codebooks in .ctr_ layout, uint8
@@ -34,6 +34,8 @@ CASES = [
     ("plainpq_d32", O.IVFADC, 32, 2000, 1, 1, 8, 64, 10, [(2000, 1)]),
     ("imi_d32", O.IMI, 32, 3000, 2, 16, 4, 64, 10, [(300, 1 << 20), (120, 40), (0, 100), (2990, 1 << 20)]),
     ("sc_d32", O.SC, 32, 3000, 1, 16, 4, 64, 10, [(300, 1 << 20), (150, 12)]),
+    # SCQuery::search_mr_ivf3: three nearest centroids per cell, kc^3 cells
+    ("sc3_d32", O.SC3, 32, 4000, 1, 10, 4, 64, 12, [(300, 1 << 20), (120, 9), (0, 100)]),
 ]
 R = 20
 
@@ -45,7 +47,7 @@ def make_case(name, mode, D, N, mc, kc, mp, kp, nq, rules, seed):
     Xf = X.astype(np.float32)
     cq, pq = W.train_codebooks(Xf[:1500], mc, kc, mp, kp, 6, seed=seed + 3,
                                zero_coarse=(kc == 1))
-    nc = 2 if mode == O.SC else 0
+    nc = {O.SC: 2, O.SC3: 3}.get(mode, 0)
     with tempfile.TemporaryDirectory() as td:
         cqp, pqp, xp = (os.path.join(td, f) for f in ("cq.ctr_", "pq.ctr_", "x.fvecs"))
         formats.write_ctr(cqp, cq, kc, mc, D)
@@ -53,8 +55,8 @@ def make_case(name, mode, D, N, mc, kc, mp, kp, nq, rules, seed):
         formats.write_vecs(xp, Xf)
         cid, codes = O.ref_encode(cqp, pqp, xp, nc, N, mc, mp)
         O.ref_build_edat(cqp, pqp, xp, nc, td, "g")
-        edat = os.path.join(td, "g_mr2_ivf.edat_" if nc else "g_ivf.edat_")
-        ncells = kc ** (2 if mode == O.SC else mc)
+        edat = os.path.join(td, "g_mr%d_ivf.edat_" % nc if nc else "g_ivf.edat_")
+        ncells = kc ** (nc or mc)
         L, pid, co, ne = formats.read_edat(edat, ncells, mp)
     ix = O.Index(D, mc, kc, mp, kp, cq, pq, L, pid, co, raw=Xf)
     out = dict(mode=mode, D=D, N=N, mc=mc, kc=kc, mp=mp, kp=kp, R=R,
@@ -87,8 +89,10 @@ def make_case(name, mode, D, N, mc, kc, mp, kp, nq, rules, seed):
 
 def main():
     O.build(ref=True)
+    only = set(sys.argv[1:])
     for k, c in enumerate(CASES):
-        make_case(*c, seed=100 + 17 * k)
+        if not only or c[0] in only:
+            make_case(*c, seed=100 + 17 * k)
 
 
 if __name__ == "__main__":

@@ -10,8 +10,11 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 # candidate count, top-R ids and distances -- equals the compiled reference's.
 # IVFADC / IMI / plain PQ: all of them.  Second candidate: the reference heap
 # orders the exactly tied cells (a,b) / (b,a) arbitrarily, so 3 of 20 differ
-# by one tied boundary cell.
-GOLDEN_SAME_AS_REF = {"imi_d32": 40, "ivf_d32": 40, "plainpq_d32": 10, "sc_d32": 17}
+# by one tied boundary cell.  Three nearest centroids: the six rank
+# permutations of a centroid triple tie (up to rounding) and only one of them
+# holds vectors, so the reference heap's arbitrary order among them moves the
+# cut on 12 of 36 queries.
+GOLDEN_SAME_AS_REF = {"imi_d32": 40, "ivf_d32": 40, "plainpq_d32": 10, "sc_d32": 17, "sc3_d32": 24}
 
 
 def same_as_reference(c, ri, ids, d, sums):

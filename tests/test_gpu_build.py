@@ -32,10 +32,18 @@ def test_build_matches_reference_file(oracle_mod, path, tmp_path):
     import formats
     import scgpu
     c = helpers.load_case(path)
-    nc = 2 if int(c["mode"]) == O.SC else 0
+    nc = {O.SC: 2, O.SC3: 3}.get(int(c["mode"]), 0)
     g = _build(scgpu, c, c["X"], nc)
     g.write_edat(tmp_path / "gpu.edat_")
-    formats.write_edat(tmp_path / "ref.edat_", c["L"], c["pid"], c["icodes"])
+    if nc == 3:
+        # the reference buckets nc = 3 rows by a misaligned id window (its
+        # defect, pinned in test_oracle_golden); the file must be the
+        # bucketing of each row's own triple, from the reference's codes
+        D, kc, mp, kp = (int(c[k]) for k in ("D", "kc", "mp", "kp"))
+        L, pid, co, _ = O.distribution(O.SC, kc, 1, 3, c["cid"], c["codes"])
+        formats.write_edat(tmp_path / "ref.edat_", L, pid, co)
+    else:
+        formats.write_edat(tmp_path / "ref.edat_", c["L"], c["pid"], c["icodes"])
     assert open(tmp_path / "gpu.edat_", "rb").read() == open(tmp_path / "ref.edat_", "rb").read()
     g.close()
 

@@ -38,7 +38,7 @@ def parse(path):
 
 
 @pytest.mark.parametrize("name,mode,tag", [("imi_d32", O.IMI, "imi"), ("sc_d32", O.SC, "sc"),
-                                           ("ivf_d32", O.IVFADC, "ivf")])
+                                           ("ivf_d32", O.IVFADC, "ivf"), ("sc3_d32", O.SC3, "sc3")])
 def test_search_through_dropin(driver, oracle_mod, tmp_path, name, mode, tag):
     c = helpers.load_case(os.path.join(helpers.GOLDEN, name + ".npz"))
     D, mc, kc, mp, kp = (int(c[k]) for k in ("D", "mc", "kc", "mp", "kp"))
@@ -46,7 +46,7 @@ def test_search_through_dropin(driver, oracle_mod, tmp_path, name, mode, tag):
     formats.write_ctr(tmp_path / "pq.ctr_", c["pq"], kp, mp, D)
     formats.write_edat(tmp_path / "x.edat_", c["L"], c["pid"], c["icodes"])
     formats.write_vecs(tmp_path / "q.fvecs", c["Q"])
-    T, w, R = 300, (16 if mode == O.IVFADC else 1 << 16), 20
+    T, w, R = 300, (16 if mode == O.IVFADC else 1 << 12), 20
     subprocess.run([driver, "search", tag, str(tmp_path / "cq.ctr_"), str(tmp_path / "pq.ctr_"),
                     str(tmp_path / "x.edat_"), str(tmp_path / "q.fvecs"), str(D), str(R), str(w), str(T),
                     str(tmp_path / "out.txt")], check=True)

@@ -19,8 +19,8 @@ def test_encoder_golden(oracle_mod, path):
     g = scgpu.Index(0)
     g.load_codebooks(c["cq"], kc, mc, c["pq"], kp, mp, D)
     X = c["X"].astype(np.float32)
-    if int(c["mode"]) == O.SC:
-        cid, codes = g.sc_encode(X, 2)
+    if int(c["mode"]) in (O.SC, O.SC3):
+        cid, codes = g.sc_encode(X, 2 if int(c["mode"]) == O.SC else 3)
     else:
         cid, codes = g.encode(X)
     assert np.array_equal(cid, c["cid"])

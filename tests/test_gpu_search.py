@@ -11,7 +11,7 @@ import workloads as W
 
 pytestmark = pytest.mark.gpu
 
-MODES = {O.IVFADC: 0, O.IMI: 1, O.SC: 2}
+MODES = {O.IVFADC: 0, O.IMI: 1, O.SC: 2, O.SC3: 3}
 
 
 @pytest.fixture(scope="module")
@@ -61,16 +61,17 @@ def test_golden_cases(scg, oracle_mod, path):
     assert same_as_ref >= helpers.GOLDEN_SAME_AS_REF[os.path.basename(path)[:-4]], (same_as_ref, total)
 
 
-@pytest.mark.parametrize("mode,mc,kc", [(O.IVFADC, 1, 64), (O.IMI, 2, 48), (O.SC, 1, 48)])
+@pytest.mark.parametrize("mode,mc,kc", [(O.IVFADC, 1, 64), (O.IMI, 2, 48), (O.SC, 1, 48), (O.SC3, 1, 20)])
 def test_random_index_parity(scg, oracle_mod, mode, mc, kc):
     D, mp, kp = 64, 8, 256
     mix = W.Mixture(D, 16, 20.0, "u8", seed=21 + mode)
     X = mix.sample(40000, seed=22)
     Q = mix.sample(60, seed=23)
     cq, pq = W.train_codebooks(X[:5000], mc, kc, mp, kp, 4, seed=24)
-    if mode == O.SC:
-        cid, codes = O.sc_encode(D, kc, mp, kp, 2, cq, pq, X)
-        L, pid, co, _ = O.distribution(O.SC, kc, 1, 2, cid, codes)
+    if mode in (O.SC, O.SC3):
+        nc = 2 if mode == O.SC else 3
+        cid, codes = O.sc_encode(D, kc, mp, kp, nc, cq, pq, X)
+        L, pid, co, _ = O.distribution(O.SC, kc, 1, nc, cid, codes)
     else:
         cid, codes = O.encode((D, mc, kc, mp, kp), cq, pq, X)
         L, pid, co, _ = O.distribution(mode, kc, mc, 0, cid, codes)
@@ -140,7 +141,7 @@ def test_file_loaders(scg, oracle_mod, tmp_path):
     g.close()
 
 
-@pytest.mark.parametrize("mode,mc,kc", [(O.IVFADC, 1, 64), (O.IMI, 2, 48), (O.SC, 1, 48)])
+@pytest.mark.parametrize("mode,mc,kc", [(O.IVFADC, 1, 64), (O.IMI, 2, 48), (O.SC, 1, 48), (O.SC3, 1, 20)])
 @pytest.mark.parametrize("form", ["FAST", "BF16"])
 def test_tensor_core_forms(scg, oracle_mod, mode, mc, kc, form):
     """The tensor-core forms reorder and round the float sums.  SCG_FAST
@@ -155,9 +156,10 @@ def test_tensor_core_forms(scg, oracle_mod, mode, mc, kc, form):
     X = mix.sample(30000, seed=32)
     Q = mix.sample(80, seed=33)
     cq, pq = W.train_codebooks(X[:4000], mc, kc, mp, kp, 4, seed=34)
-    if mode == O.SC:
-        cid, codes = O.sc_encode(D, kc, mp, kp, 2, cq, pq, X)
-        L, pid, co, _ = O.distribution(O.SC, kc, 1, 2, cid, codes)
+    if mode in (O.SC, O.SC3):
+        nc = 2 if mode == O.SC else 3
+        cid, codes = O.sc_encode(D, kc, mp, kp, nc, cq, pq, X)
+        L, pid, co, _ = O.distribution(O.SC, kc, 1, nc, cid, codes)
     else:
         cid, codes = O.encode((D, mc, kc, mp, kp), cq, pq, X)
         L, pid, co, _ = O.distribution(mode, kc, mc, 0, cid, codes)
