@@ -54,11 +54,13 @@ typedef struct {
     int w;          /* cell cap: popped cells (IVFADC, IMI) or non-empty cells (SC) */
     int T;          /* candidate target: stop after the cell that reaches T         */
     int precision;  /* SCG_FP32_EXACT, SCG_FAST, SCG_BF16 or SCG_FP16                */
-    int rerank;     /* 0: ADC distances.  L > 0 (R <= L <= 1024): the ADC top-L
-                       shortlist re-ranked by the exact distance of the
-                       reference's real_dist branch (query.h:307-312), needs
-                       the raw vectors.  -1 (exact distance for every
-                       candidate) is refused with SCG_ERR_ARG.               */
+    int rerank;     /* 0: ADC distances.  -1: the reference's real_dist branch
+                       (query.h:307-312, multi_query.h:255-259,
+                       sc_query.h:232-236) -- every visited candidate scored
+                       by its exact distance, the R smallest returned.
+                       L > 0 (R <= L <= 1024): only the ADC top-L shortlist
+                       re-ranked by that exact distance.  Both need the raw
+                       vectors (scg_load_raw / scg_load_raw_u8).             */
 } scg_search_params;
 
 /* Message of the last failing call on this thread (always NUL-terminated). */
