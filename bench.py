@@ -423,18 +423,19 @@ def encode_leg(scgpu, ix, cfg, rows, dev):
     import torch
     import workloads as W
     X = W.mixture_sampler(cfg, 99, dev)(rows)
-    mcp = 1 if cfg["mode"] == "sc" else cfg["mc"]
+    nc = 2 if cfg["mode"] == "sc" else 0  # the second-candidate index: SCEncoder::encode<T>, two centroids
+    mcp = nc if nc else cfg["mc"]
     out = {}
     codes = {}
     for name, method in (("tensor", scgpu.ENC_TENSOR), ("exact", scgpu.ENC_EXACT)):
         ix.set_encoder(method)
         cid = torch.empty(rows, mcp, dtype=torch.int16, device=dev)
         cod = torch.empty(rows, cfg["mp"], dtype=torch.uint8, device=dev)
-        ix.encode_device(X[:65536].data_ptr(), 65536, 0, cid.data_ptr(), cod.data_ptr())  # warm-up
+        ix.encode_device(X[:65536].data_ptr(), 65536, nc, cid.data_ptr(), cod.data_ptr())  # warm-up
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        ix.encode_device(X.data_ptr(), rows, 0, cid.data_ptr(), cod.data_ptr())
+        ix.encode_device(X.data_ptr(), rows, nc, cid.data_ptr(), cod.data_ptr())
         e1.record()
         e1.synchronize()
         out[name + "_rows_per_s"] = rows / (e0.elapsed_time(e1) / 1e3)
@@ -443,8 +444,9 @@ def encode_leg(scgpu, ix, cfg, rows, dev):
     out["same_codes"] = bool(np.array_equal(codes["tensor"][0], codes["exact"][0]) and
                              np.array_equal(codes["tensor"][1], codes["exact"][1]))
     out["rows"] = rows
-    out["what"] = ("Encoder::encode<T> codes (IVF/IMI) of rows drawn from the workload's mixture: tcgen05 "
-                   "split-BF16 distance tables + exact double re-check vs the all-double kernel")
+    out["what"] = ("%s codes of rows drawn from the workload's mixture: tcgen05 split-BF16 distance tables + "
+                   "exact double re-check vs the all-double kernel"
+                   % ("SCEncoder::encode<T> (two nearest coarse centroids)" if nc else "Encoder::encode<T> (IVF/IMI)"))
     return out
 
 
@@ -634,7 +636,10 @@ def run_workload(args, name, scgpu, dev, world, full=True):
         ix.set_phase_counters(True)
         step()
         ph = ix.last_phase_counters()
-        ph["per_query_cycles"] = {k: ph[k] / nq for k in ("sort", "rounds", "cut", "compact", "scan", "final_merge")}
+        ph["per_query_cycles"] = {k: ph[k] / nq for k in ("sort", "bisection", "rounds", "cut", "compact", "lut_fill",
+                                                          "warm_threshold", "scan", "final_merge")}
+        ph["per_query"] = {k: ph[k] / nq for k in ("pending", "round_count", "bisection_steps", "enumerated_cells",
+                                                   "full_sorts")}
         ix.set_phase_counters(False)
         out["phases"] = ph
 

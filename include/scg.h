@@ -181,12 +181,21 @@ int scg_set_scan_tuning(scg_index *h, int precision, int upl);
 /* Kernel organisation of the search: on (the default), cell selection and
  * the ADC scan run as two persistent kernels (the scan kernel holds more
  * resident warps per SM); off, as one fused kernel.  Both give identical
- * results; searches with per-query targets always use the fused kernel. */
+ * results; SCG_SC3 searches always use the fused kernel. */
 int scg_set_kernel_split(scg_index *h, int on);
 
 /* Per-query candidate targets (device pointer to nq ints) for the next
  * scg_search_device call; NULL restores the single T of the parameters. */
 int scg_set_query_targets(scg_index *h, const int *d_T);
+
+/* Rank limit M of the coarse lists (the M argument of search_multi2,
+ * multi_query.h:62-128; search_mr_ivf, sc_query.h:60-106; search_mr_ivf3):
+ * the IMI and second-candidate walks of later searches use only ranks
+ * 0..M-1 of each sorted coarse list, and stop when that grid is exhausted.
+ * 0 (the default) or M >= kc: all ranks.  The reference sorts only the top
+ * M ranks but lets its walk continue into the unsorted rest; where its walk
+ * stays inside ranks 0..M-1 the two agree.  IVFADC has no rank limit. */
+int scg_set_rank_limit(scg_index *h, int M);
 
 /* Budgets of the traversal: the most cells one query may enumerate
  * (default 131072).  Larger budgets cost device memory per resident CTA. */
@@ -252,12 +261,14 @@ int scg_kmeans(const float *X, int64_t n, int dim, int nseg, int k, int iters, u
 int scg_exact_nn(const float *dX, int64_t n, const float *dQ, int nq, int dim, int *d_ids, float *d_dists,
                  int device, void *stream);
 
-/* Encoder arithmetic for IVF/IMI codes (scg_encode, scg_encode_device with
- * nc = 0).  SCG_ENC_TENSOR (the default): distances ranked by tcgen05
+/* Encoder arithmetic (scg_encode, scg_sc_encode, scg_encode_device, and the
+ * index build).  SCG_ENC_TENSOR (the default): distances ranked by tcgen05
  * split-BF16 GEMM tiles, every centroid within the tiles' error margin of the
- * minimum re-scored with the reference's double arithmetic -- the codes are
- * the reference's.  SCG_ENC_EXACT: every distance in double (one thread per
- * row).  The second-candidate encoder always uses the exact kernel. */
+ * minimum (of the nc-th smallest, for the second candidate's nc nearest
+ * coarse centroids) re-scored with the reference's double arithmetic and its
+ * float-rounded comparisons where it has them -- the codes are the
+ * reference's.  SCG_ENC_EXACT: every distance in double (one thread per
+ * row). */
 #define SCG_ENC_EXACT 0
 #define SCG_ENC_TENSOR 1
 int scg_set_encoder(scg_index *h, int method);
@@ -286,11 +297,12 @@ int scg_cell_counts(scg_index *h, int *L, int64_t ncells);
 
 /* Diagnostics: with counters on, each search accumulates per-phase cycle
  * counts of the search kernels (thread 0 of every CTA, summed over queries):
- * [0] coarse-list sort, [1] staircase rounds, [2] cut, [3] compaction,
- * [4] scan rounds, [5] final merge, [7] merges, [8] rounds, [9] bisection
- * steps, [10] enumerated cells, and in the scan-only kernel [12] the LUT (or
- * query) staging and [13] the warm-up scores and threshold.  n is the
- * capacity of out (<= 16). */
+ * [0] coarse-list sort, [1] staircase rounds' enumeration, [2] cut,
+ * [3] compaction, [4] scan rounds, [5] final merge, [6] scan survivors,
+ * [7] merges, [8] rounds, [9] bisection steps, [10] enumerated cells,
+ * [11] complete sorts, [14] the rounds' bisections, and in the scan-only
+ * kernel [12] the LUT (or query) staging and [13] the warm-up scores and
+ * threshold.  n is the capacity of out (<= 16). */
 int scg_set_phase_counters(scg_index *h, int on);
 int scg_last_phase_counters(scg_index *h, long long *out, int n);
 

@@ -116,9 +116,11 @@ class Index:
     def cfg(self):
         return (self.dim, self.mc, self.kc, self.mp, self.kp)
 
-    def search_one(self, mode, q, w, T, order=ORDER_EXACT, real_dist=False):
+    def search_one(self, mode, q, w, T, order=ORDER_EXACT, real_dist=False, rank_limit=0):
         """All candidates of one query in visiting order plus the visited
-        non-empty cells: dict(dist, ids, cells, sum, empty)."""
+        non-empty cells: dict(dist, ids, cells, sum, empty, max_rank).
+        rank_limit > 0 confines the IMI / second-candidate walk to ranks
+        0..rank_limit-1 of each sorted coarse list."""
         q = np.ascontiguousarray(q, np.float32)
         cap = self.N
         dist = np.zeros(max(cap, 1), np.float32)
@@ -127,17 +129,21 @@ class Index:
         ncells = ctypes.c_int(0)
         s = ctypes.c_int(0)
         e = ctypes.c_int(0)
-        rc = lib().orc_search(ctypes.byref(self._s), mode, order, _p(q, _f32p), w, T,
-                              1 if real_dist else 0, _p(dist, _f32p), _p(ids, _i32p), cap,
-                              _p(cells, _i32p), cap, ctypes.byref(ncells), ctypes.byref(s),
-                              ctypes.byref(e))
+        lib().orc_set_rank_limit(int(rank_limit))
+        try:
+            rc = lib().orc_search(ctypes.byref(self._s), mode, order, _p(q, _f32p), w, T,
+                                  1 if real_dist else 0, _p(dist, _f32p), _p(ids, _i32p), cap,
+                                  _p(cells, _i32p), cap, ctypes.byref(ncells), ctypes.byref(s),
+                                  ctypes.byref(e))
+        finally:
+            lib().orc_set_rank_limit(0)
         if rc != 0:
             raise RuntimeError("orc_search failed: %d" % rc)
         n = s.value
         return dict(dist=dist[:n].copy(), ids=ids[:n].copy(), cells=cells[:ncells.value].copy(),
                     sum=n, empty=e.value, max_rank=int(lib().orc_last_max_rank()))
 
-    def search(self, mode, Q, R, w, T, order=ORDER_EXACT, real_dist=False):
+    def search(self, mode, Q, R, w, T, order=ORDER_EXACT, real_dist=False, rank_limit=0):
         """Top-R per query (ascending distance; equal distances by id), the
         way the reference's top-R step orders them.  Returns
         (ids[nq,R] padded with -1, dist[nq,R] padded with +inf, sums[nq])."""
@@ -147,7 +153,7 @@ class Index:
         out_d = np.full((nq, R), np.inf, np.float32)
         sums = np.zeros(nq, np.int32)
         for i in range(nq):
-            r = self.search_one(mode, Q[i], w, T, order, real_dist)
+            r = self.search_one(mode, Q[i], w, T, order, real_dist, rank_limit)
             m = min(R, r["sum"])
             td = np.zeros(max(m, 1), np.float32)
             ti = np.zeros(max(m, 1), np.int32)

@@ -305,6 +305,13 @@ static int cell_len(const int *L, long bid) { return bid > 0 ? L[bid] - L[bid - 
  * popped, empty cells included (IMI and second candidate; -1 otherwise). */
 static int g_max_rank = -1;
 int orc_last_max_rank(void) { return g_max_rank; }
+
+/* Rank limit of the IMI and second-candidate walks (the library's
+ * scg_set_rank_limit; the reference has none -- it sorts only the top M
+ * ranks, multi_query.h:125-128, but walks on into the rest): ranks 0..M-1
+ * of each sorted coarse list only; 0 = all. */
+static int g_rank_limit = 0;
+void orc_set_rank_limit(int M) { g_rank_limit = M; }
 static long cell_start(const int *L, long bid) { return bid > 0 ? L[bid - 1] : 0; }
 
 /* One query of PQQuery::search_ivfadc (query.h:202-325),
@@ -386,6 +393,7 @@ int orc_search(const orc_index *ix, int mode, int order, const float *q,
         heap6_alloc(&hp, order == ORC_ORDER_HEAP ? w : (int)(3 * kc2 + 8));
         void (*ins)(heap6 *, float, const int *) = (order == ORC_ORDER_HEAP) ? ref_insert6 : ex_insert6;
         void (*pop)(heap6 *, int *) = (order == ORC_ORDER_HEAP) ? ref_pop6 : ex_pop6;
+        const int lim = (g_rank_limit > 0 && g_rank_limit < kc) ? g_rank_limit : kc;
         int hv[6] = {0, 0, 0, t[0], t[0], t[0]};
         ins(&hp, 3.0f * v[0], hv);                     /* sc_query.h:316-324 */
         long i = 0, count2 = 0;
@@ -415,15 +423,15 @@ int orc_search(const orc_index *ix, int mode, int order, const float *q,
                  * predecessors are traversed */
                 const long m1 = i + kc2 - kc, m2 = i + kc2 - 1, m3 = i + kc - 1;
                 const long m4 = i + kc - kc2, m5 = i - kc + 1, m6 = i - kc2 + 1;
-                if (h1 < kc - 1 && (h2 == 0 || (m1 < size3 && trav[m1])) && (h3 == 0 || (m2 < size3 && trav[m2]))) {
+                if (h1 < lim - 1 && (h2 == 0 || (m1 < size3 && trav[m1])) && (h3 == 0 || (m2 < size3 && trav[m2]))) {
                     int nv[6] = {h1 + 1, h2, h3, t[h1 + 1], t[h2], t[h3]};
                     ins(&hp, v[h1 + 1] + v[h2] + v[h3], nv);
                 }
-                if (h2 < kc - 1 && (h3 == 0 || (m3 < size3 && trav[m3])) && (h1 == 0 || (m4 >= 0 && trav[m4]))) {
+                if (h2 < lim - 1 && (h3 == 0 || (m3 < size3 && trav[m3])) && (h1 == 0 || (m4 >= 0 && trav[m4]))) {
                     int nv[6] = {h1, h2 + 1, h3, t[h1], t[h2 + 1], t[h3]};
                     ins(&hp, v[h1] + v[h2 + 1] + v[h3], nv);
                 }
-                if (h3 < kc - 1 && (h2 == 0 || (m5 >= 0 && trav[m5])) && (h1 == 0 || (m6 >= 0 && trav[m6]))) {
+                if (h3 < lim - 1 && (h2 == 0 || (m5 >= 0 && trav[m5])) && (h1 == 0 || (m6 >= 0 && trav[m6]))) {
                     int nv[6] = {h1, h2, h3 + 1, t[h1], t[h2], t[h3 + 1]};
                     ins(&hp, v[h1] + v[h2] + v[h3 + 1], nv);
                 }
@@ -474,6 +482,7 @@ int orc_search(const orc_index *ix, int mode, int order, const float *q,
 
         int count2 = 0, h1 = 0, h2 = 0, h3, h4;
         long i = 0;
+        const int lim = (g_rank_limit > 0 && g_rank_limit < kc) ? g_rank_limit : kc;
         if (two) {
             /* multi_query.h:133-149 */
             ins(&hp, v1[0] + v2[0], 0, 0, t1[0], t2[0]);
@@ -482,8 +491,10 @@ int orc_search(const orc_index *ix, int mode, int order, const float *q,
              * (test_sc_query.cpp:160-161). */
             trav[0] = 1;
             float d0 = v1[0] + v1[1];
-            ins(&hp, d0, 0, 1, t1[0], t1[1]);
-            ins(&hp, d0, 1, 0, t1[1], t1[0]);
+            if (lim >= 2) {
+                ins(&hp, d0, 0, 1, t1[0], t1[1]);
+                ins(&hp, d0, 1, 0, t1[1], t1[0]);
+            }
         }
         for (;;) {
             /* IMI: while(count2 < w && sum < T) (multi_query.h:151);
@@ -512,9 +523,9 @@ int orc_search(const orc_index *ix, int mode, int order, const float *q,
                 /* multi_query.h:175-204, sc_query.h:154-185: push (h1+1,h2)
                  * once (h1+1,h2-1) is traversed, (h1,h2+1) once (h1-1,h2+1)
                  * is traversed. */
-                if (h1 < kc - 1 && (h2 == 0 || ((size_t)(i + kc - 1) < grid && trav[i + kc - 1])))
+                if (h1 < lim - 1 && (h2 == 0 || ((size_t)(i + kc - 1) < grid && trav[i + kc - 1])))
                     ins(&hp, v1[h1 + 1] + v2[h2], h1 + 1, h2, t1[h1 + 1], t2[h2]);
-                if (h2 < kc - 1 && (h1 == 0 || (i - kc + 1 >= 0 && trav[i - kc + 1])))
+                if (h2 < lim - 1 && (h1 == 0 || (i - kc + 1 >= 0 && trav[i - kc + 1])))
                     ins(&hp, v1[h1] + v2[h2 + 1], h1, h2 + 1, t1[h1], t2[h2 + 1]);
             }
         }

@@ -60,6 +60,9 @@ int orc_search(const orc_index *ix, int mode, int order, const float *q,
  * included; -1 for IVFADC). */
 int orc_last_max_rank(void);
 
+/* Rank limit of the IMI and second-candidate walks (0 = all ranks). */
+void orc_set_rank_limit(int M);
+
 void orc_topk(const float *dist, const int *ids, int n, int R,
               float *out_d, int *out_i);
 

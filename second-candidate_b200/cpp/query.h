@@ -39,9 +39,15 @@ protected:
     float *raw_data = nullptr;
 
     /* One query through the device search; fills the reference-style
-     * outputs.  Returns false (after printing) on a library error. */
+     * outputs.  M > 0: the walk uses only ranks 0..M-1 of each sorted
+     * coarse list.  Returns false (after printing) on a library error. */
     bool run_one(int mode, float *query, int R, int w, int T, bool real_dist, float *&dist, int *&result,
-                 int &sum, int *empty = nullptr, double *t_tables = nullptr, double *t_search = nullptr) {
+                 int &sum, int *empty = nullptr, double *t_tables = nullptr, double *t_search = nullptr,
+                 int M = 0) {
+        if (scg_set_rank_limit(h, M) != SCG_OK) {
+            std::cerr << scg_message() << std::endl;
+            return false;
+        }
         scg_search_params p;
         p.mode = mode;
         p.R = R;
@@ -159,7 +165,10 @@ public:
     }
 
     /* Additions of the B200 build: the batched entry point and the handle. */
-    int search_batch(int mode, const float *Q, int nq, int R, int w, int T, int *ids, float *dists, int *sums) {
+    int search_batch(int mode, const float *Q, int nq, int R, int w, int T, int *ids, float *dists, int *sums,
+                     int M = 0) {
+        int rc = scg_set_rank_limit(h, M);
+        if (rc != SCG_OK) return rc;
         scg_search_params p;
         p.mode = mode; p.R = R; p.w = w; p.T = T; p.precision = precision_; p.rerank = 0;
         return scg_search(h, &p, Q, nq, ids, dists, sums);

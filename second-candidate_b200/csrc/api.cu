@@ -407,6 +407,7 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     sa.smeta = b.smeta;
     sa.slist_w = coarse_sort_width(h->kc);
     sa.Tq = Tq;
+    sa.rank_limit = h->rank_limit;
     sa.dqc = b.dqc; sa.dqr = b.dqr; sa.qn = b.qn; sa.qsum = b.qsum;
     sa.off = h->off.as<uint32_t>(); sa.pid = h->pid.as<int>(); sa.codes = h->codes.as<uint8_t>();
     sa.dot_cr = h->dot_cr.as<float>();
@@ -819,10 +820,10 @@ int scg_search_graph(scg_index *h, const scg_search_params *p, const float *dQ, 
     cudaStream_t s = (cudaStream_t)stream;
     // everything the captured sequence reads or writes, as one key
     char key[512];
-    snprintf(key, sizeof(key), "%d %d %d %d %d %d|%p %d %p %p %p|%p %d %d %d %d %lld %d", p->mode, p->R, p->w, p->T,
-             p->precision, p->rerank, (const void *)dQ, nq, (void *)d_ids, (void *)d_dists, (void *)d_sums,
+    snprintf(key, sizeof(key), "%d %d %d %d %d %d|%p %d %p %p %p|%p %d %d %d %d %lld %d %d", p->mode, p->R, p->w,
+             p->T, p->precision, p->rerank, (const void *)dQ, nq, (void *)d_ids, (void *)d_dists, (void *)d_sums,
              (const void *)h->d_Tq, (int)h->split, h->tuned_upl[0], h->tuned_upl[1], h->cap_rec, (long long)h->N,
-             h->device);
+             h->device, h->rank_limit);
     if (!h->graph_exec || h->graph_key != key || h->graph_stream != s) {
         if (h->graph_exec) {
             cudaGraphExecDestroy(h->graph_exec);
@@ -944,6 +945,14 @@ int scg_set_kernel_split(scg_index *h, int on) {
     return SCG_OK;
 }
 
+int scg_set_rank_limit(scg_index *h, int M) {
+    if (!h) return fail(SCG_ERR_ARG, "null index");
+    if (M < 0) return fail(SCG_ERR_ARG, "rank limit must be >= 0");
+    std::lock_guard<std::mutex> g(h->mu);
+    h->rank_limit = M;
+    return SCG_OK;
+}
+
 int scg_set_query_targets(scg_index *h, const int *d_T) {
     if (!h) return fail(SCG_ERR_ARG, "null index");
     h->d_Tq = d_T;
@@ -957,9 +966,11 @@ int scg_set_cell_budget(scg_index *h, int max_cells) {
     return SCG_OK;
 }
 
-// IVF/IMI codes through tensor-core distance tables and exact re-checks
-// (encode_tc.cu), a chunk of rows at a time.
-static int encode_tc(scg_index *h, const float *dX, int64_t n, uint16_t *d_cid, uint8_t *d_codes, cudaStream_t s) {
+// Codes through tensor-core distance tables and exact re-checks
+// (encode_tc.cu), a chunk of rows at a time: IVF/IMI (nc = 0) or the second
+// candidate's nc nearest coarse centroids with float-rounded comparisons.
+static int encode_tc(scg_index *h, const float *dX, int64_t n, int nc, uint16_t *d_cid, uint8_t *d_codes,
+                     cudaStream_t s) {
     int rc;
     const int bsc = h->dim / h->mc, bsp = h->dim / h->mp;
     if (!h->enc_ready) {
@@ -995,8 +1006,10 @@ static int encode_tc(scg_index *h, const float *dX, int64_t n, uint16_t *d_cid, 
         PickArgs pa;
         pa.X = ta.Q; pa.n = nr; pa.dim = h->dim; pa.nseg = h->mc; pa.kseg = h->kc; pa.len = bsc;
         pa.C = h->cq.as<float>(); pa.tab = h->enc_tab.as<float>(); pa.segmax = h->enc_cmax.as<float>();
-        pa.cid = d_cid + (size_t)r0 * h->mc; pa.code = nullptr; pa.resid = h->enc_res.as<float>();
+        pa.cid = d_cid + (size_t)r0 * (nc ? nc : h->mc); pa.code = nullptr; pa.resid = h->enc_res.as<float>();
         pa.status = h->enc_status.as<int>();
+        pa.nbest = nc ? nc : 1;
+        pa.fcmp = nc ? 1 : 0;
         launch_pick(pa, s);
         ta.Q = h->enc_res.as<float>();
         ta.segs = 2;
@@ -1004,6 +1017,7 @@ static int encode_tc(scg_index *h, const float *dX, int64_t n, uint16_t *d_cid, 
         pa.X = h->enc_res.as<float>(); pa.nseg = h->mp; pa.kseg = h->kp; pa.len = bsp;
         pa.C = h->pq.as<float>(); pa.segmax = h->enc_rmax.as<float>();
         pa.cid = nullptr; pa.code = d_codes + (size_t)r0 * h->mp; pa.resid = nullptr;
+        pa.nbest = 1;
         launch_pick(pa, s);
         SCG_CUDA(cudaGetLastError());
     }
@@ -1235,7 +1249,7 @@ int scg_encode_device(scg_index *h, const float *dX, int64_t n, int nc, uint16_t
     int rc;
     if ((rc = set_device(h))) return rc;
     cudaStream_t s = stream ? (cudaStream_t)stream : h->stream;
-    if (nc == 0 && h->encoder == SCG_ENC_TENSOR) return n > 0 ? encode_tc(h, dX, n, d_cid, d_codes, s) : SCG_OK;
+    if (h->encoder == SCG_ENC_TENSOR) return n > 0 ? encode_tc(h, dX, n, nc, d_cid, d_codes, s) : SCG_OK;
     if (encode_smem_bytes(h->dim, mcp) > 227 * 1024)
         return fail(SCG_ERR_ARG, "dimension too large for the exact encoder's shared-memory tile");
     EncodeArgs a;
@@ -1487,6 +1501,7 @@ extern "C" int scg_search_device_noalloc(scg_index *h, const scg_search_params *
     sa.rot = rot;
     sa.upl = upl;
     sa.Tq = h->d_Tq;
+    sa.rank_limit = h->rank_limit;
     sa.dqc = dqc; sa.dqr = dqr; sa.qn = qn; sa.qsum = qsum;
     sa.off = h->off.as<uint32_t>(); sa.pid = h->pid.as<int>(); sa.codes = h->codes.as<uint8_t>();
     sa.dot_cr = h->dot_cr.as<float>();

@@ -81,6 +81,7 @@ struct scg_index {
     bool have_codebooks = false, have_csr = false, precomputed = false;
     int cap_rec = 131072;
     const int *d_Tq = nullptr;
+    int rank_limit = 0;  // scg_set_rank_limit: walk ranks < M of each coarse list (0: all)
     scg::DevBuf cq, pq, norm_c, norm_r, dot_cr, off, pid, codes, raw, vterm;
     // candidates and cells seen by the selection so far (u64 x 2): the
     // coarse prefix length rule uses their ratio instead of N / cells

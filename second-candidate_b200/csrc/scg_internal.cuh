@@ -89,6 +89,7 @@ struct SearchArgs {
     int upl;                // candidates per lane per scan chunk: 2, 4 or 8
     int shortlist;          // 1: the R best feed the exact re-rank, which orders them itself
     const int *Tq;          // optional per-query T
+    int rank_limit;         // IMI / second candidate: walk ranks < rank_limit of each list (0: all)
     const uint64_t *slist;  // optional coarse-list prefixes sorted ahead: [nq][lists][slist_w]
     const uint32_t *smeta;  // their lengths and next high words: [nq][lists][2]
     int slist_w;
@@ -149,10 +150,10 @@ size_t encode_smem_bytes(int dim, int mcp);
 // ||c||^2 of `rows` vectors of length len (the reference's float order).
 void launch_norms(const float *C, int rows, int len, float *out, cudaStream_t s);
 
-// Nearest centroid per (row, segment) from a tensor-core distance table,
+// Nearest centroid(s) per (row, segment) from a tensor-core distance table,
 // re-checked exactly: every centroid whose table value is within the
-// table's error margin of the row's minimum is scored with the reference's
-// double arithmetic and the first exact minimum wins.
+// table's error margin of the nbest-th smallest is scored with the
+// reference's double arithmetic and the nbest smallest (distance, id) win.
 struct PickArgs {
     const float *X;        // [n][dim] rows (or residuals)
     int64_t n;
@@ -164,6 +165,8 @@ struct PickArgs {
     uint8_t *code;         // [n][nseg] (PQ) or null
     float *resid;          // [n][dim] x - c for the chosen c (coarse), or null
     int *status;
+    int nbest = 1;         // centroids kept per (row, segment), 1..3 (cid holds [n][nseg][nbest])
+    int fcmp = 0;          // compare float-rounded distances (the second-candidate encoder)
 };
 void launch_pick(const PickArgs &a, cudaStream_t s);
 void launch_segmax(const float *norms, int nseg, int kseg, float *out, cudaStream_t s);

@@ -35,6 +35,8 @@
 // bound, and one radix-select merge over them gives the R best.
 #pragma once
 
+#include <type_traits>
+
 #include "exact_dist.cuh"
 
 namespace scg {
@@ -53,6 +55,7 @@ constexpr int RMAX = 1024;      // largest R
 #endif
 constexpr int WARMN = SCG_WARMN;  // candidates scored before the threshold is set
 constexpr int WWIN = 32;        // per-warp window of visited cells
+constexpr int MERGE_KPT = 16;   // survivors per thread of the final merge's register bisection
 // Candidates per lane per claimed chunk (U, a template parameter of the
 // scan: 2, 4 or 8); a warp claims 32 * U candidates at a time.
 constexpr int SBCAP = 2048;     // sorted coarse prefix capacity
@@ -166,7 +169,9 @@ __host__ __device__ inline size_t carve(int mode, int kc, int mp, int kp, int pa
 }
 
 static_assert(2 * RMAX <= WARMN, "top-R buffers live inside the warm-up scores");
+static_assert(2 * RMAX + 2 * NT <= WARMN, "the final merge's filtered survivors live inside the warm-up scores");
 static_assert(RBINS * 4 + TIECAP * 8 <= NWARP * WWIN * sizeof(CellWin), "select bins alias the cell windows");
+static_assert((1 << 10) * 4 <= NWARP * WWIN * sizeof(CellWin), "threshold bins alias the cell windows");
 static_assert(WARMN % 32 == 0, "scan chunks start at multiples of 32 (the rotated LUT relies on it)");
 
 // ---------------------------------------------------------------------------
@@ -652,6 +657,89 @@ __device__ uint32_t radix_kth_word(Word word, int n, uint64_t k, uint32_t *hist,
     return prefix;
 }
 
+// An upper bound b of the k-th smallest (1-based, 1 <= k <= n) of the n
+// 32-bit words word(i), n <= NT * KPT, less than 2^sbits above it: at least
+// k words are <= b.  The words sit in registers (KPT per thread); radix
+// passes of up to KBITS bits over the range [min, max] of the words (one
+// histogram of 2^KBITS bins in `hist` per pass) narrow the k-th smallest to
+// a bin of at most 2^sbits words, whose upper end is returned.  With ordered
+// float words and sbits = 8 the bound is within 2^-15 relative of the k-th
+// distance; on distances two or three passes suffice.
+constexpr int KBITS = 10;
+template <int KPT, class Word>
+__device__ uint32_t block_kth_bound(Word word, int n, int k, int sbits, uint32_t *hist, uint64_t *red, QState &st) {
+    __shared__ uint32_t s_red[2 * NWARP];
+    const unsigned FULL = 0xffffffffu;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    uint32_t v[KPT];
+    uint32_t mn = 0xffffffffu, mx = 0u;
+#pragma unroll
+    for (int j = 0; j < KPT; j++) {
+        const int i = tid + j * NT;
+        v[j] = i < n ? word(i) : 0u;
+        if (i < n) {
+            mn = min(mn, v[j]);
+            mx = max(mx, v[j]);
+        }
+    }
+    mn = __reduce_min_sync(FULL, mn);
+    mx = __reduce_max_sync(FULL, mx);
+    __syncthreads();  // the previous call's readers of s_red are done
+    if (lane == 0) {
+        s_red[wid] = mn;
+        s_red[NWARP + wid] = mx;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int w2 = 0; w2 < NWARP; w2++) {
+        mn = min(mn, s_red[w2]);
+        mx = max(mx, s_red[NWARP + w2]);
+    }
+    const uint32_t range = mx - mn;
+    int shift = range ? 32 - __clz(range) : 0;  // unresolved low bits of (word - min)
+    uint32_t prefix = 0;                        // resolved high bits of (word - min)
+    uint32_t need = (uint32_t)k;
+    while (shift > sbits) {
+        const int db = shift < KBITS ? shift : KBITS, hs = shift;
+        shift -= db;
+        const uint32_t nbins = 1u << db;
+        for (uint32_t b = (uint32_t)tid; b < nbins; b += NT) hist[b] = 0u;
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < KPT; j++) {
+            const uint32_t rel = v[j] - mn;
+            const bool in = tid + j * NT < n && (hs >= 32 || (rel >> hs) == (prefix >> hs));
+            if (in) atomicAdd(&hist[(rel >> shift) & (nbins - 1u)], 1u);
+        }
+        __syncthreads();
+        // the bin holding the need-th word: bins split evenly over the threads
+        constexpr int PB = (1 << KBITS) / NT;
+        const uint32_t b0 = (uint32_t)tid * PB;
+        uint32_t c[PB], mine = 0;
+#pragma unroll
+        for (int i = 0; i < PB; i++) {
+            c[i] = b0 + i < nbins ? hist[b0 + i] : 0u;
+            mine += c[i];
+        }
+        uint64_t tot;
+        uint32_t run = (uint32_t)block_exscan(mine, red, tot);
+#pragma unroll
+        for (int i = 0; i < PB; i++) {
+            if (run < need && run + c[i] >= need) {
+                st.s_bin = b0 + (uint32_t)i;
+                st.s_acc = run;
+            }
+            run += c[i];
+        }
+        __syncthreads();
+        prefix |= st.s_bin << shift;
+        need -= (uint32_t)st.s_acc;
+        __syncthreads();
+    }
+    const uint64_t b = (uint64_t)mn + prefix + ((1ull << shift) - 1ull);
+    return b < (uint64_t)mx ? (uint32_t)b : mx;
+}
+
 // The R smallest (distance, id) keys of nb pending entries by one bitonic
 // sort in top[] (room for WARMN keys, nb <= WARMN), in order; pid != null
 // turns the entries' CSR positions into ids first.
@@ -708,11 +796,33 @@ __device__ void merge_topk(uint64_t *top, uint64_t *pend, uint64_t *tmp, uint32_
         __syncthreads();
         return;
     }
-    if (na == 0 && nb <= 2 * NT) {
+    if (na == 0 && nb <= NT) {
         // few survivors: one register sort of (distance, id) keys gives the R
         // best in order
         sort_merge(top, pend, nb, R, pid, st);
         return;
+    }
+    if (na == 0 && nb <= NT * MERGE_KPT) {
+        // an upper bound b of the R-th distance (within 2^-15) keeps every
+        // entry of the R best and few others; those are sorted as above
+        auto word = [&](int i) { return (uint32_t)(pend[i] >> 32); };
+        const uint32_t b = nb <= 2 * NT ? block_kth_bound<2>(word, nb, R, 8, hist, red, st)
+                                        : block_kth_bound<MERGE_KPT>(word, nb, R, 8, hist, red, st);
+        uint64_t mine = 0;
+        for (int i = tid; i < nb; i += NT) mine += (uint32_t)(pend[i] >> 32) <= b;
+        uint64_t total;
+        uint64_t pos = block_exscan(mine, red, total);
+        if (total <= (uint64_t)(2 * NT)) {
+            uint64_t *fil = tmp + RMAX;  // past the top and tmp lists, inside the warm-up scores
+            for (int i = tid; i < nb; i += NT) {
+                const uint64_t e = pend[i];
+                if ((uint32_t)(e >> 32) <= b) fil[pos++] = e;
+            }
+            __syncthreads();
+            sort_merge(top, fil, (int)total, R, pid, st);
+            return;
+        }
+        // many entries within 2^-15 of the R-th distance: the radix select below
     }
     // radix select of the R-th smallest distance word
     uint64_t need;
@@ -1174,13 +1284,14 @@ __device__ __forceinline__ void scan_cells(const SearchArgs &a, const Smem &S, Q
         const uint32_t cnext = (ci + 1 < wci + wcn) ? W[ci - wci + 1].pre : whi;
         const uint32_t cend = min(cnext, hi);
         const float d0 = cw.d0;
-        for (uint32_t g = f; g < cend; g += WCH) {
+        // one chunk of 32 * U candidates from g; FULLC: all inside the cell
+        auto chunk = [&](uint32_t g, auto fullc) {
+            constexpr bool FULLC = decltype(fullc)::value;
             const uint32_t ff0 = g + lane;
             const uint32_t p0 = cw.start + (ff0 - cw.pre);
             CodeWords<MPC> cwd[U];
             float dist[U];
-            const bool full = g + WCH <= cend;
-            if (full) {
+            if constexpr (FULLC) {
                 const uint8_t *cp = a.codes + (size_t)p0 * MPC;
                 const float *vp = a.vterm + p0;
 #pragma unroll
@@ -1198,50 +1309,47 @@ __device__ __forceinline__ void scan_cells(const SearchArgs &a, const Smem &S, Q
                     dist[u] = __ldg(a.vterm + pu);
                 }
             }
-            bool act[U];
+            uint32_t pm = 0;  // bit u: this lane's u-th candidate is at or below tau
 #pragma unroll
             for (int u = 0; u < U; u++) {
-                act[u] = full || ff0 + 32u * u < cend;
+                const bool act = FULLC || ff0 + 32u * u < cend;
                 dist[u] = __fadd_rn(__fadd_rn(d0, dist[u]), rot_lut_sum<MPC>(cwd[u].w, roff, bsel, xl, lut_s, lane));
+                if constexpr (WARM) {
+                    if (act) warm[ff0 + 32u * u] = ((uint64_t)f2o(dist[u]) << 32) | (p0 + 32u * u);
+                } else {
+                    pm |= (act && dist[u] <= tauf ? 1u : 0u) << u;
+                }
             }
-            if constexpr (WARM) {
-#pragma unroll
-                for (int u = 0; u < U; u++)
-                    if (act[u]) warm[ff0 + 32u * u] = ((uint64_t)f2o(dist[u]) << 32) | (p0 + 32u * u);
-            } else {
-                bool anyp = false;
-#pragma unroll
-                for (int u = 0; u < U; u++) anyp |= act[u] && dist[u] <= tauf;
-                if (__any_sync(FULL, anyp)) {
+            if constexpr (!WARM) {
+                if (__any_sync(FULL, pm != 0u)) {
+                    // the chunk's survivors: one atomic for the warp, slots
+                    // in (u, lane) order
+                    unsigned m[U];
+                    uint32_t tot = 0;
 #pragma unroll
                     for (int u = 0; u < U; u++) {
-                        const bool pass = act[u] && dist[u] <= tauf;
-                        const unsigned m = __ballot_sync(FULL, pass);
-                        if (m) {
-                            uint32_t slot0 = 0;
-                            if (lane == __ffs(m) - 1) slot0 = atomicAdd((unsigned *)&st.npend, (unsigned)__popc(m));
-                            slot0 = __shfl_sync(FULL, slot0, __ffs(m) - 1);
-                            const uint32_t slot = slot0 + __popc(m & ((1u << lane) - 1));
-                            if (pass && slot < cap) out[slot] = ((uint64_t)f2o(dist[u]) << 32) | (p0 + 32u * u);
-                        }
+                        m[u] = __ballot_sync(FULL, (pm >> u) & 1u);
+                        tot += (uint32_t)__popc(m[u]);
+                    }
+                    uint32_t base = 0;
+                    if (lane == 0) base = atomicAdd((unsigned *)&st.npend, tot);
+                    base = __shfl_sync(FULL, base, 0);
+                    const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+                    for (int u = 0; u < U; u++) {
+                        const uint32_t slot = base + (uint32_t)__popc(m[u] & lt);
+                        if (((pm >> u) & 1u) && slot < cap) out[slot] = ((uint64_t)f2o(dist[u]) << 32) | (p0 + 32u * u);
+                        base += (uint32_t)__popc(m[u]);
                     }
                 }
             }
-        }
+        };
+        uint32_t g = f;
+        for (; g + WCH <= cend; g += WCH) chunk(g, std::true_type{});
+        if (g < cend) chunk(g, std::false_type{});
         f = cend;
         ci++;
     }
-}
-
-// An upper bound of the k-th smallest (1-based) high word of keys[0..n) in
-// shared memory: the word's top 24 bits by three radix passes, all low bits
-// set (at most 2^-15 relative above the k-th distance).  The scan's
-// threshold only has to bound the final R-th distance from above.
-__device__ uint32_t block_kth_hi_bound(const uint64_t *keys, int n, int k, uint32_t *hist, uint64_t *red,
-                                       QState &st) {
-    uint64_t need;
-    return radix_kth_word([&](int i) { return (uint32_t)(keys[i] >> 32); }, n, (uint64_t)k, hist, red, st, need, 3) |
-           0xffu;
 }
 
 // Resident CTAs per SM the register allocation is sized for.
@@ -1317,11 +1425,33 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
                 // the exact-distance scan keeps the query instead of a LUT
                 for (int i = tid; i < a.raw_dim; i += NT) S.lut[i] = a.Q[(size_t)q * a.raw_dim + i];
             } else if (a.rot) {
-                // rotated LUT: word c * 32 + b holds table (b mod mp) at code
-                // c, so bank b serves table b mod mp (32 / mp copies)
+                // bank-private LUT: word c * 32 + b holds table (b mod mp) at
+                // code c, so bank b serves table b mod mp (32 / mp copies)
+                if constexpr (MPC == 8 || MPC == 16 || MPC == 32) {
+                    // every entry loaded once (entry e = tid + NT j: table
+                    // e mod MPC, code e / MPC), all loads in flight together,
+                    // then its copies stored; copy r goes to bank k + MPC r',
+                    // r' = (r + code) mod (32 / MPC), so that the 32 stores of
+                    // a warp hit 32 different banks
+                    constexpr int NC = 32 / MPC;
+                    float vals[MPC];
+#pragma unroll
+                    for (int j = 0; j < MPC; j++) {
+                        const int e = tid + NT * j;
+                        vals[j] = __ldg(src + (size_t)(e & (MPC - 1)) * 256 + (e / MPC));
+                    }
+#pragma unroll
+                    for (int j = 0; j < MPC; j++) {
+                        const int e = tid + NT * j;
+                        const int k = e & (MPC - 1), cc = e / MPC;
+#pragma unroll
+                        for (int r = 0; r < NC; r++) S.lut[cc * 32 + k + MPC * ((r + cc) & (NC - 1))] = vals[j];
+                    }
+                } else {
 #pragma unroll 8
-                for (int wd = tid; wd < ROT_LUT_BYTES / 4; wd += NT)
-                    S.lut[wd] = __ldg(src + (size_t)(wd & (mp - 1)) * 256 + (wd >> 5));
+                    for (int wd = tid; wd < ROT_LUT_BYTES / 4; wd += NT)
+                        S.lut[wd] = __ldg(src + (size_t)(wd & (mp - 1)) * 256 + (wd >> 5));
+                }
             } else {
                 for (int i = tid; i < mp * kp; i += NT) S.lut[i] = src[i];
             }
@@ -1451,25 +1581,32 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
             if (!done_a) bitonic_sort64(S.LA, kcP);
             if (imi && !done_b) bitonic_sort64(S.LB, kcP);
             __syncthreads();
+            // ranks 0..lim-1 of each sorted list take part: the rank limit M
+            // of search_multi2 / search_mr_ivf / search_mr_ivf3 confines the
+            // walk to the top-M grid (kc: the whole grid; IVFADC has none)
+            const int lim = (!ivf && a.rank_limit > 0 && a.rank_limit < kc) ? a.rank_limit : kc;
+            const int kB0 = scx ? st.kA : st.kB;
             L.LA = S.LA;
             L.LB = S.LB;
-            L.kA = st.kA;
-            L.kB = scx ? st.kA : st.kB;
+            L.kA = min(st.kA, lim);
+            L.kB = ivf ? kB0 : min(kB0, lim);
             L.kc = kc;
             L.ivf = ivf;
-            const uint32_t nextB = sc ? st.nextA : st.nextB;
+            // smallest keys left outside the prefixes, within the rank limit
+            const uint32_t nextA = st.kA >= lim ? 0xffffffffu : st.nextA;
+            const uint32_t nextB = (ivf || kB0 >= lim) ? 0xffffffffu : (sc ? st.nextA : st.nextB);
             // every cell outside the prefix grid has a key >= bound
             uint32_t bound = 0xffffffffu;
             if (sc3) {
-                if (st.nextA != 0xffffffffu) {
-                    const float nx = o2f(st.nextA), a0 = L.a(0);
+                if (nextA != 0xffffffffu) {
+                    const float nx = o2f(nextA), a0 = L.a(0);
                     bound = min(f2o(__fadd_rn(__fadd_rn(nx, a0), a0)), f2o(__fadd_rn(__fadd_rn(a0, a0), nx)));
                 }
             } else {
-                if (st.nextA != 0xffffffffu) bound = min(bound, f2o(__fadd_rn(o2f(st.nextA), L.b(0))));
-                if (!ivf && nextB != 0xffffffffu) bound = min(bound, f2o(__fadd_rn(L.a(0), o2f(nextB))));
+                if (nextA != 0xffffffffu) bound = min(bound, f2o(__fadd_rn(o2f(nextA), L.b(0))));
+                if (nextB != 0xffffffffu) bound = min(bound, f2o(__fadd_rn(L.a(0), o2f(nextB))));
             }
-            const bool whole = L.kA == kc && (ivf || L.kB == kc);
+            const bool whole = L.kA == lim && (ivf || L.kB == lim);
             PHASE_MARK(0);  // lists
 
             // (2) rounds of staircase enumeration over the prefix grid
@@ -1538,6 +1675,7 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
                         it++;
                     }
                     const uint32_t tau = hi;
+                    PHASE_MARK(14);  // the round's bisection for tau
                     tau_prev = tau;  // the next round's bisection starts above tau
                     if (round == 0 && tid == 0) {
                         st.tau_gap = tau - lo_key;
@@ -1664,6 +1802,7 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
                     __syncthreads();
                     uint64_t wcnt = scx ? NEc : Ncell;
                     trig = (Ssum >= needT) || (wcnt >= needW);
+                    PHASE_MARK(1);  // the round's enumeration
                     if (trig || Ncell >= total_cells || tau >= hi_key) break;
                     // next target from the density seen so far
                     double dens = Ncell ? (double)Ssum / (double)Ncell : avg_density;
@@ -1690,7 +1829,64 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
             PHASE_MARK(1);  // staircase rounds
 
             // (3) the cut within the last round
-            if (!nothing && !qerr && trig) {
+            bool cut_done = false;
+            const int nr = nrec - r0;
+            if (!nothing && !qerr && trig && nr > 0 && nr <= 2 * NT && (!sc3 || L.kA <= NT)) {
+                // few records: sort them by (key, rank) and scan the running
+                // totals.  The enumeration wrote a round's records in rank
+                // order, so (key << 32 | index) sorts them by (key, rank).
+                uint64_t *sk = reinterpret_cast<uint64_t *>(hist);  // 2 NT keys inside the bins
+                const int n2 = next_pow2(nr);
+                for (int i = tid; i < n2; i += NT)
+                    sk[i] = i < nr ? ((uint64_t)rec_key[r0 + i] << 32) | (uint32_t)i : ~0ull;
+                if (tid == 0) st.s_bin = 0xffffffffu;
+                __syncthreads();
+                bitonic_sort64(sk, n2);
+                // thread t: sorted positions 2t and 2t + 1; candidates in
+                // bits 0..39 of the scan, non-empty cells in bits 40..63
+                uint64_t cT[2] = {0, 0}, cN[2] = {0, 0};
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const int pz = 2 * tid + j;
+                    if (pz < nr) {
+                        const uint32_t c = rec_cnt[r0 + (uint32_t)sk[pz]];
+                        cT[j] = c;
+                        cN[j] = c > 0 ? 1u : 0u;
+                    }
+                }
+                const uint64_t M40 = (1ull << 40) - 1;
+                uint64_t tot;
+                const uint64_t ex = block_exscan((cT[0] + cT[1]) | ((cN[0] + cN[1]) << 40), red, tot);
+                uint64_t accT = S0 + (ex & M40), accN = NE0 + (ex >> 40);
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const int pz = 2 * tid + j;
+                    if (pz < nr) {
+                        const uint64_t nT = accT + cT[j], nN = accN + cN[j];
+                        // the w rule counts non-empty cells (SC) or every cell
+                        const uint64_t wb = scx ? accN : N0 + (uint64_t)pz, wa = scx ? nN : N0 + (uint64_t)pz + 1;
+                        const bool before = accT >= needT || wb >= needW, after = nT >= needT || wa >= needW;
+                        if (after && !before) {
+                            // the first record at which a rule fires: the cut
+                            const uint32_t idx = (uint32_t)sk[pz];
+                            st.kappa = (uint32_t)(sk[pz] >> 32);
+                            st.rank_cut = rec_rank[r0 + idx];
+                            st.take_all = 0;
+                            st.sumv = nT;
+                            st.nv = N0 + (uint64_t)pz + 1;
+                            st.nev = nN;
+                            st.s_bin = (uint32_t)pz;
+                        }
+                        accT = nT;
+                        accN = nN;
+                    }
+                }
+                __syncthreads();
+                cut_done = st.s_bin != 0xffffffffu;
+                __syncthreads();
+            }
+            if (cut_done) {
+            } else if (!nothing && !qerr && trig) {
                 uint64_t mn = 0xffffffffull, mx = 0;
                 for (int r = r0 + tid; r < nrec; r += NT) {
                     uint64_t k = rec_key[r];
@@ -1911,7 +2107,12 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
             else scan_chunks<MPC, true, U, VAR, ROTOK>(a, S, st, c, 0u, K, 0u, S.warm, nullptr, 0u);
             __syncthreads();
             uint32_t tau = 0xffffffffu;
-            if (K > (uint32_t)R) tau = block_kth_hi_bound(S.warm, (int)K, R, S.hist2, red, st);
+            // an upper bound of the R-th warm-up distance (within 2^-15)
+            if (K > (uint32_t)R) {
+                const uint64_t *wk = S.warm;
+                tau = block_kth_bound<WARMN / NT>([&](int i) { return (uint32_t)(wk[i] >> 32); }, (int)K, R, 8,
+                                                  S.hist2, red, st);
+            }
             // the warm entries at or below tau open the pending buffer
             {
                 uint64_t mine = 0;

@@ -34,7 +34,7 @@ EXPORTS = ["scg_last_error", "scg_index_create", "scg_index_destroy", "scg_load_
            "scg_server_destroy", "scg_autotune", "scg_set_scan_tuning",
            "scg_set_kernel_split", "scg_server_wait_times", "scg_set_encoder",
            "scg_train_codebooks", "scg_build_index", "scg_write_edat", "scg_search_graph",
-           "scg_kmeans", "scg_exact_nn"]
+           "scg_kmeans", "scg_exact_nn", "scg_set_rank_limit"]
 
 
 def train_codebooks_device(dX_ptr, n, dim, mc, kc, mp, kp, iters, seed, d_cq, d_pq, device=0, stream=None):
@@ -242,6 +242,10 @@ class Index:
     def set_query_targets(self, d_T_ptr):
         _check(_lib.scg_set_query_targets(self._h, ctypes.c_void_p(d_T_ptr) if d_T_ptr else None))
 
+    def set_rank_limit(self, M):
+        """Walk only ranks 0..M-1 of each sorted coarse list (0: all)."""
+        _check(_lib.scg_set_rank_limit(self._h, int(M)))
+
     def last_query_stats(self, nq):
         nvis = np.empty(nq, np.int32)
         empty = np.empty(nq, np.int32)
@@ -255,7 +259,7 @@ class Index:
         out = np.zeros(16, np.int64)
         _check(_lib.scg_last_phase_counters(self._h, _ptr(out), 16))
         names = ["sort", "rounds", "cut", "compact", "scan", "final_merge", "pending", "merges", "round_count",
-                 "bisection_steps", "enumerated_cells", "full_sorts", "lut_fill", "warm_threshold"]
+                 "bisection_steps", "enumerated_cells", "full_sorts", "lut_fill", "warm_threshold", "bisection"]
         return {n: int(v) for n, v in zip(names, out) if n != "-"}
 
     def last_timings(self):

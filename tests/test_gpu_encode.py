@@ -88,3 +88,28 @@ def test_tensor_encoder_is_exact(oracle_mod, kind, D, mc, kc, mp, kp):
     m = min(n, 600)
     ocid, ocodes = O.encode((D, mc, kc, mp, kp), cq, pq, X[:m])
     assert np.array_equal(cid_t[:m], ocid) and np.array_equal(codes_t[:m], ocodes)
+
+
+@pytest.mark.parametrize("kind,D,kc,mp,kp,nc", [("u8", 64, 256, 8, 256, 2), ("u8", 128, 300, 8, 256, 3),
+                                                ("unit01", 960, 64, 32, 256, 2), ("ties", 32, 64, 4, 16, 2),
+                                                ("ties", 32, 64, 4, 16, 3)])
+def test_tensor_sc_encoder_is_exact(oracle_mod, kind, D, kc, mp, kp, nc):
+    """The second-candidate encoder on the tensor cores (nc nearest coarse
+    centroids from the candidates within the tables' margin of the nc-th
+    smallest, float-rounded comparisons) gives the reference's codes:
+    identical to the double-precision kernel and to the oracle, including
+    exact ties (equal distances by centroid id) and D = 960."""
+    import scgpu
+    n = 6000 if D < 960 else 1500
+    X, cq, pq = _enc_case(kind, D, 1, kc, mp, kp, n, 23 + D + nc)
+    g = scgpu.Index(0)
+    g.load_codebooks(cq, kc, 1, pq, kp, mp, D)
+    g.set_encoder(scgpu.ENC_TENSOR)
+    cid_t, codes_t = g.sc_encode(X, nc)
+    g.set_encoder(scgpu.ENC_EXACT)
+    cid_e, codes_e = g.sc_encode(X, nc)
+    g.close()
+    assert np.array_equal(cid_t, cid_e) and np.array_equal(codes_t, codes_e)
+    m = min(n, 600)
+    ocid, ocodes = O.sc_encode(D, kc, mp, kp, nc, cq, pq, X[:m])
+    assert np.array_equal(cid_t[:m], ocid) and np.array_equal(codes_t[:m], ocodes)

@@ -29,9 +29,9 @@ def gpu_index(scgpu, D, mc, kc, mp, kp, cq, pq, L, pid, codes):
     return g
 
 
-def check_against_oracle(ix, g, mode, Q, R, w, T):
+def check_against_oracle(ix, g, mode, Q, R, w, T, rank_limit=0):
     ids, d, sums = g.search(MODES[mode], Q, R, w, T)
-    oi, od, osum = ix.search(mode, Q, R, w, T, order=O.ORDER_EXACT)
+    oi, od, osum = ix.search(mode, Q, R, w, T, order=O.ORDER_EXACT, rank_limit=rank_limit)
     assert np.array_equal(sums, osum), (sums, osum)
     assert np.array_equal(d, od)
     assert np.array_equal(ids, oi)
@@ -451,4 +451,40 @@ def test_d960_m32_fp16_rerank(scg, oracle_mod):
         for j, x in enumerate(ids[i].tolist()):
             if x in dd:
                 assert d[i, j] == np.float32(dd[x])
+    g.close()
+
+
+@pytest.mark.parametrize("mode,mc,kc,Ms,Ts", [(O.IMI, 2, 48, (12, 24), (300, 5000, 10 ** 6)),
+                                              (O.SC, 1, 48, (12, 24), (300, 5000, 10 ** 6)),
+                                              (O.SC3, 1, 20, (5, 10), (300, 5000, 10 ** 6)),
+                                              (O.IMI, 2, 512, (64, 200, 300), (300, 5000))])
+def test_rank_limit_against_oracle(scg, oracle_mod, mode, mc, kc, Ms, Ts):
+    """The rank limit M (the M argument of search_multi2 / search_mr_ivf /
+    search_mr_ivf3): the walk over ranks 0..M-1 of each sorted list equals
+    the oracle's confined exact order, in the split and the fused kernels,
+    including targets that exhaust the M x M grid, and M beyond the sorted
+    prefix of a kc = 512 index."""
+    D, mp, kp = 64, 8, 64
+    mix = W.Mixture(D, 16, 20.0, "u8", seed=61 + mode + kc)
+    X = mix.sample(40000, seed=62)
+    Q = mix.sample(24, seed=63)
+    cq, pq = W.train_codebooks(X[:5000], mc, kc, mp, kp, 2, seed=64)
+    if mode in (O.SC, O.SC3):
+        nc = 2 if mode == O.SC else 3
+        cid, codes = O.sc_encode(D, kc, mp, kp, nc, cq, pq, X)
+        L, pid, co, _ = O.distribution(O.SC, kc, 1, nc, cid, codes)
+    else:
+        cid, codes = O.encode((D, mc, kc, mp, kp), cq, pq, X)
+        L, pid, co, _ = O.distribution(mode, kc, mc, 0, cid, codes)
+    ix = O.Index(D, mc, kc, mp, kp, cq, pq, L, pid, co)
+    g = gpu_index(scg, D, mc, kc, mp, kp, cq, pq, L, pid, co)
+    for split in (1, 0):
+        g.set_kernel_split(split)
+        for M in Ms:
+            g.set_rank_limit(M)
+            for T in Ts:
+                check_against_oracle(ix, g, mode, Q, 50, 1 << 20, T, rank_limit=M)
+    # the limit is per index and lasts until reset
+    g.set_rank_limit(0)
+    check_against_oracle(ix, g, mode, Q, 50, 1 << 20, 5000)
     g.close()

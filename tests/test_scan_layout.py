@@ -79,3 +79,4 @@ def test_permute_words_is_xor_of_the_index():
     words = list(range(8))
     for xw in range(8):
         assert permute_words(words, xw) == [i ^ xw for i in range(8)]
+
