@@ -513,10 +513,15 @@ def run_workload(args, name, scgpu, dev, world, full=True):
         for pv in (prec, 0):
             ix.set_scan_tuning(pv, args.upl)
         tuning = {"fixed_candidates_per_lane": args.upl}
-    for tname, pv in ((("fast", prec), ("fp32", 0)) if not (args.no_autotune or args.upl) else ()):
+    if not (args.no_autotune or args.upl):
+        # the main form: candidates per lane, coarse-prefix length, kernel
+        # organisation (and the shortlist length with a re-rank); then the
+        # exact form's candidates per lane
+        tuning["main"] = ix.autotune_ex(mode, dQ.data_ptr(), nq, R, wcap, T, d_ids.data_ptr(), d_d.data_ptr(),
+                                        d_s.data_ptr(), precision=prec, rerank=rerank)
         choice, ms = ix.autotune(mode, dQ.data_ptr(), nq, R, wcap, T, d_ids.data_ptr(), d_d.data_ptr(),
-                                 d_s.data_ptr(), precision=pv, rerank=rerank)
-        tuning[tname] = {"candidates_per_lane": choice, "ms_by_choice": dict(zip((2, 4, 8), ms))}
+                                 d_s.data_ptr(), precision=0, rerank=rerank)
+        tuning["fp32"] = {"candidates_per_lane": choice, "ms_by_choice": dict(zip((2, 4, 8), ms))}
 
     d_T = None
     if Ts is not None:
@@ -636,10 +641,10 @@ def run_workload(args, name, scgpu, dev, world, full=True):
         ix.set_phase_counters(True)
         step()
         ph = ix.last_phase_counters()
-        ph["per_query_cycles"] = {k: ph[k] / nq for k in ("sort", "bisection", "rounds", "cut", "compact", "lut_fill",
-                                                          "warm_threshold", "scan", "final_merge")}
-        ph["per_query"] = {k: ph[k] / nq for k in ("pending", "round_count", "bisection_steps", "enumerated_cells",
-                                                   "full_sorts")}
+        ph["per_query_cycles"] = {k: ph[k] / nq for k in ("select_warp", "sort", "bisection", "rounds", "cut", "compact",
+                                                          "lut_fill", "warm_threshold", "scan", "final_merge")}
+        ph["per_query"] = {k: ph[k] / nq for k in ("pending", "deferred", "round_count", "bisection_steps",
+                                                   "enumerated_cells", "full_sorts")}
         ix.set_phase_counters(False)
         out["phases"] = ph
 

@@ -174,6 +174,36 @@ int scg_query_tables_device(scg_index *h, int precision, const float *dQ, int nq
 int scg_autotune(scg_index *h, const scg_search_params *p, const float *dQ, int nq, int *d_ids,
                  float *d_dists, int *d_sums, int *choice, float *ms);
 
+/* Record of scg_autotune_ex: each knob's candidates with their best device
+ * time (ms, tables + selection + scan + re-rank of the batch) and the pick. */
+typedef struct {
+    int upl;                   /* scan candidates per lane: 2, 4 or 8          */
+    float upl_ms[3];
+    int prefix;                /* sorted coarse-prefix length: 0 (the density
+                                  rule), 128, 256 or 512                       */
+    float prefix_ms[4];
+    int split;                 /* 1: selection and scan as two kernels,
+                                  0: one fused kernel                          */
+    float split_ms[2];         /* [0] split, [1] fused                         */
+    int shortlist;             /* rerank > 0: the shortlist length to use (the
+                                  fastest tried whose top-R ids equal those of
+                                  p->rerank on >= min_agree of the queries)    */
+    int shortlist_L[5];        /* lengths tried: R, 2R, 4R, ... <= 1024        */
+    float shortlist_ms[5];
+    float shortlist_agree[5];  /* share of queries with the same top-R ids     */
+} scg_tune_record;
+
+/* Wider autotuner: on the given device batch, times the scan's candidates
+ * per lane, the sorted coarse-prefix length and the kernel organisation in
+ * turn and keeps the fastest of each for this index (the results of a
+ * search do not depend on any of them); with p->rerank > 0 it also times
+ * shortlists of R, 2R, 4R, ... <= 1024 candidates and reports the fastest one
+ * that keeps the top-R ids of p->rerank on >= min_agree of the queries
+ * (advice: the caller sets rerank).  Outputs are written as by
+ * scg_search_device.  No counterpart in the reference. */
+int scg_autotune_ex(scg_index *h, const scg_search_params *p, const float *dQ, int nq, int *d_ids,
+                    float *d_dists, int *d_sums, float min_agree, scg_tune_record *rec);
+
 /* Sets the scan's candidates per lane (2, 4 or 8) for the scan form of
  * `precision` without timing. */
 int scg_set_scan_tuning(scg_index *h, int precision, int upl);
@@ -299,10 +329,12 @@ int scg_cell_counts(scg_index *h, int *L, int64_t ncells);
  * counts of the search kernels (thread 0 of every CTA, summed over queries):
  * [0] coarse-list sort, [1] staircase rounds' enumeration, [2] cut,
  * [3] compaction, [4] scan rounds, [5] final merge, [6] scan survivors,
- * [7] merges, [8] rounds, [9] bisection steps, [10] enumerated cells,
- * [11] complete sorts, [14] the rounds' bisections, and in the scan-only
+ * [7] queries the warp-wide selection deferred, [8] rounds, [9] bisection steps, [10] enumerated cells,
+ * [11] complete sorts, [14] the rounds' bisections, in the scan-only
  * kernel [12] the LUT (or query) staging and [13] the warm-up scores and
- * threshold.  n is the capacity of out (<= 16). */
+ * threshold, and [15] the warp-wide selection (per query, every phase; the
+ * block-wide counters then cover the queries it deferred).  n is the
+ * capacity of out (<= 16). */
 int scg_set_phase_counters(scg_index *h, int on);
 int scg_last_phase_counters(scg_index *h, long long *out, int n);
 

@@ -358,6 +358,10 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
         if ((rc = ws->pool_cell.ensure(4 * (size_t)(stride * nq + over)))) return rc;
         if ((rc = ws->pool_pre.ensure(4 * (size_t)(stride * nq + over)))) return rc;
     }
+    // the selection of the split search: one warp per query where it serves
+    // the shape, the block-wide kernel for the rest (and every other shape)
+    const bool warp_sel = split && b.slist && select_warp_serves(p->mode, h->kc);
+    if (warp_sel && (rc = ws->defer.ensure(sizeof(int) * ((size_t)nq + 1)))) return rc;
     // survivors of the scan's threshold, per resident CTA
     const size_t pcap = slot > 65536 ? slot : 65536;
     if ((rc = ws->pend.ensure(8 * pcap * g_pend))) return rc;
@@ -386,6 +390,7 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
         ca.avg_density = (double)h->N / (double)(h->ncells ? h->ncells : 1);
         ca.dens_acc = h->dens.as<unsigned long long>();
         ca.max_prefix = 1024;
+        ca.fixed_prefix = h->prefix_len;
         ca.width = coarse_sort_width(h->kc);
         ca.out = b.slist;
         ca.meta = b.smeta;
@@ -441,9 +446,18 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     }
     if (nq > 0) {
         if (split) {
-            // two persistent launches, each with its own query counter
+            // persistent launches, each with its own query counter
+            if (warp_sel) {
+                SCG_CUDA(cudaMemsetAsync(ws->defer.p, 0, sizeof(int), s));
+                sa.qcounter = ws->counter.as<int>() + 3;
+                const int gw = h->num_sms * std::max(1, select_warp_blocks_per_sm());
+                if (select_warp_launch(sa, ws->defer.as<int>(), std::max(1, std::min(gw, (nq + 3) / 4)), s))
+                    return fail(SCG_ERR_CUDA, "warp-wide selection launch failed");
+                sa.qlist = ws->defer.as<int>();
+            }
             sa.qcounter = ws->counter.as<int>();
             if ((rc = search_launch(sa, 1, g_sel, s))) return rc;
+            sa.qlist = nullptr;
             SCG_CUDA(cudaEventRecord(ws->ev[4], s));
             sa.qcounter = ws->counter.as<int>() + 1;
             if ((rc = search_launch(sa, 2, g_scan, s))) return rc;
@@ -823,7 +837,7 @@ int scg_search_graph(scg_index *h, const scg_search_params *p, const float *dQ, 
     snprintf(key, sizeof(key), "%d %d %d %d %d %d|%p %d %p %p %p|%p %d %d %d %d %lld %d %d", p->mode, p->R, p->w,
              p->T, p->precision, p->rerank, (const void *)dQ, nq, (void *)d_ids, (void *)d_dists, (void *)d_sums,
              (const void *)h->d_Tq, (int)h->split, h->tuned_upl[0], h->tuned_upl[1], h->cap_rec, (long long)h->N,
-             h->device, h->rank_limit);
+             h->device, h->rank_limit * 4096 + h->prefix_len);
     if (!h->graph_exec || h->graph_key != key || h->graph_stream != s) {
         if (h->graph_exec) {
             cudaGraphExecDestroy(h->graph_exec);
@@ -935,6 +949,116 @@ int scg_autotune(scg_index *h, const scg_search_params *p, const float *dQ, int 
     }
     h->tuned_upl[form] = pick;
     if (choice) *choice = pick;
+    return SCG_OK;
+}
+
+// Best device time (ms) of the selection + scan of `reps` - 1 searches after
+// one warm-up search.
+static int tune_time(scg_index *h, const scg_search_params *p, const float *dQ, int nq, int *d_ids, float *d_dists,
+                     int *d_sums, int reps, float *ms) {
+    float t = 3.4e38f;
+    for (int rep = 0; rep < reps; rep++) {
+        int rc = run_search(h, &h->ws, nullptr, p, dQ, nq, d_ids, d_dists, d_sums, h->stream, true);
+        if (rc) return rc;
+        float a = 0, b = 0;
+        SCG_CUDA(cudaEventElapsedTime(&a, h->ws.ev[0], h->ws.ev[2]));
+        SCG_CUDA(cudaEventElapsedTime(&b, h->ws.ev[2], h->ws.ev[3]));
+        if (rep > 0 && a + b < t) t = a + b;
+    }
+    *ms = t;
+    return SCG_OK;
+}
+
+int scg_autotune_ex(scg_index *h, const scg_search_params *p, const float *dQ, int nq, int *d_ids, float *d_dists,
+                    int *d_sums, float min_agree, scg_tune_record *rec) {
+    int rc;
+    if ((rc = check_ready(h))) return rc;
+    if ((rc = check_params(h, p, nq))) return rc;
+    if (nq < 1 || !dQ || !d_ids || !d_dists || !d_sums || !rec) return fail(SCG_ERR_ARG, "autotune needs a batch and a record");
+    if (!(min_agree >= 0.0f && min_agree <= 1.0f)) return fail(SCG_ERR_ARG, "min_agree must be in [0, 1]");
+    std::lock_guard<std::mutex> g(h->mu);
+    if ((rc = set_device(h))) return rc;
+    memset(rec, 0, sizeof(*rec));
+    const int form = scan_form(p->precision) == SCG_FAST ? 1 : 0;
+    const int saved_upl = h->tuned_upl[form], saved_prefix = h->prefix_len;
+    const bool saved_split = h->split;
+    auto restore = [&]() {
+        h->tuned_upl[form] = saved_upl;
+        h->prefix_len = saved_prefix;
+        h->split = saved_split;
+    };
+    // (1) candidates per lane of the scan
+    const int ucand[3] = {2, 4, 8};
+    float best = 3.4e38f;
+    for (int i = 0; i < 3; i++) {
+        h->tuned_upl[form] = ucand[i];
+        if ((rc = tune_time(h, p, dQ, nq, d_ids, d_dists, d_sums, 3, &rec->upl_ms[i]))) { restore(); return rc; }
+        if (rec->upl_ms[i] < best) {
+            best = rec->upl_ms[i];
+            rec->upl = ucand[i];
+        }
+    }
+    h->tuned_upl[form] = rec->upl;
+    // (2) the sorted coarse-prefix length (0: the density rule); results do
+    // not depend on it, a short prefix only sends queries to a complete sort
+    const int pcand[4] = {0, 128, 256, 512};
+    best = 3.4e38f;
+    for (int i = 0; i < 4; i++) {
+        h->prefix_len = pcand[i];
+        if ((rc = tune_time(h, p, dQ, nq, d_ids, d_dists, d_sums, 3, &rec->prefix_ms[i]))) { restore(); return rc; }
+        if (rec->prefix_ms[i] < best) {
+            best = rec->prefix_ms[i];
+            rec->prefix = pcand[i];
+        }
+    }
+    h->prefix_len = rec->prefix;
+    // (3) kernel organisation: split selection + scan, or the fused kernel
+    best = 3.4e38f;
+    for (int i = 0; i < 2; i++) {
+        h->split = i == 0;
+        if ((rc = tune_time(h, p, dQ, nq, d_ids, d_dists, d_sums, 3, &rec->split_ms[i]))) { restore(); return rc; }
+        if (rec->split_ms[i] < best) {
+            best = rec->split_ms[i];
+            rec->split = i == 0 ? 1 : 0;
+        }
+    }
+    h->split = rec->split != 0;
+    // (4) the re-rank shortlist: the fastest length whose top-R ids agree
+    // with the caller's length on at least min_agree of the queries
+    if (p->rerank > 0) {
+        const int R = p->R;
+        std::vector<int> ref((size_t)nq * R), got((size_t)nq * R);
+        if ((rc = run_search(h, &h->ws, nullptr, p, dQ, nq, d_ids, d_dists, d_sums, h->stream, true))) {
+            restore();
+            return rc;
+        }
+        SCG_CUDA(cudaMemcpy(ref.data(), d_ids, sizeof(int) * ref.size(), cudaMemcpyDeviceToHost));
+        best = 3.4e38f;
+        for (int i = 0, L = R; i < 5 && L <= 1024; i++, L *= 2) {
+            scg_search_params q = *p;
+            q.rerank = L;
+            rec->shortlist_L[i] = L;
+            if ((rc = tune_time(h, &q, dQ, nq, d_ids, d_dists, d_sums, 3, &rec->shortlist_ms[i]))) {
+                restore();
+                return rc;
+            }
+            SCG_CUDA(cudaMemcpy(got.data(), d_ids, sizeof(int) * got.size(), cudaMemcpyDeviceToHost));
+            int same = 0;
+            for (int qi = 0; qi < nq; qi++) {
+                std::vector<int> x(ref.begin() + (size_t)qi * R, ref.begin() + (size_t)(qi + 1) * R);
+                std::vector<int> y(got.begin() + (size_t)qi * R, got.begin() + (size_t)(qi + 1) * R);
+                std::sort(x.begin(), x.end());
+                std::sort(y.begin(), y.end());
+                same += x == y ? 1 : 0;
+            }
+            rec->shortlist_agree[i] = (float)same / (float)nq;
+            if (rec->shortlist_agree[i] >= min_agree && rec->shortlist_ms[i] < best) {
+                best = rec->shortlist_ms[i];
+                rec->shortlist = L;
+            }
+        }
+        if (rec->shortlist == 0) rec->shortlist = p->rerank;
+    }
     return SCG_OK;
 }
 

@@ -117,6 +117,7 @@ __global__ void __launch_bounds__(CS_THREADS) k_coarse_prefix(CoarseArgs a) {
     int M = 1;
     while (M < 4 * (int)sqrt(c0) + 1) M <<= 1;
     if (M < 128) M = 128;
+    if (a.fixed_prefix > 0) M = a.fixed_prefix;  // the autotuner's choice
     if (M > a.max_prefix) M = a.max_prefix;
     uint32_t vm = 0xffffffffu;
     if (M < a.kc) {
@@ -211,6 +212,7 @@ __global__ void __launch_bounds__(256) k_coarse_prefix_block(CoarseArgs a) {
     int M = 1;
     while (M < 4 * (int)sqrt(c0) + 1) M <<= 1;
     if (M < 128) M = 128;
+    if (a.fixed_prefix > 0) M = a.fixed_prefix;  // the autotuner's choice
     if (M > a.max_prefix) M = a.max_prefix;
     auto block_count = [&](uint32_t lim) {
         int cnt = 0;

@@ -42,6 +42,7 @@ struct Workspace {
     DevBuf dqc, dqr, qn, qsum, nvis, empty, status, counter;
     DevBuf rec_key, rec_rank, rec_cnt, vis_cell, vis_pre, pend, phase, sl_ids, sl_d, slist, smeta;
     DevBuf qmeta, pool_cell, pool_pre;  // selection -> scan hand-off of the split kernels
+    DevBuf defer;  // queries the warp-wide selection left to the block-wide one: [0] count, [1..nq]
     int *h_status = nullptr;  // pinned copy of the status word
     // events: before tables, after tables, after selection + scan, after
     // re-rank, between the selection and scan kernels (split launches)
@@ -82,6 +83,7 @@ struct scg_index {
     int cap_rec = 131072;
     const int *d_Tq = nullptr;
     int rank_limit = 0;  // scg_set_rank_limit: walk ranks < M of each coarse list (0: all)
+    int prefix_len = 0;  // sorted coarse-prefix length (0: the density rule; scg_autotune_ex)
     scg::DevBuf cq, pq, norm_c, norm_r, dot_cr, off, pid, codes, raw, vterm;
     // candidates and cells seen by the selection so far (u64 x 2): the
     // coarse prefix length rule uses their ratio instead of N / cells

@@ -119,6 +119,7 @@ struct SearchArgs {
     uint32_t *pool_over;                     // allocation counter of the overflow area
     uint32_t pool_over_cap;
     int *qcounter;                           // dynamic query counter
+    const int *qlist;                        // optional: qlist[0] queries qlist[1..] instead of 0..nq-1
     // outputs
     int *out_ids;
     float *out_d;
@@ -136,6 +137,13 @@ int search_launch(const SearchArgs &a, int part, int grid, cudaStream_t s);
 int search_max_blocks_per_sm(int mode, int kc, int mp, int kp, int upl, int part, int rot, int qdim = 0);
 // Whether searches in `precision` on this shape use the rotated LUT.
 bool search_rot_form(int precision, int mp, int kp);
+// Warp-per-query cell selection (part 1) for IVFADC, IMI and the
+// second-candidate walk with coarse prefixes sorted ahead: whether it serves
+// the shape, its launch (queries it cannot finish are appended to
+// defer[1..], defer[0] counting them) and its resident CTAs per SM.
+bool select_warp_serves(int mode, int kc);
+int select_warp_launch(const SearchArgs &a, int *defer, int grid, cudaStream_t s);
+int select_warp_blocks_per_sm();
 
 struct EncodeArgs {
     int dim, mc, kc, mp, kp, nc;  // nc = 0: IVF/IMI encoder; nc >= 2: SC encoder
@@ -181,6 +189,7 @@ struct CoarseArgs {
     double avg_density;  // N / cells, for the prefix length rule
     const unsigned long long *dens_acc;  // optional: candidates, cells seen so far
     int max_prefix;
+    int fixed_prefix;    // > 0: this prefix length instead of the density rule
     int width;           // stride of a list in out
     uint64_t *out;       // [nq][lists][width] sorted prefix keys
     uint32_t *meta;      // [nq][lists][2]: prefix length, smallest high word after it

@@ -1409,7 +1409,12 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
         st.tau_T = 0;
     }
     for (;;) {
-        if (tid == 0) s_q = atomicAdd(a.qcounter, 1);
+        if (tid == 0) {
+            // a query list (the queries the warp-wide selection deferred):
+            // qlist[0] entries follow it; else the whole batch
+            const int i = atomicAdd(a.qcounter, 1);
+            s_q = a.qlist ? (i < a.qlist[0] ? a.qlist[1 + i] : a.nq) : i;
+        }
         __syncthreads();
         const int q = s_q;
         if (q >= a.nq) break;

@@ -34,7 +34,7 @@ EXPORTS = ["scg_last_error", "scg_index_create", "scg_index_destroy", "scg_load_
            "scg_server_destroy", "scg_autotune", "scg_set_scan_tuning",
            "scg_set_kernel_split", "scg_server_wait_times", "scg_set_encoder",
            "scg_train_codebooks", "scg_build_index", "scg_write_edat", "scg_search_graph",
-           "scg_kmeans", "scg_exact_nn", "scg_set_rank_limit"]
+           "scg_kmeans", "scg_exact_nn", "scg_set_rank_limit", "scg_autotune_ex"]
 
 
 def train_codebooks_device(dX_ptr, n, dim, mc, kc, mp, kp, iters, seed, d_cq, d_pq, device=0, stream=None):
@@ -63,6 +63,15 @@ class ScgError(RuntimeError):
 class SearchParams(ctypes.Structure):
     _fields_ = [("mode", ctypes.c_int), ("R", ctypes.c_int), ("w", ctypes.c_int),
                 ("T", ctypes.c_int), ("precision", ctypes.c_int), ("rerank", ctypes.c_int)]
+
+
+class TuneRecord(ctypes.Structure):
+    """scg_tune_record (include/scg.h)."""
+    _fields_ = [("upl", ctypes.c_int), ("upl_ms", ctypes.c_float * 3),
+                ("prefix", ctypes.c_int), ("prefix_ms", ctypes.c_float * 4),
+                ("split", ctypes.c_int), ("split_ms", ctypes.c_float * 2),
+                ("shortlist", ctypes.c_int), ("shortlist_L", ctypes.c_int * 5),
+                ("shortlist_ms", ctypes.c_float * 5), ("shortlist_agree", ctypes.c_float * 5)]
 
 
 _lib = None
@@ -221,6 +230,25 @@ class Index:
                                  ctypes.c_void_p(d_d), ctypes.c_void_p(d_sums), ctypes.byref(c), _ptr(ms)))
         return c.value, ms.tolist()
 
+    def autotune_ex(self, mode, dQ_ptr, nq, R, w, T, d_ids, d_d, d_sums, precision=FP32_EXACT, rerank=0,
+                    min_agree=0.99):
+        """The wider autotuner (scg_autotune_ex): returns its record as a dict
+        (each knob's candidates, their ms and the pick)."""
+        p = SearchParams(mode, R, w, T, precision, rerank)
+        r = TuneRecord()
+        _check(_lib.scg_autotune_ex(self._h, ctypes.byref(p), ctypes.c_void_p(dQ_ptr), nq, ctypes.c_void_p(d_ids),
+                                    ctypes.c_void_p(d_d), ctypes.c_void_p(d_sums), ctypes.c_float(min_agree),
+                                    ctypes.byref(r)))
+        out = {"candidates_per_lane": {"pick": r.upl, "ms_by_choice": dict(zip((2, 4, 8), list(r.upl_ms)))},
+               "coarse_prefix": {"pick": r.prefix, "ms_by_choice": dict(zip((0, 128, 256, 512), list(r.prefix_ms)))},
+               "kernel_split": {"pick": r.split, "ms_by_choice": {1: r.split_ms[0], 0: r.split_ms[1]}}}
+        if rerank > 0:
+            out["shortlist"] = {"pick": r.shortlist,
+                                "by_length": {int(L): {"ms": float(m), "agree": float(a)}
+                                              for L, m, a in zip(r.shortlist_L, r.shortlist_ms, r.shortlist_agree)
+                                              if L > 0}}
+        return out
+
     def build_index_device(self, dX_ptr, n, nc=0, stream=None):
         """Encodes device rows and loads the CSR built on the device."""
         _check(_lib.scg_build_index(self._h, ctypes.c_void_p(dX_ptr), ctypes.c_int64(n), nc,
@@ -258,8 +286,8 @@ class Index:
     def last_phase_counters(self):
         out = np.zeros(16, np.int64)
         _check(_lib.scg_last_phase_counters(self._h, _ptr(out), 16))
-        names = ["sort", "rounds", "cut", "compact", "scan", "final_merge", "pending", "merges", "round_count",
-                 "bisection_steps", "enumerated_cells", "full_sorts", "lut_fill", "warm_threshold", "bisection"]
+        names = ["sort", "rounds", "cut", "compact", "scan", "final_merge", "pending", "deferred", "round_count",
+                 "bisection_steps", "enumerated_cells", "full_sorts", "lut_fill", "warm_threshold", "bisection", "select_warp"]
         return {n: int(v) for n, v in zip(names, out) if n != "-"}
 
     def last_timings(self):
