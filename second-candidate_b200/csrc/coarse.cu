@@ -93,6 +93,34 @@ __device__ __forceinline__ void sort_out(const uint64_t *buf, uint64_t *dst, int
     for (int r = 0; r < P; r++) dst[r * 32 + lane] = v[r];
 }
 
+// The sorts of 128 and 256 keys out of line: each prefix length runs one
+// of them, and the kernel body stays small in the instruction cache.
+template <int P>
+__device__ __noinline__ void sort_out_far(const uint64_t *buf, uint64_t *dst, int lane) {
+    sort_out<P>(buf, dst, lane);
+}
+
+// Longer prefixes (512 or 1024 keys, rare): a bitonic sort in the warp's
+// shared buffer with few registers, then the copy to dst.
+__device__ __noinline__ void sort_out_smem(uint64_t *buf, uint64_t *dst, int n, int lane) {
+    for (int k = 2; k <= n; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = lane; i < n; i += 32) {
+                const int ixj = i ^ j;
+                if (ixj > i) {
+                    const uint64_t x = buf[i], y = buf[ixj];
+                    if ((x > y) == ((i & k) == 0)) {
+                        buf[i] = y;
+                        buf[ixj] = x;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+    for (int i = lane; i < n; i += 32) dst[i] = buf[i];
+}
+
 template <int P>
 __global__ void __launch_bounds__(CS_THREADS) k_coarse_prefix(CoarseArgs a) {
     __shared__ uint64_t buf[CS_THREADS / 32][CS_CAP];
@@ -104,11 +132,14 @@ __global__ void __launch_bounds__(CS_THREADS) k_coarse_prefix(CoarseArgs a) {
     const int q = list / nlists, part = list - q * nlists;
     const float base = a.imi ? a.qn[2 * q + part] : a.qsum[q];
     const float *row = a.dqc + (size_t)q * a.mc * a.kc + (size_t)part * a.kc;
-    uint64_t v[P];
+    // the high words (ordered keys) only: the centroid id of element
+    // r * 32 + lane is its position; positions past kc hold 0xffffffff,
+    // above every key (the ordered form of any float is below it)
+    uint32_t v[P];
 #pragma unroll
     for (int r = 0; r < P; r++) {
         const int i = r * 32 + lane;
-        v[r] = i < a.kc ? (((uint64_t)f2o(__fadd_rn(base, row[i])) << 32) | (uint32_t)i) : ~0ull;
+        v[r] = i < a.kc ? f2o(__fadd_rn(base, row[i])) : 0xffffffffu;
     }
     // prefix length rule of the fused kernel
     const int T = a.Tq ? a.Tq[q] : a.T;
@@ -119,17 +150,16 @@ __global__ void __launch_bounds__(CS_THREADS) k_coarse_prefix(CoarseArgs a) {
     if (M < 128) M = 128;
     if (a.fixed_prefix > 0) M = a.fixed_prefix;  // the autotuner's choice
     if (M > a.max_prefix) M = a.max_prefix;
-    uint32_t vm = 0xffffffffu;
+    uint32_t vm = 0xfffffffeu;  // every key
     if (M < a.kc) {
-        // vm = the M-th smallest high word (binary search on the value,
-        // between the list's smallest and largest high words)
+        // vm: a high word with exactly M keys at or below it if one exists
+        // (the bisection stops there), else the M-th smallest (ties)
         uint32_t lo = 0xffffffffu, hi = 0;
 #pragma unroll
         for (int r = 0; r < P; r++) {
-            if (v[r] != ~0ull) {
-                const uint32_t hw = (uint32_t)(v[r] >> 32);
-                lo = hw < lo ? hw : lo;
-                hi = hw > hi ? hw : hi;
+            if (r * 32 + lane < a.kc) {
+                lo = v[r] < lo ? v[r] : lo;
+                hi = v[r] > hi ? v[r] : hi;
             }
         }
         lo = __reduce_min_sync(FULL, lo);
@@ -138,9 +168,13 @@ __global__ void __launch_bounds__(CS_THREADS) k_coarse_prefix(CoarseArgs a) {
             const uint32_t mid = lo + ((hi - lo) >> 1);
             int cnt = 0;
 #pragma unroll
-            for (int r = 0; r < P; r++) cnt += (uint32_t)(v[r] >> 32) <= mid;
+            for (int r = 0; r < P; r++) cnt += v[r] <= mid ? 1 : 0;
             cnt = __reduce_add_sync(FULL, cnt);
-            if (cnt >= M) hi = mid;
+            if (cnt == M) {
+                lo = hi = mid;
+                break;
+            }
+            if (cnt > M) hi = mid;
             else lo = mid + 1;
         }
         vm = lo;
@@ -151,11 +185,10 @@ __global__ void __launch_bounds__(CS_THREADS) k_coarse_prefix(CoarseArgs a) {
     uint32_t nxt = 0xffffffffu;
 #pragma unroll
     for (int r = 0; r < P; r++) {
-        const uint32_t hw = (uint32_t)(v[r] >> 32);
-        const bool in = v[r] != ~0ull && hw <= vm;
-        if (!in && v[r] != ~0ull && hw < nxt) nxt = hw;
+        const bool in = v[r] <= vm;
+        if (!in && v[r] < nxt) nxt = v[r];
         const unsigned m = __ballot_sync(FULL, in);
-        if (in) b[c + __popc(m & ((1u << lane) - 1))] = v[r];
+        if (in) b[c + __popc(m & ((1u << lane) - 1))] = ((uint64_t)v[r] << 32) | (uint32_t)(r * 32 + lane);
         c += __popc(m);
     }
     nxt = __reduce_min_sync(FULL, nxt);
@@ -167,10 +200,9 @@ __global__ void __launch_bounds__(CS_THREADS) k_coarse_prefix(CoarseArgs a) {
     switch (c2) {
         case 32: sort_out<1>(b, dst, lane); break;
         case 64: sort_out<2>(b, dst, lane); break;
-        case 128: sort_out<4>(b, dst, lane); break;
-        case 256: sort_out<8>(b, dst, lane); break;
-        case 512: sort_out<16>(b, dst, lane); break;
-        default: sort_out<32>(b, dst, lane); break;
+        case 128: sort_out_far<4>(b, dst, lane); break;
+        case 256: sort_out_far<8>(b, dst, lane); break;
+        default: sort_out_smem(b, dst, c2, lane); break;
     }
     if (lane == 0) {
         a.meta[2 * list] = (uint32_t)c;

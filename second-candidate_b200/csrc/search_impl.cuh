@@ -918,6 +918,34 @@ __device__ __forceinline__ void permute_words(const uint32_t *w, uint32_t *r, ui
     }
 }
 
+// The fast form's table sum of one candidate: a tree over the n entries
+// (pairs (k, k + 1), then (k, k + 2), ...), its two halves summed side by
+// side with packed two-wide adds (add.rn.f32x2: each element an ordinary
+// round-to-nearest add, so the float is the one of scalar adds in the same
+// tree), then one add of the halves.
+template <int N>
+__device__ __forceinline__ float tree_sum(float (&v)[N]) {
+    if constexpr (N < 4) {
+#pragma unroll
+        for (int s2 = 1; s2 < N; s2 <<= 1)
+#pragma unroll
+            for (int k = 0; k + s2 < N; k += 2 * s2) v[k] = __fadd_rn(v[k], v[k + s2]);
+        return v[0];
+    } else {
+        constexpr int H = N / 2;
+        uint64_t p[H];
+#pragma unroll
+        for (int j = 0; j < H; j++) asm("mov.b64 %0, {%1, %2};" : "=l"(p[j]) : "f"(v[j]), "f"(v[j + H]));
+#pragma unroll
+        for (int s2 = 1; s2 < H; s2 <<= 1)
+#pragma unroll
+            for (int k = 0; k + s2 < H; k += 2 * s2) asm("add.rn.f32x2 %0, %0, %1;" : "+l"(p[k]) : "l"(p[k + s2]));
+        float lo, hi;
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(p[0]));
+        return __fadd_rn(lo, hi);
+    }
+}
+
 // One float of shared memory at a 32-bit shared-window address.
 __device__ __forceinline__ float lds_f32(uint32_t addr) {
     float v;
@@ -944,11 +972,7 @@ __device__ __forceinline__ float rot_lut_sum(const uint32_t *w, const uint32_t *
         else ro = lut_s + (((uint32_t)lane - xl + ((uint32_t)s2 ^ xl)) << 2);
         v[s2] = lds_f32(ro + (cb << 7));
     }
-#pragma unroll
-    for (int s2 = 1; s2 < MPC; s2 <<= 1)
-#pragma unroll
-        for (int k = 0; k + s2 < MPC; k += 2 * s2) v[k] = __fadd_rn(v[k], v[k + s2]);
-    return v[0];
+    return tree_sum<MPC>(v);
 }
 
 // Warp-centric ADC scan of the candidates [first, limit), cut into chunks of
@@ -1155,11 +1179,7 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
 #pragma unroll
                                     for (int k = 0; k < MPC; k++) v[k] = S.lut[k * c.kp + cwd[u].code(k)];
                                 }
-#pragma unroll
-                                for (int s2 = 1; s2 < MPC; s2 <<= 1)
-#pragma unroll
-                                    for (int k = 0; k + s2 < MPC; k += 2 * s2) v[k] = __fadd_rn(v[k], v[k + s2]);
-                                d = __fadd_rn(d, v[0]);
+                                d = __fadd_rn(d, tree_sum<MPC>(v));
                             } else {
                                 for (int k = 0; k < cwd[u].n(c.mp); k++)
                                     d = __fadd_rn(d, S.lut[k * c.kp + cwd[u].code(k)]);

@@ -11,10 +11,10 @@ import workloads as W
 pytestmark = pytest.mark.gpu
 
 
-def _index(scgpu, raw=False):
-    D, mc, kc, mp, kp = 64, 2, 64, 8, 256
+def _index(scgpu, raw=False, kc=64):
+    D, mc, mp, kp = 64, 2, 8, 256
     mix = W.Mixture(D, 16, 20.0, "u8", seed=131)
-    X = mix.sample(40000, seed=132)
+    X = mix.sample(40000 if kc <= 64 else 120000, seed=132)
     cq, pq = W.train_codebooks(X[:5000], mc, kc, mp, kp, 3, seed=133)
     cid, codes = O.encode((D, mc, kc, mp, kp), cq, pq, X)
     L, pid, co, _ = O.distribution(O.IMI, kc, mc, 0, cid, codes)
@@ -27,11 +27,13 @@ def _index(scgpu, raw=False):
     return g, mix, D
 
 
-@pytest.mark.parametrize("prec", ["FAST", "FP32_EXACT"])
-def test_autotune_ex_keeps_results_and_reports_every_choice(prec):
+@pytest.mark.parametrize("prec,kc", [("FAST", 64), ("FP32_EXACT", 64), ("FAST", 1024)])
+def test_autotune_ex_keeps_results_and_reports_every_choice(prec, kc):
+    """kc = 1024: the coarse-prefix lengths tried (the density rule, 128,
+    256, 512) are all shorter than the lists."""
     import torch
     import scgpu
-    g, mix, D = _index(scgpu)
+    g, mix, D = _index(scgpu, kc=kc)
     pv = getattr(scgpu, prec)
     nq, R, T = 400, 50, 3000
     Q = mix.sample(nq, seed=140)
