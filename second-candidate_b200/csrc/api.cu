@@ -704,8 +704,11 @@ int scg_search_device(scg_index *h, const scg_search_params *p, const float *dQ,
     return run_search(h, &h->ws, nullptr, p, dQ, nq, d_ids, d_dists, d_sums, s, true);
 }
 
-// Smallest chunk of the host-buffer search with pageable buffers (at most 4
-// chunks per batch).
+// Smallest chunk of the host-buffer search with page-locked and with
+// pageable buffers (at most 4 chunks per batch).
+#ifndef SCG_HOST_CHUNK_PINNED
+#define SCG_HOST_CHUNK_PINNED 2048
+#endif
 #ifndef SCG_HOST_CHUNK_MIN
 #define SCG_HOST_CHUNK_MIN 1024
 #endif
@@ -725,12 +728,12 @@ int scg_search(scg_index *h, const scg_search_params *p, const float *Q, int nq,
     if ((rc = h->sums.ensure(sizeof(int) * (size_t)nq))) return rc;
     if ((rc = h->ws.nvis.ensure(sizeof(int) * (size_t)nq))) return rc;
     if ((rc = h->ws.empty.ensure(sizeof(int) * (size_t)nq))) return rc;
-    // With page-locked caller buffers the batch is one launch sequence on one
-    // stream between its two copies: the copies take about a tenth of the
-    // search, and smaller launches would each leave a tail of idle SMs.  With
-    // pageable buffers (staged copies that block the host) the batch runs in
-    // chunks alternating over two streams, every chunk enqueued before the
-    // first copy-out, so that staging overlaps the search of other chunks.
+    // The batch runs in chunks alternating over two streams (each with its
+    // own workspace), so that one chunk's copies overlap another chunk's
+    // search and the next chunk's kernels fill the tail of the previous
+    // one's.  With page-locked caller buffers every chunk copies its results
+    // out as soon as it is done; with pageable buffers (staged copies that
+    // block the host) every chunk is enqueued before the first copy-out.
     auto pinned = [](const void *ptr) {
         if (!ptr) return true;
         cudaPointerAttributes at;
@@ -742,7 +745,7 @@ int scg_search(scg_index *h, const scg_search_params *p, const float *Q, int nq,
     };
     const bool eager_out = pinned(ids) && pinned(dists) && pinned(sums);
     const bool q_pinned = pinned(Q);
-    const int nch = (eager_out && q_pinned) ? 1 : std::max(1, std::min(4, nq / SCG_HOST_CHUNK_MIN));
+    const int nch = std::max(1, std::min(4, nq / ((eager_out && q_pinned) ? SCG_HOST_CHUNK_PINNED : SCG_HOST_CHUNK_MIN)));
     const int per = (nq + nch - 1) / nch;
     size_t off_b[8];
     size_t total = 0;
