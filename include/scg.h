@@ -328,7 +328,9 @@ int scg_cell_counts(scg_index *h, int *L, int64_t ncells);
 /* Diagnostics: with counters on, each search accumulates per-phase cycle
  * counts of the search kernels (thread 0 of every CTA, summed over queries):
  * [0] coarse-list sort, [1] staircase rounds' enumeration, [2] cut,
- * [3] compaction, [4] scan rounds, [5] final merge, [6] scan survivors,
+ * [3] compaction, [4] scan rounds, [5] final merge inside the scan kernel
+ * (for a query handed to the warp-wide merge kernel: the hand-off only),
+ * [6] scan survivors,
  * [7] queries the warp-wide selection deferred, [8] rounds, [9] bisection steps, [10] enumerated cells,
  * [11] complete sorts, [14] the rounds' bisections, in the scan-only
  * kernel [12] the LUT (or query) staging and [13] the warm-up scores and

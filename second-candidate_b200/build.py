@@ -8,7 +8,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libscgpu.so")
 SOURCES = ["search_u4.cu", "search_u2.cu", "search_u8.cu", "search_sel.cu", "api.cu", "tables.cu", "tables_tc.cu", "search.cu",
-           "encode.cu", "rerank.cu", "server.cu", "coarse.cu", "encode_tc.cu", "train.cu", "build_index.cu", "gt.cu", "select_warp.cu"]
+           "encode.cu", "rerank.cu", "server.cu", "coarse.cu", "encode_tc.cu", "train.cu", "build_index.cu", "gt.cu", "select_warp.cu", "merge_warp.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
          "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]

@@ -37,6 +37,17 @@ int set_device(scg_index *h) {
     return SCG_OK;
 }
 
+// A blocking host-to-device copy ordered before later work on stream s.  A
+// plain cudaMemcpy runs on the legacy stream, which the index's non-blocking
+// streams do not wait for, and from pageable memory it may return before its
+// DMA has landed: a kernel launched next on s could read the buffer's tail
+// before it arrives.
+cudaError_t copy_in(void *dst, const void *src, size_t bytes, cudaStream_t s) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    return e;
+}
+
 bool read_file(const char *path, std::vector<unsigned char> &buf) {
     std::ifstream f(path, std::ios::binary | std::ios::ate);
     if (!f) return false;
@@ -362,6 +373,12 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     // the shape, the block-wide kernel for the rest (and every other shape)
     const bool warp_sel = split && b.slist && select_warp_serves(p->mode, h->kc);
     if (warp_sel && (rc = ws->defer.ensure(sizeof(int) * ((size_t)nq + 1)))) return rc;
+    // the top-R of the split scan: one warp per query in a merge kernel
+    // (outputs in order, R <= 256), else inside the scan kernel
+    const bool warp_merge = split && !rr && R <= 256;
+    if (warp_merge && ((rc = ws->surv.ensure(sizeof(uint64_t) * (size_t)nq * SURV_CAP)) ||
+                       (rc = ws->surv_n.ensure(sizeof(int) * (size_t)nq))))
+        return rc;
     // survivors of the scan's threshold, per resident CTA
     const size_t pcap = slot > 65536 ? slot : 65536;
     if ((rc = ws->pend.ensure(8 * pcap * g_pend))) return rc;
@@ -460,7 +477,16 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
             sa.qlist = nullptr;
             SCG_CUDA(cudaEventRecord(ws->ev[4], s));
             sa.qcounter = ws->counter.as<int>() + 1;
+            if (warp_merge) {
+                sa.surv = ws->surv.as<uint64_t>();
+                sa.surv_n = ws->surv_n.as<int>();
+                sa.surv_cap = SURV_CAP;
+            }
             if ((rc = search_launch(sa, 2, g_scan, s))) return rc;
+            if (warp_merge) {
+                merge_warp_launch(sa.surv, sa.surv_n, SURV_CAP, sa.pid, nq, R, s_ids, s_d, h->num_sms, s);
+                SCG_CUDA(cudaGetLastError());
+            }
         } else if ((rc = search_launch(sa, 0, g_fused, s))) {
             return rc;
         }
@@ -558,8 +584,8 @@ int scg_load_codebooks(scg_index *h, const float *cq, int kc, int mc, const floa
     if ((rc = set_device(h))) return rc;
     if ((rc = h->cq.ensure(sizeof(float) * (size_t)kc * dim))) return rc;
     if ((rc = h->pq.ensure(sizeof(float) * (size_t)kp * dim))) return rc;
-    SCG_CUDA(cudaMemcpy(h->cq.p, cq, sizeof(float) * (size_t)kc * dim, cudaMemcpyHostToDevice));
-    SCG_CUDA(cudaMemcpy(h->pq.p, pq, sizeof(float) * (size_t)kp * dim, cudaMemcpyHostToDevice));
+    SCG_CUDA(copy_in(h->cq.p, cq, sizeof(float) * (size_t)kc * dim, h->stream));
+    SCG_CUDA(copy_in(h->pq.p, pq, sizeof(float) * (size_t)kp * dim, h->stream));
     h->dim = dim; h->mc = mc; h->kc = kc; h->mp = mp; h->kp = kp;
     h->have_codebooks = true;
     h->enc_ready = false;
@@ -603,10 +629,10 @@ int scg_load_csr(scg_index *h, const int *L, const int *pid, const uint8_t *code
     if ((rc = h->off.ensure(sizeof(uint32_t) * off.size()))) return rc;
     if ((rc = h->pid.ensure(sizeof(int) * (size_t)(N ? N : 1)))) return rc;
     if ((rc = h->codes.ensure((size_t)(N ? N : 1) * h->mp))) return rc;
-    SCG_CUDA(cudaMemcpy(h->off.p, off.data(), sizeof(uint32_t) * off.size(), cudaMemcpyHostToDevice));
+    SCG_CUDA(copy_in(h->off.p, off.data(), sizeof(uint32_t) * off.size(), h->stream));
     if (N) {
-        SCG_CUDA(cudaMemcpy(h->pid.p, pid, sizeof(int) * (size_t)N, cudaMemcpyHostToDevice));
-        SCG_CUDA(cudaMemcpy(h->codes.p, codes, (size_t)N * h->mp, cudaMemcpyHostToDevice));
+        SCG_CUDA(copy_in(h->pid.p, pid, sizeof(int) * (size_t)N, h->stream));
+        SCG_CUDA(copy_in(h->codes.p, codes, (size_t)N * h->mp, h->stream));
     }
     h->N = N;
     h->ncells = ncells;
@@ -662,7 +688,7 @@ static int load_raw(scg_index *h, const void *X, int64_t N, size_t elem, bool u8
     if ((rc = set_device(h))) return rc;
     const size_t bytes = elem * (size_t)N * h->dim;
     if ((rc = h->raw.ensure(bytes ? bytes : 16))) return rc;
-    if (bytes) SCG_CUDA(cudaMemcpy(h->raw.p, X, bytes, cudaMemcpyHostToDevice));
+    if (bytes) SCG_CUDA(copy_in(h->raw.p, X, bytes, h->stream));
     h->raw_rows = N;
     h->raw_u8 = u8;
     return SCG_OK;
@@ -1400,7 +1426,7 @@ static int encode_host(scg_index *h, const float *X, int64_t n, int nc, uint16_t
     if ((rc = x.ensure(sizeof(float) * (size_t)n * h->dim))) return rc;
     if ((rc = c.ensure(sizeof(uint16_t) * (size_t)n * ncid))) { x.release(); return rc; }
     if ((rc = k.ensure((size_t)n * h->mp))) { x.release(); c.release(); return rc; }
-    cudaError_t e = cudaMemcpy(x.p, X, sizeof(float) * (size_t)n * h->dim, cudaMemcpyHostToDevice);
+    cudaError_t e = copy_in(x.p, X, sizeof(float) * (size_t)n * h->dim, h->stream);
     if (e == cudaSuccess) {
         rc = scg_encode_device(h, x.as<float>(), n, nc, c.as<uint16_t>(), k.as<uint8_t>(), nullptr);
         if (rc == SCG_OK) {

@@ -43,6 +43,7 @@ struct Workspace {
     DevBuf rec_key, rec_rank, rec_cnt, vis_cell, vis_pre, pend, phase, sl_ids, sl_d, slist, smeta;
     DevBuf qmeta, pool_cell, pool_pre;  // selection -> scan hand-off of the split kernels
     DevBuf defer;  // queries the warp-wide selection left to the block-wide one: [0] count, [1..nq]
+    DevBuf surv, surv_n;  // survivors the scan kernel hands to the merge kernel: [nq][SURV_CAP], [nq]
     int *h_status = nullptr;  // pinned copy of the status word
     // events: before tables, after tables, after selection + scan, after
     // re-rank, between the selection and scan kernels (split launches)

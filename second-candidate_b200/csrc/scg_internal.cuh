@@ -112,6 +112,12 @@ struct SearchArgs {
     int cap_rec;
     uint64_t *pend;                          // [slots][pcap] scan survivors
     uint32_t pcap;
+    // optional hand-off to the merge kernel (scan-only kernel): a query with
+    // at most surv_cap survivors copies them to surv[q] and sets surv_n[q];
+    // surv_n[q] = -1: the scan kernel merged and wrote the outputs itself
+    uint64_t *surv;                          // [nq][surv_cap]
+    int *surv_n;                             // [nq]
+    int surv_cap;
     // selection -> scan hand-off of the split kernels (parts 1 and 2)
     QMeta *qmeta;                            // [nq]
     uint32_t *pool_cell, *pool_pre;          // [nq * pool_stride + pool_over_cap] visited lists
@@ -142,6 +148,11 @@ bool search_rot_form(int precision, int mp, int kp);
 // the shape, its launch (queries it cannot finish are appended to
 // defer[1..], defer[0] counting them) and its resident CTAs per SM.
 bool select_warp_serves(int mode, int kc);
+// Top-R of the survivors handed over by the scan-only kernel, one warp per
+// query (R <= 256, outputs in (distance, id) order).
+constexpr int SURV_CAP = 1024;
+void merge_warp_launch(const uint64_t *surv, const int *surv_n, int cap, const int *pid, int nq, int R,
+                       int *out_ids, float *out_d, int nsm, cudaStream_t s);
 int select_warp_launch(const SearchArgs &a, int *defer, int grid, cudaStream_t s);
 int select_warp_blocks_per_sm();
 

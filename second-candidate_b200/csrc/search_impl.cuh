@@ -364,6 +364,7 @@ struct QState {
     uint64_t thr;
     uint32_t next_flat;  // next unclaimed candidate of the scan (shared claims)
     int top_sorted;      // top[0..ncur) is already in (distance, id) order
+    int handed;          // the survivors went to the merge kernel (no outputs here)
     double dens_est;     // candidates per cell seen by this CTA's last query
     uint32_t tau_gap;    // first-round tau - lowest key of that query (0: none)
     int tau_T;           // and its candidate target
@@ -897,6 +898,10 @@ struct ScanCtx {
     int raw_dim;
     bool raw_u8, raw_vec;
     const float *qv;
+    // survivor slots below scap go to sq (the query's hand-off to the merge
+    // kernel), the others to the pending buffer
+    uint64_t *sq;
+    uint32_t scap;
 };
 
 // The MPC / 4 code words of one candidate with word i moved to i ^ xw (log
@@ -1214,7 +1219,7 @@ __device__ __forceinline__ void scan_chunks(const SearchArgs &a, const Smem &S, 
                         if (lane == __ffs(m) - 1) slot0 = atomicAdd((unsigned *)&st.npend, (unsigned)__popc(m));
                         slot0 = __shfl_sync(FULL, slot0, __ffs(m) - 1);
                         const uint32_t slot = slot0 + __popc(m & ((1u << lane) - 1));
-                        if (pass && slot < cap) out[slot] = ((uint64_t)du << 32) | pos[u];
+                        if (pass && slot < cap) (slot < c.scap ? c.sq : out)[slot] = ((uint64_t)du << 32) | pos[u];
                     }
                 }
             }
@@ -1358,7 +1363,8 @@ __device__ __forceinline__ void scan_cells(const SearchArgs &a, const Smem &S, Q
 #pragma unroll
                     for (int u = 0; u < U; u++) {
                         const uint32_t slot = base + (uint32_t)__popc(m[u] & lt);
-                        if (((pm >> u) & 1u) && slot < cap) out[slot] = ((uint64_t)f2o(dist[u]) << 32) | (p0 + 32u * u);
+                        if (((pm >> u) & 1u) && slot < cap)
+                            (slot < c.scap ? c.sq : out)[slot] = ((uint64_t)f2o(dist[u]) << 32) | (p0 + 32u * u);
                         base += (uint32_t)__popc(m[u]);
                     }
                 }
@@ -2093,7 +2099,10 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
         // scored into shared memory; their R-th smallest distance bounds the
         // final R-th distance from above, so the rest of the scan keeps only
         // candidates at or below it, appended to a per-CTA buffer; one merge
-        // over that buffer (merge_topk) gives the R best.
+        // over that buffer (merge_topk) gives the R best.  The scan-only
+        // kernel with a hand-off buffer (a.surv) writes the first surv_cap
+        // survivors of query q to surv[q] instead and, when they all fit,
+        // leaves the merge to k_merge_warp (surv_n[q] = their count).
         uint64_t *top = S.top, *tmpk = S.tmp;
         uint64_t *pend_g = a.pend + (size_t)blockIdx.x * a.pcap;
         if (tid == 0) {
@@ -2101,6 +2110,7 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
             st.npend = 0;
             st.next_flat = 0;
             st.top_sorted = 0;
+            st.handed = 0;
         }
         __syncthreads();
         if (!qerr2 && nvis > 0) {
@@ -2125,6 +2135,9 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
             c.qv = S.lut;
             c.qs = qs;
             c.dqc = dqc;
+            const bool hand = PART == 2 && a.surv != nullptr;
+            c.sq = hand ? a.surv + (size_t)q * a.surv_cap : nullptr;
+            c.scap = hand ? (uint32_t)a.surv_cap : 0u;
             const uint32_t K = Svis < (uint32_t)WARMN ? Svis : (uint32_t)WARMN;
             constexpr bool ROTOK = PART == 0 || VAR == V_FAST256;
             constexpr bool CELLS = VAR == V_FAST256 && (MPC == 8 || MPC == 16 || MPC == 32);
@@ -2146,7 +2159,10 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
                 uint64_t p = block_exscan(mine, red, tot);
                 for (int i = tid; i < (int)K; i += NT) {
                     uint64_t e = S.warm[i];
-                    if ((uint32_t)(e >> 32) <= tau) pend_g[p++] = e;
+                    if ((uint32_t)(e >> 32) <= tau) {
+                        (p < c.scap ? c.sq : pend_g)[p] = e;
+                        p++;
+                    }
                 }
                 if (tid == 0) {
                     st.npend = (int)tot;
@@ -2165,13 +2181,26 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
                     atomicOr(a.status, ST_CELL_BUDGET);
                 }
                 __syncthreads();
+            } else if (c.scap && (uint32_t)st.npend <= c.scap) {
+                // every survivor is in the query's hand-off slots: the merge
+                // kernel finishes the query
+                COUNT(6, st.npend);
+                if (tid == 0) {
+                    a.surv_n[q] = st.npend;
+                    st.handed = 1;
+                }
             } else if (st.npend > 0) {
                 COUNT(6, st.npend);
+                // the first slots went to the hand-off buffer
+                for (uint32_t i = (uint32_t)tid; i < c.scap; i += NT) pend_g[i] = c.sq[i];
+                if (c.scap) __syncthreads();
                 merge_topk(top, pend_g, tmpk, S.hist2, S.ties2, R, a.pid, red, st, a.status);
             }
         }
         __syncthreads();
         PHASE_MARK(5);  // final merge
+        if (st.handed) continue;  // uniform: read after the barrier
+        if (PART == 2 && a.surv && tid == 0) a.surv_n[q] = -1;  // outputs written here
         // (6) outputs: the R best sorted by (distance, id) (a shortlist for
         // the exact re-rank in any order: the re-rank sorts it itself)
         {

@@ -35,6 +35,8 @@ struct WarpSmem {
     uint64_t lb[KW];  // sorted prefix of list B (IMI)
     uint32_t rkey[RW], rcell[RW], rcnt[RW];  // enumerated cells in rank order
     uint16_t rowp[KW];  // per row of A: columns already enumerated
+    uint16_t rowq[KW];  // per row of A: first record of the round's new cells
+    uint16_t rows0[KW];  // per row of A: first new column of the round
 };
 
 __device__ __forceinline__ uint64_t shfl64(uint64_t v, int src) {
@@ -100,6 +102,49 @@ __device__ __forceinline__ void warp_sort(uint64_t (&v)[P], int lane) {
     }
 }
 
+// The same network on 32-bit keys.
+template <int P>
+__device__ __forceinline__ void warp_sort32(uint32_t (&v)[P], int lane) {
+    constexpr int n = 32 * P;
+#pragma unroll
+    for (int k = 2; k <= n; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            if (j >= 32) {
+                const int rj = j >> 5;
+#pragma unroll
+                for (int r = 0; r < P; r++) {
+                    const int pr = r ^ rj;
+                    if (pr > r) {
+                        const bool asc = ((r * 32) & k) == 0;
+                        const uint32_t x = v[r], y = v[pr];
+                        v[r] = asc ? min(x, y) : max(x, y);
+                        v[pr] = asc ? max(x, y) : min(x, y);
+                    }
+                }
+            } else {
+                const bool lower = (lane & j) == 0;
+#pragma unroll
+                for (int r = 0; r < P; r++) {
+                    const bool asc = ((r * 32 + lane) & k) == 0;
+                    const uint32_t o = __shfl_xor_sync(0xffffffffu, v[r], j);
+                    v[r] = (lower == asc) ? min(v[r], o) : max(v[r], o);
+                }
+            }
+        }
+    }
+}
+
+template <int P>
+__device__ __forceinline__ void sort_buf32(uint32_t *buf, int lane) {
+    uint32_t v[P];
+#pragma unroll
+    for (int r = 0; r < P; r++) v[r] = buf[r * 32 + lane];
+    warp_sort32<P>(v, lane);
+#pragma unroll
+    for (int r = 0; r < P; r++) buf[r * 32 + lane] = v[r];
+}
+
 // Sorts the n2 (a power of two, 32..RW) keys of buf in place.
 template <int P>
 __device__ __forceinline__ void sort_buf(uint64_t *buf, int lane) {
@@ -134,6 +179,16 @@ __global__ void __launch_bounds__(WS_WARPS * 32, 6) k_select_warp(SearchArgs a, 
         q = __shfl_sync(FULL, q, 0);
         if (q >= a.nq) break;
         const long long t0 = clock64();
+        long long tp = t0;
+        // optional phase cycles (lane 0): [0] prefixes, [14] bisections,
+        // [1] enumeration, [2] cut, [3] compaction
+        auto mark = [&](int i) {
+            if (a.phase_cycles && lane == 0) {
+                const long long t = clock64();
+                atomicAdd((unsigned long long *)&a.phase_cycles[i], (unsigned long long)(t - tp));
+                tp = t;
+            }
+        };
         const int T = a.Tq ? a.Tq[q] : a.T;
         const int w = a.w;
         // IMI and SC test the rules before each pop (multi_query.h:151,
@@ -202,6 +257,7 @@ __global__ void __launch_bounds__(WS_WARPS * 32, 6) k_select_warp(SearchArgs a, 
         if (nextB != INF) bound = min(bound, f2o(__fadd_rn(L.a(0), o2f(nextB))));
         const bool whole = kA == lim && (ivf || kB == lim);
 
+        mark(0);
         // (2) rounds of staircase enumeration over the prefix grid; lane l
         // owns the rows [l * rpl, l * rpl + rpl) of list A
         const int rpl = (kA + 31) / 32;
@@ -209,11 +265,28 @@ __global__ void __launch_bounds__(WS_WARPS * 32, 6) k_select_warp(SearchArgs a, 
         const uint64_t grid_cells = (uint64_t)kA * kB, total_cells = grid_cells - (sc ? 1 : 0);
         const uint32_t lo_key = f2o(__fadd_rn(L.a(0), L.b(0)));
         const uint32_t hi_key = f2o(__fadd_rn(L.a(kA - 1), L.b(kB - 1)));
-        auto count_at = [&](uint32_t tau) -> uint64_t {
+        // staircase count at tau, each row's count searched only between its
+        // counts at the bisection's current ends (rlo, rhi): cc[i] gets the
+        // lane's row counts
+        int rlo[KW / 32], rhi[KW / 32];
+        auto count_at = [&](uint32_t tau, int (&cc)[KW / 32]) -> uint64_t {
             uint32_t c = 0;
 #pragma unroll 8
-            for (int i = 0; i < KW / 32; i++)
-                if (i < rpl && hb + i < kA) c += (uint32_t)L.row_count(L.a(hb + i), tau);
+            for (int i = 0; i < KW / 32; i++) {
+                cc[i] = 0;
+                const int h = hb + i;
+                if (i < rpl && h < kA) {
+                    const float av = L.a(h);
+                    int lo2 = rlo[i], hi2 = rhi[i];  // the count lies in [lo2, hi2]
+                    while (lo2 < hi2) {
+                        const int mid = (lo2 + hi2 + 1) >> 1;
+                        if (f2o(__fadd_rn(av, L.b(mid - 1))) <= tau) lo2 = mid;
+                        else hi2 = mid - 1;
+                    }
+                    cc[i] = lo2;
+                    c += (uint32_t)lo2;
+                }
+            }
             return (uint64_t)__reduce_add_sync(FULL, c);
         };
         const double dloc = dens_est > 1e-9 ? dens_est : (avg_density > 1e-9 ? avg_density : 1e-9);
@@ -239,30 +312,48 @@ __global__ void __launch_bounds__(WS_WARPS * 32, 6) k_select_warp(SearchArgs a, 
             uint32_t lo = round == 0 ? lo_key : tau_prev + 1, hi = hi_key;
             const uint64_t thi = target + target / 4 + 32;
             if (lo > hi) lo = hi;
+            // row counts at the ends: at tau_prev (the enumerated columns;
+            // row 0 of SC starts at 1, below every key >= lo_key) and at
+            // hi_key (every column: the last row's last key is the largest)
+#pragma unroll 8
+            for (int i = 0; i < KW / 32; i++) {
+                const int h = hb + i;
+                rlo[i] = (i < rpl && h < kA) ? (int)W.rowp[h] : 0;
+                rhi[i] = kB;
+            }
+            int cc[KW / 32];
+            auto take = [&](uint64_t c, uint32_t mid) {
+                // the probe's counts become the bracket's new end
+                if (c >= target) {
+                    hi = mid;
+#pragma unroll 8
+                    for (int i = 0; i < KW / 32; i++) rhi[i] = cc[i];
+                } else {
+                    lo = mid + 1;
+#pragma unroll 8
+                    for (int i = 0; i < KW / 32; i++) rlo[i] = cc[i];
+                }
+            };
             int it = 0;
             const int tp = tau_T;
             const uint32_t gap0 = (4ll * (tp > T ? tp - T : T - tp) <= (long long)tp) ? tau_gap : 0u;
             if (round == 0 && gap0 != 0u && lo < hi) {
                 // first probe where this warp's previous query ended
                 const uint32_t mid = (hi - lo > gap0) ? lo + gap0 : hi - 1;
-                const uint64_t c = count_at(mid);
-                if (c >= target) hi = mid;
-                else lo = mid + 1;
+                const uint64_t c = count_at(mid, cc);
+                take(c, mid);
                 if (c >= target && c <= thi) lo = hi;
                 it++;
             }
             while (lo < hi && it < 40) {
                 const uint32_t mid = lo + ((hi - lo) >> 1);
-                const uint64_t c = count_at(mid);
-                if (c >= target) {
-                    hi = mid;
-                    if (c <= thi) break;
-                } else {
-                    lo = mid + 1;
-                }
+                const uint64_t c = count_at(mid, cc);
+                take(c, mid);
+                if (c >= target && c <= thi) break;
                 it++;
             }
             const uint32_t tau = hi;
+            mark(14);
             tau_prev = tau;
             if (round == 0) {
                 tau_gap = tau - lo_key;
@@ -276,9 +367,9 @@ __global__ void __launch_bounds__(WS_WARPS * 32, 6) k_select_warp(SearchArgs a, 
                 cn[i] = 0;
                 const int h = hb + i;
                 if (i < rpl && h < kA) {
+                    // the row's count at tau = hi: the bracket's upper end
                     const int p0 = W.rowp[h];
-                    int c = L.row_count(L.a(h), tau);
-                    cn[i] = c < p0 ? p0 : c;
+                    cn[i] = rhi[i] < p0 ? p0 : rhi[i];
                     mine += (uint32_t)(cn[i] - p0);
                 }
             }
@@ -291,28 +382,37 @@ __global__ void __launch_bounds__(WS_WARPS * 32, 6) k_select_warp(SearchArgs a, 
                 break;
             }
             {
+                // each row's first record and first new column, then the
+                // records spread evenly over the lanes: record r is in the
+                // last row whose first record is <= r
                 uint32_t pos = (uint32_t)nrec + base;
 #pragma unroll 8
                 for (int i = 0; i < KW / 32; i++) {
                     const int h = hb + i;
                     if (i >= rpl || h >= kA) continue;
-                    const float av = L.a(h);
-                    for (int h2 = W.rowp[h]; h2 < cn[i]; h2++) {
-                        const uint32_t rank = ((uint32_t)h << 16) | (uint32_t)h2;
-                        W.rkey[pos] = f2o(__fadd_rn(av, L.b(h2)));
-                        W.rcell[pos] = cell_of(L, rank);
-                        pos++;
-                    }
+                    W.rowq[h] = (uint16_t)pos;
+                    W.rows0[h] = W.rowp[h];
+                    pos += (uint32_t)(cn[i] - W.rowp[h]);
                     W.rowp[h] = (uint16_t)cn[i];
                 }
             }
             __syncwarp();
-            // the cells' lengths, loaded by all lanes
+            // the new records with their cells' lengths
             uint64_t ls = 0;
             uint32_t lne = 0;
             const int n1 = nrec + (int)tot_new;
             for (int r = nrec + lane; r < n1; r += 32) {
-                const uint32_t cell = W.rcell[r];
+                int lo2 = 0, hi2 = kA - 1;
+                while (lo2 < hi2) {
+                    const int mid = (lo2 + hi2 + 1) >> 1;
+                    if (W.rowq[mid] <= (uint32_t)r) lo2 = mid;
+                    else hi2 = mid - 1;
+                }
+                const int h = lo2, h2 = W.rows0[h] + (r - (int)W.rowq[h]);
+                const uint32_t rank = ((uint32_t)h << 16) | (uint32_t)h2;
+                const uint32_t cell = cell_of(L, rank);
+                W.rkey[r] = f2o(__fadd_rn(L.a(h), L.b(h2)));
+                W.rcell[r] = cell;
                 uint32_t c = __ldg(a.off + cell + 1) - __ldg(a.off + cell);
                 if (sc && cell == 0) c = 0;  // sc_query.h:138-140
                 W.rcnt[r] = c;
@@ -352,6 +452,7 @@ __global__ void __launch_bounds__(WS_WARPS * 32, 6) k_select_warp(SearchArgs a, 
             atomicAdd(&a.dens_acc[1], (unsigned long long)Ncell);
         }
 
+        mark(1);
         // (3) the cut: the last round's records sorted by (key, rank) -- the
         // rank order of the enumeration, so (key << 32 | index) -- and the
         // first record at which the T rule (candidates) or the w rule (cells,
@@ -364,14 +465,42 @@ __global__ void __launch_bounds__(WS_WARPS * 32, 6) k_select_warp(SearchArgs a, 
         if (trig) {
             int n2 = 32;
             while (n2 < nr) n2 <<= 1;
-            for (int i = lane; i < n2; i += 32)
-                sb[i] = i < nr ? (((uint64_t)W.rkey[r0 + i] << 32) | (uint32_t)i) : ~0ull;
-            __syncwarp();
-            switch (n2) {
-                case 32: sort_buf<1>(sb, lane); break;
-                case 64: sort_buf<2>(sb, lane); break;
-                case 128: sort_buf<4>(sb, lane); break;
-                default: sort_buf<8>(sb, lane); break;
+            uint32_t kmin = INF, kmax = 0;
+            for (int i = lane; i < nr; i += 32) {
+                kmin = min(kmin, W.rkey[r0 + i]);
+                kmax = max(kmax, W.rkey[r0 + i]);
+            }
+            kmin = __reduce_min_sync(FULL, kmin);
+            kmax = __reduce_max_sync(FULL, kmax);
+            if (kmax - kmin < (1u << 24) - 1u) {
+                // keys within 2^24 of the smallest: (key - min) << 8 | index
+                // sorts as 32 bits (list B's buffer is free by now), then
+                // expands to the 64-bit (key, index) words
+                uint32_t *s32 = reinterpret_cast<uint32_t *>(W.lb);
+                for (int i = lane; i < n2; i += 32)
+                    s32[i] = i < nr ? ((W.rkey[r0 + i] - kmin) << 8) | (uint32_t)i : INF;
+                __syncwarp();
+                switch (n2) {
+                    case 32: sort_buf32<1>(s32, lane); break;
+                    case 64: sort_buf32<2>(s32, lane); break;
+                    case 128: sort_buf32<4>(s32, lane); break;
+                    default: sort_buf32<8>(s32, lane); break;
+                }
+                __syncwarp();
+                for (int i = lane; i < n2; i += 32) {
+                    const uint32_t x = s32[i];
+                    sb[i] = x == INF ? ~0ull : ((uint64_t)(kmin + (x >> 8)) << 32) | (x & 255u);
+                }
+            } else {
+                for (int i = lane; i < n2; i += 32)
+                    sb[i] = i < nr ? (((uint64_t)W.rkey[r0 + i] << 32) | (uint32_t)i) : ~0ull;
+                __syncwarp();
+                switch (n2) {
+                    case 32: sort_buf<1>(sb, lane); break;
+                    case 64: sort_buf<2>(sb, lane); break;
+                    case 128: sort_buf<4>(sb, lane); break;
+                    default: sort_buf<8>(sb, lane); break;
+                }
             }
             __syncwarp();
             // lane l: sorted positions [l * pp, l * pp + pp)
@@ -427,6 +556,7 @@ __global__ void __launch_bounds__(WS_WARPS * 32, 6) k_select_warp(SearchArgs a, 
             continue;
         }
 
+        mark(2);
         // (4) the visited non-empty cells -> (cell, prefix) list in the
         // query's pool region: the earlier rounds in rank order, then the
         // last round (up to the cut) in key order
@@ -473,6 +603,7 @@ __global__ void __launch_bounds__(WS_WARPS * 32, 6) k_select_warp(SearchArgs a, 
             }
             if (lane == 0) vp[nvis] = runc;
         }
+        mark(3);
         finish(off, nvis, runc, err, runc, nv - nev);
     }
 }

@@ -35,7 +35,7 @@ namespace {
 constexpr int TM = 128;            // queries per tile (TMEM lanes)
 constexpr int TN = 256;            // entries per tile (TMEM columns)
 constexpr int TK = 64;             // K elements staged per chunk
-constexpr int TC_THREADS = 128;
+constexpr int TC_THREADS = 256;  // 8 warps: warp w reads TMEM lanes 32 (w % 4).., columns half w / 4
 constexpr int A_BYTES = TM * TK * 2;
 constexpr int B_BYTES = TN * TK * 2;
 constexpr int OFF_A0 = 0;
@@ -271,10 +271,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tables_tc(TablesArgs a, int c
     }
 
     if (!failed) {
-        const int q = q0 + warp * 32 + lane;
-        const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
+        // warp w: TMEM lanes (queries) 32 (w % 4) .. + 31 (the lanes a warp
+        // may read), columns [TN / 2 (w / 4), TN / 2 (w / 4 + 1))
+        const int wq = warp & 3, half = warp >> 2;
+        const int q = q0 + wq * 32 + lane;
+        const uint32_t lane_base = tmem + ((uint32_t)(wq * 32) << 16);
         const bool vec = (outstride % 4) == 0 && (outoff % 4) == 0;
-        for (int c = 0; c < TN && e0 + c < seglen; c += 16) {
+        for (int c = half * (TN / 2); c < (half + 1) * (TN / 2) && e0 + c < seglen; c += 16) {
             float v[16];
             tmem_load16(lane_base + (uint32_t)c, v);
             if (q < a.nq) {
