@@ -54,6 +54,12 @@ constexpr int RMAX = 1024;      // largest R
 #define SCG_WARMN 4096
 #endif
 constexpr int WARMN = SCG_WARMN;  // candidates scored before the threshold is set
+// The threshold is within 2^SCG_WARM_SBITS ordered-float steps above the R-th
+// warm-up distance (2^(SCG_WARM_SBITS - 23) relative).  15 (0.4%) leaves
+// one radix pass where 8 took two, for a few more survivors.
+#ifndef SCG_WARM_SBITS
+#define SCG_WARM_SBITS 15
+#endif
 constexpr int WWIN = 32;        // per-warp window of visited cells
 constexpr int MERGE_KPT = 16;   // survivors per thread of the final merge's register bisection
 // Candidates per lane per claimed chunk (U, a template parameter of the
@@ -2145,10 +2151,11 @@ __global__ void __launch_bounds__(NT, PART == 2   ? (VAR == V_FAST256 ? SCG_SCAN
             else scan_chunks<MPC, true, U, VAR, ROTOK>(a, S, st, c, 0u, K, 0u, S.warm, nullptr, 0u);
             __syncthreads();
             uint32_t tau = 0xffffffffu;
-            // an upper bound of the R-th warm-up distance (within 2^-15)
+            // an upper bound of the R-th warm-up distance (within
+            // 2^(SCG_WARM_SBITS - 23) of it, relative)
             if (K > (uint32_t)R) {
                 const uint64_t *wk = S.warm;
-                tau = block_kth_bound<WARMN / NT>([&](int i) { return (uint32_t)(wk[i] >> 32); }, (int)K, R, 8,
+                tau = block_kth_bound<WARMN / NT>([&](int i) { return (uint32_t)(wk[i] >> 32); }, (int)K, R, SCG_WARM_SBITS,
                                                   S.hist2, red, st);
             }
             // the warm entries at or below tau open the pending buffer
