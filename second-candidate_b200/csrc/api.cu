@@ -266,9 +266,10 @@ int reserve_search(scg_index *h, Workspace *ws, int mode, int grid) {
 // entries (or fewer when T, w or N bound its list below that: each visited
 // non-empty cell holds a candidate, so a list has at most min(T, w, N) cells
 // plus its closing prefix); longer lists take a range of a shared overflow
-// area (128 entries per query with per-query targets, whose long lists the
-// host cannot bound).  Should that run out, the batch is searched again by
-// the fused kernel.
+// area (64 entries per query, 128 with per-query targets, whose long lists
+// the host cannot bound; 65,536 at least).  Should that run out, the batch
+// is searched again by the fused kernel, which stalls a request loop, so
+// the area is generous (8 bytes per entry).
 constexpr int64_t POOL_SLOT = 128;
 
 static void pool_dims(const scg_index *h, const scg_search_params *p, int nq, bool per_query_T, int64_t *stride,
@@ -280,9 +281,14 @@ static void pool_dims(const scg_index *h, const scg_search_params *p, int nq, bo
     }
     b = std::min<int64_t>(b, h->N > 0 ? h->N : 1);
     *stride = b + 1;
-    *over = std::max<int64_t>(65536, (per_query_T ? 128 : 16) * (int64_t)nq);
+    *over = std::max<int64_t>(65536, (per_query_T ? 128 : 64) * (int64_t)nq);
 }
 
+// Every per-query buffer of the split kernels for batches of up to nq
+// queries: the visited-list pool, the deferred-query list and the survivors
+// handed to the merge kernel.  The request loop reserves them per slot when
+// it starts, so that no request grows a workspace (a cudaFree waits for the
+// whole device, every other slot included).
 int reserve_pool(scg_index *h, Workspace *ws, int nq) {
     int64_t stride, over;
     pool_dims(h, nullptr, nq, false, &stride, &over);
@@ -290,6 +296,9 @@ int reserve_pool(scg_index *h, Workspace *ws, int nq) {
     if ((rc = ws->qmeta.ensure(sizeof(QMeta) * (size_t)nq))) return rc;
     if ((rc = ws->pool_cell.ensure(4 * (size_t)(stride * nq + over)))) return rc;
     if ((rc = ws->pool_pre.ensure(4 * (size_t)(stride * nq + over)))) return rc;
+    if ((rc = ws->defer.ensure(sizeof(int) * ((size_t)nq + 1)))) return rc;
+    if ((rc = ws->surv.ensure(sizeof(uint64_t) * (size_t)nq * SURV_CAP))) return rc;
+    if ((rc = ws->surv_n.ensure(sizeof(int) * (size_t)nq))) return rc;
     return SCG_OK;
 }
 

@@ -154,6 +154,50 @@ __global__ void k_query_norms(const float *__restrict__ Q, int nq, int dim, int 
     qsum[q] = (mc == 2) ? __fadd_rn(__fadd_rn(0.0f, n[0]), n[1]) : n[0];
 }
 
+// The same norms with the rows staged in shared memory: a block copies qb
+// query rows with coalesced loads (row stride dim + 1 words, so threads
+// summing neighbouring rows read different banks), then thread (row, part)
+// adds its part in the order above.  One thread per query reading its own
+// row straight from global memory touched a different 512-byte row per lane
+// and left most SMs idle at 10,000 queries.
+constexpr int QN_THREADS = 256;
+constexpr int QN_MAX_ROWS = 64;
+constexpr int QN_SMEM_WORDS = 12288;  // 48 KB: no opt-in needed
+
+__global__ void __launch_bounds__(QN_THREADS) k_query_norms_staged(const float *__restrict__ Q, int nq, int dim,
+                                                                   int mc, int qb, float *__restrict__ qn,
+                                                                   float *__restrict__ qsum) {
+    extern __shared__ float rows[];
+    __shared__ float part_sum[QN_MAX_ROWS][2];
+    const int q0 = blockIdx.x * qb;
+    const int nr = min(qb, nq - q0);
+    const int ld = dim + 1;
+    const float *src = Q + (size_t)q0 * dim;
+    for (int i = threadIdx.x; i < nr * dim; i += QN_THREADS) {
+        const int r = i / dim;
+        rows[r * ld + (i - r * dim)] = __ldg(src + i);
+    }
+    __syncthreads();
+    const int parts = mc < 2 ? 1 : 2;
+    const int bsc = dim / mc;
+    const int t = threadIdx.x;
+    if (t < nr * parts) {
+        const int r = t / parts, i = t - r * parts;
+        const float *x = rows + r * ld + i * bsc;
+        float d = 0.0f;
+        for (int j = 0; j < bsc; j++) d = __fadd_rn(d, __fmul_rn(x[j], x[j]));
+        part_sum[r][i] = d;
+    }
+    __syncthreads();
+    if (t < nr) {
+        const float n0 = part_sum[t][0], n1 = parts == 2 ? part_sum[t][1] : 0.0f;
+        const int q = q0 + t;
+        qn[2 * q] = n0;
+        qn[2 * q + 1] = n1;
+        qsum[q] = (mc == 2) ? __fadd_rn(__fadd_rn(0.0f, n0), n1) : n0;
+    }
+}
+
 // Per-vector term of the fast ADC form, in CSR order:
 //   vterm[p] = sum_k ( ||r_k(c_k)||^2 + 2<c_part(k), r_k(c_k)> )
 // so that ||q - c - r||^2 = q_sum + dqc(cell) + vterm + sum_k (-2<q_k, r_k>).
@@ -226,7 +270,14 @@ void launch_tables_exact(const TablesArgs &a, cudaStream_t s) {
 
 void launch_query_norms(const TablesArgs &a, cudaStream_t s) {
     if (a.nq <= 0 || !a.qn) return;
-    k_query_norms<<<(a.nq + 127) / 128, 128, 0, s>>>(a.Q, a.nq, a.dim, a.mc, a.qn, a.qsum);
+    const int qb = std::min(QN_MAX_ROWS, QN_SMEM_WORDS / (a.dim + 1));
+    if (qb >= 1) {
+        const size_t smem = sizeof(float) * (size_t)qb * (a.dim + 1);
+        k_query_norms_staged<<<(a.nq + qb - 1) / qb, QN_THREADS, smem, s>>>(a.Q, a.nq, a.dim, a.mc, qb, a.qn,
+                                                                           a.qsum);
+    } else {
+        k_query_norms<<<(a.nq + 127) / 128, 128, 0, s>>>(a.Q, a.nq, a.dim, a.mc, a.qn, a.qsum);
+    }
 }
 
 }  // namespace scg

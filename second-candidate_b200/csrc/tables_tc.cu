@@ -42,8 +42,9 @@ constexpr int OFF_A0 = 0;
 constexpr int OFF_A1 = OFF_A0 + A_BYTES;
 constexpr int OFF_B0 = OFF_A1 + A_BYTES;
 constexpr int OFF_B1 = OFF_B0 + B_BYTES;
-constexpr int OFF_BAR = OFF_B1 + B_BYTES;
-// 96 KB + control words: at most two CTAs per SM, so two 256-column TMEM
+constexpr int OFF_NORM = OFF_B1 + B_BYTES;  // the tile's TN centroid norms (fp32)
+constexpr int OFF_BAR = OFF_NORM + TN * 4;
+// 97 KB + control words: at most two CTAs per SM, so two 256-column TMEM
 // allocations never exceed the SM's 512 columns.
 constexpr int TC_SMEM = OFF_BAR + 64;
 constexpr long long WAIT_CYCLES = 1ll << 30;  // ~0.5 s at the boost clock
@@ -147,31 +148,49 @@ __device__ __forceinline__ void pack8(const float (&x)[8], uint4 &hi, uint4 &lo)
 
 // Stages rows [0, rows) x K groups [0, ngroups) of one operand: row r is
 // src + r * ld (valid when r < nrows), elements k0 .. k0 + 8 * ngroups of it
-// (valid when < len).
+// (valid when < len).  A thread loads SB groups before it converts and
+// stores any of them, so a batch costs one global-load round trip instead of
+// one per group (the stores to shared memory would otherwise keep the next
+// group's loads from being issued early).
+constexpr int SB = 8;
+
 template <int FMT, bool SPLIT>
 __device__ __forceinline__ void stage(const float *__restrict__ src, int nrows, size_t ld, int len, int k0, int rows,
                                       int ngroups, unsigned char *hi, unsigned char *lo) {
     // whole groups of 8 load as two float4 when every row starts 16-byte aligned
     const bool vec = ((reinterpret_cast<uintptr_t>(src) & 15) == 0) && (ld % 4 == 0);
-    for (int u = threadIdx.x; u < rows * ngroups; u += TC_THREADS) {
-        const int r = u % rows, g = u / rows;
-        float x[8];
-        const int kb = k0 + g * 8;
-        const float *p = src + (size_t)r * ld + kb;
-        if (vec && r < nrows && kb + 8 <= len) {
-            const float4 v0 = __ldg(reinterpret_cast<const float4 *>(p));
-            const float4 v1 = __ldg(reinterpret_cast<const float4 *>(p) + 1);
-            x[0] = v0.x; x[1] = v0.y; x[2] = v0.z; x[3] = v0.w;
-            x[4] = v1.x; x[5] = v1.y; x[6] = v1.z; x[7] = v1.w;
-        } else {
+    const int total = rows * ngroups;
+    for (int u0 = threadIdx.x; u0 < total; u0 += SB * TC_THREADS) {
+        float x[SB][8];
 #pragma unroll
-            for (int j = 0; j < 8; j++) x[j] = (r < nrows && kb + j < len) ? __ldg(p + j) : 0.0f;
+        for (int b = 0; b < SB; b++) {
+            const int u = u0 + b * TC_THREADS;
+            const int r = u % rows, g = u / rows;
+            const int kb = k0 + g * 8;
+            const bool row_ok = u < total && r < nrows;
+            const float *p = src + (size_t)r * ld + kb;
+            if (vec && row_ok && kb + 8 <= len) {
+                const float4 v0 = __ldg(reinterpret_cast<const float4 *>(p));
+                const float4 v1 = __ldg(reinterpret_cast<const float4 *>(p) + 1);
+                x[b][0] = v0.x; x[b][1] = v0.y; x[b][2] = v0.z; x[b][3] = v0.w;
+                x[b][4] = v1.x; x[b][5] = v1.y; x[b][6] = v1.z; x[b][7] = v1.w;
+            } else {
+#pragma unroll
+                for (int j = 0; j < 8; j++) x[b][j] = (row_ok && kb + j < len) ? __ldg(p + j) : 0.0f;
+            }
         }
-        uint4 h, l;
-        pack8<FMT, SPLIT>(x, h, l);
-        const size_t off = ((size_t)g * rows + r) * 16;
-        *(uint4 *)(hi + off) = h;
-        if (SPLIT) *(uint4 *)(lo + off) = l;
+#pragma unroll
+        for (int b = 0; b < SB; b++) {
+            const int u = u0 + b * TC_THREADS;
+            if (u < total) {
+                const int r = u % rows, g = u / rows;
+                uint4 h, l;
+                pack8<FMT, SPLIT>(x[b], h, l);
+                const size_t off = ((size_t)g * rows + r) * 16;
+                *(uint4 *)(hi + off) = h;
+                if (SPLIT) *(uint4 *)(lo + off) = l;
+            }
+        }
     }
 }
 
@@ -229,6 +248,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tables_tc(TablesArgs a, int c
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
+    // the tile's centroid norms for the epilogue (0 for the fast form's LUT
+    // and past the segment's end), read once here instead of per lane there
+    float *snorm = (float *)(tsm + OFF_NORM);
+    for (int t = threadIdx.x; t < TN; t += TC_THREADS)
+        snorm[t] = (lut_only || e0 + t >= seglen) ? 0.0f : __ldg(norm + e0 + t);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
@@ -284,11 +308,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tables_tc(TablesArgs a, int c
                 float *dst = out + (size_t)q * outstride + outoff + e0 + c;
                 float r[16];
 #pragma unroll
-                for (int j = 0; j < 16; j++) {
-                    const int e = e0 + c + j;
-                    const float nv = (lut_only || e >= seglen) ? 0.0f : __ldg(norm + e);
-                    r[j] = __fsub_rn(__fsub_rn(nv, v[j]), v[j]);
-                }
+                for (int j = 0; j < 16; j++) r[j] = __fsub_rn(__fsub_rn(snorm[c + j], v[j]), v[j]);
                 if (vec && e0 + c + 16 <= seglen) {
 #pragma unroll
                     for (int j = 0; j < 16; j += 4) *(float4 *)(dst + j) = make_float4(r[j], r[j + 1], r[j + 2], r[j + 3]);
