@@ -381,6 +381,14 @@ int scg_server_stats(scg_server *s, long long *completed, int *max_inflight, int
  * Tickets not yet waited for are released. */
 int scg_server_destroy(scg_server *s);
 
+/* cudaMalloc calls the library has made for its own device buffers in this
+ * process so far (index arrays, search workspaces, arenas; never the
+ * caller's buffers).  A server reserves every per-slot buffer at
+ * scg_server_create, so serving requests of up to max_batch queries adds
+ * none: a cudaFree inside the request loop would wait for every slot.  No
+ * counterpart in the reference (it allocates no device memory). */
+int scg_device_allocations(long long *count);
+
 /* Index facts: dim, mc, kc, mp, kp, N (any pointer may be NULL). */
 int scg_index_info(scg_index *h, int *dim, int *mc, int *kc, int *mp, int *kp, int64_t *N);
 

@@ -1050,12 +1050,16 @@ int scg_autotune_ex(scg_index *h, const scg_search_params *p, const float *dQ, i
         }
     }
     h->prefix_len = rec->prefix;
-    // (3) kernel organisation: split selection + scan, or the fused kernel
+    // (3) kernel organisation: split selection + scan, or the fused kernel.
+    // A split run whose visited lists outgrew the pool is searched again by
+    // the fused kernel, and its events then time only that second search:
+    // such a split never wins (it costs its own kernels on top).
     best = 3.4e38f;
     for (int i = 0; i < 2; i++) {
         h->split = i == 0;
         if ((rc = tune_time(h, p, dQ, nq, d_ids, d_dists, d_sums, 3, &rec->split_ms[i]))) { restore(); return rc; }
-        if (rec->split_ms[i] < best) {
+        const bool fell_back = i == 0 && !h->ws.last_split;
+        if (!fell_back && rec->split_ms[i] < best) {
             best = rec->split_ms[i];
             rec->split = i == 0 ? 1 : 0;
         }

@@ -3,12 +3,17 @@
 // server.cu (the request loop).
 #pragma once
 
+#include <atomic>
 #include <mutex>
 #include <string>
 
 #include "scg_internal.cuh"
 
 namespace scg {
+
+// cudaMalloc calls made for the library's own device buffers in this
+// process (scg_device_allocations).
+inline std::atomic<long long> g_device_allocs{0};
 
 // Grow-only device buffer.
 struct DevBuf {
@@ -21,6 +26,7 @@ struct DevBuf {
         n = 0;
         cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
         if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc");
+        g_device_allocs.fetch_add(1, std::memory_order_relaxed);
         n = bytes;
         return SCG_OK;
     }

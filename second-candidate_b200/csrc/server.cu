@@ -384,6 +384,12 @@ int scg_server_stats(scg_server *s, long long *completed, int *max_inflight, int
     return SCG_OK;
 }
 
+int scg_device_allocations(long long *count) {
+    if (!count) return fail(SCG_ERR_ARG, "null output pointer");
+    *count = g_device_allocs.load(std::memory_order_relaxed);
+    return SCG_OK;
+}
+
 int scg_server_destroy(scg_server *s) {
     if (!s) return SCG_OK;
     {

@@ -34,7 +34,8 @@ EXPORTS = ["scg_last_error", "scg_index_create", "scg_index_destroy", "scg_load_
            "scg_server_destroy", "scg_autotune", "scg_set_scan_tuning",
            "scg_set_kernel_split", "scg_server_wait_times", "scg_set_encoder",
            "scg_train_codebooks", "scg_build_index", "scg_write_edat", "scg_search_graph",
-           "scg_kmeans", "scg_exact_nn", "scg_set_rank_limit", "scg_autotune_ex"]
+           "scg_kmeans", "scg_exact_nn", "scg_set_rank_limit", "scg_autotune_ex",
+           "scg_device_allocations"]
 
 
 def train_codebooks_device(dX_ptr, n, dim, mc, kc, mp, kp, iters, seed, d_cq, d_pq, device=0, stream=None):
@@ -317,6 +318,14 @@ class Index:
         _check(_lib.scg_encode_device(self._h, ctypes.c_void_p(dX_ptr), ctypes.c_int64(n), nc,
                                       ctypes.c_void_p(d_cid), ctypes.c_void_p(d_codes),
                                       ctypes.c_void_p(stream) if stream else None))
+
+
+def device_allocations():
+    """cudaMalloc calls the library has made for its own buffers so far."""
+    load()
+    c = ctypes.c_longlong()
+    _check(_lib.scg_device_allocations(ctypes.byref(c)))
+    return c.value
 
 
 class Server:

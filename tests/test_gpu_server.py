@@ -99,3 +99,24 @@ def test_admission_by_memory(index):
     with pytest.raises(scgpu.ScgError):
         srv.submit(2, small[0], 10, 1 << 20, 2000)
     srv.close()
+
+
+def test_requests_make_no_device_allocation(index):
+    """The server reserves every per-slot device buffer when it starts, so
+    requests of up to max_batch queries, of any size, k and arithmetic form,
+    make no cudaMalloc: growing a workspace inside the request loop means a
+    cudaFree, which waits for the work of every slot."""
+    import scgpu
+    g, mix = index
+    srv = scgpu.Server(g, slots=2, max_batch=1024, max_R=100, arena_bytes=256 << 20)
+    before = scgpu.device_allocations()
+    forms = [scgpu.FAST, scgpu.FP32_EXACT, scgpu.BF16]
+    tickets = []
+    for i, nq in enumerate([1, 7, 64, 333, 1024, 1024, 500, 1000, 12]):
+        Q = mix.sample(nq, seed=900 + i)
+        tickets.append(srv.submit(scgpu.IMI, Q, [1, 10, 100][i % 3], 1 << 20, 4000, precision=forms[(i // 3) % 3]))
+    for t in tickets:
+        assert srv.wait(t) is not None
+    after = scgpu.device_allocations()
+    srv.close()
+    assert after == before, (before, after)
