@@ -629,6 +629,8 @@ struct CodeWords<0> {
             atomicAdd((unsigned long long *)&a.phase_cycles[(i)], (unsigned long long)(v));        \
     } while (0)
 
+constexpr int RK_BATCH = 8;  // words per thread in flight in the radix passes of radix_kth_word
+
 // The k-th smallest (1-based) of n 32-bit words word(i): a radix select of
 // 4 x 8 bits over RBINS = NT bins (one per thread).  Returns the word;
 // `need` becomes how many entries equal to it complete the k smallest.  With
@@ -644,9 +646,18 @@ __device__ uint32_t radix_kth_word(Word word, int n, uint64_t k, uint32_t *hist,
     for (int sh = 24; sh >= 32 - 8 * npass; sh -= 8) {
         hist[tid] = 0;
         __syncthreads();
-        for (int i = tid; i < n; i += NT) {
-            const uint32_t v = word(i);
-            if (sh == 24 || (v >> (sh + 8)) == (prefix >> (sh + 8))) atomicAdd(&hist[(v >> sh) & 255u], 1u);
+        // RK_BATCH words loaded before their histogram adds: the words may
+        // live in global memory, and one load per add waits out a round trip
+        for (int i0 = tid; i0 < n; i0 += RK_BATCH * NT) {
+            uint32_t vb[RK_BATCH];
+#pragma unroll
+            for (int j = 0; j < RK_BATCH; j++) vb[j] = i0 + j * NT < n ? word(i0 + j * NT) : 0u;
+#pragma unroll
+            for (int j = 0; j < RK_BATCH; j++) {
+                const uint32_t v = vb[j];
+                if (i0 + j * NT < n && (sh == 24 || (v >> (sh + 8)) == (prefix >> (sh + 8))))
+                    atomicAdd(&hist[(v >> sh) & 255u], 1u);
+            }
         }
         __syncthreads();
         const uint64_t cnt = hist[tid];
@@ -839,18 +850,40 @@ __device__ void merge_topk(uint64_t *top, uint64_t *pend, uint64_t *tmp, uint32_
     const uint32_t v = prefix;
     // keep everything below v; gather the entries equal to v
     uint64_t mine = 0;
-    for (int i = tid; i < n; i += NT) mine += ((uint32_t)((i < na ? top[i] : pend[i - na]) >> 32) < v);
+    for (int i0 = tid; i0 < n; i0 += RK_BATCH * NT) {
+        uint32_t hb[RK_BATCH];
+#pragma unroll
+        for (int j = 0; j < RK_BATCH; j++) {
+            const int i = i0 + j * NT;
+            hb[j] = i < n ? (uint32_t)((i < na ? top[i] : pend[i - na]) >> 32) : 0xffffffffu;
+        }
+#pragma unroll
+        for (int j = 0; j < RK_BATCH; j++) mine += hb[j] < v;
+    }
     uint64_t total;
     uint64_t pos = block_exscan(mine, red, total);
     if (tid == 0) st.nties = 0;
     __syncthreads();
-    for (int i = tid; i < n; i += NT) {
-        uint64_t e = i < na ? top[i] : pend[i - na];
-        uint32_t hv = (uint32_t)(e >> 32);
-        if (hv < v) tmp[pos++] = i < na ? e : as_id(e);
-        else if (hv == v) {
-            int slot = atomicAdd(&st.nties, 1);
-            if (slot < TIECAP) ties[slot] = i < na ? e : as_id(e);
+    // the same entries in the same order per thread as the count above, so
+    // that pos runs through this thread's range of the exclusive scan
+    for (int i0 = tid; i0 < n; i0 += RK_BATCH * NT) {
+        uint64_t eb[RK_BATCH];
+#pragma unroll
+        for (int j = 0; j < RK_BATCH; j++) {
+            const int i = i0 + j * NT;
+            eb[j] = i < n ? (i < na ? top[i] : pend[i - na]) : ~0ull;
+        }
+#pragma unroll
+        for (int j = 0; j < RK_BATCH; j++) {
+            const int i = i0 + j * NT;
+            if (i >= n) continue;
+            const uint64_t e = eb[j];
+            const uint32_t hv = (uint32_t)(e >> 32);
+            if (hv < v) tmp[pos++] = i < na ? e : as_id(e);
+            else if (hv == v) {
+                int slot = atomicAdd(&st.nties, 1);
+                if (slot < TIECAP) ties[slot] = i < na ? e : as_id(e);
+            }
         }
     }
     __syncthreads();
