@@ -563,10 +563,11 @@ def run_workload(args, name, scgpu, dev, world, full=True):
     clocks.mark(True)
     gc.collect()
     gc.disable()
-    times, kern = [], []
+    times, kern, launches = [], [], 0
     for _ in range(args.steps):
         times += time_steps(step, flush, stream, 1)
         kern.append(ix.last_timings())
+        launches += ix.last_launches()  # this step's kernels, counted by the library
     torch.cuda.synchronize()
     gc.enable()
     clocks.mark(False)
@@ -611,7 +612,7 @@ def run_workload(args, name, scgpu, dev, world, full=True):
                                 else "k_search (fused selection + ADC scan + top-R)"),
                      "alg_bytes_per_launch": alg_bytes, "scan_ms": scan_ms if split else search_ms},
         "candidates_per_query": float(sums.mean()), "cells_per_query": float(nvis.mean() + empty.mean()),
-        "gpu_launches": (5 if split else 4) * args.steps + (args.steps if rerank else 0),
+        "gpu_launches": launches,
     }
     if not full:
         if d_T is not None:

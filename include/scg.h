@@ -321,6 +321,14 @@ int scg_last_query_stats(scg_index *h, int *nvis, int *empty, int nq);
  * the last chunk on the index's own stream.  n is the capacity of ms. */
 int scg_last_timings(scg_index *h, float *ms, int n);
 
+/* Kernels the index's last search launched on its own stream: the tables,
+ * query norms, coarse prefixes, selection, scan, top-R merge and re-rank
+ * kernels that ran (and the per-vector term when that call built it; a
+ * search the pool sent to the fused kernel counts both runs).  After
+ * scg_search (host buffers) the figure is that of the last chunk on the
+ * index's own stream.  No counterpart in the reference (no GPU code). */
+int scg_last_launches(scg_index *h, int *count);
+
 /* Copies the cell lengths back as the reference's inclusive prefix L[ncells]
  * (the array PQQuery::entropy reads, query.cpp:168-182). */
 int scg_cell_counts(scg_index *h, int *L, int64_t ncells);

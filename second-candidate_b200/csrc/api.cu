@@ -392,7 +392,13 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     const size_t pcap = slot > 65536 ? slot : 65536;
     if ((rc = ws->pend.ensure(8 * pcap * g_pend))) return rc;
 
-    if (scan_form(p->precision) == SCG_FAST && (rc = ensure_vterm(h, s))) return rc;
+    // kernels this call launches (scg_last_launches)
+    int nl = 0;
+    if (scan_form(p->precision) == SCG_FAST) {
+        const bool had_vterm = h->have_vterm;
+        if ((rc = ensure_vterm(h, s))) return rc;
+        if (!had_vterm) nl++;
+    }
     TablesArgs ta;
     memset(&ta, 0, sizeof(ta));
     ta.dim = h->dim; ta.mc = h->mc; ta.kc = h->kc; ta.mp = h->mp; ta.kp = h->kp; ta.nq = nq;
@@ -407,6 +413,7 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
     SCG_CUDA(cudaMemsetAsync(ws->counter.p, 0, sizeof(int) * 4, s));
     SCG_CUDA(cudaEventRecord(ws->ev[0], s));
     launch_tables(ta, p->precision, s);
+    if (nq > 0) nl += 2;  // the tables and the query norms
     if (b.slist) {
         CoarseArgs ca;
         ca.dqc = b.dqc; ca.qn = b.qn; ca.qsum = b.qsum;
@@ -421,6 +428,7 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
         ca.out = b.slist;
         ca.meta = b.smeta;
         launch_coarse_prefix(ca, s);
+        if (nq > 0) nl++;
     }
     SCG_CUDA(cudaEventRecord(ws->ev[1], s));
 
@@ -480,9 +488,11 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
                 if (select_warp_launch(sa, ws->defer.as<int>(), std::max(1, std::min(gw, (nq + 3) / 4)), s))
                     return fail(SCG_ERR_CUDA, "warp-wide selection launch failed");
                 sa.qlist = ws->defer.as<int>();
+                nl++;
             }
             sa.qcounter = ws->counter.as<int>();
             if ((rc = search_launch(sa, 1, g_sel, s))) return rc;
+            nl++;
             sa.qlist = nullptr;
             SCG_CUDA(cudaEventRecord(ws->ev[4], s));
             sa.qcounter = ws->counter.as<int>() + 1;
@@ -492,12 +502,16 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
                 sa.surv_cap = SURV_CAP;
             }
             if ((rc = search_launch(sa, 2, g_scan, s))) return rc;
+            nl++;
             if (warp_merge) {
                 merge_warp_launch(sa.surv, sa.surv_n, SURV_CAP, sa.pid, nq, R, s_ids, s_d, h->num_sms, s);
                 SCG_CUDA(cudaGetLastError());
+                nl++;
             }
         } else if ((rc = search_launch(sa, 0, g_fused, s))) {
             return rc;
+        } else {
+            nl++;
         }
     }
     SCG_CUDA(cudaEventRecord(ws->ev[2], s));
@@ -506,16 +520,21 @@ int run_search(scg_index *h, Workspace *ws, const ReqBufs *rb, const scg_search_
         launch_rerank(dQ, nq, h->dim, h->raw.p, h->raw_u8 ? 1 : 0, h->raw_rows, s_ids, R, p->R, d_ids, d_d,
                       ws->status.as<int>(), s);
         SCG_CUDA(cudaGetLastError());
+        nl++;
     }
     SCG_CUDA(cudaEventRecord(ws->ev[3], s));
     ws->last_nq = nq;
     ws->last_split = split && nq > 0;
+    ws->last_launches = nl;
     int *dst = h_stat ? h_stat : ws->h_status;
     SCG_CUDA(cudaMemcpyAsync(dst, ws->status.p, sizeof(int), cudaMemcpyDeviceToHost, s));
     if (!wait) return SCG_OK;
     SCG_CUDA(cudaStreamSynchronize(s));
-    if (split && (*dst & ST_POOL))  // the visited lists outgrew the pool
-        return run_search(h, ws, rb, p, dQ, nq, d_ids, d_d, d_sums, s, true, h_stat, false);
+    if (split && (*dst & ST_POOL)) {  // the visited lists outgrew the pool
+        rc = run_search(h, ws, rb, p, dQ, nq, d_ids, d_d, d_sums, s, true, h_stat, false);
+        ws->last_launches += nl;
+        return rc;
+    }
     return status_result(*dst);
 }
 
@@ -1487,6 +1506,14 @@ int scg_last_timings(scg_index *h, float *ms, int n) {
         SCG_CUDA(cudaEventElapsedTime(&t[4], h->ws.ev[4], h->ws.ev[2]));
     }
     for (int i = 0; i < n && i < 5; i++) ms[i] = t[i];
+    return SCG_OK;
+}
+
+int scg_last_launches(scg_index *h, int *count) {
+    if (!h || !count) return fail(SCG_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> g(h->mu);
+    if (h->ws.last_nq <= 0) return fail(SCG_ERR_STATE, "no search has run");
+    *count = h->ws.last_launches;
     return SCG_OK;
 }
 

@@ -55,6 +55,7 @@ struct Workspace {
     // re-rank, between the selection and scan kernels (split launches)
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     bool last_split = false;
+    int last_launches = 0;  // kernels the last run_search on this workspace launched
     int last_nq = 0;
     bool phase_on = false;
     int init();

@@ -35,7 +35,7 @@ EXPORTS = ["scg_last_error", "scg_index_create", "scg_index_destroy", "scg_load_
            "scg_set_kernel_split", "scg_server_wait_times", "scg_set_encoder",
            "scg_train_codebooks", "scg_build_index", "scg_write_edat", "scg_search_graph",
            "scg_kmeans", "scg_exact_nn", "scg_set_rank_limit", "scg_autotune_ex",
-           "scg_device_allocations"]
+           "scg_device_allocations", "scg_last_launches"]
 
 
 def train_codebooks_device(dX_ptr, n, dim, mc, kc, mp, kp, iters, seed, d_cq, d_pq, device=0, stream=None):
@@ -297,6 +297,12 @@ class Index:
         ms = np.zeros(5, np.float32)
         _check(_lib.scg_last_timings(self._h, _ptr(ms), 5))
         return tuple(float(x) for x in ms)
+
+    def last_launches(self):
+        """Kernels the last search launched on the index's own stream."""
+        c = ctypes.c_int()
+        _check(_lib.scg_last_launches(self._h, ctypes.byref(c)))
+        return c.value
 
     def encode(self, X):
         X = np.ascontiguousarray(X, np.float32)
